@@ -1,0 +1,338 @@
+"""Benchmark of the DRIFTER operator path on B200.
+
+Step = one baroclinic step of the coupled DG model on C2 (128x128x16 hexes, N=4, 200x200 km,
+seeded 32-Gaussian bathymetry, M2 tide on the west boundary, linear T stratification):
+5 LSRK45 3D stages (FP32 bulk) + 20 FP64 barotropic predictor-corrector subcycles, one CUDA
+graph. Metric: 3D DOF-stage updates per second (DOF = node x 3D prognostic variable).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 (torchrun): independent replicas, one per GPU (the path is single-GPU by design; no
+collective on the data path). Rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "DOF-stage/s (mixed-precision DG step, C2)"
+UNIT = "DOF-stage/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--small", action="store_true", help="C2 physics on a 32x32x16 mesh (quick)")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 GPU comparison run")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    return ap.parse_args()
+
+
+def dist_init(n):
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        backend = "nccl"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        if not sm:
+            return None
+        maxsm = float(self.rows[-1][2])
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows if len(r) >= 9
+                          for i, v in enumerate(r[5:9]) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": maxsm, "reasons": reasons,
+                "samples": len(sm)}
+
+
+def gpu_smi_id(local):
+    """nvidia-smi --id for the CUDA device `local` (PCI bus id), or the ordinal."""
+    try:
+        import torch
+        p = torch.cuda.get_device_properties(local)
+        return f"{p.pci_domain_id:08X}:{p.pci_bus_id:02X}:{p.pci_device_id:02X}.0"
+    except Exception:
+        return str(local)
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic(name):
+    """DRAM bytes per launch from a committed ncu summary (profiles/<name>.md), or None."""
+    p = os.path.join(ROOT, "profiles", name)
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.strip().startswith("dram_bytes_per_launch_full_size:"):
+            try:
+                return float(line.split(":")[1])
+            except ValueError:
+                return None
+    return None
+
+
+def make_case(small):
+    from drifter_b200 import configs
+    if small:
+        return configs.c2(nx=32, ny=32, nz=16, Lx=50e3)
+    return configs.c2()
+
+
+def cpu_baseline(seconds=12.0, threads=1):
+    """Reference CPU path (SimulationDriver::step, non-split SSPRK3 over the dense-Kronecker
+    element RHS, src/solver/simulation_driver.cpp:108) on C2-shaped N=4 elements."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as O
+    order, nd = 4, 125
+    rng = np.random.default_rng(0)
+    nel = 64 * max(1, threads)
+    h = np.full((nel, nd), 500.0) + rng.uniform(0, 50, (nel, nd))
+    f = np.full((nel, nd), 1e-4)
+    H = h.copy()
+    st = dict(Hu=H * 0.1 * rng.standard_normal((nel, nd)), Hv=H * 0.1 * rng.standard_normal((nel, nd)),
+              eta=np.zeros((nel, nd)), HT=H * 10.0, HS=H * 35.0, omega=np.zeros((nel, nd)))
+    done, t0 = 0, time.perf_counter()
+    while True:
+        st = O.compat_ssprk3(order, 1.0, st, h, f, nthreads=threads)
+        done += 1
+        el = time.perf_counter() - t0
+        if el > seconds:
+            break
+    rate = nel * nd * 4 * 3 * done / el
+    return rate, dict(sample=f"{done} SSPRK3 steps x {nel} N=4 elements ({nel*nd*4} DOFs), "
+                      f"{el:.1f} s", threads=threads)
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    vals = []
+    for _ in range(args.warmup):
+        cpu_baseline(seconds=2.0, threads=threads)
+    for _ in range(args.steps):
+        v, meta = cpu_baseline(seconds=max(2.0, 60.0 / max(args.steps, 1)), threads=threads)
+        vals.append(v)
+    value = float(np.mean(vals))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "reference non-split SSPRK3 DG step (dense Kronecker element RHS) "
+                               "on C2-shaped N=4 elements", "threads": threads},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": meta["sample"]},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank, world, local):
+    import torch
+    torch.cuda.set_device(local)
+    from drifter_b200 import launch_count
+    from drifter_b200.dg import OceanModel
+
+    case = make_case(args.small)
+    cfg = case["cfg"]
+    model = OceanModel(cfg, case["h"], case["f"], case["taux"], case["tauy"])
+    stream = torch.cuda.Stream()  # a real (non-legacy) stream: graphs are captured on it
+    model.set_stream(stream.cuda_stream)
+    model.upload_state(case["q"], case["eta"])
+    dt, nsub = case["dt"], case["nsub"]
+    ndof = 4 * cfg.n3
+    for _ in range(args.warmup):
+        model.step(dt, nsub, 1)
+    torch.cuda.synchronize()
+
+    clocks = ClockSampler(gpu_smi_id(local))
+    clocks.start()
+    time.sleep(0.3)
+    barrier(world)
+    torch.cuda.synchronize()
+    l0 = launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    model.step(dt, nsub, args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    launches = launch_count() - l0
+    ms = e0.elapsed_time(e1)
+    ck = clocks.stop()
+    ms_max = max_over_ranks(ms, world)
+    ms_step = ms_max / args.steps
+    value = world * ndof * 5 * args.steps / (ms_max / 1e3)
+
+    # dominant kernel: the fused 3D stage, timed alone with CUDA events on the model's stream
+    st = model.time_stage(nrep=5 * args.steps)
+    peak, peak_kind = measured_peaks()
+    achieved = st["alg_bytes"] / (st["ms"] / 1e3) / 1e9
+    traffic = profile_traffic("dg3d_stage_c2_mixed.md")
+
+    # end to end through the C ABI: per step upload the surface stress from pinned host memory,
+    # run the step, read back the surface elevation and the diagnostics
+    taux = torch.from_numpy(case["taux"]).pin_memory().numpy()
+    tauy = torch.from_numpy(case["tauy"]).pin_memory().numpy()
+    eta_out = torch.empty(cfg.n2, dtype=torch.float64).pin_memory().numpy()
+    torch.cuda.synchronize()
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        model.set_forcing(taux, tauy)
+        model.step(dt, nsub, 1)
+        model.download_surface(eta_out)
+        model.diagnostics()
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world)
+    e2e = {"value": world * ndof * 5 * args.steps / e2e_s, "unit": UNIT,
+           "h2d_bytes_per_step": 2 * 8 * cfg.n2, "d2h_bytes_per_step": 8 * cfg.n2 + 80}
+
+    # FP64 GPU form of the same step and the mixed-precision surface error against it
+    fp64 = None
+    if not args.no_fp64:
+        sm = model.download_state()
+        nsteps_done = args.warmup + 2 * args.steps
+        del model
+        torch.cuda.synchronize()
+        from drifter_b200.dg import DGConfig
+        cfg64 = DGConfig(**{**cfg.__dict__, "precision": "fp64"})
+        m64 = OceanModel(cfg64, case["h"], case["f"], case["taux"], case["tauy"])
+        m64.set_stream(stream.cuda_stream)
+        m64.upload_state(case["q"], case["eta"])
+        m64.step(dt, nsub, args.warmup)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        m64.step(dt, nsub, 2 * args.steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms64 = max_over_ranks(e0.elapsed_time(e1), world) / (2 * args.steps)
+        s64 = m64.download_state()
+        err = float(np.linalg.norm(sm["eta"] - s64["eta"]) / np.linalg.norm(s64["eta"]))
+        fp64 = {"value": world * ndof * 5 / (ms64 / 1e3), "ms_per_step": ms64,
+                "eta_rel_err_mixed_vs_fp64": err, "steps_compared": nsteps_done}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        v, meta = cpu_baseline(seconds=12.0, threads=1)
+        cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "port", "sample": meta["sample"]}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (3D bulk) + f64 (barotropic)",
+            "data": "synthetic",
+            "config": {"workload": case["name"] + " coupled DG baroclinic step (5 LSRK45 stages + "
+                                                  f"{nsub} FP64 barotropic subcycles)",
+                       "dofs": ndof, "dt_s": dt, "l2": "inputs > L2 (state 2.1 GB)",
+                       "parallelism": f"replicas x{world}"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "kernel": "dg3d_stage_kernel<float,5>", "kernel_ms": st["ms"],
+                         "alg_bytes_per_launch": st["alg_bytes"],
+                         "peak_source": f"{peak_kind} MEASURED_PEAKS.json hbm_gbs"},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "fp64_gpu": fp64,
+            "gpu_launches": int(launches),
+            "clocks": ck,
+        }
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_init(args.gpus)
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank, world)
+        else:
+            run_ours(args, rank, world, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

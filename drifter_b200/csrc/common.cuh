@@ -1,0 +1,118 @@
+// Shared runtime pieces of libdrifter_b200: status codes, error capture, launch
+// accounting, and the nodal basis tables kept in constant memory.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/drifter_b200.h"
+
+namespace drf {
+
+// ----------------------------------------------------------------------------- errors
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string &m) : std::runtime_error(m), code(c) {}
+};
+void set_last_error(const std::string &msg);
+std::atomic<uint64_t> &launch_counter();
+
+#define DRF_CUDA(call)                                                                       \
+    do {                                                                                     \
+        cudaError_t e_ = (call);                                                             \
+        if (e_ != cudaSuccess)                                                               \
+            throw ::drf::Error(DRF_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+#define DRF_CHECK(cond, code, msg)                  \
+    do {                                            \
+        if (!(cond)) throw ::drf::Error(code, msg); \
+    } while (0)
+
+// After every kernel launch: count it and surface launch-configuration errors.
+#define DRF_LAUNCHED()                                  \
+    do {                                                \
+        ::drf::launch_counter().fetch_add(1);           \
+        DRF_CUDA(cudaGetLastError());                   \
+    } while (0)
+
+// C-ABI wrapper: converts exceptions into status codes.
+template <class F>
+int guard(F &&f) {
+    try {
+        f();
+        return DRF_OK;
+    } catch (const Error &e) {
+        set_last_error(e.what());
+        return e.code;
+    } catch (const std::bad_alloc &) {
+        set_last_error("host allocation failed");
+        return DRF_E_NOMEM;
+    } catch (const std::exception &e) {
+        set_last_error(e.what());
+        return DRF_E_INVALID;
+    }
+}
+
+// ----------------------------------------------------------------------------- basis (host)
+// Legendre-Gauss-Lobatto basis on [-1, 1] computed in FP64 on the host: nodes, weights,
+// derivative matrix D (D[i][m] = l_m'(x_i)), its square D2 = D*D, and the integration
+// matrix S[k][m] = int_{-1}^{x_k} l_m(x) dx.
+struct HostBasis {
+    int order = 0, np = 0;
+    std::vector<double> x, w, D, D2, S;
+};
+HostBasis make_lgl_basis(int order);
+
+constexpr int MAXNP = 6;
+
+// Basis tables for device code (both precisions), uploaded once per process.
+struct DevBasis {
+    double D[MAXNP * MAXNP], D2[MAXNP * MAXNP], S[MAXNP * MAXNP], w[MAXNP], x[MAXNP];
+    float Df[MAXNP * MAXNP], D2f[MAXNP * MAXNP], Sf[MAXNP * MAXNP], wf[MAXNP], xf[MAXNP];
+};
+
+// Device-memory RAII buffer.
+template <class T>
+struct DevBuf {
+    T *p = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    explicit DevBuf(size_t count) { alloc(count); }
+    void alloc(size_t count) {
+        release();
+        n = count;
+        if (count) {
+            cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+            if (e != cudaSuccess) {
+                p = nullptr;
+                n = 0;
+                (void)cudaGetLastError();
+                throw Error(DRF_E_NOMEM, "cudaMalloc of " + std::to_string(count * sizeof(T)) +
+                                             " bytes failed: " + cudaGetErrorString(e));
+            }
+        }
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    ~DevBuf() { release(); }
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    DevBuf(DevBuf &&o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+    DevBuf &operator=(DevBuf &&o) noexcept {
+        release();
+        p = o.p; n = o.n; o.p = nullptr; o.n = 0;
+        return *this;
+    }
+};
+
+bool all_finite(const double *x, size_t n);
+
+}  // namespace drf

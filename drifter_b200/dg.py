@@ -1,0 +1,218 @@
+"""Host-side mirror of DRIFTER's DG operator/solver interfaces over the C ABI.
+
+Names and argument meaning follow the reference classes:
+  * PrimitiveEquationsSolver.compute_rhs  (include/physics/primitive_equations.hpp:240)
+  * ModeSplittingSolver.step              (include/physics/mode_splitting.hpp:241)
+  * NumericalFluxFactory fluxes           (include/flux/numerical_flux.hpp:180-210)
+  * OceanModel = SimulationDriver-like coupled model (include/solver/simulation_driver.hpp:92-127)
+Errors raise DrfError (the reference throws std::invalid_argument / std::runtime_error).
+All compute runs in libdrifter_b200.so on the GPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _abi
+from ._abi import check, dptr, dptr_array, lib
+
+COMPAT_DEFAULTS = dict(g=9.81, rho0=1025.0, alpha=2e-4, beta=7.6e-4, nu_h=1.0, nu_v=1e-4,
+                       kappa_v_T=1e-5, kappa_v_S=1e-5)
+
+
+def _compat_params(p: dict | None) -> np.ndarray:
+    d = dict(COMPAT_DEFAULTS)
+    d.update(p or {})
+    return np.array([d["g"], d["rho0"], d["alpha"], d["beta"], d["nu_h"], d["nu_v"],
+                     d["kappa_v_T"], d["kappa_v_S"]], dtype=np.float64)
+
+
+def _c(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def numerical_flux(kind: str, UL, UR, normals, g: float = 9.81) -> np.ndarray:
+    """F*(U_L, U_R, n) for batches of shallow-water states (h, hu, hv); kind in lf/hllc/roe."""
+    UL, UR, nr = _c(UL).reshape(-1, 3), _c(UR).reshape(-1, 3), _c(normals).reshape(-1, 2)
+    if not (len(UL) == len(UR) == len(nr)):
+        raise ValueError("UL, UR and normals must have the same length")
+    F = np.empty_like(UL)
+    check(lib().drf_sw_flux_batch(_abi.FLUX[kind], len(UL), dptr(UL), dptr(UR), dptr(nr), g,
+                                  dptr(F)))
+    return F
+
+
+class PrimitiveEquationsSolver:
+    """Element-local primitive-equation tendencies with the reference's semantics.
+
+    `compute_rhs(states)` takes a dict of [nel, (N+1)^3] arrays Hu, Hv, eta, HT, HS, omega and
+    returns dHu_dt, dHv_dt, deta_dt, dHT_dt, dHS_dt (PrimitiveTendencies).
+    """
+
+    def __init__(self, order: int, bathymetry, coriolis, constants: dict | None = None):
+        self.order = order
+        self.h = _c(bathymetry)
+        self.f = _c(coriolis)
+        self.params = _compat_params(constants)
+
+    def compute_rhs(self, states: dict) -> dict:
+        ins = [_c(states[k]) for k in ("Hu", "Hv", "eta", "HT", "HS", "omega")]
+        nel = ins[0].shape[0]
+        outs = [np.empty_like(ins[0]) for _ in range(5)]
+        check(lib().drf_compat_compute_rhs(self.order, nel, dptr_array(ins), dptr(self.h),
+                                           dptr(self.f), dptr(self.params), dptr_array(outs)))
+        return dict(zip(("dHu_dt", "dHv_dt", "deta_dt", "dHT_dt", "dHS_dt"), outs))
+
+
+STATE12 = ("Hu", "Hv", "eta", "HT", "HS", "H", "u", "v", "T", "S", "omega", "rho")
+
+
+class ModeSplittingSolver:
+    """Per-element barotropic/baroclinic split step with the reference's semantics."""
+
+    def __init__(self, order: int, bathymetry, coriolis, subcycles: int = 30,
+                 constants: dict | None = None):
+        self.order = order
+        self.h = _c(bathymetry)
+        self.f = _c(coriolis)
+        self.subcycles = subcycles
+        self.params = _compat_params(constants)
+
+    def step(self, dt_3d: float, full_state: dict) -> None:
+        arrs = [np.ascontiguousarray(full_state[k], dtype=np.float64) for k in STATE12]
+        nel = arrs[0].shape[0]
+        check(lib().drf_compat_modesplit_step(self.order, nel, dt_3d, self.subcycles,
+                                              dptr_array(arrs), dptr(self.h), dptr(self.f),
+                                              dptr(self.params)))
+        for k, a in zip(STATE12, arrs):
+            full_state[k] = a
+
+
+@dataclass
+class DGConfig:
+    nx: int
+    ny: int
+    nz: int
+    order: int
+    Lx: float
+    Ly: float
+    g: float = 9.81
+    rho0: float = 1025.0
+    nu_h: float = 1.0
+    nu_v: float = 1e-4
+    kappa_v_T: float = 1e-5
+    kappa_v_S: float = 1e-5
+    cd: float = 2.5e-3
+    flux2d: str = "lf"
+    precision: str = "mixed"
+    bc: tuple = ("wall", "wall", "wall", "wall")
+    tide_amp: float = 0.0
+    tide_period: float = 44714.0
+
+    @property
+    def np_(self) -> int:
+        return self.order + 1
+
+    @property
+    def n3(self) -> int:
+        return self.nx * self.ny * self.nz * self.np_ ** 3
+
+    @property
+    def n2(self) -> int:
+        return self.nx * self.ny * self.np_ ** 2
+
+
+class OceanModel:
+    """Coupled sigma-coordinate DG model resident on the GPU (one CUDA stream)."""
+
+    def __init__(self, cfg: DGConfig, h, f, taux, tauy):
+        self.cfg = cfg
+        mesh = _abi.MeshDesc(cfg.nx, cfg.ny, cfg.nz, cfg.order, cfg.Lx, cfg.Ly)
+        prm = _abi.DGParams()
+        prm.g, prm.rho0, prm.nu_h, prm.nu_v = cfg.g, cfg.rho0, cfg.nu_h, cfg.nu_v
+        prm.kappa_v_T, prm.kappa_v_S, prm.cd = cfg.kappa_v_T, cfg.kappa_v_S, cfg.cd
+        prm.flux2d = _abi.FLUX[cfg.flux2d]
+        prm.precision = _abi.PREC[cfg.precision]
+        for s in range(4):
+            prm.bc[s] = _abi.BC[cfg.bc[s]]
+        prm.tide_amp, prm.tide_period = cfg.tide_amp, cfg.tide_period
+        self._keep = [_c(h), _c(f), _c(taux), _c(tauy)]
+        hd = C.c_void_p()
+        check(lib().drf_dg_create(C.byref(mesh), C.byref(prm), *[dptr(a) for a in self._keep],
+                                  C.byref(hd)))
+        self.handle = hd
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().drf_dg_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_ptr: int | None):
+        check(lib().drf_dg_set_stream(self.handle, C.c_void_p(stream_ptr or 0)))
+
+    def sync(self):
+        check(lib().drf_dg_sync(self.handle))
+
+    def upload_state(self, q4, eta, t: float = 0.0):
+        qs = [_c(a) for a in q4]
+        check(lib().drf_dg_upload_state(self.handle, dptr_array(qs), dptr(_c(eta)), float(t)))
+
+    def download_state(self) -> dict:
+        n3, n2 = self.cfg.n3, self.cfg.n2
+        q = [np.empty(n3) for _ in range(4)]
+        eta, HU, HV, eavg = (np.empty(n2) for _ in range(4))
+        t = C.c_double()
+        check(lib().drf_dg_download_state(self.handle, dptr_array(q), dptr(eta), dptr(HU),
+                                          dptr(HV), dptr(eavg), C.byref(t)))
+        return dict(Hu=q[0], Hv=q[1], HT=q[2], HS=q[3], eta=eta, HU=HU, HV=HV, eta_avg=eavg,
+                    t=t.value)
+
+    def compute_rhs(self) -> dict:
+        n3, n2 = self.cfg.n3, self.cfg.n2
+        r = [np.empty(n3) for _ in range(4)]
+        om, de = np.empty(n3), np.empty(n2)
+        check(lib().drf_dg_compute_rhs(self.handle, dptr_array(r), dptr(om), dptr(de)))
+        return dict(dHu=r[0], dHv=r[1], dHT=r[2], dHS=r[3], omega=om, deta=de)
+
+    def compute_rhs2d(self, Fx, Fy, time: float) -> tuple:
+        n2 = self.cfg.n2
+        ke, ku, kv = np.empty(n2), np.empty(n2), np.empty(n2)
+        check(lib().drf_dg_compute_rhs2d(self.handle, dptr(_c(Fx)), dptr(_c(Fy)), time,
+                                         dptr(ke), dptr(ku), dptr(kv)))
+        return ke, ku, kv
+
+    def step(self, dt: float, nsub: int, nsteps: int = 1):
+        """nsteps baroclinic steps, each one CUDA graph (ModeSplittingSolver::step)."""
+        check(lib().drf_dg_step_modesplit(self.handle, dt, nsub, nsteps))
+
+    def rk_step(self, scheme: str, dt: float, nsteps: int = 1):
+        check(lib().drf_dg_rk_step(self.handle, _abi.RK[scheme], dt, nsteps))
+
+    def set_forcing(self, taux, tauy):
+        self._forcing = (_c(taux), _c(tauy))
+        check(lib().drf_dg_set_forcing(self.handle, dptr(self._forcing[0]), dptr(self._forcing[1])))
+
+    def download_surface(self, out: np.ndarray | None = None) -> np.ndarray:
+        out = np.empty(self.cfg.n2) if out is None else out
+        check(lib().drf_dg_download_surface(self.handle, dptr(out)))
+        return out
+
+    def diagnostics(self) -> dict:
+        out = np.empty(10)
+        check(lib().drf_dg_diagnostics(self.handle, dptr(out)))
+        keys = ("mass", "mass_unweighted", "energy", "heat", "salt", "max_speed", "max_eta",
+                "min_eta", "max_T", "min_T")
+        return dict(zip(keys, out.tolist()))
+
+    def time_stage(self, nrep: int = 20) -> dict:
+        ms, ab, nd = C.c_double(), C.c_double(), C.c_double()
+        check(lib().drf_dg_time_stage(self.handle, nrep, C.byref(ms), C.byref(ab), C.byref(nd)))
+        return dict(ms=ms.value, alg_bytes=ab.value, ndof=nd.value)

@@ -1,0 +1,153 @@
+/* drifter_b200 — B200-native (sm_100a) matrix-free operator path of DRIFTER.
+ *
+ * C ABI of libdrifter_b200.so. Plain pointers and sizes only; every call returns an int
+ * status (0 = OK, see DRF_E_*); the message of the last failure on the calling thread is
+ * available from drf_last_error(). Handles are opaque, own their device memory and one
+ * CUDA stream each, and must not be shared between host threads.
+ *
+ * Array layouts (all host arrays are FP64, caller-owned):
+ *   3D nodal field  : [column][layer][k][j][i], column = ex + nx*ey, node = i + np*(j + np*k),
+ *                     np = order + 1 (LGL nodes) — size nx*ny*nz*np^3.
+ *   2D nodal field  : [column][j][i] — size nx*ny*np^2.
+ *   compat fields   : [element][dof], dof = i + np*(j + np*k) (the reference's element
+ *                     vectors, include/dg/basis_hexahedron.hpp:255).
+ */
+#ifndef DRIFTER_B200_H
+#define DRIFTER_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    DRF_OK = 0,
+    DRF_E_INVALID = 1,   /* bad argument (the reference throws std::invalid_argument) */
+    DRF_E_CUDA = 2,      /* CUDA runtime failure */
+    DRF_E_NOMEM = 3,     /* device allocation failed */
+    DRF_E_NONFINITE = 4, /* NaN/Inf found in an input or a result */
+    DRF_E_UNSUPPORTED = 5,
+    DRF_E_TIMEOUT = 6    /* a bounded device wait gave up */
+};
+
+enum { DRF_FLUX_LF = 0, DRF_FLUX_HLLC = 1, DRF_FLUX_ROE = 2 };
+enum { DRF_PREC_FP64 = 0, DRF_PREC_MIXED = 1 };
+enum { DRF_BC_WALL = 0, DRF_BC_TIDE = 1 };
+enum { DRF_RK_EULER = 0, DRF_RK_MIDPOINT = 1, DRF_RK_SSP3 = 2, DRF_RK_RK4 = 3, DRF_RK_LSRK45 = 4,
+       DRF_RK_DOPRI = 5 };
+
+/* Copies the last error message of the calling thread into buf (NUL-terminated). */
+int drf_last_error(char *buf, size_t n);
+/* Library version string and the number of kernels this library has launched. */
+const char *drf_version(void);
+uint64_t drf_kernel_launch_count(void);
+
+/* ------------------------------------------------------------------ fluxes
+ * Batched shallow-water numerical flux F*(U_L, U_R, n) on the GPU, U = (h, hu, hv).
+ * Replaces NumericalFluxFunc (include/flux/numerical_flux.hpp:25) as produced by
+ * NumericalFluxFactory::shallow_water_{lax_friedrichs,hllc,roe}
+ * (src/flux/numerical_flux.cpp:134-190; LaxFriedrichsFlux::flux
+ * include/flux/numerical_flux.hpp:222, ShallowWaterHLLCFlux::flux :272,
+ * ShallowWaterRoeFlux::flux src/flux/numerical_flux.cpp:13).
+ * UL, UR, F: n x 3; normals: n x 2 (nx, ny). */
+int drf_sw_flux_batch(int kind, int64_t n, const double *UL, const double *UR,
+                      const double *normals, double g, double *F);
+
+/* ------------------------------------------------------------------ DG, reference semantics
+ * compat params (8 doubles): g, rho0, alpha, beta, nu_h, nu_v, kappa_v_T, kappa_v_S
+ * (OceanConstants include/physics/primitive_equations.hpp:41, DiffusivityParams :106). */
+
+/* PrimitiveEquationsSolver::compute_rhs (include/physics/primitive_equations.hpp:240,
+ * src/physics/primitive_equations.cpp:428): element-local tendencies of nel elements.
+ * in6 = {Hu, Hv, eta, HT, HS, omega}, out5 = {dHu, dHv, deta, dHT, dHS}, h/f: per node. */
+int drf_compat_compute_rhs(int order, int nel, const double *const *in6, const double *h,
+                           const double *f, const double *params8, double *const *out5);
+
+/* ModeSplittingSolver::step (include/physics/mode_splitting.hpp:241,
+ * src/physics/mode_splitting.cpp:434) on nel elements, in place.
+ * st12 = {Hu, Hv, eta, HT, HS, H, u, v, T, S, omega, rho}. */
+int drf_compat_modesplit_step(int order, int nel, double dt, int nsub, double *const *st12,
+                              const double *h, const double *f, const double *params8);
+
+/* ------------------------------------------------------------------ DG, coupled model */
+typedef struct drf_dg drf_dg;
+
+typedef struct {
+    int32_t nx, ny, nz; /* hexes in x, y (columns) and sigma (layers) */
+    int32_t order;      /* polynomial order N, np = N + 1 LGL nodes per direction (1..5) */
+    double Lx, Ly;      /* basin extent [m] */
+} drf_mesh_desc;
+
+typedef struct {
+    double g, rho0;                        /* 9.81, 1025 */
+    double nu_h, nu_v, kappa_v_T, kappa_v_S; /* DiffusivityParams defaults 1, 1e-4, 1e-5, 1e-5 */
+    double cd;                             /* quadratic bottom drag (BottomFriction, 2.5e-3) */
+    int32_t flux2d;                        /* DRF_FLUX_* for the barotropic face flux */
+    int32_t precision;                     /* DRF_PREC_FP64 or DRF_PREC_MIXED */
+    int32_t bc[4];                         /* west, east, south, north: DRF_BC_* */
+    double tide_amp, tide_period;          /* tidal elevation on DRF_BC_TIDE sides */
+} drf_dg_params;
+
+/* Creates the model: h (bathymetry > 0), f (Coriolis), taux/tauy (surface stress, N/m^2)
+ * are 2D nodal fields. Replaces PrimitiveEquationsSolver/ModeSplittingSolver::initialize
+ * (src/physics/primitive_equations.cpp:697, src/physics/mode_splitting.cpp:347) and
+ * SimulationDriver::initialize (src/solver/simulation_driver.cpp:29). */
+int drf_dg_create(const drf_mesh_desc *mesh, const drf_dg_params *params, const double *h,
+                  const double *f, const double *taux, const double *tauy, drf_dg **out);
+int drf_dg_destroy(drf_dg *m);
+/* Uses the given cudaStream_t for all work of this model (NULL = the model's own stream). */
+int drf_dg_set_stream(drf_dg *m, void *cuda_stream);
+int drf_dg_sync(drf_dg *m);
+
+/* Host FP64 state in/out. q = {Hu, Hv, HT, HS} 3D fields, eta 2D. On upload the barotropic
+ * transports are the depth integrals of Hu, Hv. (SimulationDriver::pack_state/unpack_state,
+ * src/solver/simulation_driver.cpp:199,215.) Any output pointer may be NULL. */
+int drf_dg_upload_state(drf_dg *m, const double *const *q4, const double *eta, double t);
+int drf_dg_download_state(drf_dg *m, double *const *q4, double *eta, double *HU, double *HV,
+                          double *eta_avg, double *t);
+
+/* Coupled right-hand side at the current state (eta frozen): R = {dHu, dHv, dHT, dHS},
+ * omega (3D sigma velocity), deta (2D, -int div(Hu) dsigma). Maps
+ * PrimitiveEquationsSolver::compute_rhs + apply_interface_fluxes + the column diagnosis
+ * VerticalVelocityDiagnosis::diagnose_omega (src/physics/vertical_velocity.cpp:55). */
+int drf_dg_compute_rhs(drf_dg *m, double *const *r4, double *omega, double *deta);
+
+/* Barotropic operator (2D, FP64) with forcing Fx, Fy at time t on the current state. */
+int drf_dg_compute_rhs2d(drf_dg *m, const double *Fx, const double *Fy, double time,
+                         double *ke, double *khu, double *khv);
+
+/* nsteps baroclinic steps: LSRK45 3D stages (include/solver/time_stepper.hpp:56-61) plus
+ * nsub barotropic predictor-corrector subcycles per step, each step replayed as one CUDA
+ * graph. Maps ModeSplittingSolver::step (include/physics/mode_splitting.hpp:241). */
+int drf_dg_step_modesplit(drf_dg *m, double dt, int nsub, int nsteps);
+
+/* Non-split RK over (Hu, Hv, HT, HS, eta): TimeStepper::step
+ * (include/solver/time_stepper.hpp:18) with the scheme of DRF_RK_*. */
+int drf_dg_rk_step(drf_dg *m, int scheme, double dt, int nsteps);
+
+/* FP64 diagnostics (SimulationDriver::compute_diagnostics, src/solver/simulation_driver.cpp:237):
+ * out[10] = {mass_weighted, mass_unweighted, energy, heat, salt, max_speed, max_eta,
+ *            min_eta, max_T, min_T}. */
+int drf_dg_diagnostics(drf_dg *m, double *out10);
+
+/* Device-side timing of the dominant 3D stage kernel: runs nrep stage launches on the
+ * model's stream between CUDA events; *ms = mean per launch. Also reports the bytes the
+ * stage moves by the algorithmic model (*alg_bytes) and the number of 3D DOFs (*ndof). */
+int drf_dg_time_stage(drf_dg *m, int nrep, double *ms, double *alg_bytes, double *ndof);
+
+/* Replaces the surface stress fields (WindStress::compute, src/physics/primitive_equations.cpp:695)
+ * for the following steps; asynchronous on the model's stream (pinned host memory recommended;
+ * the caller keeps the buffers alive until the next drf_dg_sync). */
+int drf_dg_set_forcing(drf_dg *m, const double *taux, const double *tauy);
+/* Copies the 2D surface elevation to the host (synchronous). */
+int drf_dg_download_surface(drf_dg *m, double *eta);
+
+/* Size and pointer introspection for the bench (device-resident timing). */
+int drf_dg_info(drf_dg *m, int64_t *n3d_nodes, int64_t *n2d_nodes, int *precision);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DRIFTER_B200_H */

@@ -1,0 +1,187 @@
+"""ORACLE binding — test infrastructure only (tests/, __graft_entry__.smoke(), bench.py's
+CPU-baseline leg). ctypes access to oracle/_build/liboracle.so, the FP64 CPU restatement of
+the reference algorithms. Never imported by the drifter_b200 package.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "_build", "liboracle.so")
+_dp = C.POINTER(C.c_double)
+_lib = None
+
+
+def build() -> str:
+    subprocess.check_call(["make", "-s", "-C", HERE])
+    return LIB
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build()
+        _lib = C.CDLL(LIB)
+        _lib.orc_last_error.restype = C.c_char_p
+        _lib.orc_phys_create.restype = C.c_void_p
+        for name in ("orc_phys_destroy", "orc_phys_set_state", "orc_phys_get_state",
+                     "orc_phys_rhs", "orc_phys_rhs2d", "orc_phys_split_steps",
+                     "orc_phys_rk_steps", "orc_phys_diagnostics"):
+            getattr(_lib, name).argtypes = None
+        _lib.orc_phys_destroy.argtypes = [C.c_void_p]
+    return _lib
+
+
+def _p(a):
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_dp)
+
+
+def _pa(arrs):
+    return (_dp * len(arrs))(*[_p(a) for a in arrs])
+
+
+def _chk(rc):
+    if rc != 0:
+        raise RuntimeError("oracle: " + lib().orc_last_error().decode())
+
+
+def _c(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def basis(order: int, kind: str = "lgl"):
+    np_ = order + 1
+    x, w, D, S = np.empty(np_), np.empty(np_), np.empty(np_ * np_), np.empty(np_ * np_)
+    _chk(lib().orc_basis(order, 0 if kind == "lgl" else 1, _p(x), _p(w), _p(D), _p(S)))
+    return x, w, D.reshape(np_, np_), S.reshape(np_, np_)
+
+
+def dense_3d(order: int):
+    nd = (order + 1) ** 3
+    a, b, c = (np.empty(nd * nd) for _ in range(3))
+    _chk(lib().orc_dense_3d(order, _p(a), _p(b), _p(c)))
+    return a.reshape(nd, nd), b.reshape(nd, nd), c.reshape(nd, nd)
+
+
+FLUX = {"lf": 0, "hllc": 1, "roe": 2}
+
+
+def sw_flux(kind, UL, UR, nx, ny, g=9.81):
+    F = np.empty(3)
+    _chk(lib().orc_sw_flux(FLUX[kind], _p(_c(UL)), _p(_c(UR)), C.c_double(nx), C.c_double(ny),
+                           C.c_double(g), _p(F)))
+    return F
+
+
+def compat_params(p=None):
+    d = dict(g=9.81, rho0=1025.0, alpha=2e-4, beta=7.6e-4, nu_h=1.0, nu_v=1e-4, kappa_v_T=1e-5,
+             kappa_v_S=1e-5)
+    d.update(p or {})
+    return np.array([d[k] for k in ("g", "rho0", "alpha", "beta", "nu_h", "nu_v", "kappa_v_T",
+                                    "kappa_v_S")])
+
+
+def compat_rhs(order, states, h, f, params=None):
+    ins = [_c(states[k]) for k in ("Hu", "Hv", "eta", "HT", "HS", "omega")]
+    outs = [np.empty_like(ins[0]) for _ in range(5)]
+    _chk(lib().orc_compat_rhs(order, ins[0].shape[0], _pa(ins), _p(_c(h)), _p(_c(f)),
+                              _p(compat_params(params)), _pa(outs)))
+    return dict(zip(("dHu_dt", "dHv_dt", "deta_dt", "dHT_dt", "dHS_dt"), outs))
+
+
+STATE12 = ("Hu", "Hv", "eta", "HT", "HS", "H", "u", "v", "T", "S", "omega", "rho")
+
+
+def compat_modesplit(order, dt, nsub, state, h, f, params=None):
+    arrs = [_c(state[k]).copy() for k in STATE12]
+    _chk(lib().orc_compat_modesplit(order, arrs[0].shape[0], C.c_double(dt), nsub, _pa(arrs),
+                                    _p(_c(h)), _p(_c(f)), _p(compat_params(params))))
+    return dict(zip(STATE12, arrs))
+
+
+def compat_ssprk3(order, dt, state, h, f, params=None, nthreads=1):
+    """SimulationDriver::step without mode splitting on nel elements (in place on copies)."""
+    arrs = [_c(state[k]).copy() for k in ("Hu", "Hv", "eta", "HT", "HS", "omega")]
+    _chk(lib().orc_compat_ssprk3(order, arrs[0].shape[0], C.c_double(dt), _pa(arrs), _p(_c(h)),
+                                 _p(_c(f)), _p(compat_params(params)), nthreads))
+    return dict(zip(("Hu", "Hv", "eta", "HT", "HS", "omega"), arrs))
+
+
+BCS = {"wall": 0, "tide": 1}
+RK = {"euler": 0, "midpoint": 1, "ssp3": 2, "rk4": 3, "lsrk45": 4, "dopri": 5}
+
+
+class PhysOracle:
+    """FP64 CPU model of the coupled DG scheme (same spec as the GPU OceanModel)."""
+
+    def __init__(self, cfg, h, f, taux, tauy):
+        self.cfg = cfg
+        iv = np.array([cfg.nx, cfg.ny, cfg.nz, cfg.order, FLUX[cfg.flux2d]] +
+                      [BCS[b] for b in cfg.bc], dtype=np.int32)
+        dv = np.array([cfg.Lx, cfg.Ly, cfg.g, cfg.rho0, cfg.nu_h, cfg.nu_v, cfg.kappa_v_T,
+                       cfg.kappa_v_S, cfg.cd, cfg.tide_amp, cfg.tide_period])
+        self._keep = [_c(h), _c(f), _c(taux), _c(tauy)]
+        L = lib()
+        L.orc_phys_create.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp, _dp]
+        self.h = L.orc_phys_create(iv.ctypes.data, _p(dv), *[_p(a) for a in self._keep])
+        if not self.h:
+            raise RuntimeError("oracle: " + L.orc_last_error().decode())
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_phys_destroy(C.c_void_p(self.h))
+            self.h = None
+
+    def set_state(self, q4, eta, t=0.0):
+        qs = [_c(a) for a in q4]
+        _chk(lib().orc_phys_set_state(C.c_void_p(self.h), _pa(qs), _p(_c(eta)), C.c_double(t)))
+
+    def get_state(self):
+        n3, n2 = self.cfg.n3, self.cfg.n2
+        q = [np.empty(n3) for _ in range(4)]
+        eta, HU, HV, eavg = (np.empty(n2) for _ in range(4))
+        t = C.c_double()
+        _chk(lib().orc_phys_get_state(C.c_void_p(self.h), _pa(q), _p(eta), _p(HU), _p(HV),
+                                      _p(eavg), C.byref(t)))
+        return dict(Hu=q[0], Hv=q[1], HT=q[2], HS=q[3], eta=eta, HU=HU, HV=HV, eta_avg=eavg,
+                    t=t.value)
+
+    def rhs(self):
+        n3, n2 = self.cfg.n3, self.cfg.n2
+        r = [np.empty(n3) for _ in range(4)]
+        om, de = np.empty(n3), np.empty(n2)
+        _chk(lib().orc_phys_rhs(C.c_void_p(self.h), _pa(r), _p(om), _p(de)))
+        return dict(dHu=r[0], dHv=r[1], dHT=r[2], dHS=r[3], omega=om, deta=de)
+
+    def rhs2d(self, Fx, Fy, time):
+        n2 = self.cfg.n2
+        a, b, c = np.empty(n2), np.empty(n2), np.empty(n2)
+        _chk(lib().orc_phys_rhs2d(C.c_void_p(self.h), _p(_c(Fx)), _p(_c(Fy)), C.c_double(time),
+                                  _p(a), _p(b), _p(c)))
+        return a, b, c
+
+    def split_steps(self, dt, nsub, nsteps=1):
+        _chk(lib().orc_phys_split_steps(C.c_void_p(self.h), C.c_double(dt), nsub, nsteps))
+
+    def rk_steps(self, scheme, dt, nsteps=1):
+        _chk(lib().orc_phys_rk_steps(C.c_void_p(self.h), RK[scheme], C.c_double(dt), nsteps))
+
+    def diagnostics(self):
+        out = np.empty(10)
+        _chk(lib().orc_phys_diagnostics(C.c_void_p(self.h), _p(out)))
+        keys = ("mass", "mass_unweighted", "energy", "heat", "salt", "max_speed", "max_eta",
+                "min_eta", "max_T", "min_T")
+        return dict(zip(keys, out.tolist()))
+
+
+def rk_ode(scheme, lam, U0, T, nsteps):
+    out = C.c_double()
+    _chk(lib().orc_rk_ode(RK[scheme], C.c_double(lam), C.c_double(U0), C.c_double(T), nsteps,
+                          C.byref(out)))
+    return out.value

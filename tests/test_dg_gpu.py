@@ -1,0 +1,205 @@
+"""GPU parity of the DG path against the FP64 oracle, through the C ABI.
+
+Tolerances: FP64 kernels 1e-10 relative to the field's max magnitude (sum-factorized vs dense
+products, FMA contraction); mixed precision (FP32 3D bulk) 2e-4 on 3D fields; the surface
+elevation of the mixed run is held to the stated 1e-6 relative error against the FP64 oracle.
+"""
+import numpy as np
+import pytest
+
+import pyoracle as O
+from drifter_b200 import configs, launch_count
+from drifter_b200.dg import ModeSplittingSolver, OceanModel, PrimitiveEquationsSolver, numerical_flux
+
+pytestmark = pytest.mark.gpu
+
+
+def relerr(a, b):
+    den = max(np.abs(b).max(), 1e-300)
+    return np.abs(a - b).max() / den
+
+
+# ---------------------------------------------------------------- fluxes
+@pytest.mark.parametrize("kind", ["lf", "hllc", "roe"])
+def test_flux_batch_matches_oracle(kind):
+    rng = np.random.default_rng(3)
+    n = 257
+    UL = np.stack([rng.uniform(0.5, 3, n), rng.normal(0, 1, n), rng.normal(0, 1, n)], 1)
+    UR = np.stack([rng.uniform(0.5, 3, n), rng.normal(0, 1, n), rng.normal(0, 1, n)], 1)
+    UL[:8, 0] = 1e-12  # dry cells
+    th = rng.uniform(0, 2 * np.pi, n)
+    nr = np.stack([np.cos(th), np.sin(th)], 1)
+    F = numerical_flux(kind, UL, UR, nr)
+    ref = np.array([O.sw_flux(kind, UL[i], UR[i], nr[i, 0], nr[i, 1]) for i in range(n)])
+    assert np.isfinite(F).all()
+    np.testing.assert_allclose(F, ref, rtol=1e-12, atol=1e-12)
+
+
+def test_flux_batch_empty():
+    assert numerical_flux("lf", np.zeros((0, 3)), np.zeros((0, 3)), np.zeros((0, 2))).shape == (0, 3)
+
+
+# ---------------------------------------------------------------- reference-semantics DG
+def _compat_state(order, nel, seed=1):
+    rng = np.random.default_rng(seed)
+    nd = (order + 1) ** 3
+    h = 100.0 + rng.uniform(0, 20, (nel, nd))
+    f = 1e-4 + 1e-6 * rng.standard_normal((nel, nd))
+    eta = 0.1 * rng.standard_normal((nel, nd))
+    H = eta + h
+    u, v = 0.2 * rng.standard_normal((2, nel, nd))
+    T = 10.0 + rng.standard_normal((nel, nd))
+    S = 35.0 + 0.1 * rng.standard_normal((nel, nd))
+    om = 1e-4 * rng.standard_normal((nel, nd))
+    st = dict(Hu=H * u, Hv=H * v, eta=eta, HT=H * T, HS=H * S, H=H, u=u, v=v, T=T, S=S, omega=om,
+              rho=np.zeros((nel, nd)))
+    return st, h, f
+
+
+@pytest.mark.parametrize("order", [1, 2, 3, 4, 5])
+def test_compat_rhs_matches_oracle(order):
+    st, h, f = _compat_state(order, 9)
+    gpu = PrimitiveEquationsSolver(order, h, f).compute_rhs(st)
+    ref = O.compat_rhs(order, st, h, f)
+    for k in ref:
+        assert relerr(gpu[k], ref[k]) < 1e-11, k
+
+
+@pytest.mark.parametrize("order,nsub", [(2, 7), (3, 20), (4, 5)])
+def test_compat_modesplit_matches_oracle(order, nsub):
+    st, h, f = _compat_state(order, 6, seed=order)
+    ref = O.compat_modesplit(order, 5.0, nsub, st, h, f)
+    gst = {k: v.copy() for k, v in st.items()}
+    ModeSplittingSolver(order, h, f, subcycles=nsub).step(5.0, gst)
+    for k in ref:
+        assert relerr(gst[k], ref[k]) < 1e-11, k
+
+
+def test_compat_empty_batch():
+    st, h, f = _compat_state(3, 0)
+    out = PrimitiveEquationsSolver(3, h, f).compute_rhs(st)
+    assert out["dHu_dt"].shape == (0, 64)
+
+
+# ---------------------------------------------------------------- coupled model
+def _pair(case):
+    cfg = case["cfg"]
+    gpu = OceanModel(cfg, case["h"], case["f"], case["taux"], case["tauy"])
+    gpu.upload_state(case["q"], case["eta"])
+    ref = O.PhysOracle(cfg, case["h"], case["f"], case["taux"], case["tauy"])
+    ref.set_state(case["q"], case["eta"])
+    return gpu, ref
+
+
+def _tidal_small(precision, order=3, nx=5, ny=4, nz=3, flux2d="lf"):
+    case = configs.c2(nx=nx, ny=ny, nz=nz, order=order, precision=precision, Lx=40e3, flux2d=flux2d)
+    case = configs.perturb(case)
+    case["taux"][:] = 0.05
+    return case
+
+
+@pytest.mark.parametrize("order", [2, 3, 4])
+def test_phys_rhs_fp64_matches_oracle(order):
+    case = _tidal_small("fp64", order=order)
+    gpu, ref = _pair(case)
+    g, r = gpu.compute_rhs(), ref.rhs()
+    assert relerr(g["omega"], r["omega"]) < 1e-10
+    assert relerr(g["deta"], r["deta"]) < 1e-10
+    for k in ("dHu", "dHv", "dHT", "dHS"):
+        assert relerr(g[k], r[k]) < 1e-10, k
+
+
+def test_phys_rhs_mixed_matches_oracle():
+    case = _tidal_small("mixed", order=4)
+    gpu, ref = _pair(case)
+    g, r = gpu.compute_rhs(), ref.rhs()
+    for k in ("dHu", "dHv", "omega"):
+        assert relerr(g[k], r[k]) < 2e-4, k
+
+
+@pytest.mark.parametrize("flux2d", ["lf", "hllc", "roe"])
+def test_phys_rhs2d_matches_oracle(flux2d):
+    case = _tidal_small("fp64", flux2d=flux2d)
+    gpu, ref = _pair(case)
+    rng = np.random.default_rng(1)
+    Fx, Fy = 1e-3 * rng.standard_normal((2, case["cfg"].n2))
+    g = gpu.compute_rhs2d(Fx, Fy, 1234.5)
+    r = ref.rhs2d(Fx, Fy, 1234.5)
+    for a, b in zip(g, r):
+        assert relerr(a, b) < 1e-11
+
+
+@pytest.mark.parametrize("flux2d", ["lf", "hllc", "roe"])
+def test_split_step_fp64_matches_oracle(flux2d):
+    case = _tidal_small("fp64", flux2d=flux2d)
+    gpu, ref = _pair(case)
+    gpu.step(case["dt"], case["nsub"], 3)
+    ref.split_steps(case["dt"], case["nsub"], 3)
+    g, r = gpu.download_state(), ref.get_state()
+    assert abs(g["t"] - r["t"]) < 1e-9
+    for k in ("eta", "HU", "HV", "eta_avg"):
+        assert relerr(g[k], r[k]) < 1e-10, k
+    for k in ("Hu", "Hv", "HT", "HS"):
+        assert relerr(g[k], r[k]) < 1e-10, k
+
+
+def test_c1_mixed_eta_error_within_1e6():
+    """C1 in full (16x16x4, N=3, 20 subcycles, 100 steps): mixed-precision surface elevation
+    against the FP64 oracle; the target is <= 1e-6 relative."""
+    case = configs.c1(precision="mixed")
+    gpu, ref = _pair(case)
+    gpu.step(case["dt"], case["nsub"], case["steps"])
+    ref.split_steps(case["dt"], case["nsub"], case["steps"])
+    g, r = gpu.download_state(), ref.get_state()
+    err = np.linalg.norm(g["eta"] - r["eta"]) / np.linalg.norm(r["eta"])
+    assert np.abs(r["eta"]).max() > 1e-4  # the wind has set up a surface slope
+    assert err <= 1e-6, err
+    # and the FP64 GPU form matches to rounding
+    case64 = configs.c1(precision="fp64")
+    g64 = OceanModel(case64["cfg"], case64["h"], case64["f"], case64["taux"], case64["tauy"])
+    g64.upload_state(case64["q"], case64["eta"])
+    g64.step(case64["dt"], case64["nsub"], case64["steps"])
+    s64 = g64.download_state()
+    assert np.linalg.norm(s64["eta"] - r["eta"]) / np.linalg.norm(r["eta"]) < 1e-10
+
+
+@pytest.mark.parametrize("scheme", ["euler", "midpoint", "ssp3", "rk4", "lsrk45", "dopri"])
+def test_rk_step_matches_oracle(scheme):
+    case = _tidal_small("fp64", nx=3, ny=3, nz=2)
+    gpu, ref = _pair(case)
+    dt = case["dt"] / case["nsub"]
+    gpu.rk_step(scheme, dt, 2)
+    ref.rk_steps(scheme, dt, 2)
+    g, r = gpu.download_state(), ref.get_state()
+    for k in ("eta", "Hu", "Hv", "HT", "HU"):
+        assert relerr(g[k], r[k]) < 1e-10, k
+
+
+def test_diagnostics_match_oracle():
+    case = _tidal_small("fp64")
+    gpu, ref = _pair(case)
+    gpu.step(case["dt"], case["nsub"], 2)
+    ref.split_steps(case["dt"], case["nsub"], 2)
+    g, r = gpu.diagnostics(), ref.diagnostics()
+    for k in r:
+        assert abs(g[k] - r[k]) <= 1e-10 * max(abs(r[k]), 1e-12), k
+
+
+def test_lake_at_rest_stays_at_rest_on_gpu():
+    case = configs.c1(nx=6, ny=5, nz=3)
+    case["taux"][:] = 0.0
+    gpu = OceanModel(case["cfg"], case["h"], case["f"], case["taux"], case["tauy"])
+    gpu.upload_state(case["q"], case["eta"])
+    before = launch_count()
+    gpu.step(case["dt"], case["nsub"], 4)
+    s = gpu.download_state()
+    assert launch_count() > before
+    assert np.abs(s["eta"]).max() < 1e-12 and np.abs(s["Hu"]).max() < 1e-8
+
+
+def test_time_stage_reports_positive_rate():
+    case = configs.c1(nx=8, ny=8, nz=4, precision="mixed")
+    gpu = OceanModel(case["cfg"], case["h"], case["f"], case["taux"], case["tauy"])
+    gpu.upload_state(case["q"], case["eta"])
+    r = gpu.time_stage(5)
+    assert r["ms"] > 0 and r["alg_bytes"] > 0 and r["ndof"] == 4 * case["cfg"].n3
