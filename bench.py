@@ -37,6 +37,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--small", action="store_true", help="C2 physics on a 32x32x16 mesh (quick)")
+    ap.add_argument("--mid", action="store_true", help="C2 physics on a 64x64x16 mesh (profiling)")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 GPU comparison run")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     return ap.parse_args()
@@ -150,8 +151,10 @@ def profile_traffic(name):
     return None
 
 
-def make_case(small):
+def make_case(small, mid=False):
     from drifter_b200 import configs
+    if mid:
+        return configs.c2(nx=64, ny=64, nz=16, Lx=100e3)
     if small:
         return configs.c2(nx=32, ny=32, nz=16, Lx=50e3)
     return configs.c2()
@@ -212,7 +215,7 @@ def run_ours(args, rank, world, local):
     from drifter_b200 import launch_count
     from drifter_b200.dg import OceanModel
 
-    case = make_case(args.small)
+    case = make_case(args.small, args.mid)
     cfg = case["cfg"]
     model = OceanModel(cfg, case["h"], case["f"], case["taux"], case["tauy"])
     stream = torch.cuda.Stream()  # a real (non-legacy) stream: graphs are captured on it
