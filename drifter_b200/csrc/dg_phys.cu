@@ -10,7 +10,8 @@
 // Kernel map (one baroclinic step, graph-captured):
 //   dg3d_stage x5 (one CTA per water column: load column -> horizontal divergence ->
 //   omega column scan in shared memory -> RHS -> LSRK update -> FP64 column increments)
-//   baro_force, (baro_pred, baro_corr) x nsub, baro_finish, correct3d.
+//   baro_force, (baro_pred, baro_corr) x nsub, baro_finish; the transport correction the
+//   barotropic step leaves is folded into the next step's first stage.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -63,6 +64,7 @@ struct StageArgs {
     T *qout[4];
     T *res[4];
     const double *eta, *h, *f, *taux, *tauy, *tdev;
+    const double *corrU, *corrV;  // pending transport correction added to Hu, Hv on load (or null)
     double toff;
     double *dHU3, *dHV3;
     T *omega_out;
@@ -73,47 +75,70 @@ struct StageArgs {
     Geo G;
 };
 
+template <typename T>
+__device__ __forceinline__ T sel4(const T (&x)[4], int v) {
+    return v == 0 ? x[0] : (v == 1 ? x[1] : (v == 2 ? x[2] : x[3]));
+}
+
+// Shared-memory plan of the stage kernel for one water column (ncn = nz*(N+1)^3 nodes):
+//   sQ[4][ncn] state, sR[4][ncn] right-hand side (sR[0] first holds the horizontal
+//   divergence and the layer integrals), sOm[ncn] omega, per layer x 2D-node scratch, and the
+//   column's 2D fields.
+template <typename T>
+__host__ __device__ inline size_t stage_smem_elems(int nz, int np) {
+    const int np2 = np * np, ncn = nz * np2 * np;
+    return (size_t)9 * ncn + (size_t)2 * nz * np2 + 4 * np2;
+}
+
+// One CTA per water column; work is organised in pencils (lines of N+1 nodes) so every
+// thread applies the 1D operators to registers, with the operator entries read as
+// warp-uniform constants: x pencils (j,k,layer), y pencils (i,k,layer), z pencils (i,j,layer).
 template <typename T, int NP>
-__global__ void __launch_bounds__(256) dg3d_stage_kernel(StageArgs<T> a) {
+__global__ void __launch_bounds__(512) dg3d_stage_kernel(StageArgs<T> a) {
     constexpr int NP2 = NP * NP, NP3 = NP2 * NP, N = NP - 1;
     using B = BT<T>;
     const Geo &G = a.G;
-    const int nz = G.nz, ncn = nz * NP3;
+    const int nz = G.nz, ncn = nz * NP3, npen = nz * NP2;
     const int c = blockIdx.x, ex = c % G.nx, ey = c / G.nx;
     const size_t base = (size_t)c * ncn;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T *sQ = reinterpret_cast<T *>(smem_raw);  // [4][ncn]
-    T *sU = sQ + 4 * ncn, *sV = sU + ncn, *sOm = sV + ncn, *sW = sOm + ncn, *sW2 = sW + ncn;
-    T *sBase = sW2 + ncn;                     // [nz][NP2]
-    T *sIH = sBase + nz * NP2;                // [NP2]
-    T *sItot = sIH + NP2;                     // [NP2]
-    double *sEta = reinterpret_cast<double *>(
-        (reinterpret_cast<uintptr_t>(sItot + NP2) + 15) & ~uintptr_t(15));
-    double *sH = sEta + NP2;
+    T *sR = sQ + 4 * ncn;                     // [4][ncn]
+    T *sOm = sR + 4 * ncn;                    // [ncn]
+    T *sL1 = sOm + ncn;                       // [nz][NP2]
+    T *sL2 = sL1 + nz * NP2;                  // [nz][NP2]
+    T *sIH = sL2 + nz * NP2, *sHt = sIH + NP2, *sEt = sHt + NP2, *sItot = sEt + NP2;
+    T *sD = sR;                               // divergence / layer integrals
 
     const double tnow = a.tdev[0] + a.toff;
-    const double etide = tide_at(G, tnow);
+    const T etide = (T)tide_at(G, tnow);
+    const T cx = (T)G.cx, cy = (T)G.cy, cs = (T)G.cs;
+    const T Lx = (T)G.Lx, Ly = (T)G.Ly, Ls = (T)G.Ls;
+    const T g = (T)G.g;
 
-    for (int n = threadIdx.x; n < ncn; n += blockDim.x) {
-#pragma unroll
-        for (int v = 0; v < 4; ++v) sQ[v * ncn + n] = a.qin[v][base + n];
-    }
+    // ---- load the column (and apply a pending transport correction to Hu, Hv)
     for (int t = threadIdx.x; t < NP2; t += blockDim.x) {
         const double e = a.eta[(size_t)c * NP2 + t];
         const double H = e + a.h[(size_t)c * NP2 + t];
-        sEta[t] = e;
-        sH[t] = H;
+        sEt[t] = (T)e;
+        sHt[t] = (T)H;
         sIH[t] = (T)(1.0 / H);
     }
-    __syncthreads();
     for (int n = threadIdx.x; n < ncn; n += blockDim.x) {
-        const int an = (n % NP3) % NP2;
-        sU[n] = sQ[n] * sIH[an];
-        sV[n] = sQ[ncn + n] * sIH[an];
+        T q0 = a.qin[0][base + n], q1 = a.qin[1][base + n];
+        if (a.corrU) {
+            const int an = n % NP2;
+            q0 += (T)a.corrU[(size_t)c * NP2 + an];
+            q1 += (T)a.corrV[(size_t)c * NP2 + an];
+        }
+        sQ[n] = q0;
+        sQ[ncn + n] = q1;
+        sQ[2 * ncn + n] = a.qin[2][base + n];
+        sQ[3 * ncn + n] = a.qin[3][base + n];
     }
     __syncthreads();
 
-    // horizontal neighbour (or ghost) state across side s for own node (ez, i, j, k).
+    // state across horizontal side s at own node (ez,i,j,k): q+ (4), eta+, H+
     auto outside = [&](int s, int ez, int i, int j, int k, int n, T qp[4], T &etap, T &Hp) {
         int nc = -1, ni = i, nj = j;
         if (s == 0 && ex > 0) { nc = c - 1; ni = N; }
@@ -123,237 +148,334 @@ __global__ void __launch_bounds__(256) dg3d_stage_kernel(StageArgs<T> a) {
         const int an = i + NP * j;
         if (nc >= 0) {
             const size_t nb = (size_t)nc * ncn + (size_t)ez * NP3 + ni + NP * (nj + NP * k);
+            const size_t n2 = (size_t)nc * NP2 + ni + NP * nj;
 #pragma unroll
             for (int v = 0; v < 4; ++v) qp[v] = a.qin[v][nb];
-            const size_t n2 = (size_t)nc * NP2 + ni + NP * nj;
+            if (a.corrU) {
+                qp[0] += (T)a.corrU[n2];
+                qp[1] += (T)a.corrV[n2];
+            }
             const double e = a.eta[n2];
             etap = (T)e;
             Hp = (T)(e + a.h[n2]);
             return;
         }
         if (G.bc[s] == DRF_BC_TIDE) {
-            const double Hpd = etide + a.h[(size_t)c * NP2 + an];
-            etap = (T)etide;
-            Hp = (T)Hpd;
-            const T r = (T)Hpd * sIH[an];
+            etap = etide;
+            Hp = etide + (T)a.h[(size_t)c * NP2 + an];
+            const T r = Hp * sIH[an];
 #pragma unroll
             for (int v = 0; v < 4; ++v) qp[v] = sQ[v * ncn + n] * r;
         } else {
-            etap = (T)sEta[an];
-            Hp = (T)sH[an];
+            etap = sEt[an];
+            Hp = sHt[an];
 #pragma unroll
             for (int v = 0; v < 4; ++v) qp[v] = sQ[v * ncn + n];
             if (s <= 1) qp[0] = -qp[0]; else qp[1] = -qp[1];
         }
     };
 
-    const T cx = (T)G.cx, cy = (T)G.cy, cs = (T)G.cs;
-    const T Lx = (T)G.Lx, Ly = (T)G.Ly, Ls = (T)G.Ls;
-
-    // ---- horizontal divergence of (Hu, Hv), central face flux
-    for (int n = threadIdx.x; n < ncn; n += blockDim.x) {
-        const int ez = n / NP3, ln = n % NP3, i = ln % NP, j = (ln / NP) % NP, k = ln / NP2;
-        const int eb = ez * NP3;
-        T sx = 0, sy = 0;
+    // ---- horizontal divergence of (Hu, Hv) with central face flux: x pencils
+    for (int p = threadIdx.x; p < npen; p += blockDim.x) {
+        const int ez = p / NP2, j = p % NP, k = (p / NP) % NP;
+        const int e0 = ez * NP3 + NP * (j + NP * k);
+        T q[NP];
 #pragma unroll
-        for (int m = 0; m < NP; ++m) {
-            sx += B::D(i * NP + m) * sQ[eb + m + NP * (j + NP * k)];
-            sy += B::D(j * NP + m) * sQ[ncn + eb + i + NP * (m + NP * k)];
-        }
-        T d = cx * sx + cy * sy;
-        if (i == 0 || i == N || j == 0 || j == N) {
+        for (int m = 0; m < NP; ++m) q[m] = sQ[e0 + m];
 #pragma unroll
-            for (int s = 0; s < 4; ++s) {
-                const bool on = (s == 0 && i == 0) || (s == 1 && i == N) || (s == 2 && j == 0) ||
-                                (s == 3 && j == N);
-                if (!on) continue;
+        for (int i = 0; i < NP; ++i) {
+            T s = 0;
+#pragma unroll
+            for (int m = 0; m < NP; ++m) s += B::D(i * NP + m) * q[m];
+            T d = cx * s;
+            if (i == 0 || i == N) {
+                const int side = i == 0 ? 0 : 1;
                 T qp[4], ep, Hp;
-                outside(s, ez, i, j, k, n, qp, ep, Hp);
-                const int comp = s <= 1 ? 0 : 1;
-                const T nrm = (s == 0 || s == 2) ? T(-1) : T(1);
-                const T L = s <= 1 ? Lx : Ly;
-                const T qm = sQ[comp * ncn + n];
-                const T fm = qm * nrm;
-                const T fs = T(0.5) * (qm + qp[comp]) * nrm;
-                d += L * (fs - fm);
+                outside(side, ez, i, j, k, e0 + i, qp, ep, Hp);
+                const T nrm = i == 0 ? T(-1) : T(1);
+                d += Lx * (T(0.5) * (q[i] + qp[0]) * nrm - q[i] * nrm);
             }
+            sD[e0 + i] = d;
         }
-        sW[n] = d;
     }
     __syncthreads();
-    // ---- layer integrals J_k = (dsig/2) sum_m S[k][m] delta_m
+    // y pencils
+    for (int p = threadIdx.x; p < npen; p += blockDim.x) {
+        const int ez = p / NP2, i = p % NP, k = (p / NP) % NP;
+        const int e0 = ez * NP3 + i + NP2 * k;
+        T q[NP];
+#pragma unroll
+        for (int m = 0; m < NP; ++m) q[m] = sQ[ncn + e0 + NP * m];
+#pragma unroll
+        for (int j = 0; j < NP; ++j) {
+            T s = 0;
+#pragma unroll
+            for (int m = 0; m < NP; ++m) s += B::D(j * NP + m) * q[m];
+            T d = cy * s;
+            if (j == 0 || j == N) {
+                const int side = j == 0 ? 2 : 3;
+                T qp[4], ep, Hp;
+                outside(side, ez, i, j, k, e0 + NP * j, qp, ep, Hp);
+                const T nrm = j == 0 ? T(-1) : T(1);
+                d += Ly * (T(0.5) * (q[j] + qp[1]) * nrm - q[j] * nrm);
+            }
+            sD[e0 + NP * j] += d;
+        }
+    }
+    __syncthreads();
+    // ---- layer integrals J_k = (dsig/2) sum_m S[k][m] delta_m: z pencils
     const T hds = (T)(0.5 * G.dsig);
-    for (int t = threadIdx.x; t < nz * NP2; t += blockDim.x) {
-        const int ez = t / NP2, an = t % NP2;
+    for (int p = threadIdx.x; p < npen; p += blockDim.x) {
+        const int ez = p / NP2, an = p % NP2;
+        const int e0 = ez * NP3 + an;
         T del[NP];
 #pragma unroll
-        for (int m = 0; m < NP; ++m) del[m] = sW[ez * NP3 + an + NP2 * m];
+        for (int m = 0; m < NP; ++m) del[m] = sD[e0 + NP2 * m];
 #pragma unroll
         for (int k = 0; k < NP; ++k) {
             T s = 0;
 #pragma unroll
             for (int m = 0; m < NP; ++m) s += B::S(k * NP + m) * del[m];
-            sW[ez * NP3 + an + NP2 * k] = (k == 0) ? T(0) : hds * s;
+            sD[e0 + NP2 * k] = (k == 0) ? T(0) : hds * s;
         }
     }
     __syncthreads();
     for (int an = threadIdx.x; an < NP2; an += blockDim.x) {
         T Ib = 0;
         for (int ez = 0; ez < nz; ++ez) {
-            sBase[ez * NP2 + an] = Ib;
-            Ib = Ib + sW[ez * NP3 + an + NP2 * N];
+            sL1[ez * NP2 + an] = Ib;
+            Ib = Ib + sD[ez * NP3 + an + NP2 * N];
         }
         sItot[an] = Ib;
         if (a.mode == 1 && a.deta_out) a.deta_out[(size_t)c * NP2 + an] = -(double)Ib;
     }
     __syncthreads();
-    for (int n = threadIdx.x; n < ncn; n += blockDim.x) {
-        const int ez = n / NP3, ln = n % NP3, an = ln % NP2, k = ln / NP2;
-        const T I = sBase[ez * NP2 + an] + sW[n];
-        T s1 = (T)(G.dsig * (ez + 0.5 * ((double)B::x(k) + 1.0)));
-        if (ez == nz - 1 && k == N) s1 = T(1);
-        const T Hw = -I + s1 * sItot[an];
-        const T om = Hw * sIH[an];
-        sOm[n] = om;
-        if (a.mode == 1 && a.omega_out) a.omega_out[base + n] = om;
+    for (int p = threadIdx.x; p < npen; p += blockDim.x) {
+        const int ez = p / NP2, an = p % NP2;
+        const int e0 = ez * NP3 + an;
+        const T Ib = sL1[ez * NP2 + an], It = sItot[an], iH = sIH[an];
+#pragma unroll
+        for (int k = 0; k < NP; ++k) {
+            const T I = Ib + sD[e0 + NP2 * k];
+            T s1 = (T)(G.dsig * (ez + 0.5 * ((double)B::x(k) + 1.0)));
+            if (ez == nz - 1 && k == N) s1 = T(1);
+            const T om = (-I + s1 * It) * iH;
+            sOm[e0 + NP2 * k] = om;
+            if (a.mode == 1 && a.omega_out) a.omega_out[base + e0 + NP2 * k] = om;
+        }
     }
     __syncthreads();
 
-    // ---- right-hand side and stage update
-    const T g = (T)G.g;
-    for (int n = threadIdx.x; n < ncn; n += blockDim.x) {
-        const int ez = n / NP3, ln = n % NP3, i = ln % NP, j = (ln / NP) % NP, k = ln / NP2;
-        const int an = i + NP * j, eb = ez * NP3;
-        const T iH = sIH[an], Hh = (T)sH[an];
-        T r[4];
+    // ---- right-hand side, x pencils: advection d/dx, pressure, horizontal diffusion xx, x faces.
+    // Variables are processed one at a time to keep few values live per thread.
+    const T nh = (T)G.nu_h;
+    const bool hdiff = G.nu_h > 0.0;
+    for (int p = threadIdx.x; p < npen; p += blockDim.x) {
+        const int ez = p / NP2, j = p % NP, k = (p / NP) % NP;
+        const int e0 = ez * NP3 + NP * (j + NP * k);
+        T u[NP];
 #pragma unroll
+        for (int m = 0; m < NP; ++m) u[m] = sQ[e0 + m] * sIH[m + NP * j];
+        // both end faces: outside state, normal velocities and LF speed
+        T qp0[4], qpN[4], ep0, epN, Hp0, HpN;
+        outside(0, ez, 0, j, k, e0, qp0, ep0, Hp0);
+        outside(1, ez, N, j, k, e0 + N, qpN, epN, HpN);
+        const T unm0 = -u[0], unp0 = -qp0[0] / Hp0, lam0 = fmax(fabs(unm0), fabs(unp0));
+        const T unmN = u[N], unpN = qpN[0] / HpN, lamN = fmax(fabs(unmN), fabs(unpN));
+#pragma unroll 1
         for (int v = 0; v < 4; ++v) {
-            const T *q = sQ + v * ncn + eb;
-            T ax = 0, ay = 0, as = 0;
+            T q[NP];
 #pragma unroll
-            for (int m = 0; m < NP; ++m) {
-                const int px = m + NP * (j + NP * k), py = i + NP * (m + NP * k), pz = an + NP2 * m;
-                ax += B::D(i * NP + m) * q[px] * sU[eb + px];
-                ay += B::D(j * NP + m) * q[py] * sV[eb + py];
-                as += B::D(k * NP + m) * q[pz] * sOm[eb + pz];
-            }
-            r[v] = -(cx * ax + cy * ay + cs * as);
-        }
-        const T fa = (T)a.f[(size_t)c * NP2 + an];
-        T gex = 0, gey = 0;
+            for (int m = 0; m < NP; ++m) q[m] = sQ[v * ncn + e0 + m];
 #pragma unroll
-        for (int m = 0; m < NP; ++m) {
-            gex += B::D(i * NP + m) * (T)sEta[m + NP * j];
-            gey += B::D(j * NP + m) * (T)sEta[i + NP * m];
-        }
-        const T Hu = sQ[n], Hv = sQ[ncn + n];
-        r[0] += fa * Hv - g * Hh * cx * gex;
-        r[1] += -fa * Hu - g * Hh * cy * gey;
-        if (G.nu_h > 0.0) {
-            T uxx = 0, uyy = 0, vxx = 0, vyy = 0;
+            for (int i = 0; i < NP; ++i) {
+                T s = 0;
 #pragma unroll
-            for (int l = 0; l < NP; ++l) {
-                const int px = eb + l + NP * (j + NP * k), py = eb + i + NP * (l + NP * k);
-                uxx += B::D2(i * NP + l) * sU[px];
-                uyy += B::D2(j * NP + l) * sU[py];
-                vxx += B::D2(i * NP + l) * sV[px];
-                vyy += B::D2(j * NP + l) * sV[py];
-            }
-            const T nh = (T)G.nu_h;
-            r[0] += nh * Hh * (cx * cx * uxx + cy * cy * uyy);
-            r[1] += nh * Hh * (cx * cx * vxx + cy * cy * vyy);
-        }
-        {
-            const T kap[4] = {(T)G.nu_v, (T)G.nu_v, (T)G.kT, (T)G.kS};
+                for (int m = 0; m < NP; ++m) s += B::D(i * NP + m) * (q[m] * u[m]);
+                T r = -cx * s;
+                const T Hh = sHt[i + NP * j];
+                if (v == 0) {
+                    T ge = 0;
 #pragma unroll
-            for (int v = 0; v < 4; ++v) {
-                if (!(kap[v] > T(0))) continue;
-                const T *q = sQ + v * ncn + eb;
-                T szz = 0;
-#pragma unroll
-                for (int l = 0; l < NP; ++l) szz += B::D2(k * NP + l) * (q[an + NP2 * l] * iH);
-                r[v] += kap[v] * iH * cs * cs * szz;
-            }
-        }
-        if (i == 0 || i == N || j == 0 || j == N) {
-#pragma unroll
-            for (int s = 0; s < 4; ++s) {
-                const bool on = (s == 0 && i == 0) || (s == 1 && i == N) || (s == 2 && j == 0) ||
-                                (s == 3 && j == N);
-                if (!on) continue;
-                T qp[4], ep, Hp;
-                outside(s, ez, i, j, k, n, qp, ep, Hp);
-                const T nx = s == 0 ? T(-1) : (s == 1 ? T(1) : T(0));
-                const T ny = s == 2 ? T(-1) : (s == 3 ? T(1) : T(0));
-                const T L = s <= 1 ? Lx : Ly;
-                const T unm = (Hu * nx + Hv * ny) * iH;
-                const T unp = (qp[0] * nx + qp[1] * ny) / Hp;
-                const T lam = fmax(fabs(unm), fabs(unp));
-#pragma unroll
-                for (int v = 0; v < 4; ++v) {
-                    const T qm = sQ[v * ncn + n];
-                    const T fs = T(0.5) * (qm * unm + qp[v] * unp) - T(0.5) * lam * (qp[v] - qm);
-                    r[v] -= L * (fs - qm * unm);
+                    for (int m = 0; m < NP; ++m) ge += B::D(i * NP + m) * sEt[m + NP * j];
+                    r -= g * Hh * cx * ge;
                 }
-                const T pj = g * Hh * T(0.5) * (ep - (T)sEta[an]);
-                r[0] -= L * pj * nx;
-                r[1] -= L * pj * ny;
+                if (v <= 1 && hdiff) {
+                    T xx = 0;
+#pragma unroll
+                    for (int m = 0; m < NP; ++m)
+                        xx += B::D2(i * NP + m) * (v == 0 ? u[m] : q[m] * sIH[m + NP * j]);
+                    r += nh * Hh * (cx * cx * xx);
+                }
+                if (i == 0 || i == N) {
+                    const T qm = q[i];
+                    const T qpv = i == 0 ? sel4(qp0, v) : sel4(qpN, v);
+                    const T unm = i == 0 ? unm0 : unmN, unp = i == 0 ? unp0 : unpN;
+                    const T lam = i == 0 ? lam0 : lamN;
+                    const T fs = T(0.5) * (qm * unm + qpv * unp) - T(0.5) * lam * (qpv - qm);
+                    r -= Lx * (fs - qm * unm);
+                    if (v == 0) {
+                        const T nx = i == 0 ? T(-1) : T(1);
+                        const T ep = i == 0 ? ep0 : epN;
+                        r -= Lx * (g * Hh * T(0.5) * (ep - sEt[i + NP * j])) * nx;
+                    }
+                }
+                sR[v * ncn + e0 + i] = r;
             }
         }
-        if (k == 0 || k == N) {
-            const T nrm = k == 0 ? T(-1) : T(1);
-            const T wm = sOm[n] * nrm;
-            const bool interior = (k == 0 && ez > 0) || (k == N && ez < nz - 1);
-            if (interior) {
-                const int n2 = k == 0 ? (ez - 1) * NP3 + an + NP2 * N : (ez + 1) * NP3 + an;
-                const T wp = sOm[n2] * nrm;
-                const T lam = fmax(fabs(wm), fabs(wp));
+    }
+    __syncthreads();
+    // ---- y pencils: advection d/dy, pressure, horizontal diffusion yy, y faces
+    for (int p = threadIdx.x; p < npen; p += blockDim.x) {
+        const int ez = p / NP2, i = p % NP, k = (p / NP) % NP;
+        const int e0 = ez * NP3 + i + NP2 * k;
+        T w[NP];
 #pragma unroll
-                for (int v = 0; v < 4; ++v) {
-                    const T qm = sQ[v * ncn + n], qpp = sQ[v * ncn + n2];
-                    const T fs = T(0.5) * (qm * wm + qpp * wp) - T(0.5) * lam * (qpp - qm);
-                    r[v] -= Ls * (fs - qm * wm);
+        for (int m = 0; m < NP; ++m) w[m] = sQ[ncn + e0 + NP * m] * sIH[i + NP * m];
+        T qp0[4], qpN[4], ep0, epN, Hp0, HpN;
+        outside(2, ez, i, 0, k, e0, qp0, ep0, Hp0);
+        outside(3, ez, i, N, k, e0 + NP * N, qpN, epN, HpN);
+        const T unm0 = -w[0], unp0 = -qp0[1] / Hp0, lam0 = fmax(fabs(unm0), fabs(unp0));
+        const T unmN = w[N], unpN = qpN[1] / HpN, lamN = fmax(fabs(unmN), fabs(unpN));
+#pragma unroll 1
+        for (int v = 0; v < 4; ++v) {
+            T q[NP];
+#pragma unroll
+            for (int m = 0; m < NP; ++m) q[m] = sQ[v * ncn + e0 + NP * m];
+#pragma unroll
+            for (int j = 0; j < NP; ++j) {
+                T s = 0;
+#pragma unroll
+                for (int m = 0; m < NP; ++m) s += B::D(j * NP + m) * (q[m] * w[m]);
+                T r = -cy * s;
+                const T Hh = sHt[i + NP * j];
+                if (v == 1) {
+                    T ge = 0;
+#pragma unroll
+                    for (int m = 0; m < NP; ++m) ge += B::D(j * NP + m) * sEt[i + NP * m];
+                    r -= g * Hh * cy * ge;
                 }
-            } else {
+                if (v <= 1 && hdiff) {
+                    T yy = 0;
 #pragma unroll
-                for (int v = 0; v < 4; ++v) r[v] -= Ls * (T(0) - sQ[v * ncn + n] * wm);
+                    for (int m = 0; m < NP; ++m)
+                        yy += B::D2(j * NP + m) * (v == 1 ? w[m] : q[m] * sIH[i + NP * m]);
+                    r += nh * Hh * (cy * cy * yy);
+                }
+                if (j == 0 || j == N) {
+                    const T qm = q[j];
+                    const T qpv = j == 0 ? sel4(qp0, v) : sel4(qpN, v);
+                    const T unm = j == 0 ? unm0 : unmN, unp = j == 0 ? unp0 : unpN;
+                    const T lam = j == 0 ? lam0 : lamN;
+                    const T fs = T(0.5) * (qm * unm + qpv * unp) - T(0.5) * lam * (qpv - qm);
+                    r -= Ly * (fs - qm * unm);
+                    if (v == 1) {
+                        const T ny = j == 0 ? T(-1) : T(1);
+                        const T ep = j == 0 ? ep0 : epN;
+                        r -= Ly * (g * Hh * T(0.5) * (ep - sEt[i + NP * j])) * ny;
+                    }
+                }
+                sR[v * ncn + e0 + NP * j] += r;
+            }
+        }
+    }
+    __syncthreads();
+    // ---- z pencils: advection d/dsigma, Coriolis, vertical diffusion, sigma faces, surface
+    // and bed stresses, then the LSRK update and the FP64 column increments
+    for (int p = threadIdx.x; p < npen; p += blockDim.x) {
+        const int ez = p / NP2, an = p % NP2;
+        const int e0 = ez * NP3 + an;
+        const T iH = sIH[an], fa = (T)a.f[(size_t)c * NP2 + an];
+        const bool bed = ez == 0, top = ez == nz - 1;
+        T om[NP];
+#pragma unroll
+        for (int m = 0; m < NP; ++m) om[m] = sOm[e0 + NP2 * m];
+        // bed stress (only the bottom layer's k = 0 node) and surface stress
+        T fbx = 0, fby = 0;
+        if (bed) {
+            const T uu = sQ[e0] * iH, vv = sQ[ncn + e0] * iH;
+            const T sp = sqrt(uu * uu + vv * vv);
+            fbx = -Ls * (T)G.cd * sp * uu;
+            fby = -Ls * (T)G.cd * sp * vv;
+        }
+        T fsx = 0, fsy = 0;
+        if (top) {
+            fsx = Ls * (T)(a.taux[(size_t)c * NP2 + an] / G.rho0);
+            fsy = Ls * (T)(a.tauy[(size_t)c * NP2 + an] / G.rho0);
+        }
+        const T w0 = om[0] * T(-1), wN = om[N];
+        const int nb0 = (ez - 1) * NP3 + an + NP2 * N, nbN = (ez + 1) * NP3 + an;
+        const T wp0 = bed ? T(0) : sOm[nb0] * T(-1), wpN = top ? T(0) : sOm[nbN];
+        const T lam0 = fmax(fabs(w0), fabs(wp0)), lamN = fmax(fabs(wN), fabs(wpN));
+        T incU = 0, incV = 0;
+#pragma unroll 1
+        for (int v = 0; v < 4; ++v) {
+            const T kp = v <= 1 ? (T)G.nu_v : (v == 2 ? (T)G.kT : (T)G.kS);
+            T q[NP];
+#pragma unroll
+            for (int m = 0; m < NP; ++m) q[m] = sQ[v * ncn + e0 + NP2 * m];
+#pragma unroll
+            for (int k = 0; k < NP; ++k) {
+                const int n = e0 + NP2 * k;
+                T s = 0, z2 = 0;
+#pragma unroll
+                for (int m = 0; m < NP; ++m) {
+                    s += B::D(k * NP + m) * (q[m] * om[m]);
+                    z2 += B::D2(k * NP + m) * (q[m] * iH);
+                }
+                T r = sR[v * ncn + n] - cs * s;
+                if (kp > T(0)) r += kp * iH * cs * cs * z2;
+                if (v == 0) r += fa * sQ[ncn + n];
+                if (v == 1) r += -fa * sQ[n];
                 if (k == 0) {
-                    const T uu = Hu * iH, vv = Hv * iH;
-                    const T sp = sqrt(uu * uu + vv * vv);
-                    r[0] -= Ls * (T)G.cd * sp * uu;
-                    r[1] -= Ls * (T)G.cd * sp * vv;
+                    const T wm = w0;
+                    if (!bed) {
+                        const T qpp = sQ[v * ncn + nb0];
+                        const T fs = T(0.5) * (q[0] * wm + qpp * wp0) - T(0.5) * lam0 * (qpp - q[0]);
+                        r -= Ls * (fs - q[0] * wm);
+                    } else {
+                        r -= Ls * (T(0) - q[0] * wm);
+                        if (v == 0) r += fbx;
+                        if (v == 1) r += fby;
+                    }
+                }
+                if (k == N) {
+                    const T wm = wN;
+                    if (!top) {
+                        const T qpp = sQ[v * ncn + nbN];
+                        const T fs = T(0.5) * (q[N] * wm + qpp * wpN) - T(0.5) * lamN * (qpp - q[N]);
+                        r -= Ls * (fs - q[N] * wm);
+                    } else {
+                        r -= Ls * (T(0) - q[N] * wm);
+                        if (v == 0) r += fsx;
+                        if (v == 1) r += fsy;
+                    }
+                }
+                const size_t gi = base + n;
+                if (a.mode == 1) {
+                    a.res[v][gi] = r;
                 } else {
-                    r[0] += Ls * (T)(a.taux[(size_t)c * NP2 + an] / G.rho0);
-                    r[1] += Ls * (T)(a.tauy[(size_t)c * NP2 + an] / G.rho0);
+                    const T rn = (a.first ? T(0) : a.A * a.res[v][gi]) + a.dt * r;
+                    a.res[v][gi] = rn;
+                    a.qout[v][gi] = q[k] + a.B * rn;
+                    if (v == 0) incU += B::w(k) * (a.B * rn);
+                    if (v == 1) incV += B::w(k) * (a.B * rn);
                 }
             }
         }
-        const size_t gi = base + n;
-        if (a.mode == 1) {
-#pragma unroll
-            for (int v = 0; v < 4; ++v) a.res[v][gi] = r[v];
-        } else {
-            T rn[4];
-#pragma unroll
-            for (int v = 0; v < 4; ++v) {
-                rn[v] = (a.first ? T(0) : a.A * a.res[v][gi]) + a.dt * r[v];
-                a.res[v][gi] = rn[v];
-                a.qout[v][gi] = sQ[v * ncn + n] + a.B * rn[v];
-            }
-            sW[n] = B::w(k) * (a.B * rn[0]);
-            sW2[n] = B::w(k) * (a.B * rn[1]);
+        if (a.mode == 0) {
+            sL1[ez * NP2 + an] = incU;
+            sL2[ez * NP2 + an] = incV;
         }
     }
     if (a.mode == 0) {
         __syncthreads();
         for (int an = threadIdx.x; an < NP2; an += blockDim.x) {
             double su = 0.0, sv = 0.0;
-            for (int ez = 0; ez < nz; ++ez)
-#pragma unroll
-                for (int k = 0; k < NP; ++k) {
-                    su += (double)sW[ez * NP3 + an + NP2 * k];
-                    sv += (double)sW2[ez * NP3 + an + NP2 * k];
-                }
+            for (int ez = 0; ez < nz; ++ez) {
+                su += (double)sL1[ez * NP2 + an];
+                sv += (double)sL2[ez * NP2 + an];
+            }
             const size_t i2 = (size_t)c * NP2 + an;
             const double hd = 0.5 * G.dsig;
             a.dHU3[i2] = (a.first ? 0.0 : a.dHU3[i2]) + hd * su;
@@ -363,40 +485,64 @@ __global__ void __launch_bounds__(256) dg3d_stage_kernel(StageArgs<T> a) {
 }
 
 // ------------------------------------------------------------------------- barotropic (FP64)
+// One CTA per tile of BARO_CPB water columns (one thread per 2D node): the column's state is
+// staged in shared memory with 1/H computed once per node; element-local derivatives read the
+// tile, face fluxes read the neighbouring column's face node from global memory.
+constexpr int BARO_CPB = 8;
+
 struct BaroArgs {
     const double *e, *hu, *hv, *h, *f, *Fx, *Fy, *tdev;
     double toff;
     Geo G;
+    int64_t ncol;
 };
 
 template <int NP>
-__device__ void baro_phi(const BaroArgs &a, int c, int an, double &re, double &ru, double &rv) {
+__device__ __forceinline__ bool baro_tile_phi(const BaroArgs &a, double &re, double &ru,
+                                              double &rv, int64_t &t) {
     constexpr int NP2 = NP * NP, N = NP - 1;
+    __shared__ double sE[BARO_CPB * NP2], sU[BARO_CPB * NP2], sV[BARO_CPB * NP2],
+        sI[BARO_CPB * NP2], sD[NP2];
     const Geo &G = a.G;
-    const int ex = c % G.nx, ey = c / G.nx, i = an % NP, j = an / NP;
-    const size_t o = (size_t)c * NP2;
-    const double H = a.e[o + an] + a.h[o + an];
+    const int lc = threadIdx.x / NP2, an = threadIdx.x % NP2, i = an % NP, j = an / NP;
+    const int64_t c = (int64_t)blockIdx.x * BARO_CPB + lc;
+    const bool valid = c < a.ncol;
+    if (threadIdx.x < NP2) sD[threadIdx.x] = cB.D[threadIdx.x];
+    t = c * NP2 + an;
+    double H = 1.0;
+    if (valid) {
+        const double e = a.e[t];
+        H = e + a.h[t];
+        sE[threadIdx.x] = e;
+        sU[threadIdx.x] = a.hu[t];
+        sV[threadIdx.x] = a.hv[t];
+        sI[threadIdx.x] = 1.0 / H;
+    }
+    __syncthreads();
+    if (!valid) return false;
+    const int b0 = lc * NP2;
     double dhu = 0, dhv = 0, auu = 0, auv = 0, avu = 0, avv = 0, gex = 0, gey = 0;
 #pragma unroll
     for (int m = 0; m < NP; ++m) {
-        const size_t px = o + m + NP * j, py = o + i + NP * m;
-        const double Hx = a.e[px] + a.h[px], Hy = a.e[py] + a.h[py];
-        const double dxm = cB.D[i * NP + m], dym = cB.D[j * NP + m];
-        dhu += dxm * a.hu[px];
-        dhv += dym * a.hv[py];
-        auu += dxm * a.hu[px] * a.hu[px] / Hx;
-        avu += dxm * a.hv[px] * a.hu[px] / Hx;
-        auv += dym * a.hu[py] * a.hv[py] / Hy;
-        avv += dym * a.hv[py] * a.hv[py] / Hy;
-        gex += dxm * a.e[px];
-        gey += dym * a.e[py];
+        const int px = b0 + m + NP * j, py = b0 + i + NP * m;
+        const double dxm = sD[i * NP + m], dym = sD[j * NP + m];
+        const double ux = sU[px], vx = sV[px], ix = sI[px];
+        const double uy = sU[py], vy = sV[py], iy = sI[py];
+        dhu += dxm * ux;
+        dhv += dym * vy;
+        auu += dxm * ux * ux * ix;
+        avu += dxm * vx * ux * ix;
+        auv += dym * uy * vy * iy;
+        avv += dym * vy * vy * iy;
+        gex += dxm * sE[px];
+        gey += dym * sE[py];
     }
+    const double hu0 = sU[threadIdx.x], hv0 = sV[threadIdx.x];
     re = -(G.cx * dhu + G.cy * dhv);
-    ru = -(G.cx * auu + G.cy * auv) - G.g * H * G.cx * gex + a.f[o + an] * a.hv[o + an] +
-         (a.Fx ? a.Fx[o + an] : 0.0);
-    rv = -(G.cx * avu + G.cy * avv) - G.g * H * G.cy * gey - a.f[o + an] * a.hu[o + an] +
-         (a.Fy ? a.Fy[o + an] : 0.0);
-    if (!(i == 0 || i == N || j == 0 || j == N)) return;
+    ru = -(G.cx * auu + G.cy * auv) - G.g * H * G.cx * gex + a.f[t] * hv0 + (a.Fx ? a.Fx[t] : 0.0);
+    rv = -(G.cx * avu + G.cy * avv) - G.g * H * G.cy * gey - a.f[t] * hu0 + (a.Fy ? a.Fy[t] : 0.0);
+    if (!(i == 0 || i == N || j == 0 || j == N)) return true;
+    const int ex = (int)(c % G.nx), ey = (int)(c / G.nx);
     const double etide = tide_at(G, a.tdev[0] + a.toff);
 #pragma unroll
     for (int s = 0; s < 4; ++s) {
@@ -406,17 +552,18 @@ __device__ void baro_phi(const BaroArgs &a, int c, int an, double &re, double &r
         const double nx = s == 0 ? -1.0 : (s == 1 ? 1.0 : 0.0);
         const double ny = s == 2 ? -1.0 : (s == 3 ? 1.0 : 0.0);
         const double L = s <= 1 ? G.Lx : G.Ly;
-        int nc = -1, ni = i, nj = j;
+        int64_t nc = -1;
+        int ni = i, nj = j;
         if (s == 0 && ex > 0) { nc = c - 1; ni = N; }
         if (s == 1 && ex < G.nx - 1) { nc = c + 1; ni = 0; }
         if (s == 2 && ey > 0) { nc = c - G.nx; nj = N; }
         if (s == 3 && ey < G.ny - 1) { nc = c + G.nx; nj = 0; }
-        double UL[3] = {H, a.hu[o + an], a.hv[o + an]}, UR[3];
+        double UL[3] = {H, hu0, hv0}, UR[3];
         if (nc >= 0) {
-            const size_t q = (size_t)nc * NP2 + ni + NP * nj;
+            const int64_t q = nc * NP2 + ni + NP * nj;
             UR[0] = a.e[q] + a.h[q]; UR[1] = a.hu[q]; UR[2] = a.hv[q];
         } else if (G.bc[s] == DRF_BC_TIDE) {
-            UR[0] = etide + a.h[o + an];
+            UR[0] = etide + a.h[t];
             const double r = UR[0] / H;
             UR[1] = UL[1] * r; UR[2] = UL[2] * r;
         } else {
@@ -430,26 +577,24 @@ __device__ void baro_phi(const BaroArgs &a, int c, int an, double &re, double &r
         ru -= L * (Fs[1] - Fm[1]);
         rv -= L * (Fs[2] - Fm[2]);
     }
+    return true;
 }
 
 template <int NP>
-__global__ void baro_rhs_kernel(BaroArgs a, int64_t n2, double *ke, double *ku, double *kv) {
-    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (t >= n2) return;
+__global__ void baro_rhs_kernel(BaroArgs a, double *ke, double *ku, double *kv) {
     double re, ru, rv;
-    baro_phi<NP>(a, (int)(t / (NP * NP)), (int)(t % (NP * NP)), re, ru, rv);
+    int64_t t;
+    if (!baro_tile_phi<NP>(a, re, ru, rv, t)) return;
     ke[t] = re; ku[t] = ru; kv[t] = rv;
 }
 
 // F = (3D-integrated increment)/dt - Phi(U^n); keeps HU^n, HV^n for the transport correction.
 template <int NP>
-__global__ void baro_force_kernel(BaroArgs a, int64_t n2, double dt, const double *dHU3,
-                                  const double *dHV3, double *Fx, double *Fy, double *HUo,
-                                  double *HVo) {
-    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (t >= n2) return;
+__global__ void baro_force_kernel(BaroArgs a, double dt, const double *dHU3, const double *dHV3,
+                                  double *Fx, double *Fy, double *HUo, double *HVo) {
     double re, ru, rv;
-    baro_phi<NP>(a, (int)(t / (NP * NP)), (int)(t % (NP * NP)), re, ru, rv);
+    int64_t t;
+    if (!baro_tile_phi<NP>(a, re, ru, rv, t)) return;
     Fx[t] = dHU3[t] / dt - ru;
     Fy[t] = dHV3[t] / dt - rv;
     HUo[t] = a.hu[t];
@@ -457,12 +602,11 @@ __global__ void baro_force_kernel(BaroArgs a, int64_t n2, double dt, const doubl
 }
 
 template <int NP>
-__global__ void baro_pred_kernel(BaroArgs a, int64_t n2, double dtb, double *k1e, double *k1u,
-                                 double *k1v, double *es, double *us, double *vs) {
-    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (t >= n2) return;
+__global__ void baro_pred_kernel(BaroArgs a, double dtb, double *k1e, double *k1u, double *k1v,
+                                 double *es, double *us, double *vs) {
     double re, ru, rv;
-    baro_phi<NP>(a, (int)(t / (NP * NP)), (int)(t % (NP * NP)), re, ru, rv);
+    int64_t t;
+    if (!baro_tile_phi<NP>(a, re, ru, rv, t)) return;
     k1e[t] = re; k1u[t] = ru; k1v[t] = rv;
     es[t] = a.e[t] + dtb * re;
     us[t] = a.hu[t] + dtb * ru;
@@ -470,13 +614,12 @@ __global__ void baro_pred_kernel(BaroArgs a, int64_t n2, double dtb, double *k1e
 }
 
 template <int NP>
-__global__ void baro_corr_kernel(BaroArgs a, int64_t n2, double dtb, const double *k1e,
-                                 const double *k1u, const double *k1v, double *e, double *hu,
-                                 double *hv, double *esum, int first) {
-    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (t >= n2) return;
+__global__ void baro_corr_kernel(BaroArgs a, double dtb, const double *k1e, const double *k1u,
+                                 const double *k1v, double *e, double *hu, double *hv,
+                                 double *esum, int first) {
     double re, ru, rv;
-    baro_phi<NP>(a, (int)(t / (NP * NP)), (int)(t % (NP * NP)), re, ru, rv);
+    int64_t t;
+    if (!baro_tile_phi<NP>(a, re, ru, rv, t)) return;
     const double hd = 0.5 * dtb;
     const double en = e[t] + hd * (k1e[t] + re);
     e[t] = en;
@@ -487,14 +630,14 @@ __global__ void baro_corr_kernel(BaroArgs a, int64_t n2, double dtb, const doubl
 
 __global__ void baro_finish_kernel(int64_t n2, int nsub, double dt, const double *esum,
                                    double *eta_avg, const double *HU, const double *HV,
-                                   const double *HUo, const double *HVo, double *dHU3, double *dHV3,
-                                   double *tdev) {
+                                   const double *HUo, const double *HVo, const double *dHU3,
+                                   const double *dHV3, double *corrU, double *corrV, double *tdev) {
     const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (t == 0) tdev[0] = tdev[0] + dt;
     if (t >= n2) return;
     eta_avg[t] = esum[t] / nsub;
-    dHU3[t] = HU[t] - (HUo[t] + dHU3[t]);
-    dHV3[t] = HV[t] - (HVo[t] + dHV3[t]);
+    corrU[t] = HU[t] - (HUo[t] + dHU3[t]);
+    corrV[t] = HV[t] - (HVo[t] + dHV3[t]);
 }
 
 template <typename T, int NP>
@@ -654,8 +797,10 @@ struct drf_dg {
     double *h = nullptr, *f = nullptr, *taux = nullptr, *tauy = nullptr, *eta = nullptr,
            *HU = nullptr, *HV = nullptr, *eta_avg = nullptr, *esum = nullptr, *Fx = nullptr,
            *Fy = nullptr, *HUo = nullptr, *HVo = nullptr, *k1[3] = {}, *us[3] = {}, *dHU3 = nullptr,
-           *dHV3 = nullptr, *tdev = nullptr, *scratch2 = nullptr;
+           *dHV3 = nullptr, *tdev = nullptr, *scratch2 = nullptr, *corrU = nullptr,
+           *corrV = nullptr;
     int cur = 0;
+    bool pending = false;  // a transport correction in corrU/corrV is not yet in q(cur)
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     double graph_dt = 0.0;
     int graph_nsub = 0;
@@ -675,9 +820,16 @@ struct drf_dg {
         if (own) cudaStreamDestroy(own);
     }
 
+    int stage_threads() const {
+        const int npen = G.nz * np2;
+        int bs = ((npen + 31) / 32) * 32;
+        return bs < 64 ? 64 : (bs > 512 ? 512 : bs);
+    }
+
     template <typename T, int NP>
     void launch_stage(int in, int out, int s, double dt, int mode, void *const *rout,
-                      T *omega_out, double *deta_out, const double *eta_use, double toff) {
+                      T *omega_out, double *deta_out, const double *eta_use, double toff,
+                      bool with_corr = false) {
         StageArgs<T> a{};
         for (int v = 0; v < 4; ++v) {
             a.qin[v] = (const T *)q(in, v);
@@ -690,9 +842,30 @@ struct drf_dg {
         a.omega_out = omega_out; a.deta_out = deta_out;
         a.A = (T)LSRK_A[s]; a.B = (T)LSRK_B[s]; a.dt = (T)dt;
         a.mode = mode; a.first = (s == 0);
+        a.corrU = with_corr ? corrU : nullptr;
+        a.corrV = with_corr ? corrV : nullptr;
         a.G = G;
-        dg3d_stage_kernel<T, NP><<<ncol, 256, smem, stream>>>(a);
+        dg3d_stage_kernel<T, NP><<<ncol, stage_threads(), smem, stream>>>(a);
         DRF_LAUNCHED();
+    }
+
+    // folds a pending transport correction into the current state buffer
+    template <typename T, int NP>
+    void materialize_t() {
+        if (!pending) return;
+        correct3d_kernel<T, NP><<<blocks_for(n3), 256, 0, stream>>>(n3, G.nz, (T *)q(cur, 0),
+                                                                  (T *)q(cur, 1), corrU, corrV);
+        DRF_LAUNCHED();
+        DRF_CUDA(cudaMemsetAsync(corrU, 0, n2 * 8, stream));
+        DRF_CUDA(cudaMemsetAsync(corrV, 0, n2 * 8, stream));
+        pending = false;
+    }
+    void materialize() {
+        with_types([&](auto tv, auto npc) {
+            using T = decltype(tv);
+            constexpr int NP = decltype(npc)::value;
+            this->template materialize_t<T, NP>();
+        });
     }
 
     template <int NP>
@@ -700,7 +873,7 @@ struct drf_dg {
         BaroArgs b{};
         b.e = e; b.hu = u; b.hv = v; b.h = h; b.f = f;
         b.Fx = forced ? Fx : nullptr; b.Fy = forced ? Fy : nullptr;
-        b.tdev = tdev; b.toff = toff; b.G = G;
+        b.tdev = tdev; b.toff = toff; b.G = G; b.ncol = ncol;
         return b;
     }
 
@@ -710,29 +883,29 @@ struct drf_dg {
         int src = in;
         for (int s = 0; s < 5; ++s) {
             const int dst = (s % 2 == 0) ? out : in;
-            launch_stage<T, NP>(src, dst, s, dt, 0, nullptr, nullptr, nullptr, eta, 0.0);
+            // stage 0 folds in the transport correction left by the previous step
+            launch_stage<T, NP>(src, dst, s, dt, 0, nullptr, nullptr, nullptr, eta, 0.0, s == 0);
             src = dst;
         }
         // after 5 stages the state is in `out`
-        const unsigned nb2 = blocks_for(n2);
-        baro_force_kernel<NP><<<nb2, 256, 0, stream>>>(baro<NP>(eta, HU, HV, false, 0.0), n2, dt,
-                                                       dHU3, dHV3, Fx, Fy, HUo, HVo);
+        const unsigned nbt = (unsigned)((ncol + BARO_CPB - 1) / BARO_CPB);
+        const int bt = BARO_CPB * NP * NP;
+        baro_force_kernel<NP><<<nbt, bt, 0, stream>>>(baro<NP>(eta, HU, HV, false, 0.0), dt, dHU3,
+                                                      dHV3, Fx, Fy, HUo, HVo);
         DRF_LAUNCHED();
         const double dtb = dt / nsub;
         for (int m = 0; m < nsub; ++m) {
-            baro_pred_kernel<NP><<<nb2, 256, 0, stream>>>(baro<NP>(eta, HU, HV, true, m * dtb), n2,
-                                                          dtb, k1[0], k1[1], k1[2], us[0], us[1], us[2]);
+            baro_pred_kernel<NP><<<nbt, bt, 0, stream>>>(baro<NP>(eta, HU, HV, true, m * dtb), dtb,
+                                                         k1[0], k1[1], k1[2], us[0], us[1], us[2]);
             DRF_LAUNCHED();
-            baro_corr_kernel<NP><<<nb2, 256, 0, stream>>>(
-                baro<NP>(us[0], us[1], us[2], true, m * dtb + dtb), n2, dtb, k1[0], k1[1], k1[2],
-                eta, HU, HV, esum, m == 0);
+            baro_corr_kernel<NP><<<nbt, bt, 0, stream>>>(
+                baro<NP>(us[0], us[1], us[2], true, m * dtb + dtb), dtb, k1[0], k1[1], k1[2], eta,
+                HU, HV, esum, m == 0);
             DRF_LAUNCHED();
         }
-        baro_finish_kernel<<<nb2, 256, 0, stream>>>(n2, nsub, dt, esum, eta_avg, HU, HV, HUo, HVo,
-                                                    dHU3, dHV3, tdev);
-        DRF_LAUNCHED();
-        correct3d_kernel<T, NP><<<blocks_for(n3), 256, 0, stream>>>(n3, G.nz, (T *)q(out, 0),
-                                                                  (T *)q(out, 1), dHU3, dHV3);
+        baro_finish_kernel<<<blocks_for(n2), 256, 0, stream>>>(n2, nsub, dt, esum, eta_avg, HU, HV,
+                                                               HUo, HVo, dHU3, dHV3, corrU, corrV,
+                                                               tdev);
         DRF_LAUNCHED();
     }
 
@@ -847,7 +1020,7 @@ int drf_dg_create(const drf_mesh_desc *mesh, const drf_dg_params *params, const 
         m->stream = m->own;
         // shared memory of the stage kernel: 9 column arrays + per-layer bases + 2D scalars
         const int ncn = mesh->nz * m->np3;
-        m->smem = (size_t)(9 * ncn + mesh->nz * m->np2 + 2 * m->np2) * m->tsz + 16 + 2 * m->np2 * 8 + 16;
+        m->smem = stage_smem_elems<double>(mesh->nz, m->np) * m->tsz;
         int dev = 0, maxsm = 0;
         DRF_CUDA(cudaGetDevice(&dev));
         DRF_CUDA(cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
@@ -861,7 +1034,7 @@ int drf_dg_create(const drf_mesh_desc *mesh, const drf_dg_params *params, const 
         });
         m->q3.alloc((size_t)16 * m->n3 * m->tsz);
         DRF_CUDA(cudaMemset(m->q3.p, 0, m->q3.n));
-        const int n2arrays = 25;
+        const int n2arrays = 27;
         m->d2.alloc((size_t)n2arrays * m->n2 + 8);
         DRF_CUDA(cudaMemset(m->d2.p, 0, m->d2.n * 8));
         double *p = m->d2.p;
@@ -872,6 +1045,7 @@ int drf_dg_create(const drf_mesh_desc *mesh, const drf_dg_params *params, const 
         for (int i = 0; i < 3; ++i) m->k1[i] = take();
         for (int i = 0; i < 3; ++i) m->us[i] = take();
         m->dHU3 = take(); m->dHV3 = take(); m->scratch2 = take();
+        m->corrU = take(); m->corrV = take();
         m->tdev = p;
         DRF_CUDA(cudaMemcpy(m->h, h, m->n2 * 8, cudaMemcpyHostToDevice));
         DRF_CUDA(cudaMemcpy(m->f, f, m->n2 * 8, cudaMemcpyHostToDevice));
@@ -938,6 +1112,9 @@ int drf_dg_upload_state(drf_dg *m, const double *const *q4, const double *eta, d
         DRF_CUDA(cudaMemcpyAsync(m->HU, hu.data(), m->n2 * 8, cudaMemcpyHostToDevice, m->stream));
         DRF_CUDA(cudaMemcpyAsync(m->HV, hv.data(), m->n2 * 8, cudaMemcpyHostToDevice, m->stream));
         DRF_CUDA(cudaMemcpyAsync(m->tdev, &t, 8, cudaMemcpyHostToDevice, m->stream));
+        DRF_CUDA(cudaMemsetAsync(m->corrU, 0, m->n2 * 8, m->stream));
+        DRF_CUDA(cudaMemsetAsync(m->corrV, 0, m->n2 * 8, m->stream));
+        m->pending = false;
         DRF_CUDA(cudaStreamSynchronize(m->stream));
         m->drop_graphs();
     });
@@ -947,6 +1124,7 @@ int drf_dg_download_state(drf_dg *m, double *const *q4, double *eta, double *HU,
                           double *eta_avg, double *t) {
     return guard([&] {
         check_model(m);
+        m->materialize();
         DRF_CUDA(cudaStreamSynchronize(m->stream));
         if (q4)
             for (int v = 0; v < 4; ++v)
@@ -962,6 +1140,7 @@ int drf_dg_download_state(drf_dg *m, double *const *q4, double *eta, double *HU,
 int drf_dg_compute_rhs(drf_dg *m, double *const *r4, double *omega, double *deta) {
     return guard([&] {
         check_model(m);
+        m->materialize();
         void *rout[4] = {m->tmp(0), m->tmp(1), m->tmp(2), m->tmp(3)};
         m->with_types([&](auto tv, auto npc) {
             using T = decltype(tv);
@@ -990,9 +1169,9 @@ int drf_dg_compute_rhs2d(drf_dg *m, const double *Fx, const double *Fy, double t
         DRF_CUDA(cudaStreamSynchronize(m->stream));
         dispatch_np(m->np, [&](auto npc) {
             constexpr int NP = decltype(npc)::value;
-            baro_rhs_kernel<NP><<<blocks_for(m->n2), 256, 0, m->stream>>>(
-                m->baro<NP>(m->eta, m->HU, m->HV, true, time - tcur), m->n2, m->k1[0], m->k1[1],
-                m->k1[2]);
+            baro_rhs_kernel<NP><<<(unsigned)((m->ncol + BARO_CPB - 1) / BARO_CPB), BARO_CPB * NP * NP,
+                                  0, m->stream>>>(m->baro<NP>(m->eta, m->HU, m->HV, true, time - tcur),
+                                                  m->k1[0], m->k1[1], m->k1[2]);
         });
         DRF_LAUNCHED();
         DRF_CUDA(cudaStreamSynchronize(m->stream));
@@ -1034,8 +1213,9 @@ int drf_dg_step_modesplit(drf_dg *m, double dt, int nsub, int nsteps) {
         }
         for (int s = 0; s < nsteps; ++s) {
             DRF_CUDA(cudaGraphLaunch(m->graph[m->cur], m->stream));
-            launch_counter().fetch_add(5 + 3 + 2 * (uint64_t)nsub);
+            launch_counter().fetch_add(5 + 2 + 2 * (uint64_t)nsub);
             m->cur = 1 - m->cur;
+            m->pending = true;
         }
     });
 }
@@ -1045,6 +1225,7 @@ int drf_dg_rk_step(drf_dg *m, int scheme, double dt, int nsteps) {
         check_model(m);
         DRF_CHECK(scheme >= 0 && scheme <= 5, DRF_E_INVALID, "unknown RK scheme");
         DRF_CHECK(dt > 0.0 && std::isfinite(dt), DRF_E_INVALID, "dt must be positive");
+        m->materialize();
         // Stage storage: up to 6 RHS evaluations of (q[4], eta). The 3D parts live in a
         // separately allocated buffer; this path is the generic (non-split) reference driver.
         const int nk = scheme == DRF_RK_DOPRI ? 6 : (scheme == DRF_RK_RK4 ? 4 : 2);
@@ -1179,6 +1360,7 @@ int drf_dg_diagnostics(drf_dg *m, double *out10) {
     return guard([&] {
         check_model(m);
         DRF_CHECK(out10, DRF_E_INVALID, "null output");
+        m->materialize();
         const unsigned nb3 = blocks_for(m->n3), nb2 = blocks_for(m->n2);
         DevBuf<double> part((size_t)nb3 * 6 + (size_t)nb2 * 5);
         const double dx = m->mesh.Lx / m->mesh.nx, dy = m->mesh.Ly / m->mesh.ny;
@@ -1220,6 +1402,7 @@ int drf_dg_time_stage(drf_dg *m, int nrep, double *ms, double *alg_bytes, double
     return guard([&] {
         check_model(m);
         DRF_CHECK(nrep >= 1 && ms, DRF_E_INVALID, "bad arguments");
+        m->materialize();
         cudaEvent_t e0, e1;
         DRF_CUDA(cudaEventCreate(&e0));
         DRF_CUDA(cudaEventCreate(&e1));
