@@ -72,8 +72,47 @@ struct StageArgs {
     T A, B, dt;
     int mode;   // 0: LSRK stage update, 1: write the right-hand side into res[]
     int first;  // 1: A = 0 stage (res not read, column increments overwritten)
+    int bulk;   // 1: column blocks are 16-byte aligned -> staged with cp.async.bulk
+    int *err;   // device status word (DRF_E_TIMEOUT when a bounded wait gives up)
     Geo G;
 };
+
+// ---- TMA bulk copy (global -> shared) completed on an mbarrier, with bounded waits
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    uint64_t g;
+    asm volatile("cvta.to.global.u64 %0, %1;" : "=l"(g) : "l"(src));
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_addr(dst)),
+        "l"(g), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+// Spins on the barrier's phase with an iteration limit; false when it gave up.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t phase) {
+    const uint32_t a = smem_addr(bar);
+    for (long it = 0; it < (1L << 24); ++it) {
+        uint32_t done;
+        asm volatile(
+            "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+            : "=r"(done)
+            : "r"(a), "r"(phase)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
 
 template <typename T>
 __device__ __forceinline__ T sel4(const T (&x)[4], int v) {
@@ -81,13 +120,12 @@ __device__ __forceinline__ T sel4(const T (&x)[4], int v) {
 }
 
 // Shared-memory plan of the stage kernel for one water column (ncn = nz*(N+1)^3 nodes):
-//   sQ[4][ncn] state, sR[4][ncn] right-hand side (sR[0] first holds the horizontal
-//   divergence and the layer integrals), sOm[ncn] omega, per layer x 2D-node scratch, and the
-//   column's 2D fields.
-template <typename T>
-__host__ __device__ inline size_t stage_smem_elems(int nz, int np) {
+//   two mbarriers (16 B), sQ[4][ncn] state, sRes[4][ncn] LSRK 2N register, sR[4][ncn]
+//   right-hand side (sR[0] first holds the horizontal divergence and the layer integrals),
+//   sOm[ncn] omega, per layer x 2D-node scratch, and the column's 2D fields.
+inline size_t stage_smem_bytes(int nz, int np, size_t tsz) {
     const int np2 = np * np, ncn = nz * np2 * np;
-    return (size_t)9 * ncn + (size_t)2 * nz * np2 + 4 * np2;
+    return 16 + ((size_t)13 * ncn + (size_t)2 * nz * np2 + 4 * np2) * tsz;
 }
 
 // One CTA per water column; work is organised in pencils (lines of N+1 nodes) so every
@@ -102,21 +140,48 @@ __global__ void __launch_bounds__(512) dg3d_stage_kernel(StageArgs<T> a) {
     const int c = blockIdx.x, ex = c % G.nx, ey = c / G.nx;
     const size_t base = (size_t)c * ncn;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    T *sQ = reinterpret_cast<T *>(smem_raw);  // [4][ncn]
-    T *sR = sQ + 4 * ncn;                     // [4][ncn]
-    T *sOm = sR + 4 * ncn;                    // [ncn]
-    T *sL1 = sOm + ncn;                       // [nz][NP2]
-    T *sL2 = sL1 + nz * NP2;                  // [nz][NP2]
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw);
+    T *sQ = reinterpret_cast<T *>(smem_raw + 16);  // [4][ncn]
+    T *sRes = sQ + 4 * ncn;                        // [4][ncn]
+    T *sR = sRes + 4 * ncn;                        // [4][ncn]
+    T *sOm = sR + 4 * ncn;                         // [ncn]
+    T *sL1 = sOm + ncn;                            // [nz][NP2]
+    T *sL2 = sL1 + nz * NP2;                       // [nz][NP2]
     T *sIH = sL2 + nz * NP2, *sHt = sIH + NP2, *sEt = sHt + NP2, *sItot = sEt + NP2;
-    T *sD = sR;                               // divergence / layer integrals
+    T *sD = sR;                                    // divergence / layer integrals
+    __shared__ int s_ok;
 
     const double tnow = a.tdev[0] + a.toff;
     const T etide = (T)tide_at(G, tnow);
     const T cx = (T)G.cx, cy = (T)G.cy, cs = (T)G.cs;
     const T Lx = (T)G.Lx, Ly = (T)G.Ly, Ls = (T)G.Ls;
     const T g = (T)G.g;
+    const bool need_res = a.mode == 0 && !a.first;
 
-    // ---- load the column (and apply a pending transport correction to Hu, Hv)
+    // ---- stage the column: state (and the 2N register) by TMA bulk copies when aligned
+    if (a.bulk) {
+        if (threadIdx.x == 0) {
+            mbar_init(&bars[0], 1);
+            mbar_init(&bars[1], 1);
+            const uint32_t bytes = (uint32_t)(ncn * sizeof(T));
+            mbar_expect_tx(&bars[0], 4 * bytes);
+#pragma unroll
+            for (int v = 0; v < 4; ++v) bulk_g2s(sQ + v * ncn, a.qin[v] + base, bytes, &bars[0]);
+            if (need_res) {
+                mbar_expect_tx(&bars[1], 4 * bytes);
+#pragma unroll
+                for (int v = 0; v < 4; ++v) bulk_g2s(sRes + v * ncn, a.res[v] + base, bytes, &bars[1]);
+            }
+        }
+    } else {
+        for (int n = threadIdx.x; n < ncn; n += blockDim.x) {
+#pragma unroll
+            for (int v = 0; v < 4; ++v) sQ[v * ncn + n] = a.qin[v][base + n];
+            if (need_res)
+#pragma unroll
+                for (int v = 0; v < 4; ++v) sRes[v * ncn + n] = a.res[v][base + n];
+        }
+    }
     for (int t = threadIdx.x; t < NP2; t += blockDim.x) {
         const double e = a.eta[(size_t)c * NP2 + t];
         const double H = e + a.h[(size_t)c * NP2 + t];
@@ -124,17 +189,18 @@ __global__ void __launch_bounds__(512) dg3d_stage_kernel(StageArgs<T> a) {
         sHt[t] = (T)H;
         sIH[t] = (T)(1.0 / H);
     }
-    for (int n = threadIdx.x; n < ncn; n += blockDim.x) {
-        T q0 = a.qin[0][base + n], q1 = a.qin[1][base + n];
-        if (a.corrU) {
+    if (threadIdx.x == 0) s_ok = a.bulk ? (int)mbar_wait(&bars[0], 0) : 1;
+    __syncthreads();
+    if (!s_ok) {
+        if (threadIdx.x == 0) atomicExch(a.err, DRF_E_TIMEOUT);
+        return;
+    }
+    if (a.corrU) {  // pending transport correction of the previous step
+        for (int n = threadIdx.x; n < ncn; n += blockDim.x) {
             const int an = n % NP2;
-            q0 += (T)a.corrU[(size_t)c * NP2 + an];
-            q1 += (T)a.corrV[(size_t)c * NP2 + an];
+            sQ[n] += (T)a.corrU[(size_t)c * NP2 + an];
+            sQ[ncn + n] += (T)a.corrV[(size_t)c * NP2 + an];
         }
-        sQ[n] = q0;
-        sQ[ncn + n] = q1;
-        sQ[2 * ncn + n] = a.qin[2][base + n];
-        sQ[3 * ncn + n] = a.qin[3][base + n];
     }
     __syncthreads();
 
@@ -175,10 +241,14 @@ __global__ void __launch_bounds__(512) dg3d_stage_kernel(StageArgs<T> a) {
         }
     };
 
-    // ---- horizontal divergence of (Hu, Hv) with central face flux: x pencils
+    // ---- horizontal divergence of (Hu, Hv) with central face flux: x pencils (both face
+    // neighbours fetched up front so their latencies overlap)
     for (int p = threadIdx.x; p < npen; p += blockDim.x) {
         const int ez = p / NP2, j = p % NP, k = (p / NP) % NP;
         const int e0 = ez * NP3 + NP * (j + NP * k);
+        T qa[4], qb[4], ea, eb, Ha, Hb;
+        outside(0, ez, 0, j, k, e0, qa, ea, Ha);
+        outside(1, ez, N, j, k, e0 + N, qb, eb, Hb);
         T q[NP];
 #pragma unroll
         for (int m = 0; m < NP; ++m) q[m] = sQ[e0 + m];
@@ -188,13 +258,8 @@ __global__ void __launch_bounds__(512) dg3d_stage_kernel(StageArgs<T> a) {
 #pragma unroll
             for (int m = 0; m < NP; ++m) s += B::D(i * NP + m) * q[m];
             T d = cx * s;
-            if (i == 0 || i == N) {
-                const int side = i == 0 ? 0 : 1;
-                T qp[4], ep, Hp;
-                outside(side, ez, i, j, k, e0 + i, qp, ep, Hp);
-                const T nrm = i == 0 ? T(-1) : T(1);
-                d += Lx * (T(0.5) * (q[i] + qp[0]) * nrm - q[i] * nrm);
-            }
+            if (i == 0) d += Lx * (T(0.5) * (q[0] + qa[0]) * T(-1) - q[0] * T(-1));
+            if (i == N) d += Lx * (T(0.5) * (q[N] + qb[0]) - q[N]);
             sD[e0 + i] = d;
         }
     }
@@ -203,6 +268,9 @@ __global__ void __launch_bounds__(512) dg3d_stage_kernel(StageArgs<T> a) {
     for (int p = threadIdx.x; p < npen; p += blockDim.x) {
         const int ez = p / NP2, i = p % NP, k = (p / NP) % NP;
         const int e0 = ez * NP3 + i + NP2 * k;
+        T qa[4], qb[4], ea, eb, Ha, Hb;
+        outside(2, ez, i, 0, k, e0, qa, ea, Ha);
+        outside(3, ez, i, N, k, e0 + NP * N, qb, eb, Hb);
         T q[NP];
 #pragma unroll
         for (int m = 0; m < NP; ++m) q[m] = sQ[ncn + e0 + NP * m];
@@ -212,13 +280,8 @@ __global__ void __launch_bounds__(512) dg3d_stage_kernel(StageArgs<T> a) {
 #pragma unroll
             for (int m = 0; m < NP; ++m) s += B::D(j * NP + m) * q[m];
             T d = cy * s;
-            if (j == 0 || j == N) {
-                const int side = j == 0 ? 2 : 3;
-                T qp[4], ep, Hp;
-                outside(side, ez, i, j, k, e0 + NP * j, qp, ep, Hp);
-                const T nrm = j == 0 ? T(-1) : T(1);
-                d += Ly * (T(0.5) * (q[j] + qp[1]) * nrm - q[j] * nrm);
-            }
+            if (j == 0) d += Ly * (T(0.5) * (q[0] + qa[1]) * T(-1) - q[0] * T(-1));
+            if (j == N) d += Ly * (T(0.5) * (q[N] + qb[1]) - q[N]);
             sD[e0 + NP * j] += d;
         }
     }
@@ -382,6 +445,14 @@ __global__ void __launch_bounds__(512) dg3d_stage_kernel(StageArgs<T> a) {
     __syncthreads();
     // ---- z pencils: advection d/dsigma, Coriolis, vertical diffusion, sigma faces, surface
     // and bed stresses, then the LSRK update and the FP64 column increments
+    if (a.bulk && need_res) {
+        if (threadIdx.x == 0) s_ok = (int)mbar_wait(&bars[1], 0);
+        __syncthreads();
+        if (!s_ok) {
+            if (threadIdx.x == 0) atomicExch(a.err, DRF_E_TIMEOUT);
+            return;
+        }
+    }
     for (int p = threadIdx.x; p < npen; p += blockDim.x) {
         const int ez = p / NP2, an = p % NP2;
         const int e0 = ez * NP3 + an;
@@ -455,7 +526,7 @@ __global__ void __launch_bounds__(512) dg3d_stage_kernel(StageArgs<T> a) {
                 if (a.mode == 1) {
                     a.res[v][gi] = r;
                 } else {
-                    const T rn = (a.first ? T(0) : a.A * a.res[v][gi]) + a.dt * r;
+                    const T rn = (a.first ? T(0) : a.A * sRes[v * ncn + n]) + a.dt * r;
                     a.res[v][gi] = rn;
                     a.qout[v][gi] = q[k] + a.B * rn;
                     if (v == 0) incU += B::w(k) * (a.B * rn);
@@ -794,6 +865,7 @@ struct drf_dg {
     cudaStream_t stream = nullptr, own = nullptr;
     DevBuf<unsigned char> q3;  // [2 ping-pong][4 vars] + [4 res] + [4 tmp] of n3 values each
     DevBuf<double> d2;         // 2D FP64 arrays
+    DevBuf<int> errbuf;        // device status word written by bounded waits
     double *h = nullptr, *f = nullptr, *taux = nullptr, *tauy = nullptr, *eta = nullptr,
            *HU = nullptr, *HV = nullptr, *eta_avg = nullptr, *esum = nullptr, *Fx = nullptr,
            *Fy = nullptr, *HUo = nullptr, *HVo = nullptr, *k1[3] = {}, *us[3] = {}, *dHU3 = nullptr,
@@ -844,6 +916,8 @@ struct drf_dg {
         a.mode = mode; a.first = (s == 0);
         a.corrU = with_corr ? corrU : nullptr;
         a.corrV = with_corr ? corrV : nullptr;
+        a.bulk = ((size_t)G.nz * np3 * sizeof(T)) % 16 == 0;
+        a.err = errbuf.p;
         a.G = G;
         dg3d_stage_kernel<T, NP><<<ncol, stage_threads(), smem, stream>>>(a);
         DRF_LAUNCHED();
@@ -971,6 +1045,17 @@ void from_device(drf_dg *m, double *dst, const void *src) {
 
 void check_model(drf_dg *m) { DRF_CHECK(m != nullptr, DRF_E_INVALID, "null model handle"); }
 
+// surfaces a status word set on the device (a bounded wait that gave up)
+void check_device_status(drf_dg *m) {
+    int st = 0;
+    DRF_CUDA(cudaMemcpyAsync(&st, m->errbuf.p, sizeof(int), cudaMemcpyDeviceToHost, m->stream));
+    DRF_CUDA(cudaStreamSynchronize(m->stream));
+    if (st != 0) {
+        DRF_CUDA(cudaMemsetAsync(m->errbuf.p, 0, sizeof(int), m->stream));
+        throw Error(st, "a device-side wait gave up (status " + std::to_string(st) + ")");
+    }
+}
+
 }  // namespace
 }  // namespace drf
 
@@ -1020,7 +1105,7 @@ int drf_dg_create(const drf_mesh_desc *mesh, const drf_dg_params *params, const 
         m->stream = m->own;
         // shared memory of the stage kernel: 9 column arrays + per-layer bases + 2D scalars
         const int ncn = mesh->nz * m->np3;
-        m->smem = stage_smem_elems<double>(mesh->nz, m->np) * m->tsz;
+        m->smem = stage_smem_bytes(mesh->nz, m->np, m->tsz);
         int dev = 0, maxsm = 0;
         DRF_CUDA(cudaGetDevice(&dev));
         DRF_CUDA(cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
@@ -1032,6 +1117,8 @@ int drf_dg_create(const drf_mesh_desc *mesh, const drf_dg_params *params, const 
             DRF_CUDA(cudaFuncSetAttribute(dg3d_stage_kernel<T, NP>,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)m->smem));
         });
+        m->errbuf.alloc(1);
+        DRF_CUDA(cudaMemset(m->errbuf.p, 0, sizeof(int)));
         m->q3.alloc((size_t)16 * m->n3 * m->tsz);
         DRF_CUDA(cudaMemset(m->q3.p, 0, m->q3.n));
         const int n2arrays = 27;
@@ -1076,6 +1163,7 @@ int drf_dg_sync(drf_dg *m) {
     return guard([&] {
         check_model(m);
         DRF_CUDA(cudaStreamSynchronize(m->stream));
+        check_device_status(m);
     });
 }
 
@@ -1125,7 +1213,7 @@ int drf_dg_download_state(drf_dg *m, double *const *q4, double *eta, double *HU,
     return guard([&] {
         check_model(m);
         m->materialize();
-        DRF_CUDA(cudaStreamSynchronize(m->stream));
+        check_device_status(m);
         if (q4)
             for (int v = 0; v < 4; ++v)
                 if (q4[v]) from_device(m, q4[v], m->q(m->cur, v));
