@@ -259,16 +259,28 @@ def run_ours(args, rank, world, local):
     eta_out = torch.empty(cfg.n2, dtype=torch.float64).pin_memory().numpy()
     torch.cuda.synchronize()
     barrier(world)
+    calls = {"set_forcing": 0.0, "step": 0.0, "download_surface": 0.0, "diagnostics": 0.0}
     t0 = time.perf_counter()
     for _ in range(args.steps):
+        ta = time.perf_counter()
         model.set_forcing(taux, tauy)
+        tb = time.perf_counter()
         model.step(dt, nsub, 1)
+        tc = time.perf_counter()
         model.download_surface(eta_out)
+        td = time.perf_counter()
         model.diagnostics()
+        te = time.perf_counter()
+        calls["set_forcing"] += tb - ta
+        calls["step"] += tc - tb
+        calls["download_surface"] += td - tc
+        calls["diagnostics"] += te - td
     torch.cuda.synchronize()
     e2e_s = max_over_ranks(time.perf_counter() - t0, world)
     e2e = {"value": world * ndof * 5 * args.steps / e2e_s, "unit": UNIT,
-           "h2d_bytes_per_step": 2 * 8 * cfg.n2, "d2h_bytes_per_step": 8 * cfg.n2 + 80}
+           "h2d_bytes_per_step": 2 * 8 * cfg.n2, "d2h_bytes_per_step": 8 * cfg.n2 + 80,
+           "ms_per_step": 1e3 * e2e_s / args.steps,
+           "host_ms_per_call": {k: round(1e3 * v / args.steps, 3) for k, v in calls.items()}}
 
     # FP64 GPU form of the same step and the mixed-precision surface error against it
     fp64 = None

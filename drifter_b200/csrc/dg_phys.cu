@@ -829,6 +829,40 @@ __global__ void diag2d_kernel(int64_t n2, int nz, const double *eta, const doubl
         for (int q = 0; q < 5; ++q) part[blockIdx.x * 5 + q] = red[q][0];
 }
 
+// second pass: one block folds the per-block partials (fixed order -> deterministic)
+__global__ void diag_final_kernel(const double *p3, unsigned nb3, const double *p2, unsigned nb2,
+                                  double *out) {
+    __shared__ double red[11][256];
+    double v[11] = {0, 0, 0, 0, -1e300, 1e300, 0, 0, 0, -1e300, 1e300};
+    for (unsigned b = threadIdx.x; b < nb3; b += blockDim.x) {
+        v[0] += p3[b * 6]; v[1] += p3[b * 6 + 1]; v[2] += p3[b * 6 + 2];
+        v[3] = fmax(v[3], p3[b * 6 + 3]); v[4] = fmax(v[4], p3[b * 6 + 4]);
+        v[5] = fmin(v[5], p3[b * 6 + 5]);
+    }
+    for (unsigned b = threadIdx.x; b < nb2; b += blockDim.x) {
+        v[6] += p2[b * 5]; v[7] += p2[b * 5 + 1]; v[8] += p2[b * 5 + 2];
+        v[9] = fmax(v[9], p2[b * 5 + 3]); v[10] = fmin(v[10], p2[b * 5 + 4]);
+    }
+    for (int q = 0; q < 11; ++q) red[q][threadIdx.x] = v[q];
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s)
+            for (int q = 0; q < 11; ++q) {
+                const double a = red[q][threadIdx.x], b = red[q][threadIdx.x + s];
+                red[q][threadIdx.x] = (q == 3 || q == 4 || q == 9) ? fmax(a, b)
+                                      : (q == 5 || q == 10)        ? fmin(a, b)
+                                                                   : a + b;
+            }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        // {mass_w, mass_u, energy, heat, salt, max_speed, max_eta, min_eta, max_T, min_T}
+        out[0] = red[6][0]; out[1] = red[7][0]; out[2] = red[0][0] + red[8][0];
+        out[3] = red[1][0]; out[4] = red[2][0]; out[5] = red[3][0];
+        out[6] = red[9][0]; out[7] = red[10][0]; out[8] = red[4][0]; out[9] = red[5][0];
+    }
+}
+
 template <class F>
 void dispatch_np(int np, F &&f) {
     switch (np) {
@@ -866,6 +900,7 @@ struct drf_dg {
     DevBuf<unsigned char> q3;  // [2 ping-pong][4 vars] + [4 res] + [4 tmp] of n3 values each
     DevBuf<double> d2;         // 2D FP64 arrays
     DevBuf<int> errbuf;        // device status word written by bounded waits
+    DevBuf<double> diag;       // diagnostics partials
     double *h = nullptr, *f = nullptr, *taux = nullptr, *tauy = nullptr, *eta = nullptr,
            *HU = nullptr, *HV = nullptr, *eta_avg = nullptr, *esum = nullptr, *Fx = nullptr,
            *Fy = nullptr, *HUo = nullptr, *HVo = nullptr, *k1[3] = {}, *us[3] = {}, *dHU3 = nullptr,
@@ -1450,7 +1485,9 @@ int drf_dg_diagnostics(drf_dg *m, double *out10) {
         DRF_CHECK(out10, DRF_E_INVALID, "null output");
         m->materialize();
         const unsigned nb3 = blocks_for(m->n3), nb2 = blocks_for(m->n2);
-        DevBuf<double> part((size_t)nb3 * 6 + (size_t)nb2 * 5);
+        if (m->diag.n < (size_t)nb3 * 6 + (size_t)nb2 * 5 + 10)
+            m->diag.alloc((size_t)nb3 * 6 + (size_t)nb2 * 5 + 10);
+        double *p3 = m->diag.p, *p2 = p3 + (size_t)nb3 * 6, *res10 = p2 + (size_t)nb2 * 5;
         const double dx = m->mesh.Lx / m->mesh.nx, dy = m->mesh.Ly / m->mesh.ny;
         m->with_types([&](auto tv, auto npc) {
             using T = decltype(tv);
@@ -1458,28 +1495,17 @@ int drf_dg_diagnostics(drf_dg *m, double *out10) {
             const int c = m->cur;
             diag3d_kernel<T, NP><<<nb3, 256, 0, m->stream>>>(
                 m->n3, m->G.nz, (const T *)m->q(c, 0), (const T *)m->q(c, 1), (const T *)m->q(c, 2),
-                (const T *)m->q(c, 3), m->eta, m->h, 0.125 * dx * dy * m->G.dsig, part.p);
+                (const T *)m->q(c, 3), m->eta, m->h, 0.125 * dx * dy * m->G.dsig, p3);
             DRF_LAUNCHED();
             diag2d_kernel<NP><<<nb2, 256, 0, m->stream>>>(m->n2, m->G.nz, m->eta, m->h,
-                                                         0.25 * dx * dy, m->G.g, part.p + (size_t)nb3 * 6);
+                                                         0.25 * dx * dy, m->G.g, p2);
             DRF_LAUNCHED();
         });
-        std::vector<double> hp(part.n);
-        DRF_CUDA(cudaMemcpyAsync(hp.data(), part.p, part.n * 8, cudaMemcpyDeviceToHost, m->stream));
+        diag_final_kernel<<<1, 256, 0, m->stream>>>(p3, nb3, p2, nb2, res10);
+        DRF_LAUNCHED();
+        double vals[10];
+        DRF_CUDA(cudaMemcpyAsync(vals, res10, sizeof(vals), cudaMemcpyDeviceToHost, m->stream));
         DRF_CUDA(cudaStreamSynchronize(m->stream));
-        double en = 0, heat = 0, salt = 0, um = 0, Tmax = -1e300, Tmin = 1e300;
-        for (unsigned b = 0; b < nb3; ++b) {
-            en += hp[b * 6]; heat += hp[b * 6 + 1]; salt += hp[b * 6 + 2];
-            um = std::max(um, hp[b * 6 + 3]); Tmax = std::max(Tmax, hp[b * 6 + 4]);
-            Tmin = std::min(Tmin, hp[b * 6 + 5]);
-        }
-        double mw = 0, mu = 0, pe = 0, emax = -1e300, emin = 1e300;
-        const double *p2 = hp.data() + (size_t)nb3 * 6;
-        for (unsigned b = 0; b < nb2; ++b) {
-            mw += p2[b * 5]; mu += p2[b * 5 + 1]; pe += p2[b * 5 + 2];
-            emax = std::max(emax, p2[b * 5 + 3]); emin = std::min(emin, p2[b * 5 + 4]);
-        }
-        const double vals[10] = {mw, mu, en + pe, heat, salt, um, emax, emin, Tmax, Tmin};
         std::memcpy(out10, vals, sizeof(vals));
         for (int i = 0; i < 10; ++i)
             DRF_CHECK(std::isfinite(vals[i]), DRF_E_NONFINITE, "non-finite diagnostic (model blew up)");
