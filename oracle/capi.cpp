@@ -177,4 +177,115 @@ int orc_rk_ode(int scheme, double lam, double U0, double T, int nsteps, double *
     })
 }
 
+// ----------------------------------------------------------------------------- Bezier
+struct BzHandle {
+    BzSystem S;
+    CSR A;
+    BzMG M;
+};
+
+void *orc_bz_build(int nx, int ny, double x0, double y0, double Lx, double Ly, double lambda,
+                   double eps, const double *dgauss) {
+    try {
+        auto *h = new BzHandle();
+        BzGrid g;
+        g.nx = nx; g.ny = ny; g.x0 = x0; g.y0 = y0; g.Lx = Lx; g.Ly = Ly;
+        g.lambda = lambda; g.eps = eps;
+        bz_build(h->S, g, dgauss);
+        return h;
+    } catch (const std::exception &e) {
+        g_err = e.what();
+        return nullptr;
+    }
+}
+void orc_bz_destroy(void *h) { delete static_cast<BzHandle *>(h); }
+
+int orc_bz_info(void *hd, long *ndof, double *alpha, double *dTWd) {
+    ORC_TRY({
+        auto *h = static_cast<BzHandle *>(hd);
+        *ndof = h->S.ndof; *alpha = h->S.alpha; *dTWd = h->S.dTWd;
+    })
+}
+
+int orc_bz_element_mats(double dx, double dy, double *H, double *B) {
+    ORC_TRY({
+        element_hessian(dx, dy, 4, H);
+        element_mass(dx, dy, 4, B);
+    })
+}
+
+int orc_bz_vec(void *hd, int which, double *out) {
+    ORC_TRY({
+        auto *h = static_cast<BzHandle *>(hd);
+        const BVec &v = which == 0 ? h->S.b : h->S.BtWd;
+        std::memcpy(out, v.data(), sizeof(double) * v.size());
+    })
+}
+
+static const CSR &pick(BzHandle *h, int which) {
+    return which == 0 ? h->S.H : which == 1 ? h->S.BtWB : which == 2 ? h->S.Q : h->A;
+}
+
+long orc_bz_nnz(void *hd, int which) {
+    auto *h = static_cast<BzHandle *>(hd);
+    const CSR &M = pick(h, which);
+    return M.rp.empty() ? 0 : M.rp.back();
+}
+long orc_bz_rows(void *hd, int which) { return pick(static_cast<BzHandle *>(hd), which).n; }
+
+int orc_bz_csr(void *hd, int which, long *rp, long *ci, double *v) {
+    ORC_TRY({
+        const CSR &M = pick(static_cast<BzHandle *>(hd), which);
+        std::memcpy(rp, M.rp.data(), sizeof(long) * M.rp.size());
+        std::memcpy(ci, M.ci.data(), sizeof(long) * M.ci.size());
+        std::memcpy(v, M.v.data(), sizeof(double) * M.v.size());
+    })
+}
+
+int orc_bz_constraints(void *hd, int edge_ngauss) {
+    ORC_TRY({
+        auto *h = static_cast<BzHandle *>(hd);
+        bz_constraints(h->S, edge_ngauss, h->A);
+    })
+}
+
+int orc_bz_objective(void *hd, const double *x, double *parts, double *obj) {
+    ORC_TRY(*obj = bz_objective(static_cast<BzHandle *>(hd)->S, x, parts))
+}
+
+int orc_bz_mg_setup(void *hd, int coarsest_n, int *nlevels) {
+    ORC_TRY({
+        auto *h = static_cast<BzHandle *>(hd);
+        bz_mg_setup(h->S, h->M, coarsest_n);
+        *nlevels = (int)h->M.lv.size();
+    })
+}
+
+int orc_bz_level_info(void *hd, int l, int *n, double *K, double *rho, double *binv) {
+    ORC_TRY({
+        auto *h = static_cast<BzHandle *>(hd);
+        const BzLevel &L = h->M.lv.at(l);
+        *n = L.n;
+        if (K) std::memcpy(K, L.K, sizeof(L.K));
+        if (rho) std::memcpy(rho, L.rho.data(), sizeof(double) * L.rho.size());
+        if (binv && !L.binv.empty()) std::memcpy(binv, L.binv.data(), sizeof(double) * L.binv.size());
+    })
+}
+
+int orc_bz_level_apply(void *hd, int l, const double *x, double *y) {
+    ORC_TRY(bz_level_apply(static_cast<BzHandle *>(hd)->M, l, x, y))
+}
+
+int orc_bz_mg_vcycle(void *hd, const double *r, double *z) {
+    ORC_TRY(bz_mg_vcycle(static_cast<BzHandle *>(hd)->M, r, z))
+}
+
+int orc_bz_pcg(void *hd, int precond, const double *b, double *x, double tol, int maxit,
+               int *iters, double *relres) {
+    ORC_TRY({
+        auto *h = static_cast<BzHandle *>(hd);
+        *iters = bz_pcg(h->S, &h->M, precond, b, x, tol, maxit, relres);
+    })
+}
+
 }  // extern "C"

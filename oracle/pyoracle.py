@@ -185,3 +185,110 @@ def rk_ode(scheme, lam, U0, T, nsteps):
     _chk(lib().orc_rk_ode(RK[scheme], C.c_double(lam), C.c_double(U0), C.c_double(T), nsteps,
                           C.byref(out)))
     return out.value
+
+
+# ----------------------------------------------------------------------------- Bezier smoother
+def gauss01_4():
+    a = np.sqrt(3 / 7 - 2 / 7 * np.sqrt(6 / 5))
+    b = np.sqrt(3 / 7 + 2 / 7 * np.sqrt(6 / 5))
+    return np.array([0.5 * (1 - b), 0.5 * (1 - a), 0.5 * (1 + a), 0.5 * (1 + b)])
+
+
+def gauss_points(nx, ny, x0, y0, Lx, Ly):
+    """Physical coordinates of the 4x4 data Gauss points, layout [ey][ex][qj][qi]."""
+    p = gauss01_4()
+    dx, dy = Lx / nx, Ly / ny
+    ex = np.arange(nx)[None, :, None, None]
+    ey = np.arange(ny)[:, None, None, None]
+    X = x0 + (ex + p[None, None, None, :]) * dx
+    Y = y0 + (ey + p[None, None, :, None]) * dy
+    X = np.broadcast_to(X, (ny, nx, 4, 4))
+    Y = np.broadcast_to(Y, (ny, nx, 4, 4))
+    return X.reshape(-1).copy(), Y.reshape(-1).copy()
+
+
+class BezierOracle:
+    """Uniform-grid cubic Bezier smoother system (Q, b, constraints, multigrid, PCG)."""
+
+    def __init__(self, nx, ny, Lx, Ly, dgauss, lam=1.0, eps=1e-4, x0=0.0, y0=0.0):
+        L = lib()
+        L.orc_bz_build.restype = C.c_void_p
+        L.orc_bz_build.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
+                                   C.c_double, C.c_double, C.c_double, _dp]
+        L.orc_bz_destroy.argtypes = [C.c_void_p]
+        for fn in ("orc_bz_nnz", "orc_bz_rows"):
+            getattr(L, fn).restype = C.c_long
+            getattr(L, fn).argtypes = [C.c_void_p, C.c_int]
+        self.d = _c(dgauss)
+        self.h = L.orc_bz_build(nx, ny, x0, y0, Lx, Ly, lam, eps, _p(self.d))
+        if not self.h:
+            raise RuntimeError("oracle: " + L.orc_last_error().decode())
+        n, a, d = C.c_long(), C.c_double(), C.c_double()
+        _chk(L.orc_bz_info(C.c_void_p(self.h), C.byref(n), C.byref(a), C.byref(d)))
+        self.ndof, self.alpha, self.dTWd = n.value, a.value, d.value
+        self.nx, self.ny = nx, ny
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_bz_destroy(C.c_void_p(self.h))
+            self.h = None
+
+    def vec(self, which="b"):
+        out = np.empty(self.ndof)
+        _chk(lib().orc_bz_vec(C.c_void_p(self.h), 0 if which == "b" else 1, _p(out)))
+        return out
+
+    def csr(self, which):
+        import scipy.sparse as sp
+        w = {"H": 0, "BtWB": 1, "Q": 2, "A": 3}[which]
+        L = lib()
+        nnz, rows = L.orc_bz_nnz(C.c_void_p(self.h), w), L.orc_bz_rows(C.c_void_p(self.h), w)
+        rp = np.empty(rows + 1, dtype=np.int64)
+        ci = np.empty(nnz, dtype=np.int64)
+        v = np.empty(nnz)
+        _chk(L.orc_bz_csr(C.c_void_p(self.h), w, rp.ctypes.data_as(C.c_void_p),
+                          ci.ctypes.data_as(C.c_void_p), _p(v)))
+        return sp.csr_matrix((v, ci, rp), shape=(rows, self.ndof))
+
+    def constraints(self, edge_ngauss=4):
+        _chk(lib().orc_bz_constraints(C.c_void_p(self.h), edge_ngauss))
+        return self.csr("A")
+
+    def objective(self, x):
+        parts, obj = np.empty(2), C.c_double()
+        _chk(lib().orc_bz_objective(C.c_void_p(self.h), _p(_c(x)), _p(parts), C.byref(obj)))
+        return obj.value, parts[0], parts[1]
+
+    def mg_setup(self, coarsest_n=2):
+        nl = C.c_int()
+        _chk(lib().orc_bz_mg_setup(C.c_void_p(self.h), coarsest_n, C.byref(nl)))
+        self.nlevels = nl.value
+        return nl.value
+
+    def level(self, l):
+        n = C.c_int()
+        K = np.empty(256)
+        _chk(lib().orc_bz_level_info(C.c_void_p(self.h), l, C.byref(n), _p(K), None, None))
+        nd = 3 * n.value + 1
+        rho = np.empty(nd)
+        binv = np.zeros(9 * 256)
+        _chk(lib().orc_bz_level_info(C.c_void_p(self.h), l, C.byref(n), _p(K), _p(rho), _p(binv)))
+        return dict(n=n.value, K=K.reshape(16, 16), rho=rho, binv=binv.reshape(9, 16, 16))
+
+    def level_apply(self, l, x):
+        y = np.empty_like(_c(x))
+        _chk(lib().orc_bz_level_apply(C.c_void_p(self.h), l, _p(_c(x)), _p(y)))
+        return y
+
+    def vcycle(self, r):
+        z = np.empty(self.ndof)
+        _chk(lib().orc_bz_mg_vcycle(C.c_void_p(self.h), _p(_c(r)), _p(z)))
+        return z
+
+    def pcg(self, b=None, precond="mg", tol=1e-10, maxit=2000, x0=None):
+        b = self.vec("b") if b is None else _c(b)
+        x = np.zeros(self.ndof) if x0 is None else _c(x0).copy()
+        it, rr = C.c_int(), C.c_double()
+        _chk(lib().orc_bz_pcg(C.c_void_p(self.h), {"none": 0, "jacobi": 1, "mg": 2}[precond],
+                              _p(b), _p(x), C.c_double(tol), maxit, C.byref(it), C.byref(rr)))
+        return x, it.value, rr.value

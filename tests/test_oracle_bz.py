@@ -1,0 +1,144 @@
+"""Pins the Bezier-smoother oracle against the reference's published known answer and its
+multigrid test assertions (CPU only)."""
+import json
+import os
+
+import numpy as np
+import pytest
+import scipy.sparse.linalg as spl
+
+import pyoracle as O
+
+GOLD = json.load(open(os.path.join(os.path.dirname(__file__), "golden",
+                                   "reference_known_answers.json")))
+
+
+def doc_case(n=16, L=1000.0, lam=1.0):
+    X, Y = O.gauss_points(n, n, 0, 0, L, L)
+    d = np.exp(np.sin(2 * np.pi * X / L) * np.sin(2 * np.pi * Y / L))
+    return O.BezierOracle(n, n, L, L, d, lam=lam, eps=1e-4)
+
+
+def schur_solve(B, tol=1e-13):
+    """Constrained minimiser by CG on S = A Q^-1 A^T (the reference's Schur path,
+    src/bathymetry/cg_cubic_bezier_bathymetry_smoother.cpp:305); exact Q^-1 by SuperLU."""
+    Q = B.csr("Q").tocsc()
+    A = B.constraints(4).tocsr()
+    b = B.vec("b")
+    lu = spl.splu(Q)
+    rhs = A @ lu.solve(b)
+    lam = np.zeros(A.shape[0])
+    r = rhs.copy()
+    p = r.copy()
+    rr = r @ r
+    r0 = np.sqrt(rr)
+    for _ in range(5000):
+        q = A @ lu.solve(A.T @ p)
+        a = rr / (p @ q)
+        lam += a * p
+        r -= a * q
+        rn = r @ r
+        if np.sqrt(rn) < tol * r0:
+            break
+        p = r + rn / rr * p
+        rr = rn
+    return lu.solve(b - A.T @ lam), A
+
+
+def test_doc_known_answer_16x16():
+    # docs/cg_bezier_solver_verification.md:32-39 (Direct column): objective 25.235,
+    # ||x|| 61.715, data residual 0.1398, 2401 DOFs. (The doc's "regularization energy 0.0040"
+    # is not alpha-consistent with its own objective: alpha * x^T H x + lambda * data = 25.235
+    # holds with x^T H x = 0.0010, which is what is asserted here through the objective.)
+    k = GOLD["bezier_doc_16x16"]
+    B = doc_case()
+    assert B.ndof == k["dofs"]
+    x, A = schur_solve(B)
+    obj, reg, dat = B.objective(x)
+    assert abs(obj - k["objective"]) < 6e-4
+    assert abs(np.linalg.norm(x) - k["x_norm"]) < 6e-4
+    assert abs(dat - k["data_residual"]) < 6e-5
+    assert np.abs(A @ x).max() < 1e-8  # constraint violation (doc: 2.45e-08)
+
+
+def test_dof_count_8x8():
+    # tests/integration/test_cg_cubic_bezier_bathymetry_smoother.cpp:935 EightByEightDofCount
+    k = GOLD["bezier_dofs"]
+    X, Y = O.gauss_points(8, 8, 0, 0, 1, 1)
+    assert O.BezierOracle(8, 8, 1.0, 1.0, X + Y).ndof == k["dofs"]
+
+
+def test_plane_reproduction():
+    # polynomial reproduction (test_cg_cubic_bezier_bathymetry_smoother.cpp:46-120): a plane
+    # has zero thin-plate energy and is fitted exactly (ridge off)
+    n, L = 4, 100.0
+    X, Y = O.gauss_points(n, n, 0, 0, L, L)
+    B = O.BezierOracle(n, n, L, L, 2.0 + 0.03 * X - 0.05 * Y, lam=1.0, eps=0.0)
+    x = spl.spsolve(B.csr("Q").tocsc(), B.vec("b"))
+    gi, gj = np.meshgrid(np.arange(3 * n + 1), np.arange(3 * n + 1))
+    plane = 2.0 + 0.03 * (gi.ravel() * L / (3 * n)) - 0.05 * (gj.ravel() * L / (3 * n))
+    np.testing.assert_allclose(x, plane, atol=1e-8)
+
+
+def _fbm_case(n, seed=3, L=5000.0):
+    rng = np.random.default_rng(seed)
+    X, Y = O.gauss_points(n, n, 0, 0, L, L)
+    d = np.zeros_like(X)
+    for _ in range(12):
+        k = rng.uniform(0.5, 6, 2) * 2 * np.pi / L
+        d += rng.normal() / (k @ k) ** 0.5 * np.sin(k[0] * X + k[1] * Y + rng.uniform(0, 6.3))
+    d = 2000 + 1500 * d / np.abs(d).max()
+    return O.BezierOracle(n, n, L, L, d, lam=1.0, eps=1e-4)
+
+
+def test_mg_transfer_and_galerkin_properties():
+    # tests/unit/test_bezier_multigrid.cpp:1130-1274,1586-1652: P rows sum to 1, subdivision
+    # weights non-negative, coarse operators symmetric
+    B = _fbm_case(8)
+    nl = B.mg_setup(2)
+    assert nl == 3
+    for l in range(nl):
+        K = B.level(l)["K"]
+        np.testing.assert_allclose(K, K.T, atol=1e-9 * np.abs(K).max())
+    # the coarse operator is the Galerkin product P^T Q_f P with the ridge kept on the diagonal
+    # (checked on dense matrices of the two finest levels)
+    fine, crs = B.level(nl - 1), B.level(nl - 2)
+    nf, nc = 3 * fine["n"] + 1, 3 * crs["n"] + 1
+    P1 = np.zeros((nf, nc))
+    Sl = np.array([[1, 0, 0, 0], [.5, .5, 0, 0], [.25, .5, .25, 0], [.125, .375, .375, .125]])
+    Sr = Sl[::-1, ::-1]
+    for f in range(nf):
+        E = min(f // 6, crs["n"] - 1)
+        k = f - 6 * E
+        P1[f, 3 * E:3 * E + 4] = Sl[k] if k <= 3 else Sr[k - 3]
+    assert np.all(P1 >= 0) and np.allclose(P1.sum(1), 1.0)  # partition of unity, non-negative
+    P = np.kron(P1, P1)  # [fj, fi] x [cj, ci] ordering matches i + nd * j
+    Qf = np.stack([B.level_apply(nl - 1, e) for e in np.eye(nf * nf)], 1)
+    Qc = np.stack([B.level_apply(nl - 2, e) for e in np.eye(nc * nc)], 1)
+    G = P.T @ Qf @ P
+    np.testing.assert_allclose(np.diag(G), np.diag(Qc), rtol=1e-10)
+    off = G - Qc
+    np.fill_diagonal(off, 0.0)
+    assert np.abs(off).max() <= 1e-4 * 4.0  # only the off-diagonal part of lambda*eps*P^T P
+
+
+def test_vcycle_is_spd_preconditioner():
+    # V-cycle yields r^T z > 0 (test_bezier_multigrid.cpp) and is symmetric (r1.Mr2 = r2.Mr1)
+    B = _fbm_case(16)
+    B.mg_setup(2)
+    rng = np.random.default_rng(0)
+    r1, r2 = rng.standard_normal((2, B.ndof))
+    z1, z2 = B.vcycle(r1), B.vcycle(r2)
+    assert r1 @ z1 > 0 and r2 @ z2 > 0
+    assert abs(r1 @ z2 - r2 @ z1) < 1e-8 * abs(r1 @ z2)
+
+
+def test_mg_pcg_matches_direct():
+    B = _fbm_case(32)
+    B.mg_setup(2)
+    x, it, rr = B.pcg(precond="mg", tol=1e-10)
+    xd = spl.spsolve(B.csr("Q").tocsc(), B.vec("b"))
+    assert rr <= 1e-10 and it < 60
+    assert np.abs(x - xd).max() / np.abs(xd).max() < 1e-8
+    x2, it2, rr2 = B.pcg(precond="jacobi", tol=1e-10, maxit=20000)
+    assert it2 > 3 * it  # multigrid is a much stronger preconditioner
