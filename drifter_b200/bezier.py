@@ -1,0 +1,109 @@
+"""Host mirror of DRIFTER's cubic Bezier smoother interfaces over the C ABI.
+
+  * BezierSmoother  ~ CGBezierSmootherBase assembly + solve (src/bathymetry/cg_bezier_smoother_base.cpp)
+  * BezierMultigridPreconditioner.setup/apply (include/bathymetry/bezier_multigrid_preconditioner.hpp:240,246)
+  * solve(...) = PCG on Q x = b (FP64) with preconditioner "none" | "jacobi" | "mg" | "cnn" | "mg+cnn"
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from ._abi import check, dptr, lib
+
+PRECOND = {"none": 0, "jacobi": 1, "mg": 2, "cnn": 3, "mg+cnn": 4}
+
+
+class BzGridDesc(C.Structure):
+    _fields_ = [("nx", C.c_int32), ("ny", C.c_int32), ("x0", C.c_double), ("y0", C.c_double),
+                ("Lx", C.c_double), ("Ly", C.c_double), ("lam", C.c_double),
+                ("ridge_epsilon", C.c_double)]
+
+
+def _setup_sigs():
+    L = lib()
+    vp, dp = C.c_void_p, C.POINTER(C.c_double)
+    sigs = {
+        "drf_bz_create": [C.POINTER(BzGridDesc), dp, C.POINTER(C.c_void_p)],
+        "drf_bz_destroy": [vp], "drf_bz_set_stream": [vp, vp],
+        "drf_bz_info": [vp, C.POINTER(C.c_int64), dp, C.POINTER(C.c_int)],
+        "drf_bz_get_rhs": [vp, dp], "drf_bz_apply_Q": [vp, dp, dp],
+        "drf_mg_setup": [vp, C.c_int, C.c_int, C.c_int], "drf_mg_apply": [vp, dp, dp],
+        "drf_pcg_solve": [vp, dp, dp, C.c_double, C.c_int, C.c_int, C.POINTER(C.c_int), dp, dp],
+    }
+    for k, a in sigs.items():
+        getattr(L, k).argtypes = a
+        getattr(L, k).restype = C.c_int
+    return L
+
+
+class BezierSmoother:
+    """Uniform-grid cubic Bezier smoother resident on the GPU."""
+
+    def __init__(self, nx, ny, Lx, Ly, dgauss, lam=1.0, ridge_epsilon=1e-4, x0=0.0, y0=0.0):
+        L = _setup_sigs()
+        self.desc = BzGridDesc(nx, ny, x0, y0, Lx, Ly, lam, ridge_epsilon)
+        d = np.ascontiguousarray(dgauss, dtype=np.float64)
+        h = C.c_void_p()
+        check(L.drf_bz_create(C.byref(self.desc), dptr(d), C.byref(h)))
+        self.h = h
+        n, a, nl = C.c_int64(), C.c_double(), C.c_int()
+        check(L.drf_bz_info(self.h, C.byref(n), C.byref(a), C.byref(nl)))
+        self.ndof, self.alpha = n.value, a.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().drf_bz_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, ptr):
+        check(lib().drf_bz_set_stream(self.h, C.c_void_p(ptr or 0)))
+
+    def rhs(self):
+        b = np.empty(self.ndof)
+        check(lib().drf_bz_get_rhs(self.h, dptr(b)))
+        return b
+
+    def apply_Q(self, x):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.empty(self.ndof)
+        check(lib().drf_bz_apply_Q(self.h, dptr(x), dptr(y)))
+        return y
+
+    def mg_setup(self, coarsest_n=2, pre=1, post=1):
+        check(lib().drf_mg_setup(self.h, coarsest_n, pre, post))
+
+    def mg_apply(self, r):
+        r = np.ascontiguousarray(r, dtype=np.float64)
+        z = np.empty(self.ndof)
+        check(lib().drf_mg_apply(self.h, dptr(r), dptr(z)))
+        return z
+
+    def solve(self, precond="mg", tol=1e-10, maxit=1000, b=None, x0=None):
+        x = np.zeros(self.ndof) if x0 is None else np.array(x0, dtype=np.float64)
+        bb = None if b is None else np.ascontiguousarray(b, dtype=np.float64)
+        it, rr, ms = C.c_int(), C.c_double(), C.c_double()
+        check(lib().drf_pcg_solve(self.h, dptr(bb) if bb is not None else None, dptr(x), tol,
+                                  maxit, PRECOND[precond], C.byref(it), C.byref(rr), C.byref(ms)))
+        return x, dict(iters=it.value, relres=rr.value, ms=ms.value)
+
+
+class BezierMultigridPreconditioner:
+    """setup()/apply() over a BezierSmoother's operator (one symmetric V-cycle per apply)."""
+
+    def __init__(self, smoother: BezierSmoother, coarsest_n=2, pre=1, post=1):
+        self.s = smoother
+        self.cfg = (coarsest_n, pre, post)
+
+    def setup(self):
+        self.s.mg_setup(*self.cfg)
+
+    def apply(self, r):
+        return self.s.mg_apply(r)

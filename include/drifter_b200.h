@@ -147,6 +147,42 @@ int drf_dg_download_surface(drf_dg *m, double *eta);
 /* Size and pointer introspection for the bench (device-resident timing). */
 int drf_dg_info(drf_dg *m, int64_t *n3d_nodes, int64_t *n2d_nodes, int *precision);
 
+/* ------------------------------------------------------------------ Bezier smoother
+ * Uniform-grid cubic Bezier bathymetry smoother: Q = alpha H + lambda (B^T W B + eps I),
+ * control points (3 nx + 1) x (3 ny + 1), point (gi, gj) at gi + (3 nx + 1) gj. */
+typedef struct drf_bz drf_bz;
+
+typedef struct {
+    int32_t nx, ny;               /* elements per direction (the GPU path needs nx == ny) */
+    double x0, y0, Lx, Ly;        /* domain */
+    double lambda, ridge_epsilon; /* CGCubicBezierSmootherConfig::lambda, ridge_epsilon */
+} drf_bz_grid_desc;
+
+/* Builds the operator and assembles b = lambda B^T W d on the GPU from the data sampled at the
+ * 4x4 Gauss points of every element (dgauss: [ey][ex][qj][qi]). Replaces
+ * CGBezierSmootherBase::assemble_hessian_global / assemble_data_fitting_global / assemble_Q /
+ * assemble_b (src/bathymetry/cg_bezier_smoother_base.cpp:260,308,396,405). */
+int drf_bz_create(const drf_bz_grid_desc *grid, const double *dgauss, drf_bz **out);
+int drf_bz_destroy(drf_bz *h);
+int drf_bz_set_stream(drf_bz *h, void *cuda_stream);
+int drf_bz_info(drf_bz *h, int64_t *ndof, double *alpha, int *nlevels);
+int drf_bz_get_rhs(drf_bz *h, double *b);
+/* y = Q x, matrix-free (the SpMV L.Q * x of src/bathymetry/bezier_multigrid_preconditioner.cpp:776). */
+int drf_bz_apply_Q(drf_bz *h, const double *x, double *y);
+/* BezierMultigridPreconditioner::setup (include/bathymetry/bezier_multigrid_preconditioner.hpp:240):
+ * levels down to coarsest_n elements per direction, pre/post colored-Schwarz sweeps. */
+int drf_mg_setup(drf_bz *h, int coarsest_n, int pre, int post);
+/* One V-cycle z = M r (BezierMultigridPreconditioner::apply, :246; the reference repeats
+ * V-cycles to a tolerance, this entry applies one symmetric cycle). */
+int drf_mg_apply(drf_bz *h, const double *r, double *z);
+/* PCG on Q x = b to ||r|| <= tol ||b|| (FP64). b NULL = the assembled right-hand side; x holds
+ * the initial guess and returns the solution. kind: 0 none, 1 Jacobi, 2 multigrid V-cycle,
+ * 3 learned CNN, 4 CNN-corrected multigrid. Maps the PCG loop of
+ * solve_with_constraints_iterative (src/bathymetry/cg_cubic_bezier_bathymetry_smoother.cpp:479-558)
+ * with Q in place of the Schur operator. *ms = device time of the solve. */
+int drf_pcg_solve(drf_bz *h, const double *b, double *x, double tol, int maxit, int kind,
+                  int *iters, double *relres, double *ms);
+
 #ifdef __cplusplus
 }
 #endif
