@@ -119,3 +119,49 @@ def perturb(case: dict, seed: int = 7, amp_u: float = 0.05, amp_eta: float = 0.0
     out = dict(case)
     out.update(q=q, eta=eta)
     return out
+
+
+def gauss01_4() -> np.ndarray:
+    a = np.sqrt(3 / 7 - 2 / 7 * np.sqrt(6 / 5))
+    b = np.sqrt(3 / 7 + 2 / 7 * np.sqrt(6 / 5))
+    return np.array([0.5 * (1 - b), 0.5 * (1 - a), 0.5 * (1 + a), 0.5 * (1 + b)])
+
+
+def fbm_field(m: int, seed: int = SEED, beta: float = 2.0) -> np.ndarray:
+    """Periodic fractional-Brownian surface on an m x m grid with power spectrum 1/f^beta."""
+    rng = np.random.default_rng(seed)
+    kx = np.fft.fftfreq(m)[None, :]
+    ky = np.fft.fftfreq(m)[:, None]
+    k = np.sqrt(kx * kx + ky * ky)
+    k[0, 0] = 1.0
+    amp = k ** (-beta / 2.0)
+    amp[0, 0] = 0.0
+    ph = rng.uniform(0, 2 * np.pi, (m, m))
+    return np.real(np.fft.ifft2(amp * np.exp(1j * ph)))
+
+
+def c4(n: int = 512, L: float = 51200.0, seed: int = SEED, lam: float = 1.0, eps: float = 1e-4):
+    """C4: cubic Bezier smoother on an n x n grid over seeded fBm bathymetry (1/f^2 spectrum)
+    scaled to 0-4000 m, sampled at the 4x4 Gauss points of every element ([ey][ex][qj][qi])."""
+    m = 4 * n
+    f = fbm_field(m, seed)
+    f = 4000.0 * (f - f.min()) / (f.max() - f.min())
+    p = gauss01_4()
+    dx = L / n
+    ex = np.arange(n)
+    X = (ex[None, :, None, None] + p[None, None, None, :]) * dx
+    Y = (ex[:, None, None, None] + p[None, None, :, None]) * dx
+    X = np.broadcast_to(X, (n, n, 4, 4)).reshape(-1)
+    Y = np.broadcast_to(Y, (n, n, 4, 4)).reshape(-1)
+    # bilinear sampling of the periodic grid field (cell-centred samples at (i + 0.5) L / m)
+    u = X / L * m - 0.5
+    v = Y / L * m - 0.5
+    i0 = np.floor(u).astype(np.int64)
+    j0 = np.floor(v).astype(np.int64)
+    fu, fv = u - i0, v - j0
+    i0 %= m
+    j0 %= m
+    i1, j1 = (i0 + 1) % m, (j0 + 1) % m
+    d = ((1 - fu) * (1 - fv) * f[j0, i0] + fu * (1 - fv) * f[j0, i1] + (1 - fu) * fv * f[j1, i0]
+         + fu * fv * f[j1, i1])
+    return dict(n=n, L=L, lam=lam, eps=eps, d=d.copy(), name=f"C4 Bezier {n}x{n}")

@@ -8,6 +8,7 @@
 // Layout: control point (gi, gj) of a level with n elements per direction is stored at
 // gi + (3n + 1) * gj; element (ex, ey) owns control points 3ex..3ex+3 x 3ey..3ey+3 and its
 // local dof k = i + 4 j (the reference's cubic dof order, include/bathymetry/cubic_bezier_basis_2d.hpp).
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -556,7 +557,8 @@ int drf_bz_create(const drf_bz_grid_desc *g, const double *dgauss, drf_bz **out)
         up(h->Bq, h->H.Bq);
         for (auto *v : {&h->b, &h->x, &h->r, &h->z, &h->p, &h->q}) v->alloc(h->ndof);
         h->scal.alloc(S_NSLOT);
-        h->part.alloc(4096);
+        // per-block partials: the fused apply-dot writes one value per apply block
+        h->part.alloc(std::max<size_t>(4096, (size_t)nblk(h->ndof) + 16));
         h->ctl.alloc(3);
         bz_rhs_kernel<<<nblk(h->ndof), BS, 0, h->stream>>>(F.n, F.nd, h->dat.p, h->Bq.p, g->lambda, h->b.p);
         DRF_LAUNCHED();
