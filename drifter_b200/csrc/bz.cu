@@ -388,7 +388,7 @@ struct drf_bz {
     BzSetup H;  // host-side setup (element matrices, levels, transfers)
     cudaStream_t stream = nullptr, own = nullptr;
     int64_t ndof = 0;
-    DevBuf<double> dat, Bq, b, x, r, z, p, q, scal, part, mgbuf, coarse;
+    DevBuf<double> dat, Bq, b, bs, x, r, z, p, q, scal, part, mgbuf, coarse;  // b: assembled rhs, bs: rhs of the current solve
     DevBuf<int> ctl;
     struct Lv {
         DevBuf<double> K, rho, binv, x, b, r;
@@ -555,7 +555,7 @@ int drf_bz_create(const drf_bz_grid_desc *g, const double *dgauss, drf_bz **out)
         h->dat.alloc(nd);
         DRF_CUDA(cudaMemcpy(h->dat.p, dgauss, nd * 8, cudaMemcpyHostToDevice));
         up(h->Bq, h->H.Bq);
-        for (auto *v : {&h->b, &h->x, &h->r, &h->z, &h->p, &h->q}) v->alloc(h->ndof);
+        for (auto *v : {&h->b, &h->bs, &h->x, &h->r, &h->z, &h->p, &h->q}) v->alloc(h->ndof);
         h->scal.alloc(S_NSLOT);
         // per-block partials: the fused apply-dot writes one value per apply block
         h->part.alloc(std::max<size_t>(4096, (size_t)nblk(h->ndof) + 16));
@@ -670,7 +670,8 @@ int drf_pcg_solve(drf_bz *h, const double *bh, double *xh, double tol, int maxit
         cudaEvent_t e0, e1;
         DRF_CUDA(cudaEventCreate(&e0));
         DRF_CUDA(cudaEventCreate(&e1));
-        if (bh) DRF_CUDA(cudaMemcpyAsync(h->b.p, bh, n * 8, cudaMemcpyHostToDevice, h->stream));
+        if (bh) DRF_CUDA(cudaMemcpyAsync(h->bs.p, bh, n * 8, cudaMemcpyHostToDevice, h->stream));
+        else DRF_CUDA(cudaMemcpyAsync(h->bs.p, h->b.p, n * 8, cudaMemcpyDeviceToDevice, h->stream));
         DRF_CUDA(cudaMemcpyAsync(h->x.p, xh, n * 8, cudaMemcpyHostToDevice, h->stream));
         DRF_CUDA(cudaEventRecord(e0, h->stream));
         PcgCtl c = h->pctl();
@@ -680,9 +681,9 @@ int drf_pcg_solve(drf_bz *h, const double *bh, double *xh, double tol, int maxit
         DRF_CUDA(cudaMemcpyAsync(h->scal.p + S_TOL2, &tol2, 8, cudaMemcpyHostToDevice, h->stream));
         // r = b - Q x ; bb = b.b ; z = M r ; rz = r.z ; p = z
         const LevelDev L = h->levdev(h->finest());
-        bz_apply_kernel<<<nblk(n), BS, 0, h->stream>>>(L, h->x.p, h->b.p, h->r.p, 1, nullptr, nullptr);
+        bz_apply_kernel<<<nblk(n), BS, 0, h->stream>>>(L, h->x.p, h->bs.p, h->r.p, 1, nullptr, nullptr);
         DRF_LAUNCHED();
-        dot_kernel<<<h->nparts(), BS, 0, h->stream>>>(n, h->b.p, h->b.p, h->part.p, nullptr);
+        dot_kernel<<<h->nparts(), BS, 0, h->stream>>>(n, h->bs.p, h->bs.p, h->part.p, nullptr);
         DRF_LAUNCHED();
         reduce_kernel<<<1, BS, 0, h->stream>>>(h->part.p, (int)h->nparts(), h->scal.p + S_BB);
         DRF_LAUNCHED();
