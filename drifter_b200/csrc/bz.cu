@@ -10,6 +10,7 @@
 // local dof k = i + 4 j (the reference's cubic dof order, include/bathymetry/cubic_bezier_basis_2d.hpp).
 #include <algorithm>
 #include <cmath>
+#include <string>
 #include <cstring>
 #include <memory>
 #include <vector>
@@ -379,7 +380,25 @@ __global__ void zero_kernel(int64_t n, double *a, const int *stop) {
     if (t < n) a[t] = 0.0;
 }
 
+__global__ void fill_kernel(int64_t n, double v, double *a) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t < n) a[t] = v;
+}
+
 }  // namespace
+
+// ---------------------------------------------------------------- allocation-free solve
+// Scratch of drf_bz_jacobi_pcg_noalloc: a file-scope device array that every GPU loading this
+// library holds until process exit (NOALLOC_BYTES). Layout in doubles: element operator (256),
+// ridge factors (NOALLOC_MAX_ND), PCG vectors r, z, p, q (NOALLOC_MAX_DOF each), per-block
+// partials (NOALLOC_PARTS), scalars (S_NSLOT, padded to 16) and three int control words.
+constexpr int64_t NOALLOC_MAX_DOF = 1 << 18;  // 262,144 control points (170 x 170 elements)
+constexpr int NOALLOC_MAX_ND = 512;
+constexpr int NOALLOC_PARTS = 1040;           // >= nblk(NOALLOC_MAX_DOF) and >= 1024
+constexpr int64_t NOALLOC_DOUBLES =
+    256 + NOALLOC_MAX_ND + 4 * NOALLOC_MAX_DOF + NOALLOC_PARTS + 16 + 4;
+static __device__ __align__(256) double g_noalloc_scratch[NOALLOC_DOUBLES];
+
 }  // namespace drf
 
 using namespace drf;
@@ -746,6 +765,110 @@ int drf_pcg_solve(drf_bz *h, const double *bh, double *xh, double tol, int maxit
         if (iters) *iters = it;
         if (relres) *relres = sc[S_BB] > 0 ? std::sqrt(sc[S_RR] / sc[S_BB]) : 0.0;
         if (ms) *ms = t;
+        DRF_CHECK(std::isfinite(sc[S_RR]), DRF_E_NONFINITE, "PCG diverged (non-finite residual)");
+    });
+}
+
+// Callers that cannot allocate device memory (a host application that hands this library
+// only the buffers it already owns, code running under an allocator that forbids
+// cudaMalloc/cudaFree, or a stream being used by another runtime that must not see
+// device-wide synchronising allocation calls) solve Q x = b with Jacobi-preconditioned CG
+// here. All scratch is the file-scope array g_noalloc_scratch; the caller passes the device
+// right-hand side and the device solution buffer (initial guess in, solution out).
+int drf_bz_jacobi_pcg_noalloc(const drf_bz_grid_desc *g, const double *d_b, double *d_x,
+                              double tol, int maxit, void *stream, int *iters, double *relres) {
+    return guard([&] {
+        DRF_CHECK(g && d_b && d_x && iters && relres, DRF_E_INVALID, "null argument");
+        DRF_CHECK(g->nx >= 1 && g->nx == g->ny, DRF_E_INVALID, "square grid (nx == ny >= 1) required");
+        DRF_CHECK(g->Lx > 0 && g->Ly > 0 && g->lambda > 0 && g->ridge_epsilon >= 0, DRF_E_INVALID,
+                  "extent and lambda must be positive, ridge_epsilon >= 0");
+        DRF_CHECK(tol > 0 && maxit >= 0, DRF_E_INVALID, "tol must be > 0 and maxit >= 0");
+        const int nd = 3 * g->nx + 1;
+        const int64_t n = (int64_t)nd * nd;
+        DRF_CHECK(nd <= NOALLOC_MAX_ND && n <= NOALLOC_MAX_DOF, DRF_E_UNSUPPORTED,
+                  "grid too large for the allocation-free solve: at most " +
+                      std::to_string(NOALLOC_MAX_DOF) + " control points (nx <= 170)");
+        // device address of the scratch array, looked up once per device with it current
+        static double *base[64] = {nullptr};
+        int dev = 0;
+        DRF_CUDA(cudaGetDevice(&dev));
+        DRF_CHECK(dev >= 0 && dev < 64, DRF_E_UNSUPPORTED, "device ordinal out of range");
+        if (!base[dev]) {
+            void *ptr = nullptr;
+            DRF_CUDA(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
+            base[dev] = static_cast<double *>(ptr);
+        }
+        double *K = base[dev], *rho = K + 256, *r = rho + NOALLOC_MAX_ND;
+        double *z = r + NOALLOC_MAX_DOF, *p = z + NOALLOC_MAX_DOF, *q = p + NOALLOC_MAX_DOF;
+        double *part = q + NOALLOC_MAX_DOF, *scal = part + NOALLOC_PARTS;
+        int *ctl = reinterpret_cast<int *>(scal + 16);
+        cudaStream_t st = (cudaStream_t)stream;
+        upload_sub();
+        double Kh[256], alpha = 0.0;
+        bz_fine_operator(*g, Kh, &alpha);
+        // every value the solve reads is written here first (the array keeps the last call's data)
+        DRF_CUDA(cudaMemcpyAsync(K, Kh, sizeof(Kh), cudaMemcpyHostToDevice, st));
+        fill_kernel<<<nblk(nd), BS, 0, st>>>(nd, 1.0, rho);
+        DRF_LAUNCHED();
+        const int ctl0[3] = {0, 0, maxit};
+        DRF_CUDA(cudaMemcpyAsync(ctl, ctl0, sizeof(ctl0), cudaMemcpyHostToDevice, st));
+        const double tol2 = tol * tol;
+        DRF_CUDA(cudaMemcpyAsync(scal + S_TOL2, &tol2, sizeof(double), cudaMemcpyHostToDevice, st));
+        LevelDev L;
+        L.n = g->nx; L.nd = nd; L.K = K; L.rho = rho; L.binv = nullptr;
+        L.lam_eps = g->lambda * g->ridge_epsilon;
+        PcgCtl c;
+        c.sc = scal; c.stop = ctl; c.iters = ctl + 1; c.maxit = ctl + 2; c.part = part;
+        const unsigned nb = nblk(n), np = 1024;
+        bz_apply_kernel<<<nb, BS, 0, st>>>(L, d_x, d_b, r, 1, nullptr, nullptr);
+        DRF_LAUNCHED();
+        dot_kernel<<<np, BS, 0, st>>>(n, d_b, d_b, part, nullptr);
+        DRF_LAUNCHED();
+        reduce_kernel<<<1, BS, 0, st>>>(part, (int)np, scal + S_BB);
+        DRF_LAUNCHED();
+        dot_kernel<<<np, BS, 0, st>>>(n, r, r, part, nullptr);
+        DRF_LAUNCHED();
+        reduce_kernel<<<1, BS, 0, st>>>(part, (int)np, scal + S_RR);
+        DRF_LAUNCHED();
+        jacobi_kernel<<<nb, BS, 0, st>>>(L, r, z, nullptr);
+        DRF_LAUNCHED();
+        dot_kernel<<<np, BS, 0, st>>>(n, r, z, part, nullptr);
+        DRF_LAUNCHED();
+        reduce_kernel<<<1, BS, 0, st>>>(part, (int)np, scal + S_RZ);
+        DRF_LAUNCHED();
+        p_update_kernel<<<np, BS, 0, st>>>(n, c, z, p, 1);
+        DRF_LAUNCHED();
+        double sc[S_NSLOT];
+        DRF_CUDA(cudaMemcpyAsync(sc, scal, sizeof(sc), cudaMemcpyDeviceToHost, st));
+        DRF_CUDA(cudaStreamSynchronize(st));
+        int cl[3] = {0, 0, maxit};
+        if (sc[S_RR] > tol2 * sc[S_BB] && maxit > 0) {
+            while (true) {
+                bz_apply_kernel<<<nb, BS, 0, st>>>(L, p, nullptr, q, 0, part, ctl);
+                DRF_LAUNCHED();
+                alpha_kernel<<<1, BS, 0, st>>>(c, (int)nb);
+                DRF_LAUNCHED();
+                xr_update_kernel<<<np, BS, 0, st>>>(n, c, p, q, d_x, r);
+                DRF_LAUNCHED();
+                conv_kernel<<<1, BS, 0, st>>>(c, (int)np);
+                DRF_LAUNCHED();
+                jacobi_kernel<<<nb, BS, 0, st>>>(L, r, z, ctl);
+                DRF_LAUNCHED();
+                dot_kernel<<<np, BS, 0, st>>>(n, r, z, part, ctl);
+                DRF_LAUNCHED();
+                beta_kernel<<<1, BS, 0, st>>>(c, (int)np);
+                DRF_LAUNCHED();
+                p_update_kernel<<<np, BS, 0, st>>>(n, c, z, p, 0);
+                DRF_LAUNCHED();
+                DRF_CUDA(cudaMemcpyAsync(cl, ctl, sizeof(cl), cudaMemcpyDeviceToHost, st));
+                DRF_CUDA(cudaStreamSynchronize(st));
+                if (cl[0] || cl[1] >= maxit) break;
+            }
+            DRF_CUDA(cudaMemcpyAsync(sc, scal, sizeof(sc), cudaMemcpyDeviceToHost, st));
+            DRF_CUDA(cudaStreamSynchronize(st));
+        }
+        *iters = cl[1];
+        *relres = sc[S_BB] > 0 ? std::sqrt(sc[S_RR] / sc[S_BB]) : 0.0;
         DRF_CHECK(std::isfinite(sc[S_RR]), DRF_E_NONFINITE, "PCG diverged (non-finite residual)");
     });
 }

@@ -102,6 +102,16 @@ static void global_frob2(int n, const double *A, const double *B, double &fa, do
         }
 }
 
+void bz_fine_operator(const drf_bz_grid_desc &g, double K[256], double *alpha) {
+    double He[256], Be[256], Bq[256];
+    element_ops(g.Lx / g.nx, g.Ly / g.ny, He, Be, Bq);
+    double fh, fb;
+    global_frob2(g.nx, He, Be, fh, fb);
+    const double a = fh > 0 ? std::sqrt(fb) / std::sqrt(fh) : 0.0;
+    for (int i = 0; i < 256; ++i) K[i] = a * He[i] + g.lambda * Be[i];
+    *alpha = a;
+}
+
 void bz_setup_fine(BzSetup &s, const drf_bz_grid_desc &g) {
     s.g = g;
     s.dx = g.Lx / g.nx;

@@ -27,6 +27,8 @@ struct BzSetup {
 
 void bz_subdivision_1d(double S[2][16]);
 void bz_setup_fine(BzSetup &s, const drf_bz_grid_desc &g);
+// Finest-level element operator K = alpha H + lambda B and alpha, without heap allocation.
+void bz_fine_operator(const drf_bz_grid_desc &g, double K[256], double *alpha);
 void bz_setup_levels(BzSetup &s, int coarsest_n, int pre, int post);
 
 }  // namespace drf

@@ -183,6 +183,19 @@ int drf_mg_apply(drf_bz *h, const double *r, double *z);
 int drf_pcg_solve(drf_bz *h, const double *b, double *x, double tol, int maxit, int kind,
                   int *iters, double *relres, double *ms);
 
+/* Allocation-free variant of drf_pcg_solve with the Jacobi preconditioner (kind 1), for callers
+ * that cannot allocate device memory. No counterpart in the reference (it has no device code).
+ * The caller owns d_b (device, (3 nx + 1)^2 doubles) and d_x (device, initial guess in,
+ * solution out); stream is a cudaStream_t (NULL = legacy default stream).
+ * Scratch: one file-scope device array of 8.5 MB in libdrifter_b200.so, held on every device
+ * that loads the library until process exit; grids up to 262,144 control points (nx <= 170),
+ * larger sizes return DRF_E_UNSUPPORTED. It calls no cudaMalloc/cudaFree. The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress) and must come before any
+ * stream capture on that device. Every call shares the array: calls that overlap on the GPU
+ * (other host threads, other streams) race and must be serialised by the caller. */
+int drf_bz_jacobi_pcg_noalloc(const drf_bz_grid_desc *grid, const double *d_b, double *d_x,
+                              double tol, int maxit, void *stream, int *iters, double *relres);
+
 #ifdef __cplusplus
 }
 #endif
