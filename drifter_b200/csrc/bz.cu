@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "bz_host.hpp"
+#include "cnn.hpp"
 #include "common.cuh"
 
 namespace drf {
@@ -265,6 +266,57 @@ __global__ void __launch_bounds__(BS) dot_kernel(int64_t n, const double *a, con
     if (threadIdx.x == 0) part[blockIdx.x] = red[0];
 }
 
+// partial dot products a.b and a.c per block (part and part + gridDim.x)
+__global__ void __launch_bounds__(BS) dot2_kernel(int64_t n, const double *a, const double *b,
+                                                  const double *cvec, double *part, const int *stop) {
+    __shared__ double red[2][BS];
+    if (stop && *stop) return;
+    double s = 0.0, s2 = 0.0;
+    for (int64_t t = blockIdx.x * (int64_t)BS + threadIdx.x; t < n; t += (int64_t)gridDim.x * BS) {
+        s += a[t] * b[t];
+        s2 += a[t] * cvec[t];
+    }
+    red[0][threadIdx.x] = s;
+    red[1][threadIdx.x] = s2;
+    __syncthreads();
+    for (int k = BS / 2; k > 0; k >>= 1) {
+        if (threadIdx.x < k) {
+            red[0][threadIdx.x] += red[0][threadIdx.x + k];
+            red[1][threadIdx.x] += red[1][threadIdx.x + k];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        part[blockIdx.x] = red[0][0];
+        part[gridDim.x + blockIdx.x] = red[1][0];
+    }
+}
+
+// flexible CG (Notay's FCG(1)): rz = r.z, beta = -(z.q)/(p.q)
+__global__ void beta_fcg_kernel(PcgCtl c, int nparts) {
+    __shared__ double red[2][BS];
+    if (*c.stop) return;
+    double s = 0.0, s2 = 0.0;
+    for (int i = threadIdx.x; i < nparts; i += BS) {
+        s += c.part[i];
+        s2 += c.part[nparts + i];
+    }
+    red[0][threadIdx.x] = s;
+    red[1][threadIdx.x] = s2;
+    __syncthreads();
+    for (int k = BS / 2; k > 0; k >>= 1) {
+        if (threadIdx.x < k) {
+            red[0][threadIdx.x] += red[0][threadIdx.x + k];
+            red[1][threadIdx.x] += red[1][threadIdx.x + k];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        c.sc[S_RZ] = red[0][0];
+        c.sc[S_BETA] = -red[1][0] / c.sc[S_PQ];
+    }
+}
+
 __global__ void alpha_kernel(PcgCtl c, int nparts) {
     __shared__ double red[BS];
     if (*c.stop) return;
@@ -415,6 +467,8 @@ struct drf_bz {
     };
     std::vector<Lv> lv;
     bool mg_ready = false;
+    drf_cnn *cnn = nullptr;
+    double cnn_scale = 1.0;
     cudaGraphExec_t graph = nullptr;
     int graph_kind = -1, graph_chunk = 0;
 
@@ -446,6 +500,9 @@ struct drf_bz {
         } else if (kind == 1) {
             jacobi_kernel<<<nblk(n), BS, 0, stream>>>(levdev(L), rin, zout, stop);
             DRF_LAUNCHED();
+        } else if (kind == 3) {
+            cnn_precondition(cnn_net(cnn), stream, lv[finest()].n, rin, scal.p + S_RR, cnn_scale,
+                             zout, stop);
         } else {
             vcycle(rin, zout);
         }
@@ -510,10 +567,17 @@ struct drf_bz {
         conv_kernel<<<1, BS, 0, stream>>>(c, (int)nparts());
         DRF_LAUNCHED();
         precondition(kind, r.p, z.p, c.stop);
-        dot_kernel<<<nparts(), BS, 0, stream>>>(ndof, r.p, z.p, part.p, c.stop);
-        DRF_LAUNCHED();
-        beta_kernel<<<1, BS, 0, stream>>>(c, (int)nparts());
-        DRF_LAUNCHED();
+        if (kind == 3) {
+            dot2_kernel<<<nparts(), BS, 0, stream>>>(ndof, z.p, r.p, q.p, part.p, c.stop);
+            DRF_LAUNCHED();
+            beta_fcg_kernel<<<1, BS, 0, stream>>>(c, (int)nparts());
+            DRF_LAUNCHED();
+        } else {
+            dot_kernel<<<nparts(), BS, 0, stream>>>(ndof, r.p, z.p, part.p, c.stop);
+            DRF_LAUNCHED();
+            beta_kernel<<<1, BS, 0, stream>>>(c, (int)nparts());
+            DRF_LAUNCHED();
+        }
         p_update_kernel<<<nparts(), BS, 0, stream>>>(ndof, c, z.p, p.p, 0);
         DRF_LAUNCHED();
     }
@@ -666,6 +730,22 @@ int drf_mg_setup(drf_bz *h, int coarsest_n, int pre, int post) {
     });
 }
 
+int drf_bz_set_cnn(drf_bz *h, drf_cnn *net, double out_scale) {
+    return guard([&] {
+        check_bz(h);
+        DRF_CHECK(net, DRF_E_INVALID, "null network");
+        DRF_CHECK(std::isfinite(out_scale) && out_scale > 0, DRF_E_INVALID, "out_scale must be > 0");
+        h->cnn = net;
+        h->cnn_scale = out_scale;
+        cnn_prepare(cnn_net(net), h->lv[h->finest()].n);
+        if (h->graph && h->graph_kind == 3) {
+            cudaGraphExecDestroy(h->graph);
+            h->graph = nullptr;
+            h->graph_kind = -1;
+        }
+    });
+}
+
 int drf_mg_apply(drf_bz *h, const double *rh, double *zh) {
     return guard([&] {
         check_bz(h);
@@ -683,8 +763,9 @@ int drf_pcg_solve(drf_bz *h, const double *bh, double *xh, double tol, int maxit
     return guard([&] {
         check_bz(h);
         DRF_CHECK(xh && tol > 0 && maxit >= 0, DRF_E_INVALID, "bad arguments");
-        DRF_CHECK(kind >= 0 && kind <= 2, DRF_E_INVALID, "unknown preconditioner kind");
+        DRF_CHECK(kind >= 0 && kind <= 3, DRF_E_INVALID, "unknown preconditioner kind");
         DRF_CHECK(kind != 2 || h->mg_ready, DRF_E_INVALID, "multigrid preconditioner not set up");
+        DRF_CHECK(kind != 3 || h->cnn, DRF_E_INVALID, "no learned preconditioner attached (drf_bz_set_cnn)");
         const int64_t n = h->ndof;
         cudaEvent_t e0, e1;
         DRF_CUDA(cudaEventCreate(&e0));

@@ -1,0 +1,607 @@
+// Learned preconditioner for the Bezier smoother's CG: a 4-layer conv3x3 network on 3x3
+// "superpixels" of the control-point grid (space-to-depth exposes the element structure:
+// superpixel (I, J) holds the 9 control points 3I..3I+2 x 3J..3J+2 as channels), BF16
+// activations and weights with FP32 accumulation on the tensor cores (mma.sync m16n8k16,
+// implicit GEMM: M = 16 pixels of a row, N = output channels, K = 9 taps x input channels),
+// trained on the GPU by the backward kernels below with Adam.
+//
+// Channels (padded for the MMA shapes): 16 (9 used) -> 32 -> 32 -> 32 -> 16 (9 used); ReLU
+// after layers 1-3. Layouts: activations NHWC [b][h][w][c]; weights [co][tap][ci] (tap = dy*3+dx).
+#include <cuda_bf16.h>
+
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <random>
+#include <vector>
+
+#include "cnn.hpp"
+#include "common.cuh"
+
+namespace drf {
+namespace {
+
+using bf16 = __nv_bfloat16;
+constexpr int CH[5] = {16, 32, 32, 32, 16};
+constexpr int TH = 8, TW = 16;  // CTA tile: 8 rows x 16 pixels, one warp per row
+
+__device__ __forceinline__ void mma_bf16(float c[4], uint32_t a0, uint32_t a1, uint32_t a2,
+                                         uint32_t a3, uint32_t b0, uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+        "{%8,%9}, {%0,%1,%2,%3};"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+// Y = conv3x3(X, W) (+ bias) (+ ReLU); X, W bf16; Y bf16 (OUTF32 = false) or f32.
+// Shared memory: input halo (TH+2) x (TW+2) pixels with pixel stride CIN+8, and the weights
+// with output-channel stride 9*CIN+8 (both paddings remove shared-memory bank conflicts of
+// the fragment loads).
+template <int CIN, int COUT, bool RELU, bool OUTF32>
+__global__ void __launch_bounds__(256) conv3x3_kernel(int H, int W, const bf16 *__restrict__ X,
+                                                      const bf16 *__restrict__ Wt,
+                                                      const float *__restrict__ bias, void *Yv) {
+    constexpr int PS = CIN + 8, WS = 9 * CIN + 8, HP = TH + 2, WP = TW + 2;
+    __shared__ __align__(16) bf16 Xs[HP * WP * PS];
+    __shared__ __align__(16) bf16 Ws[COUT * WS];
+    const int b = blockIdx.z;
+    const int h0 = blockIdx.y * TH, w0 = blockIdx.x * TW;
+    const bf16 *Xb = X + (size_t)b * H * W * CIN;
+    // stage weights (32-bit copies)
+    for (int i = threadIdx.x; i < COUT * 9 * CIN / 2; i += blockDim.x) {
+        const int e = 2 * i, co = e / (9 * CIN), r = e % (9 * CIN);
+        *reinterpret_cast<uint32_t *>(&Ws[co * WS + r]) = reinterpret_cast<const uint32_t *>(Wt)[i];
+    }
+    // stage the input halo, zero outside the image
+    for (int i = threadIdx.x; i < HP * WP * (CIN / 2); i += blockDim.x) {
+        const int pix = i / (CIN / 2), cp = i % (CIN / 2);
+        const int hh = h0 - 1 + pix / WP, ww = w0 - 1 + pix % WP;
+        uint32_t v = 0u;
+        if (hh >= 0 && hh < H && ww >= 0 && ww < W)
+            v = reinterpret_cast<const uint32_t *>(Xb + ((size_t)hh * W + ww) * CIN)[cp];
+        *reinterpret_cast<uint32_t *>(&Xs[pix * PS + 2 * cp]) = v;
+    }
+    __syncthreads();
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32, g = lane >> 2, t = lane & 3;
+    const int h = h0 + warp;
+    float acc[COUT / 8][4];
+#pragma unroll
+    for (int j = 0; j < COUT / 8; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.f;
+#pragma unroll
+    for (int tap = 0; tap < 9; ++tap) {
+        const int dy = tap / 3, dx = tap % 3;
+        // pixel m of the strip reads halo pixel (warp + dy, m + dx)
+        const bf16 *xr0 = &Xs[((warp + dy) * WP + (g + dx)) * PS];
+        const bf16 *xr1 = &Xs[((warp + dy) * WP + (g + 8 + dx)) * PS];
+#pragma unroll
+        for (int kc = 0; kc < CIN; kc += 16) {
+            const uint32_t a0 = *reinterpret_cast<const uint32_t *>(xr0 + kc + 2 * t);
+            const uint32_t a1 = *reinterpret_cast<const uint32_t *>(xr1 + kc + 2 * t);
+            const uint32_t a2 = *reinterpret_cast<const uint32_t *>(xr0 + kc + 2 * t + 8);
+            const uint32_t a3 = *reinterpret_cast<const uint32_t *>(xr1 + kc + 2 * t + 8);
+#pragma unroll
+            for (int j = 0; j < COUT / 8; ++j) {
+                const bf16 *wr = &Ws[(8 * j + g) * WS + tap * CIN + kc];
+                const uint32_t b0 = *reinterpret_cast<const uint32_t *>(wr + 2 * t);
+                const uint32_t b1 = *reinterpret_cast<const uint32_t *>(wr + 2 * t + 8);
+                mma_bf16(acc[j], a0, a1, a2, a3, b0, b1);
+            }
+        }
+    }
+    if (h >= H) return;
+#pragma unroll
+    for (int j = 0; j < COUT / 8; ++j) {
+        const int co = 8 * j + 2 * t;
+        const float b0 = bias ? bias[co] : 0.f, b1 = bias ? bias[co + 1] : 0.f;
+#pragma unroll
+        for (int half = 0; half < 2; ++half) {
+            const int w = w0 + g + 8 * half;
+            if (w >= W) continue;
+            float v0 = acc[j][2 * half] + b0, v1 = acc[j][2 * half + 1] + b1;
+            if (RELU) { v0 = fmaxf(v0, 0.f); v1 = fmaxf(v1, 0.f); }
+            const size_t o = (((size_t)b * H + h) * W + w) * COUT + co;
+            if (OUTF32) {
+                float *Y = static_cast<float *>(Yv);
+                Y[o] = v0;
+                Y[o + 1] = v1;
+            } else {
+                bf16 *Y = static_cast<bf16 *>(Yv);
+                *reinterpret_cast<__nv_bfloat162 *>(&Y[o]) = __floats2bfloat162_rn(v0, v1);
+            }
+        }
+    }
+}
+
+// dW partials of one layer for one CTA tile: dW[co][tap][ci] += dZ[p][co] * A[p + shift][ci],
+// db[co] += dZ[p][co]; FP32, one partial row per tile (reduced in a fixed order afterwards).
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(256) dw_partial_kernel(int H, int W, const float *__restrict__ dZ,
+                                                         const bf16 *__restrict__ A, float *part) {
+    constexpr int HP = TH + 2, WP = TW + 2, NW = COUT * 9 * CIN + COUT;
+    __shared__ float dzs[TH * TW * COUT];
+    __shared__ float as[HP * WP * CIN];
+    const int b = blockIdx.z;
+    const int h0 = blockIdx.y * TH, w0 = blockIdx.x * TW;
+    for (int i = threadIdx.x; i < TH * TW * COUT; i += blockDim.x) {
+        const int p = i / COUT, co = i % COUT;
+        const int hh = h0 + p / TW, ww = w0 + p % TW;
+        dzs[i] = (hh < H && ww < W) ? dZ[(((size_t)b * H + hh) * W + ww) * COUT + co] : 0.f;
+    }
+    for (int i = threadIdx.x; i < HP * WP * CIN; i += blockDim.x) {
+        const int pix = i / CIN, ci = i % CIN;
+        const int hh = h0 - 1 + pix / WP, ww = w0 - 1 + pix % WP;
+        as[i] = (hh >= 0 && hh < H && ww >= 0 && ww < W)
+                    ? __bfloat162float(A[(((size_t)b * H + hh) * W + ww) * CIN + ci])
+                    : 0.f;
+    }
+    __syncthreads();
+    const size_t tile = ((size_t)b * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+    for (int e = threadIdx.x; e < NW; e += blockDim.x) {
+        float s = 0.f;
+        if (e < COUT * 9 * CIN) {
+            const int co = e / (9 * CIN), r = e % (9 * CIN), tap = r / CIN, ci = r % CIN;
+            const int dy = tap / 3, dx = tap % 3;
+            for (int p = 0; p < TH * TW; ++p) {
+                const int ph = p / TW, pw = p % TW;
+                s += dzs[p * COUT + co] * as[((ph + dy) * WP + (pw + dx)) * CIN + ci];
+            }
+        } else {
+            const int co = e - COUT * 9 * CIN;
+            for (int p = 0; p < TH * TW; ++p) s += dzs[p * COUT + co];
+        }
+        part[tile * NW + e] = s;
+    }
+}
+
+__global__ void reduce_cols_kernel(int nrows, int ncols, const float *part, float *out) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= ncols) return;
+    float s = 0.f;
+    for (int r = 0; r < nrows; ++r) s += part[(size_t)r * ncols + e];
+    out[e] = s;
+}
+
+// dOut = 2 (out - target) / count on the 9 used channels; per-block loss partials
+__global__ void loss_grad_kernel(int64_t npix, const float *out, const float *tgt, float *dout,
+                                 float inv_cnt, double *lpart) {
+    __shared__ double red[256];
+    double l = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < npix * 16;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int c = (int)(i % 16);
+        float d = 0.f;
+        if (c < 9) {
+            d = out[i] - tgt[i];
+            l += (double)d * d;
+        }
+        dout[i] = 2.f * d * inv_cnt;
+    }
+    red[threadIdx.x] = l;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) lpart[blockIdx.x] = red[0];
+}
+
+// dZ_{l-1} = dX * (Z_{l-1} > 0); keeps an FP32 copy (for dW) and a BF16 copy (next conv input)
+__global__ void relu_back_kernel(int64_t n, const float *dX, const bf16 *Apost, float *dZ,
+                                 bf16 *dZb) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    // A_post = relu(Z) rounded; Z > 0 <=> A_post > 0 except values that rounded to 0
+    const float v = __bfloat162float(Apost[i]) > 0.f ? dX[i] : 0.f;
+    dZ[i] = v;
+    dZb[i] = __float2bfloat16_rn(v);
+}
+
+__global__ void f32_to_bf16_kernel(int64_t n, const float *a, bf16 *b) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) b[i] = __float2bfloat16_rn(a[i]);
+}
+
+// bf16 weights of a layer and the flipped/transposed copy used by the input-gradient conv
+__global__ void cast_weights_kernel(int cin, int cout, const float *Wm, bf16 *W, bf16 *Wflip) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= cout * 9 * cin) return;
+    const int co = e / (9 * cin), r = e % (9 * cin), tap = r / cin, ci = r % cin;
+    const bf16 v = __float2bfloat16_rn(Wm[e]);
+    W[e] = v;
+    if (Wflip) Wflip[(ci * 9 + (8 - tap)) * cout + co] = v;
+}
+
+__global__ void adam_kernel(int n, float *w, float *m, float *v, const float *g, float lr,
+                            float b1, float b2, float eps, float c1, float c2) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float gi = g[i];
+    const float mi = b1 * m[i] + (1.f - b1) * gi, vi = b2 * v[i] + (1.f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    w[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+}
+
+// random crops of the device dataset into a batch (X bf16, target f32)
+__global__ void crop_kernel(int B, int ch, int cw, int H, int W, const int *sel, const float *Xd,
+                            const float *Td, bf16 *Xb, float *Tb) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= (int64_t)B * ch * cw * 16) return;
+    const int c = (int)(i % 16);
+    const int64_t p = i / 16;
+    const int w = (int)(p % cw), h = (int)((p / cw) % ch), b = (int)(p / ((int64_t)cw * ch));
+    const int k = sel[3 * b], oy = sel[3 * b + 1], ox = sel[3 * b + 2];
+    const int64_t s = ((((int64_t)k * H) + oy + h) * W + ox + w) * 16 + c;
+    Xb[i] = __float2bfloat16_rn(Xd[s]);
+    Tb[i] = Td[s];
+}
+
+// superpixel packing of a control-point field (nd x nd, nd = 3n + 1) scaled by 1/rms
+__global__ void pack_kernel(int n, const double *r, const double *rr_ptr, double inv_len, bf16 *X) {
+    const int S = n + 1, nd = 3 * n + 1;
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= (int64_t)S * S * 16) return;
+    const int c = (int)(i % 16);
+    const int64_t p = i / 16;
+    const int I = (int)(p % S), J = (int)(p / S);
+    float v = 0.f;
+    if (c < 9) {
+        const int gi = 3 * I + c % 3, gj = 3 * J + c / 3;
+        if (gi < nd && gj < nd) {
+            const double rr = *rr_ptr;
+            const double sc = rr > 0 ? 1.0 / sqrt(rr * inv_len) : 0.0;
+            v = (float)(r[gi + (int64_t)nd * gj] * sc);
+        }
+    }
+    X[i] = __float2bfloat16_rn(v);
+}
+
+__global__ void unpack_kernel(int n, const float *Y, const double *rr_ptr, double inv_len,
+                              double out_scale, double *z, const int *stop) {
+    if (stop && *stop) return;
+    const int S = n + 1, nd = 3 * n + 1;
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= (int64_t)nd * nd) return;
+    const int gi = (int)(t % nd), gj = (int)(t / nd);
+    const int I = gi / 3, J = gj / 3, c = (gi % 3) + 3 * (gj % 3);
+    const double rr = *rr_ptr;
+    const double sc = sqrt(rr * inv_len);
+    z[t] = (double)Y[((int64_t)J * S + I) * 16 + c] * sc * out_scale;
+}
+
+inline unsigned nb(int64_t n, int bs = 256) { return (unsigned)((n + bs - 1) / bs); }
+
+template <int CIN, int COUT, bool RELU, bool OUTF32>
+void conv(cudaStream_t s, int B, int H, int W, const bf16 *X, const bf16 *Wt, const float *bias,
+          void *Y) {
+    dim3 grid((W + TW - 1) / TW, (H + TH - 1) / TH, B);
+    conv3x3_kernel<CIN, COUT, RELU, OUTF32><<<grid, 256, 0, s>>>(H, W, X, Wt, bias, Y);
+    DRF_LAUNCHED();
+}
+
+void conv_layer(cudaStream_t s, int l, int B, int H, int W, const bf16 *X, const bf16 *Wt,
+                const float *bias, void *Y) {
+    switch (l) {
+    case 0: conv<16, 32, true, false>(s, B, H, W, X, Wt, bias, Y); break;
+    case 1: conv<32, 32, true, false>(s, B, H, W, X, Wt, bias, Y); break;
+    case 2: conv<32, 32, true, false>(s, B, H, W, X, Wt, bias, Y); break;
+    default: conv<32, 16, false, true>(s, B, H, W, X, Wt, bias, Y); break;
+    }
+}
+
+// input-gradient conv of layer l (l = 1..3): dX (CIN_l channels, f32) = conv(dZ_l, Wflip_l)
+void conv_back(cudaStream_t s, int l, int B, int H, int W, const bf16 *dZb, const bf16 *Wf, float *dX) {
+    switch (l) {
+    case 3: conv<16, 32, false, true>(s, B, H, W, dZb, Wf, nullptr, dX); break;
+    default: conv<32, 32, false, true>(s, B, H, W, dZb, Wf, nullptr, dX); break;
+    }
+}
+
+void dw_layer(cudaStream_t s, int l, int B, int H, int W, const float *dZ, const bf16 *A, float *part) {
+    dim3 grid((W + TW - 1) / TW, (H + TH - 1) / TH, B);
+    switch (l) {
+    case 0: dw_partial_kernel<16, 32><<<grid, 256, 0, s>>>(H, W, dZ, A, part); break;
+    case 3: dw_partial_kernel<32, 16><<<grid, 256, 0, s>>>(H, W, dZ, A, part); break;
+    default: dw_partial_kernel<32, 32><<<grid, 256, 0, s>>>(H, W, dZ, A, part); break;
+    }
+    DRF_LAUNCHED();
+}
+
+size_t layer_w(int l) { return (size_t)CH[l + 1] * 9 * CH[l]; }
+
+}  // namespace
+
+// ------------------------------------------------------------------------------ network object
+struct CnnNet {
+    cudaStream_t stream = nullptr, own = nullptr;
+    // FP32 masters (packed like the oracle: per layer W then b), Adam moments, gradients
+    DevBuf<float> wm, am, av, grad;
+    DevBuf<bf16> wb, wflip;
+    size_t off_w[4], off_b[4], off_wb[4], nparam = 0, nwb = 0;
+    int64_t adam_t = 0;
+    // activation buffers (sized on demand)
+    int64_t cap_pix = 0;
+    DevBuf<bf16> act[4], dzb;
+    DevBuf<float> out, dout, dx, dz;
+    DevBuf<float> part;
+    DevBuf<double> lpart;
+    // dataset
+    DevBuf<float> dsX, dsT;
+    DevBuf<int> sel;
+    DevBuf<bf16> bx;
+    DevBuf<float> bt;
+    int ds_n = 0, ds_h = 0, ds_w = 0;
+
+    CnnNet() {
+        size_t o = 0, ob = 0;
+        for (int l = 0; l < 4; ++l) {
+            off_w[l] = o; o += layer_w(l);
+            off_b[l] = o; o += CH[l + 1];
+            off_wb[l] = ob; ob += layer_w(l);
+        }
+        nparam = o;
+        nwb = ob;
+        for (auto *b : {&wm, &am, &av, &grad}) b->alloc(nparam);
+        wb.alloc(nwb);
+        wflip.alloc(nwb);
+        DRF_CUDA(cudaMemset(am.p, 0, nparam * 4));
+        DRF_CUDA(cudaMemset(av.p, 0, nparam * 4));
+        DRF_CUDA(cudaStreamCreateWithFlags(&own, cudaStreamNonBlocking));
+        stream = own;
+    }
+    ~CnnNet() {
+        if (own) cudaStreamDestroy(own);
+    }
+    void cast() {
+        for (int l = 0; l < 4; ++l) {
+            cast_weights_kernel<<<nb(layer_w(l)), 256, 0, stream>>>(CH[l], CH[l + 1], wm.p + off_w[l],
+                                                                    wb.p + off_wb[l], wflip.p + off_wb[l]);
+            DRF_LAUNCHED();
+        }
+    }
+    void ensure(int64_t pix) {
+        if (pix <= cap_pix) return;
+        for (int l = 0; l < 4; ++l) act[l].alloc(pix * CH[l]);
+        dzb.alloc(pix * 32);
+        out.alloc(pix * 16);
+        dout.alloc(pix * 16);
+        dx.alloc(pix * 32);
+        dz.alloc(pix * 32);
+        lpart.alloc(1024);
+        cap_pix = pix;
+    }
+    // forward from act[0]; output f32 in `out`
+    void forward(int B, int H, int W) {
+        for (int l = 0; l < 3; ++l)
+            conv_layer(stream, l, B, H, W, act[l].p, wb.p + off_wb[l], wm.p + off_b[l], act[l + 1].p);
+        conv_layer(stream, 3, B, H, W, act[3].p, wb.p + off_wb[3], wm.p + off_b[3], out.p);
+    }
+    // backward of the mean-square loss against tgt; fills grad; returns device loss partials
+    void backward(int B, int H, int W, const float *tgt) {
+        const int64_t pix = (int64_t)B * H * W;
+        loss_grad_kernel<<<1024, 256, 0, stream>>>(pix, out.p, tgt, dout.p, 1.f / (float)(pix * 9), lpart.p);
+        DRF_LAUNCHED();
+        const int tiles = ((W + TW - 1) / TW) * ((H + TH - 1) / TH) * B;
+        const float *dZ = dout.p;
+        for (int l = 3; l >= 0; --l) {
+            const size_t nw = layer_w(l) + CH[l + 1];
+            if (part.n < (size_t)tiles * nw) part.alloc((size_t)tiles * nw);
+            dw_layer(stream, l, B, H, W, dZ, act[l].p, part.p);
+            reduce_cols_kernel<<<nb(nw), 256, 0, stream>>>(tiles, (int)nw, part.p, grad.p + off_w[l]);
+            DRF_LAUNCHED();
+            if (l == 0) break;
+            // dZ_l in bf16 for the input-gradient conv
+            f32_to_bf16_kernel<<<nb(pix * CH[l + 1]), 256, 0, stream>>>(pix * CH[l + 1], dZ, dzb.p);
+            DRF_LAUNCHED();
+            conv_back(stream, l, B, H, W, dzb.p, wflip.p + off_wb[l], dx.p);
+            // dZ_{l-1} = dX * relu'(Z_{l-1}) into dz (the previous dZ is no longer read)
+            relu_back_kernel<<<nb(pix * CH[l]), 256, 0, stream>>>(pix * CH[l], dx.p, act[l].p, dz.p, dzb.p);
+            DRF_LAUNCHED();
+            dZ = dz.p;
+        }
+    }
+    double loss_host() {
+        std::vector<double> lp(1024);
+        DRF_CUDA(cudaMemcpyAsync(lp.data(), lpart.p, 1024 * 8, cudaMemcpyDeviceToHost, stream));
+        DRF_CUDA(cudaStreamSynchronize(stream));
+        double s = 0.0;
+        for (double v : lp) s += v;
+        return s;
+    }
+};
+
+// packs r (control points) and runs the network; z = rms(r) * out_scale * net(r / rms(r))
+void cnn_precondition(CnnNet *net, cudaStream_t s, int n, const double *r, const double *rr_dev,
+                      double out_scale, double *z, const int *stop) {
+    const int S = n + 1;
+    const int64_t pix = (int64_t)S * S, nd = 3 * n + 1;
+    cudaStream_t keep = net->stream;
+    net->stream = s;
+    net->ensure(pix);
+    pack_kernel<<<nb(pix * 16), 256, 0, s>>>(n, r, rr_dev, 1.0 / (double)(nd * nd), net->act[0].p);
+    DRF_LAUNCHED();
+    net->forward(1, S, S);
+    unpack_kernel<<<nb(nd * nd), 256, 0, s>>>(n, net->out.p, rr_dev, 1.0 / (double)(nd * nd), out_scale,
+                                              z, stop);
+    DRF_LAUNCHED();
+    net->stream = keep;
+}
+
+void cnn_prepare(CnnNet *net, int n) { net->ensure((int64_t)(n + 1) * (n + 1)); }
+
+}  // namespace drf
+
+using namespace drf;
+
+struct drf_cnn {
+    std::unique_ptr<CnnNet> net;
+};
+
+extern "C" {
+
+int64_t drf_cnn_nparams(void) {
+    int64_t n = 0;
+    for (int l = 0; l < 4; ++l) n += (int64_t)CH[l + 1] * 9 * CH[l] + CH[l + 1];
+    return n;
+}
+
+int drf_cnn_create(uint64_t seed, drf_cnn **out) {
+    return guard([&] {
+        DRF_CHECK(out, DRF_E_INVALID, "null argument");
+        auto h = std::make_unique<drf_cnn>();
+        h->net = std::make_unique<CnnNet>();
+        // He-normal initialisation of the used input channels, zero biases
+        std::mt19937_64 rng(seed);
+        std::vector<float> w(h->net->nparam, 0.f);
+        for (int l = 0; l < 4; ++l) {
+            const int cin_used = l == 0 ? 9 : CH[l], cout_used = l == 3 ? 9 : CH[l + 1];
+            std::normal_distribution<float> nd(0.f, std::sqrt(2.f / (9.f * cin_used)));
+            for (int co = 0; co < cout_used; ++co)
+                for (int tap = 0; tap < 9; ++tap)
+                    for (int ci = 0; ci < cin_used; ++ci)
+                        w[h->net->off_w[l] + ((size_t)co * 9 + tap) * CH[l] + ci] = nd(rng) * (l == 3 ? 0.1f : 1.f);
+        }
+        DRF_CUDA(cudaMemcpy(h->net->wm.p, w.data(), w.size() * 4, cudaMemcpyHostToDevice));
+        h->net->cast();
+        DRF_CUDA(cudaStreamSynchronize(h->net->stream));
+        *out = h.release();
+    });
+}
+
+int drf_cnn_destroy(drf_cnn *h) {
+    return guard([&] {
+        if (!h) return;
+        cudaStreamSynchronize(h->net->stream);
+        delete h;
+    });
+}
+
+int drf_cnn_get_params(drf_cnn *h, double *p) {
+    return guard([&] {
+        DRF_CHECK(h && p, DRF_E_INVALID, "null argument");
+        std::vector<float> w(h->net->nparam);
+        DRF_CUDA(cudaMemcpyAsync(w.data(), h->net->wm.p, w.size() * 4, cudaMemcpyDeviceToHost, h->net->stream));
+        DRF_CUDA(cudaStreamSynchronize(h->net->stream));
+        for (size_t i = 0; i < w.size(); ++i) p[i] = w[i];
+    });
+}
+
+int drf_cnn_set_params(drf_cnn *h, const double *p) {
+    return guard([&] {
+        DRF_CHECK(h && p, DRF_E_INVALID, "null argument");
+        DRF_CHECK(all_finite(p, h->net->nparam), DRF_E_NONFINITE, "non-finite parameter");
+        std::vector<float> w(h->net->nparam);
+        for (size_t i = 0; i < w.size(); ++i) w[i] = (float)p[i];
+        DRF_CUDA(cudaMemcpyAsync(h->net->wm.p, w.data(), w.size() * 4, cudaMemcpyHostToDevice, h->net->stream));
+        h->net->cast();
+        DRF_CUDA(cudaStreamSynchronize(h->net->stream));
+    });
+}
+
+// forward (and optional loss/gradient) of B images H x W x 16 given on the host (FP64)
+int drf_cnn_forward_backward(drf_cnn *h, int B, int H, int W, const double *X, const double *T,
+                             double *Y, double *grad, double *loss) {
+    return guard([&] {
+        DRF_CHECK(h && X && B > 0 && H > 0 && W > 0, DRF_E_INVALID, "bad arguments");
+        CnnNet &n = *h->net;
+        const int64_t pix = (int64_t)B * H * W;
+        n.ensure(pix);
+        std::vector<bf16> xb(pix * 16);
+        for (int64_t i = 0; i < pix * 16; ++i) xb[i] = __float2bfloat16_rn((float)X[i]);
+        DRF_CUDA(cudaMemcpyAsync(n.act[0].p, xb.data(), pix * 16 * 2, cudaMemcpyHostToDevice, n.stream));
+        n.forward(B, H, W);
+        if (Y) {
+            std::vector<float> y(pix * 16);
+            DRF_CUDA(cudaMemcpyAsync(y.data(), n.out.p, pix * 16 * 4, cudaMemcpyDeviceToHost, n.stream));
+            DRF_CUDA(cudaStreamSynchronize(n.stream));
+            for (int64_t i = 0; i < pix * 16; ++i) Y[i] = y[i];
+        }
+        if (T) {
+            std::vector<float> t(pix * 16);
+            for (int64_t i = 0; i < pix * 16; ++i) t[i] = (float)T[i];
+            DevBuf<float> td(pix * 16);
+            DRF_CUDA(cudaMemcpyAsync(td.p, t.data(), pix * 16 * 4, cudaMemcpyHostToDevice, n.stream));
+            n.backward(B, H, W, td.p);
+            const double l = n.loss_host() / (double)(pix * 9);
+            if (loss) *loss = l;
+            if (grad) {
+                std::vector<float> g(n.nparam);
+                DRF_CUDA(cudaMemcpyAsync(g.data(), n.grad.p, g.size() * 4, cudaMemcpyDeviceToHost, n.stream));
+                DRF_CUDA(cudaStreamSynchronize(n.stream));
+                for (size_t i = 0; i < g.size(); ++i) grad[i] = g[i];
+            }
+        }
+        DRF_CUDA(cudaStreamSynchronize(n.stream));
+    });
+}
+
+// training set of N samples H x W x 16 (inputs X, targets T), kept on the device in FP32
+int drf_cnn_set_dataset(drf_cnn *h, int N, int H, int W, const double *X, const double *T) {
+    return guard([&] {
+        DRF_CHECK(h && X && T && N > 0 && H > 0 && W > 0, DRF_E_INVALID, "bad arguments");
+        CnnNet &n = *h->net;
+        const size_t cnt = (size_t)N * H * W * 16;
+        std::vector<float> a(cnt), b(cnt);
+        for (size_t i = 0; i < cnt; ++i) { a[i] = (float)X[i]; b[i] = (float)T[i]; }
+        n.dsX.alloc(cnt);
+        n.dsT.alloc(cnt);
+        DRF_CUDA(cudaMemcpy(n.dsX.p, a.data(), cnt * 4, cudaMemcpyHostToDevice));
+        DRF_CUDA(cudaMemcpy(n.dsT.p, b.data(), cnt * 4, cudaMemcpyHostToDevice));
+        n.ds_n = N; n.ds_h = H; n.ds_w = W;
+    });
+}
+
+// Adam on random crops (batch x crop x crop) of the device dataset; returns the mean loss of
+// the last `report` steps.
+int drf_cnn_train(drf_cnn *h, int steps, int batch, int crop, double lr, uint64_t seed,
+                  double *loss) {
+    return guard([&] {
+        DRF_CHECK(h && steps >= 0 && batch > 0 && crop > 0, DRF_E_INVALID, "bad arguments");
+        CnnNet &n = *h->net;
+        DRF_CHECK(n.ds_n > 0, DRF_E_INVALID, "no dataset (drf_cnn_set_dataset)");
+        DRF_CHECK(crop <= n.ds_h && crop <= n.ds_w, DRF_E_INVALID, "crop larger than the samples");
+        const int64_t pix = (int64_t)batch * crop * crop;
+        n.ensure(pix);
+        n.sel.alloc(3 * batch);
+        n.bx.alloc(pix * 16);
+        n.bt.alloc(pix * 16);
+        std::mt19937_64 rng(seed);
+        std::vector<int> sel(3 * batch);
+        double acc = 0.0;
+        int nacc = 0;
+        const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+        for (int s = 0; s < steps; ++s) {
+            for (int b = 0; b < batch; ++b) {
+                sel[3 * b] = (int)(rng() % n.ds_n);
+                sel[3 * b + 1] = (int)(rng() % (n.ds_h - crop + 1));
+                sel[3 * b + 2] = (int)(rng() % (n.ds_w - crop + 1));
+            }
+            DRF_CUDA(cudaMemcpyAsync(n.sel.p, sel.data(), sel.size() * 4, cudaMemcpyHostToDevice, n.stream));
+            crop_kernel<<<nb(pix * 16), 256, 0, n.stream>>>(batch, crop, crop, n.ds_h, n.ds_w, n.sel.p,
+                                                          n.dsX.p, n.dsT.p, n.bx.p, n.bt.p);
+            DRF_LAUNCHED();
+            DRF_CUDA(cudaMemcpyAsync(n.act[0].p, n.bx.p, pix * 16 * 2, cudaMemcpyDeviceToDevice, n.stream));
+            n.forward(batch, crop, crop);
+            n.backward(batch, crop, crop, n.bt.p);
+            ++n.adam_t;
+            const float c1 = 1.f - std::pow(b1, (float)n.adam_t), c2 = 1.f - std::pow(b2, (float)n.adam_t);
+            adam_kernel<<<nb(n.nparam), 256, 0, n.stream>>>((int)n.nparam, n.wm.p, n.am.p, n.av.p,
+                                                           n.grad.p, (float)lr, b1, b2, eps, c1, c2);
+            DRF_LAUNCHED();
+            n.cast();
+            if (s >= steps - 10) {
+                acc += n.loss_host() / (double)(pix * 9);
+                ++nacc;
+            }
+        }
+        DRF_CUDA(cudaStreamSynchronize(n.stream));
+        if (loss) *loss = nacc ? acc / nacc : 0.0;
+    });
+}
+
+}  // extern "C"
+
+namespace drf {
+CnnNet *cnn_net(drf_cnn *h) { return h ? h->net.get() : nullptr; }
+}  // namespace drf

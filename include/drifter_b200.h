@@ -183,6 +183,29 @@ int drf_mg_apply(drf_bz *h, const double *r, double *z);
 int drf_pcg_solve(drf_bz *h, const double *b, double *x, double tol, int maxit, int kind,
                   int *iters, double *relres, double *ms);
 
+/* ------------------------------------------------------------------ learned preconditioner
+ * No counterpart in the reference. A 4-layer conv3x3 network (BF16, FP32 accumulation) on
+ * 3x3 superpixels of the control-point grid, trained on the GPU on (residual, error) pairs
+ * from the smoother's own multigrid solves, used as PCG preconditioner kind 3 (flexible CG).
+ * Images are NHWC with 16 channels (9 used: control point (3I+di, 3J+dj) -> channel di+3dj). */
+typedef struct drf_cnn drf_cnn;
+int64_t drf_cnn_nparams(void);
+int drf_cnn_create(uint64_t seed, drf_cnn **out);
+int drf_cnn_destroy(drf_cnn *h);
+/* parameters packed per layer: W [co][tap][ci] (channels 16,32,32,32,16) then bias [co] */
+int drf_cnn_get_params(drf_cnn *h, double *p);
+int drf_cnn_set_params(drf_cnn *h, const double *p);
+/* forward of B images (host FP64 in/out); with T != NULL also the mean-square loss over the 9
+ * used channels and its parameter gradient */
+int drf_cnn_forward_backward(drf_cnn *h, int B, int H, int W, const double *X, const double *T,
+                             double *Y, double *grad, double *loss);
+int drf_cnn_set_dataset(drf_cnn *h, int N, int H, int W, const double *X, const double *T);
+int drf_cnn_train(drf_cnn *h, int steps, int batch, int crop, double lr, uint64_t seed,
+                  double *loss);
+/* attaches a trained network to a smoother as preconditioner kind 3 (output scale s: z =
+ * rms(r) s net(r / rms(r))) */
+int drf_bz_set_cnn(drf_bz *h, drf_cnn *net, double out_scale);
+
 /* Allocation-free variant of drf_pcg_solve with the Jacobi preconditioner (kind 1), for callers
  * that cannot allocate device memory. No counterpart in the reference (it has no device code).
  * The caller owns d_b (device, (3 nx + 1)^2 doubles) and d_x (device, initial guess in,

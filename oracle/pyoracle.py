@@ -292,3 +292,25 @@ class BezierOracle:
         _chk(lib().orc_bz_pcg(C.c_void_p(self.h), {"none": 0, "jacobi": 1, "mg": 2}[precond],
                               _p(b), _p(x), C.c_double(tol), maxit, C.byref(it), C.byref(rr)))
         return x, it.value, rr.value
+
+
+# ----------------------------------------------------------------------------- learned preconditioner
+def cnn_nparams():
+    L = lib()
+    L.orc_cnn_nparams.restype = C.c_long
+    return int(L.orc_cnn_nparams())
+
+
+def cnn_forward_backward(params, X, T=None, round_bf16=True):
+    """CPU reference of the preconditioner network for one image X (H x W x 16)."""
+    L = lib()
+    L.orc_cnn_forward_backward.restype = C.c_double
+    L.orc_cnn_forward_backward.argtypes = [_dp, _dp, C.c_int, C.c_int, _dp, _dp, _dp, C.c_int]
+    X = _c(X)
+    H, W, _ = X.shape
+    out = np.empty_like(X)
+    grad = np.empty(cnn_nparams()) if T is not None else None
+    loss = L.orc_cnn_forward_backward(_p(_c(params)), _p(X), H, W,
+                                      _p(_c(T)) if T is not None else None, _p(out),
+                                      _p(grad) if grad is not None else None, int(round_bf16))
+    return out, grad, loss
