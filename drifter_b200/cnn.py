@@ -43,7 +43,7 @@ def to_superpixels(field: np.ndarray, n: int) -> np.ndarray:
     S = n + 1
     g = np.zeros((3 * S, 3 * S))
     g[:nd, :nd] = field.reshape(nd, nd)  # [gj][gi]
-    sp = g.reshape(S, 3, S, 3).transpose(0, 2, 3, 1).reshape(S, S, 9)  # [J][I][dj*3+di]
+    sp = g.reshape(S, 3, S, 3).transpose(0, 2, 1, 3).reshape(S, S, 9)  # [J][I][di + 3 dj]
     out = np.zeros((S, S, 16))
     out[:, :, :9] = sp
     return out
@@ -52,7 +52,7 @@ def to_superpixels(field: np.ndarray, n: int) -> np.ndarray:
 def from_superpixels(sp: np.ndarray, n: int) -> np.ndarray:
     nd = 3 * n + 1
     S = n + 1
-    g = sp[:, :, :9].reshape(S, S, 3, 3).transpose(0, 3, 1, 2).reshape(3 * S, 3 * S)
+    g = sp[:, :, :9].reshape(S, S, 3, 3).transpose(0, 2, 1, 3).reshape(3 * S, 3 * S)
     return g[:nd, :nd].reshape(-1).copy()
 
 

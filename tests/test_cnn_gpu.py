@@ -46,10 +46,16 @@ def test_gradient_matches_reference():
     assert rl2(g, go) < 2e-2
 
 
-def test_superpixel_roundtrip():
+def test_superpixel_layout():
+    # control point (gi, gj) -> superpixel (I, J) = (gi // 3, gj // 3), channel gi % 3 + 3 (gj % 3)
+    # (the layout of the library's pack/unpack kernels)
     n = 7
-    f = np.random.default_rng(2).standard_normal((3 * n + 1) ** 2)
-    assert np.array_equal(from_superpixels(to_superpixels(f, n), n), f)
+    nd = 3 * n + 1
+    f = np.random.default_rng(2).standard_normal(nd * nd)
+    sp = to_superpixels(f, n)
+    for gi, gj in ((0, 0), (4, 2), (2, 7), (21, 21), (13, 5)):
+        assert sp[gj // 3, gi // 3, gi % 3 + 3 * (gj % 3)] == f[gi + nd * gj]
+    assert np.array_equal(from_superpixels(sp, n), f)
 
 
 def test_trained_preconditioner_gains_over_plain_cg():
