@@ -161,17 +161,31 @@ def build_dataset(pairs, n):
     return np.stack(X), np.stack(T), scale
 
 
+def bathymetry_rhs(n: int, L: float, lam: float, eps: float, count: int, seed: int):
+    """Right-hand sides lambda B^T W d of smoothing problems on seeded fBm bathymetries."""
+    from . import configs
+    out = []
+    for k in range(count):
+        d = configs.c4(n=n, L=L, seed=seed * 1000 + k, lam=lam, eps=eps)["d"]
+        s = BezierSmoother(n, n, L, L, d, lam=lam, ridge_epsilon=eps)
+        out.append(s.rhs())
+        s.close()
+    return out
+
+
 def train_preconditioner(n=64, dx=100.0, lam=1.0, eps=1e-4, d=None, rhs_count=16, steps=1500,
                          seed=1, lr=2e-3, crop=48, batch=16):
     """Trains a network on a training grid of n x n elements with element size dx (the same
-    element operator as the target grid) and returns it with its output scale set."""
+    element operator as the target grid) and returns it with its output scale set. Training
+    pairs come from the multigrid iterations of smoothing problems (bathymetry right-hand
+    sides) and of random fields."""
     L = n * dx
     if d is None:
         from . import configs
         d = configs.c4(n=n, L=L, seed=seed + 101)["d"]
     s = BezierSmoother(n, n, L, L, d, lam=lam, ridge_epsilon=eps)
     s.mg_setup(2)
-    rhs = random_rhs(s, n, L, rhs_count, seed)
+    rhs = bathymetry_rhs(n, L, lam, eps, rhs_count, seed) + random_rhs(s, n, L, rhs_count // 2, seed)
     X, T, scale = build_dataset(multigrid_pairs(s, n, rhs), n)
     net = CNN(seed)
     net.set_dataset(X, T)
