@@ -30,6 +30,7 @@ def _setup_sigs():
         "drf_bz_info": [vp, C.POINTER(C.c_int64), dp, C.POINTER(C.c_int)],
         "drf_bz_get_rhs": [vp, dp], "drf_bz_apply_Q": [vp, dp, dp],
         "drf_mg_setup": [vp, C.c_int, C.c_int, C.c_int], "drf_mg_apply": [vp, dp, dp],
+        "drf_bz_precondition": [vp, C.c_int, dp, dp],
         "drf_pcg_solve": [vp, dp, dp, C.c_double, C.c_int, C.c_int, C.POINTER(C.c_int), dp, dp],
     }
     for k, a in sigs.items():
@@ -84,6 +85,12 @@ class BezierSmoother:
         r = np.ascontiguousarray(r, dtype=np.float64)
         z = np.empty(self.ndof)
         check(lib().drf_mg_apply(self.h, dptr(r), dptr(z)))
+        return z
+
+    def precondition(self, r, kind="jacobi"):
+        r = np.ascontiguousarray(r, dtype=np.float64)
+        z = np.empty(self.ndof)
+        check(lib().drf_bz_precondition(self.h, PRECOND[kind], dptr(r), dptr(z)))
         return z
 
     def solve(self, precond="mg", tol=1e-10, maxit=1000, b=None, x0=None):

@@ -746,6 +746,24 @@ int drf_bz_set_cnn(drf_bz *h, drf_cnn *net, double out_scale) {
     });
 }
 
+int drf_bz_precondition(drf_bz *h, int kind, const double *rh, double *zh) {
+    return guard([&] {
+        check_bz(h);
+        DRF_CHECK(rh && zh, DRF_E_INVALID, "null argument");
+        DRF_CHECK(kind >= 0 && kind <= 3, DRF_E_INVALID, "unknown preconditioner kind");
+        DRF_CHECK(kind != 2 || h->mg_ready, DRF_E_INVALID, "multigrid preconditioner not set up");
+        DRF_CHECK(kind != 3 || h->cnn, DRF_E_INVALID, "no learned preconditioner attached");
+        DRF_CUDA(cudaMemcpyAsync(h->r.p, rh, h->ndof * 8, cudaMemcpyHostToDevice, h->stream));
+        dot_kernel<<<h->nparts(), BS, 0, h->stream>>>(h->ndof, h->r.p, h->r.p, h->part.p, nullptr);
+        DRF_LAUNCHED();
+        reduce_kernel<<<1, BS, 0, h->stream>>>(h->part.p, (int)h->nparts(), h->scal.p + S_RR);
+        DRF_LAUNCHED();
+        h->precondition(kind, h->r.p, h->z.p, nullptr);
+        DRF_CUDA(cudaMemcpyAsync(zh, h->z.p, h->ndof * 8, cudaMemcpyDeviceToHost, h->stream));
+        DRF_CUDA(cudaStreamSynchronize(h->stream));
+    });
+}
+
 int drf_mg_apply(drf_bz *h, const double *rh, double *zh) {
     return guard([&] {
         check_bz(h);

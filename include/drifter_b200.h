@@ -175,6 +175,8 @@ int drf_mg_setup(drf_bz *h, int coarsest_n, int pre, int post);
 /* One V-cycle z = M r (BezierMultigridPreconditioner::apply, :246; the reference repeats
  * V-cycles to a tolerance, this entry applies one symmetric cycle). */
 int drf_mg_apply(drf_bz *h, const double *r, double *z);
+/* z = M r for preconditioner kind (0 none, 1 Jacobi, 2 multigrid, 3 learned). */
+int drf_bz_precondition(drf_bz *h, int kind, const double *r, double *z);
 /* PCG on Q x = b to ||r|| <= tol ||b|| (FP64). b NULL = the assembled right-hand side; x holds
  * the initial guess and returns the solution. kind: 0 none, 1 Jacobi, 2 multigrid V-cycle,
  * 3 learned CNN, 4 CNN-corrected multigrid. Maps the PCG loop of
