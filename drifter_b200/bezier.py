@@ -2,7 +2,7 @@
 
   * BezierSmoother  ~ CGBezierSmootherBase assembly + solve (src/bathymetry/cg_bezier_smoother_base.cpp)
   * BezierMultigridPreconditioner.setup/apply (include/bathymetry/bezier_multigrid_preconditioner.hpp:240,246)
-  * solve(...) = PCG on Q x = b (FP64) with preconditioner "none" | "jacobi" | "mg" | "cnn" | "mg+cnn"
+  * solve(...) = PCG on Q x = b (FP64) with preconditioner "none" | "jacobi" | "mg" | "cnn"
 """
 from __future__ import annotations
 
@@ -12,7 +12,7 @@ import numpy as np
 
 from ._abi import check, dptr, lib
 
-PRECOND = {"none": 0, "jacobi": 1, "mg": 2, "cnn": 3, "mg+cnn": 4}
+PRECOND = {"none": 0, "jacobi": 1, "mg": 2, "cnn": 3}
 
 
 class BzGridDesc(C.Structure):

@@ -147,18 +147,30 @@ def random_rhs(s: BezierSmoother, n: int, L: float, count: int, seed: int):
     return out
 
 
-def build_dataset(pairs, n):
-    X, T, ratios = [], [], []
-    for r, e in pairs:
-        sr = np.sqrt(np.mean(r * r))
-        se = np.sqrt(np.mean(e * e))
-        ratios.append(se / sr)
-    scale = float(np.median(ratios))
-    for r, e in pairs:
+def build_dataset(pairs, n, s: BezierSmoother, scale=None):
+    """Inputs r / rms(r); targets the error the Jacobi base leaves, (e - D^-1 r) / (rms(r) s)."""
+    res = [(r, e - s.precondition(r, "jacobi")) for r, e in pairs]
+    if scale is None:
+        scale = float(np.median([np.sqrt(np.mean(c * c) / np.mean(r * r)) for r, c in res]))
+    X, T = [], []
+    for r, c in res:
         sr = np.sqrt(np.mean(r * r))
         X.append(to_superpixels(r / sr, n))
-        T.append(to_superpixels(e / (sr * scale), n))
+        T.append(to_superpixels(c / (sr * scale), n))
     return np.stack(X), np.stack(T), scale
+
+
+def fcg_pairs(s: BezierSmoother, net: "CNN", rhs_list, iters: int = 8):
+    """(residual, error) pairs along flexible CG with the current network (its own residual
+    distribution), exact solutions from multigrid PCG."""
+    net.attach(s)
+    pairs = []
+    for b in rhs_list:
+        xs, _ = s.solve("mg", tol=1e-12, maxit=200, b=b)
+        for k in range(1, iters + 1):
+            x, _ = s.solve("cnn", tol=1e-30, maxit=k, b=b)
+            pairs.append((b - s.apply_Q(x), xs - x))
+    return pairs
 
 
 def bathymetry_rhs(n: int, L: float, lam: float, eps: float, count: int, seed: int):
@@ -186,10 +198,14 @@ def train_preconditioner(n=64, dx=100.0, lam=1.0, eps=1e-4, d=None, rhs_count=16
     s = BezierSmoother(n, n, L, L, d, lam=lam, ridge_epsilon=eps)
     s.mg_setup(2)
     rhs = bathymetry_rhs(n, L, lam, eps, rhs_count, seed) + random_rhs(s, n, L, rhs_count // 2, seed)
-    X, T, scale = build_dataset(multigrid_pairs(s, n, rhs), n)
+    X, T, scale = build_dataset(multigrid_pairs(s, n, rhs), n, s)
     net = CNN(seed)
     net.set_dataset(X, T)
     loss = net.train(steps, batch=batch, crop=min(crop, n + 1), lr=lr, seed=seed)
     net.out_scale = scale
+    # second round: add the residuals the network meets inside flexible CG
+    X2, T2, _ = build_dataset(fcg_pairs(s, net, rhs[: max(2, rhs_count // 2)]), n, s, scale)
+    net.set_dataset(np.concatenate([X, X2]), np.concatenate([T, T2]))
+    loss = net.train(steps // 2, batch=batch, crop=min(crop, n + 1), lr=lr * 0.5, seed=seed + 1)
     s.close()
-    return net, dict(loss=loss, scale=scale, pairs=len(X))
+    return net, dict(loss=loss, scale=scale, pairs=len(X) + len(X2))

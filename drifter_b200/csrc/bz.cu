@@ -501,8 +501,12 @@ struct drf_bz {
             jacobi_kernel<<<nblk(n), BS, 0, stream>>>(levdev(L), rin, zout, stop);
             DRF_LAUNCHED();
         } else if (kind == 3) {
-            cnn_precondition(cnn_net(cnn), stream, lv[finest()].n, rin, scal.p + S_RR, cnn_scale,
-                             zout, stop);
+            // Jacobi base (positive definite: a descent direction for any residual) plus the
+            // learned correction of the error it leaves
+            jacobi_kernel<<<nblk(n), BS, 0, stream>>>(levdev(L), rin, zout, stop);
+            DRF_LAUNCHED();
+            cnn_precondition(cnn_net(cnn), stream, lv[L].n, rin, scal.p + S_RR, cnn_scale, zout, 1,
+                             stop);
         } else {
             vcycle(rin, zout);
         }

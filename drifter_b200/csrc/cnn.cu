@@ -257,8 +257,9 @@ __global__ void pack_kernel(int n, const double *r, const double *rr_ptr, double
     X[i] = __float2bfloat16_rn(v);
 }
 
+// z (+)= rms(r) out_scale Y on the control points (add = 1 adds to a base already in z)
 __global__ void unpack_kernel(int n, const float *Y, const double *rr_ptr, double inv_len,
-                              double out_scale, double *z, const int *stop) {
+                              double out_scale, double *z, int add, const int *stop) {
     if (stop && *stop) return;
     const int S = n + 1, nd = 3 * n + 1;
     const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -267,7 +268,8 @@ __global__ void unpack_kernel(int n, const float *Y, const double *rr_ptr, doubl
     const int I = gi / 3, J = gj / 3, c = (gi % 3) + 3 * (gj % 3);
     const double rr = *rr_ptr;
     const double sc = sqrt(rr * inv_len);
-    z[t] = (double)Y[((int64_t)J * S + I) * 16 + c] * sc * out_scale;
+    const double v = (double)Y[((int64_t)J * S + I) * 16 + c] * sc * out_scale;
+    z[t] = add ? z[t] + v : v;
 }
 
 inline unsigned nb(int64_t n, int bs = 256) { return (unsigned)((n + bs - 1) / bs); }
@@ -411,9 +413,9 @@ struct CnnNet {
     }
 };
 
-// packs r (control points) and runs the network; z = rms(r) * out_scale * net(r / rms(r))
+// packs r (control points) and runs the network; z (+)= rms(r) * out_scale * net(r / rms(r))
 void cnn_precondition(CnnNet *net, cudaStream_t s, int n, const double *r, const double *rr_dev,
-                      double out_scale, double *z, const int *stop) {
+                      double out_scale, double *z, int add, const int *stop) {
     const int S = n + 1;
     const int64_t pix = (int64_t)S * S, nd = 3 * n + 1;
     cudaStream_t keep = net->stream;
@@ -423,7 +425,7 @@ void cnn_precondition(CnnNet *net, cudaStream_t s, int n, const double *r, const
     DRF_LAUNCHED();
     net->forward(1, S, S);
     unpack_kernel<<<nb(nd * nd), 256, 0, s>>>(n, net->out.p, rr_dev, 1.0 / (double)(nd * nd), out_scale,
-                                              z, stop);
+                                              z, add, stop);
     DRF_LAUNCHED();
     net->stream = keep;
 }

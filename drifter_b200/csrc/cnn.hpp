@@ -8,8 +8,9 @@ namespace drf {
 struct CnnNet;
 CnnNet *cnn_net(drf_cnn *h);
 void cnn_prepare(CnnNet *net, int n);
-// z = rms(r) * out_scale * net(r / rms(r)) on the control-point grid of n x n elements;
-// rr_dev points to r.r on the device; kernels return early when *stop is set.
+// z (+)= rms(r) * out_scale * net(r / rms(r)) on the control-point grid of n x n elements
+// (add = 1 adds to the base already in z); rr_dev points to r.r on the device; kernels return
+// early when *stop is set.
 void cnn_precondition(CnnNet *net, cudaStream_t s, int n, const double *r, const double *rr_dev,
-                      double out_scale, double *z, const int *stop);
+                      double out_scale, double *z, int add, const int *stop);
 }  // namespace drf

@@ -179,7 +179,7 @@ int drf_mg_apply(drf_bz *h, const double *r, double *z);
 int drf_bz_precondition(drf_bz *h, int kind, const double *r, double *z);
 /* PCG on Q x = b to ||r|| <= tol ||b|| (FP64). b NULL = the assembled right-hand side; x holds
  * the initial guess and returns the solution. kind: 0 none, 1 Jacobi, 2 multigrid V-cycle,
- * 3 learned CNN, 4 CNN-corrected multigrid. Maps the PCG loop of
+ * 3 learned (Jacobi plus the network's correction, flexible CG). Maps the PCG loop of
  * solve_with_constraints_iterative (src/bathymetry/cg_cubic_bezier_bathymetry_smoother.cpp:479-558)
  * with Q in place of the Schur operator. *ms = device time of the solve. */
 int drf_pcg_solve(drf_bz *h, const double *b, double *x, double tol, int maxit, int kind,
@@ -188,7 +188,8 @@ int drf_pcg_solve(drf_bz *h, const double *b, double *x, double tol, int maxit, 
 /* ------------------------------------------------------------------ learned preconditioner
  * No counterpart in the reference. A 4-layer conv3x3 network (BF16, FP32 accumulation) on
  * 3x3 superpixels of the control-point grid, trained on the GPU on (residual, error) pairs
- * from the smoother's own multigrid solves, used as PCG preconditioner kind 3 (flexible CG).
+ * from the smoother's own multigrid solves; PCG preconditioner kind 3 is z = D^-1 r + the
+ * network's correction (flexible CG).
  * Images are NHWC with 16 channels (9 used: control point (3I+di, 3J+dj) -> channel di+3dj). */
 typedef struct drf_cnn drf_cnn;
 int64_t drf_cnn_nparams(void);
@@ -204,8 +205,8 @@ int drf_cnn_forward_backward(drf_cnn *h, int B, int H, int W, const double *X, c
 int drf_cnn_set_dataset(drf_cnn *h, int N, int H, int W, const double *X, const double *T);
 int drf_cnn_train(drf_cnn *h, int steps, int batch, int crop, double lr, uint64_t seed,
                   double *loss);
-/* attaches a trained network to a smoother as preconditioner kind 3 (output scale s: z =
- * rms(r) s net(r / rms(r))) */
+/* attaches a trained network to a smoother as preconditioner kind 3 (output scale s:
+ * z = D^-1 r + rms(r) s net(r / rms(r))) */
 int drf_bz_set_cnn(drf_bz *h, drf_cnn *net, double out_scale);
 
 /* Allocation-free variant of drf_pcg_solve with the Jacobi preconditioner (kind 1), for callers

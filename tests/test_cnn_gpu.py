@@ -70,6 +70,7 @@ def test_trained_preconditioner_gains_over_plain_cg():
     s.mg_setup(2)
     net.attach(s)
     x_cnn, i_cnn = s.solve("cnn", tol=1e-10, maxit=2000)
+    assert np.isfinite(x_cnn).all()
     x_cg, i_cg = s.solve("none", tol=1e-10, maxit=5000)
     x_j, i_j = s.solve("jacobi", tol=1e-10, maxit=5000)
     x_mg, i_mg = s.solve("mg", tol=1e-10, maxit=200)
