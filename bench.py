@@ -40,6 +40,7 @@ def parse():
     ap.add_argument("--mid", action="store_true", help="C2 physics on a 64x64x16 mesh (profiling)")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 GPU comparison run")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--no-cg", action="store_true", help="skip the C4 Bezier CG comparison")
     return ap.parse_args()
 
 
@@ -185,6 +186,41 @@ def cpu_baseline(seconds=12.0, threads=1):
                       f"{el:.1f} s", threads=threads)
 
 
+def run_cg(stream, reps=3):
+    """C4 Bezier smoother: PCG time-to-1e-10 per preconditioner (device time of whole solves,
+    CUDA events inside the library), the learned network trained on a 64x64 grid first."""
+    from drifter_b200 import configs
+    from drifter_b200.bezier import BezierSmoother
+    from drifter_b200.cnn import train_preconditioner
+    c = configs.c4()
+    t0 = time.perf_counter()
+    net, info = train_preconditioner(n=64, dx=c["L"] / c["n"], lam=c["lam"], eps=c["eps"],
+                                     steps=1500, rhs_count=16, seed=1)
+    train_s = time.perf_counter() - t0
+    s = BezierSmoother(c["n"], c["n"], c["L"], c["L"], c["d"], lam=c["lam"], ridge_epsilon=c["eps"])
+    s.set_stream(stream.cuda_stream)
+    s.mg_setup(2)
+    net.attach(s)
+    out = {"workload": c["name"] + " cubic Bezier, lambda=1, eps=1e-4, FP64 PCG to 1e-10",
+           "dofs": s.ndof, "train_s": round(train_s, 2), "train_loss": info["loss"]}
+    sols = {}
+    for pc in ("mg", "cnn", "jacobi", "none"):
+        s.solve(pc, tol=1e-10, maxit=5000)  # warm-up (graph capture)
+        best = None
+        for _ in range(reps):
+            x, inf = s.solve(pc, tol=1e-10, maxit=5000)
+            if best is None or inf["ms"] < best["ms"]:
+                best = inf
+        sols[pc] = x
+        out[pc] = {"iters": best["iters"], "ms": round(best["ms"], 3), "relres": best["relres"]}
+    out["cnn_vs_mg_speedup"] = round(out["mg"]["ms"] / out["cnn"]["ms"], 3)
+    out["cnn_vs_mg_solution_rel_diff"] = float(np.abs(sols["cnn"] - sols["mg"]).max() /
+                                               np.abs(sols["mg"]).max())
+    s.close()
+    net.close()
+    return out
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -306,6 +342,12 @@ def run_ours(args, rank, world, local):
         fp64 = {"value": world * ndof * 5 / (ms64 / 1e3), "ms_per_step": ms64,
                 "eta_rel_err_mixed_vs_fp64": err, "steps_compared": nsteps_done}
 
+    # Bezier smoother CG on C4 (512x512, 2.36 M control points): time to the FP64 1e-10 residual
+    # with the multigrid and the learned preconditioner (plus Jacobi and none for reference)
+    cg = None
+    if not args.no_cg:
+        cg = run_cg(stream)
+
     cpu = None
     if rank == 0 and not args.no_cpu:
         v, meta = cpu_baseline(seconds=12.0, threads=1)
@@ -329,6 +371,7 @@ def run_ours(args, rank, world, local):
             "cpu_baseline": cpu,
             "e2e": e2e,
             "fp64_gpu": fp64,
+            "cg": cg,
             "gpu_launches": int(launches),
             "clocks": ck,
         }
