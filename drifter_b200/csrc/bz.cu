@@ -23,13 +23,25 @@ namespace drf {
 namespace {
 
 constexpr int BS = 256;
+// color steps with at least this many elements use one thread per element, smaller ones one
+// thread per dof
+constexpr int64_t ELEM_THREAD_MIN_ELEMS = 65536;
 inline unsigned nblk(int64_t n) { return (unsigned)((n + BS - 1) / BS); }
+
+// asynchronous 8-byte global -> shared copy (zero fill when !valid; src must still be a
+// valid address then, it is not read); every copy of a thread completes at cp_async_wait_all
+__device__ __forceinline__ void cp_async8(double *smem_dst, const double *gsrc, bool valid) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(gsrc), "r"(valid ? 8 : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 struct LevelDev {
     int n, nd;
-    const double *K;     // 256, row-major
+    const double *K;     // 256, transposed: K[k * 16 + a] = K_ak (lanes of one row read one bank each)
     const double *rho;   // nd
-    const double *binv;  // 9 x 256
+    const double *binv;  // 9 x 256, each block transposed like K
     double lam_eps;
 };
 
@@ -38,8 +50,8 @@ __device__ __forceinline__ double ridge(const LevelDev &L, int gi, int gj) {
 }
 
 // (Q_l x) at control point (gi, gj): gather over the <= 2 x 2 elements containing it
-__device__ __forceinline__ double row_apply(const LevelDev &L, const double *__restrict__ K,
-                                            const double *__restrict__ x, int gi, int gj) {
+__device__ __forceinline__ double row_apply(const LevelDev &L, const double *K, const double *x,
+                                            int gi, int gj) {
     double s = ridge(L, gi, gj) * x[gi + (int64_t)L.nd * gj];
     const int ex1 = min(gi / 3, L.n - 1), ey1 = min(gj / 3, L.n - 1);
     const int ex0 = (gi % 3 == 0 && gi > 0) ? gi / 3 - 1 : ex1;
@@ -48,11 +60,11 @@ __device__ __forceinline__ double row_apply(const LevelDev &L, const double *__r
         for (int ex = ex0; ex <= ex1; ++ex) {
             const int a = (gi - 3 * ex) + 4 * (gj - 3 * ey);
             const double *xr = x + (3 * ex) + (int64_t)L.nd * (3 * ey);
-            const double *Kr = K + a * 16;
+            const double *Kc = K + a;
 #pragma unroll
             for (int bj = 0; bj < 4; ++bj)
 #pragma unroll
-                for (int bi = 0; bi < 4; ++bi) s += Kr[bi + 4 * bj] * xr[bi + (int64_t)L.nd * bj];
+                for (int bi = 0; bi < 4; ++bi) s += Kc[16 * (bi + 4 * bj)] * xr[bi + (int64_t)L.nd * bj];
         }
     return s;
 }
@@ -90,19 +102,156 @@ __global__ void __launch_bounds__(BS) bz_apply_kernel(LevelDev L, const double *
     }
 }
 
+// ---------------------------------------------------------------- operator apply, tiled
+// y = Q x (mode 0, with the block's partial of x.y in part[block]) or y = b - Q x (mode 1).
+// One thread per element computes the dofs the element owns (local ai, aj < 3; ai = 3 / aj = 3
+// too on the last element column / row of the grid) as its contributions plus those of the
+// elements left, below and diagonally below-left of it; x is staged in shared memory over the
+// tile and a one-element margin below and left, K (transposed) beside it, and the owned dofs
+// are written row by row from a shared staging tile.
+template <int TI, int TJ>
+struct ApplyTile {
+    static constexpr int WX = 3 * TI + 4, WY = 3 * TJ + 4;  // x: 3 TI bx - 3 .. 3 TI (bx + 1)
+    static constexpr int OX = 3 * TI + 1, OY = 3 * TJ + 1;  // owned dofs (+ the grid's last)
+};
+
+template <int TI, int TJ>
+__global__ void __launch_bounds__(TI *TJ) bz_apply_tile_kernel(LevelDev L, const double *__restrict__ x,
+                                                               const double *__restrict__ b,
+                                                               double *__restrict__ y, int mode,
+                                                               double *__restrict__ part,
+                                                               const int *__restrict__ stop) {
+    using T = ApplyTile<TI, TJ>;
+    __shared__ __align__(16) double Ks[256];
+    __shared__ double xt[T::WY * T::WX];
+    __shared__ double ys[T::OY * T::OX];
+    __shared__ double red[TI * TJ / 32];
+    if (stop && *stop) return;
+    for (int i = threadIdx.x; i < 256; i += TI * TJ) cp_async8(Ks + i, L.K + i, true);
+    const int X0 = 3 * TI * (int)blockIdx.x - 3, Y0 = 3 * TJ * (int)blockIdx.y - 3;
+    for (int idx = threadIdx.x; idx < T::WX * T::WY; idx += TI * TJ) {
+        const int u = idx % T::WX, v = idx / T::WX;
+        const int gi = X0 + u, gj = Y0 + v;
+        const bool in = gi >= 0 && gi < L.nd && gj >= 0 && gj < L.nd;
+        cp_async8(xt + idx, in ? x + gi + (int64_t)L.nd * gj : x, in);
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    const int ti = threadIdx.x % TI, tj = threadIdx.x / TI;
+    const int ex = TI * blockIdx.x + ti, ey = TJ * blockIdx.y + tj;
+    if (ex < L.n && ey < L.n) {
+        // x of element (ex - dx, ey - dy), dx, dy in {0, 1}: tile origin (3 ti + 3 - 3 dx, 3 tj + 3 - 3 dy)
+        const double *x0 = xt + (3 * tj + 3) * T::WX + 3 * ti + 3;
+        double s[9];
+#pragma unroll
+        for (int a = 0; a < 9; ++a) s[a] = 0.0;
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+            const double xk = x0[(k / 4) * T::WX + k % 4];
+            const double *Kk = Ks + 16 * k;
+#pragma unroll
+            for (int aj = 0; aj < 3; ++aj)
+#pragma unroll
+                for (int ai = 0; ai < 3; ++ai) s[ai + 3 * aj] += Kk[ai + 4 * aj] * xk;
+        }
+        const bool hx = ex > 0, hy = ey > 0;
+        if (hx) {
+#pragma unroll
+            for (int k = 0; k < 16; ++k) {
+                const double xk = x0[(k / 4) * T::WX + k % 4 - 3];
+#pragma unroll
+                for (int aj = 0; aj < 3; ++aj) s[3 * aj] += Ks[16 * k + 3 + 4 * aj] * xk;
+            }
+        }
+        if (hy) {
+#pragma unroll
+            for (int k = 0; k < 16; ++k) {
+                const double xk = x0[(k / 4 - 3) * T::WX + k % 4];
+#pragma unroll
+                for (int ai = 0; ai < 3; ++ai) s[ai] += Ks[16 * k + ai + 12] * xk;
+            }
+        }
+        if (hx && hy) {
+#pragma unroll
+            for (int k = 0; k < 16; ++k) s[0] += Ks[16 * k + 15] * x0[(k / 4 - 3) * T::WX + k % 4 - 3];
+        }
+        double *y0 = ys + (3 * tj) * T::OX + 3 * ti;
+#pragma unroll
+        for (int aj = 0; aj < 3; ++aj)
+#pragma unroll
+            for (int ai = 0; ai < 3; ++ai) y0[aj * T::OX + ai] = s[ai + 3 * aj];
+        // the grid's last column / row of dofs: this element and the one below / left of it
+        if (ex == L.n - 1) {
+            double t[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+            for (int k = 0; k < 16; ++k) {
+                const double xk = x0[(k / 4) * T::WX + k % 4];
+#pragma unroll
+                for (int aj = 0; aj < 4; ++aj) t[aj] += Ks[16 * k + 3 + 4 * aj] * xk;
+            }
+            if (hy)
+                for (int k = 0; k < 16; ++k) t[0] += Ks[16 * k + 15] * x0[(k / 4 - 3) * T::WX + k % 4];
+#pragma unroll
+            for (int aj = 0; aj < 3; ++aj) y0[aj * T::OX + 3] = t[aj];
+            if (ey == L.n - 1) y0[3 * T::OX + 3] = t[3];
+        }
+        if (ey == L.n - 1) {
+            double t[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+            for (int k = 0; k < 16; ++k) {
+                const double xk = x0[(k / 4) * T::WX + k % 4];
+#pragma unroll
+                for (int ai = 0; ai < 3; ++ai) t[ai] += Ks[16 * k + ai + 12] * xk;
+            }
+            if (hx)
+                for (int k = 0; k < 16; ++k) t[0] += Ks[16 * k + 15] * x0[(k / 4) * T::WX + k % 4 - 3];
+#pragma unroll
+            for (int ai = 0; ai < 3; ++ai) y0[3 * T::OX + ai] = t[ai];
+        }
+    }
+    __syncthreads();
+    double dot = 0.0;
+    for (int idx = threadIdx.x; idx < T::OX * T::OY; idx += TI * TJ) {
+        const int u = idx % T::OX, v = idx / T::OX;
+        const int gi = 3 * TI * blockIdx.x + u, gj = 3 * TJ * blockIdx.y + v;
+        if (gi >= L.nd || gj >= L.nd) continue;
+        if ((u == 3 * TI && gi != L.nd - 1) || (v == 3 * TJ && gj != L.nd - 1)) continue;
+        const double xv = xt[(v + 3) * T::WX + u + 3];
+        const double q = ys[idx] + L.lam_eps * L.rho[gi] * L.rho[gj] * xv;
+        const int64_t I = gi + (int64_t)L.nd * gj;
+        if (mode == 0) {
+            y[I] = q;
+            dot += xv * q;
+        } else {
+            y[I] = b[I] - q;
+        }
+    }
+    if (part) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) dot += __shfl_xor_sync(0xffffffffu, dot, o);
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x / 32] = dot;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double t = 0.0;
+            for (int w = 0; w < TI * TJ / 32; ++w) t += red[w];
+            part[blockIdx.x + gridDim.x * blockIdx.y] = t;
+        }
+    }
+}
+
 __device__ __forceinline__ int elem_class(int e, int n) { return e == 0 ? 0 : (e == n - 1 ? 2 : 1); }
 
-// colored Schwarz, part 1: residual at the dofs of every element of one color
-__global__ void __launch_bounds__(BS) bz_smooth_res_kernel(LevelDev L, int color,
-                                                           const double *__restrict__ x,
-                                                           const double *__restrict__ b, double *r) {
-    __shared__ double K[256];
-    for (int i = threadIdx.x; i < 256; i += blockDim.x) K[i] = L.K[i];
-    __syncthreads();
+// ---------------------------------------------------------------- per-dof bodies
+// Shared by the grid-wide kernels (one work item per thread) and the single-CTA coarse V-cycle
+// (work items strided over the block). x, b, r may be written earlier in the same launch by
+// other threads of the block, so none of them is declared __restrict__ here.
+
+// colored Schwarz residual at dof a of the ce-th element of one color
+__device__ __forceinline__ void schwarz_res_item(const LevelDev &L, const double *K, int color,
+                                                 const double *x, const double *b, double *r,
+                                                 int64_t t) {
     const int px = color & 1, py = color >> 1;
-    const int ncx = (L.n - px + 1) / 2, ncy = (L.n - py + 1) / 2;
-    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (t >= (int64_t)ncx * ncy * 16) return;
+    const int ncx = (L.n - px + 1) / 2;
     const int ce = (int)(t / 16), a = (int)(t % 16);
     const int ex = px + 2 * (ce % ncx), ey = py + 2 * (ce / ncx);
     const int gi = 3 * ex + a % 4, gj = 3 * ey + a / 4;
@@ -110,79 +259,68 @@ __global__ void __launch_bounds__(BS) bz_smooth_res_kernel(LevelDev L, int color
     r[I] = b[I] - row_apply(L, K, x, gi, gj);
 }
 
-// colored Schwarz, part 2: x_e += Binv_class(e) r_e for every element of one color
-__global__ void __launch_bounds__(BS) bz_smooth_upd_kernel(LevelDev L, int color,
-                                                           const double *__restrict__ r, double *x) {
+// x_e += Binv_class(e) r_e at dof a of the ce-th element of one color
+__device__ __forceinline__ void schwarz_upd_item(const LevelDev &L, int color, const double *r,
+                                                 double *x, int64_t t) {
     const int px = color & 1, py = color >> 1;
-    const int ncx = (L.n - px + 1) / 2, ncy = (L.n - py + 1) / 2;
-    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (t >= (int64_t)ncx * ncy * 16) return;
+    const int ncx = (L.n - px + 1) / 2;
     const int ce = (int)(t / 16), a = (int)(t % 16);
     const int ex = px + 2 * (ce % ncx), ey = py + 2 * (ce / ncx);
-    const double *Bi = L.binv + (elem_class(ex, L.n) + 3 * elem_class(ey, L.n)) * 256 + a * 16;
+    const double *Bi = L.binv + (elem_class(ex, L.n) + 3 * elem_class(ey, L.n)) * 256 + a;
     const double *re = r + 3 * ex + (int64_t)L.nd * (3 * ey);
     double s = 0.0;
 #pragma unroll
-    for (int k = 0; k < 16; ++k) s += Bi[k] * re[(k % 4) + (int64_t)L.nd * (k / 4)];
+    for (int k = 0; k < 16; ++k) s += Bi[16 * k] * re[(k % 4) + (int64_t)L.nd * (k / 4)];
     x[(3 * ex + a % 4) + (int64_t)L.nd * (3 * ey + a / 4)] += s;
 }
 
-// 1D prolongation weights: fine index f -> 4 weights on coarse 3E..3E+3
-__constant__ double cSub[2][16];
+// 1D transfer between a level of nc elements and its refinement, as tables built on the host
+// from the Bezier subdivision (the uniform grid is square, one table serves both directions):
+// prolongation row of fine index f: coarse fc0[f] .. fc0[f] + 3 with weights fw[4 f ..];
+// restriction row of coarse index c (the transpose): fine cf0[c] .. cf0[c] + 7 with weights
+// cw[8 c ..], zero where f does not touch c. Lanes of neighbouring indices read neighbouring
+// table entries (no divergent constant-memory reads).
+struct TransferDev {
+    const int *fc0, *cf0;
+    const double *fw, *cw;
+};
 
-__device__ __forceinline__ int p1_row(int f, int nc, double w[4]) {
-    int E = f / 6;
-    if (E > nc - 1) E = nc - 1;
-    const int k = f - 6 * E;
-    const double *row = k <= 3 ? &cSub[0][k * 4] : &cSub[1][(k - 3) * 4];
-#pragma unroll
-    for (int c = 0; c < 4; ++c) w[c] = row[c];
-    return 3 * E;
-}
-
-// weight of coarse index c in the row of fine index f (0 if none)
-__device__ __forceinline__ double p1_weight(int f, int c, int nc) {
-    double w[4];
-    const int c0 = p1_row(f, nc, w);
-    const int d = c - c0;
-    return (d >= 0 && d <= 3) ? w[d] : 0.0;
-}
-
-// r_c = P^T r_f (separable sums over the <= 13 fine indices per direction)
-__global__ void __launch_bounds__(BS) bz_restrict_kernel(int ncel, int ndc, int ndf,
-                                                         const double *__restrict__ rf, double *rc,
-                                                         double *xc_zero) {
-    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (t >= (int64_t)ndc * ndc) return;
+// r_c = P^T r_f at coarse dof t (fine rows ascending, columns ascending within a row)
+__device__ __forceinline__ void restrict_item(const TransferDev &T, int ndc, int ndf, const double *rf,
+                                              double *rc, double *xc_zero, int64_t t) {
     const int ci = (int)(t % ndc), cj = (int)(t / ndc);
-    const int Ex1 = min(ci / 3, ncel - 1), Ey1 = min(cj / 3, ncel - 1);
-    const int Ex0 = (ci % 3 == 0 && ci > 0) ? ci / 3 - 1 : Ex1;
-    const int Ey0 = (cj % 3 == 0 && cj > 0) ? cj / 3 - 1 : Ey1;
-    const int fi0 = 6 * Ex0, fi1 = min(6 * Ex1 + 6, ndf - 1);
-    const int fj0 = 6 * Ey0, fj1 = min(6 * Ey1 + 6, ndf - 1);
+    const int fi0 = T.cf0[ci], fj0 = T.cf0[cj];
+    const double *wx = T.cw + 8 * ci, *wy = T.cw + 8 * cj;
+    double w[8];
+#pragma unroll
+    for (int p = 0; p < 8; ++p) w[p] = wx[p];
     double s = 0.0;
-    for (int fj = fj0; fj <= fj1; ++fj) {
-        const double wy = p1_weight(fj, cj, ncel);
-        if (wy == 0.0) continue;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        const double wq = wy[q];
+        if (wq == 0.0) continue;
+        const double *row = rf + fi0 + (int64_t)ndf * (fj0 + q);
         double sx = 0.0;
-        for (int fi = fi0; fi <= fi1; ++fi) {
-            const double wx = p1_weight(fi, ci, ncel);
-            if (wx != 0.0) sx += wx * rf[fi + (int64_t)ndf * fj];
-        }
-        s += wy * sx;
+#pragma unroll
+        for (int p = 0; p < 8; ++p)
+            if (w[p] != 0.0) sx += w[p] * row[p];
+        s += wq * sx;
     }
     rc[t] = s;
     xc_zero[t] = 0.0;
 }
 
-// x_f += P e_c
-__global__ void __launch_bounds__(BS) bz_prolong_kernel(int ncel, int ndc, int ndf,
-                                                        const double *__restrict__ ec, double *xf) {
-    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (t >= (int64_t)ndf * ndf) return;
+// x_f += P e_c at fine dof t
+__device__ __forceinline__ void prolong_item(const TransferDev &T, int ndc, int ndf, const double *ec,
+                                             double *xf, int64_t t) {
     const int fi = (int)(t % ndf), fj = (int)(t / ndf);
+    const int cx0 = T.fc0[fi], cy0 = T.fc0[fj];
     double wx[4], wy[4];
-    const int cx0 = p1_row(fi, ncel, wx), cy0 = p1_row(fj, ncel, wy);
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        wx[a] = T.fw[4 * fi + a];
+        wy[a] = T.fw[4 * fj + a];
+    }
     double s = 0.0;
 #pragma unroll
     for (int b = 0; b < 4; ++b)
@@ -191,16 +329,314 @@ __global__ void __launch_bounds__(BS) bz_prolong_kernel(int ncel, int ndc, int n
     xf[t] += s;
 }
 
-// coarsest level: x = C^-1 b (one block, dense)
-__global__ void bz_coarse_kernel(int n2, const double *__restrict__ Cinv, const double *__restrict__ b,
-                                 double *x) {
-    extern __shared__ double sb[];
-    for (int i = threadIdx.x; i < n2; i += blockDim.x) sb[i] = b[i];
+__global__ void __launch_bounds__(BS) bz_restrict_kernel(TransferDev T, int ndc, int ndf,
+                                                         const double *__restrict__ rf, double *rc,
+                                                         double *xc_zero) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t < (int64_t)ndc * ndc) restrict_item(T, ndc, ndf, rf, rc, xc_zero, t);
+}
+
+__global__ void __launch_bounds__(BS) bz_prolong_kernel(TransferDev T, int ndc, int ndf,
+                                                        const double *__restrict__ ec, double *xf) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t < (int64_t)ndf * ndf) prolong_item(T, ndc, ndf, ec, xf, t);
+}
+
+// ---------------------------------------------------------------- fine-level Schwarz sweep
+// One color step of the multiplicative Schwarz smoother on a level with many elements, split
+// in two launches so that every residual of the color is formed before any update (Jacobi
+// within a color, as the per-dof form):
+//   bz_color_solve_kernel: one thread per element e of the color; z_e = Binv_class(e)(b - Q x)_e
+//     from x staged in shared memory (the 3x3-element neighbourhood of every element of the
+//     tile), K and the interior block inverse staged beside it (warp-wide broadcast reads);
+//   bz_color_update_kernel: x_e += z_e.
+// Shared tile: columns 3(px + 2 TI bx) - 3 .. + 6 TI + 3 and the same in y; column u is stored
+// at u + u / 6, so that lanes six columns apart (neighbouring elements of one color) hit
+// distinct bank pairs.
+template <int TI, int TJ>
+struct SchwarzTile {
+    static constexpr int WX = 6 * TI + 4, WY = 6 * TJ + 4;
+    static constexpr int WXP = WX + WX / 6 + 1;
+    static constexpr int ZS = 17;  // padded row of the per-element staging
+    static constexpr size_t smem_bytes() { return (size_t)(512 + WY * WXP) * sizeof(double); }
+    static_assert(TI * TJ * ZS <= WX * WY, "staging must fit in the tile");
+};
+
+template <int TI, int TJ>
+__global__ void __launch_bounds__(TI *TJ) bz_color_solve_kernel(LevelDev L, int color,
+                                                                const double *__restrict__ x,
+                                                                const double *__restrict__ b,
+                                                                double *__restrict__ zc) {
+    using T = SchwarzTile<TI, TJ>;
+    extern __shared__ __align__(16) double smem[];
+    double *Ks = smem, *Bs = smem + 256, *tile = smem + 512;
+    for (int i = threadIdx.x; i < 256; i += TI * TJ) {
+        cp_async8(Ks + i, L.K + i, true);
+        cp_async8(Bs + i, L.binv + 4 * 256 + i, true);
+    }
+    const int px = color & 1, py = color >> 1;
+    const int ncx = (L.n - px + 1) / 2, ncy = (L.n - py + 1) / 2;
+    const int X0 = 3 * (px + 2 * TI * (int)blockIdx.x) - 3;
+    const int Y0 = 3 * (py + 2 * TJ * (int)blockIdx.y) - 3;
+    for (int idx = threadIdx.x; idx < T::WX * T::WY; idx += TI * TJ) {
+        const int u = idx % T::WX, v = idx / T::WX;
+        const int gi = X0 + u, gj = Y0 + v;
+        const bool in = gi >= 0 && gi < L.nd && gj >= 0 && gj < L.nd;
+        cp_async8(tile + v * T::WXP + u + u / 6, in ? x + gi + (int64_t)L.nd * gj : x, in);
+    }
+    const int ti = threadIdx.x % TI, tj = threadIdx.x / TI;
+    const int i = blockIdx.x * TI + ti, j = blockIdx.y * TJ + tj;
+    const bool valid = i < ncx && j < ncy;
+    const int ex = px + 2 * i, ey = py + 2 * j;
+    // this element's right-hand side, in flight while the tile arrives
+    double bv[16];
+#pragma unroll
+    for (int a = 0; a < 16; ++a)
+        bv[a] = valid ? b[(3 * ex + a % 4) + (int64_t)L.nd * (3 * ey + a / 4)] : 0.0;
+    cp_async_wait_all();
     __syncthreads();
-    for (int i = threadIdx.x; i < n2; i += blockDim.x) {
-        double s = 0.0;
-        for (int k = 0; k < n2; ++k) s += Cinv[(int64_t)i * n2 + k] * sb[k];
-        x[i] = s;
+    // element origin at tile column 6 ti + 3, row 6 tj + 3; local column c >= 0 from 6 ti lies
+    // at 7 ti + c + c / 6
+    const double *tl = tile + (6 * tj) * T::WXP + 7 * ti;
+    double s[16];
+#pragma unroll
+    for (int a = 0; a < 16; ++a) s[a] = 0.0;
+    if (valid) {
+        double rx[4], ry[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            rx[q] = L.rho[3 * ex + q];
+            ry[q] = L.rho[3 * ey + q];
+        }
+#pragma unroll
+        for (int a = 0; a < 16; ++a) {
+            const int c = 3 + a % 4, rr = 3 + a / 4;
+            s[a] = L.lam_eps * rx[a % 4] * ry[a / 4] * tl[rr * T::WXP + c + c / 6];
+        }
+#pragma unroll
+        for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll
+            for (int dx = -1; dx <= 1; ++dx) {
+                if (ex + dx < 0 || ex + dx >= L.n || ey + dy < 0 || ey + dy >= L.n) continue;
+#pragma unroll
+                for (int k = 0; k < 16; ++k) {
+                    const int c = 3 + 3 * dx + k % 4, rr = 3 + 3 * dy + k / 4;
+                    const double xk = tl[rr * T::WXP + c + c / 6];
+                    const double *Kk = Ks + 16 * k;
+                    // rows of the neighbour that are dofs of this element
+#pragma unroll
+                    for (int aj2 = 0; aj2 < 4; ++aj2)
+#pragma unroll
+                        for (int ai2 = 0; ai2 < 4; ++ai2) {
+                            const int ai = ai2 + 3 * dx, aj = aj2 + 3 * dy;
+                            if (ai < 0 || ai > 3 || aj < 0 || aj > 3) continue;
+                            s[ai + 4 * aj] += Kk[ai2 + 4 * aj2] * xk;
+                        }
+                }
+            }
+    }
+    __syncthreads();  // tile reads done: the tile now stages per-element vectors
+    double *zs = tile;
+    if (valid) {
+        double r[16], z[16];
+#pragma unroll
+        for (int a = 0; a < 16; ++a) {
+            r[a] = bv[a] - s[a];
+            z[a] = 0.0;
+        }
+        const int cls = elem_class(ex, L.n) + 3 * elem_class(ey, L.n);
+        const double *Bi = cls == 4 ? Bs : L.binv + cls * 256;
+#pragma unroll
+        for (int k = 0; k < 16; ++k)
+#pragma unroll
+            for (int a = 0; a < 16; ++a) z[a] += Bi[k * 16 + a] * r[k];
+#pragma unroll
+        for (int a = 0; a < 16; ++a) zs[threadIdx.x * T::ZS + a] = z[a];
+    }
+    __syncthreads();
+    // z of element (i, j) of the color at zc[(i + ncx j) * 16 + a]
+    for (int idx = threadIdx.x; idx < TI * TJ * 16; idx += TI * TJ) {
+        const int el = idx / 16, a = idx % 16;
+        const int ii = blockIdx.x * TI + el % TI, jj = blockIdx.y * TJ + el / TI;
+        if (ii < ncx && jj < ncy) zc[((int64_t)ii + (int64_t)ncx * jj) * 16 + a] = zs[el * T::ZS + a];
+    }
+}
+
+// The same color step with one thread per dof of an element (16 lanes per element): each lane
+// forms the residual of its row from the shared x tile (gathering over the one, two or four
+// elements that contain the dof), the element's residual is exchanged through shared memory and
+// each lane forms one row of Binv_class(e) r_e. Shorter per-thread work than the element-per-
+// thread form; the tile is (6 TI + 4) x (6 TJ + 4) control points, unpadded.
+template <int TI, int TJ>
+struct SchwarzDofTile {
+    static constexpr int WX = 6 * TI + 4, WY = 6 * TJ + 4, NT = TI * TJ * 16;
+    static constexpr size_t smem_bytes() { return (size_t)(256 + WX * WY + TI * TJ * 17) * sizeof(double); }
+};
+
+template <int TI, int TJ>
+__global__ void __launch_bounds__(TI *TJ * 16) bz_color_solve_dof_kernel(LevelDev L, int color,
+                                                                         const double *__restrict__ x,
+                                                                         const double *__restrict__ b,
+                                                                         double *__restrict__ zc) {
+    using T = SchwarzDofTile<TI, TJ>;
+    extern __shared__ __align__(16) double smem[];
+    double *Ks = smem, *xt = smem + 256, *rs = smem + 256 + T::WX * T::WY;
+    for (int i = threadIdx.x; i < 256; i += T::NT) cp_async8(Ks + i, L.K + i, true);
+    const int px = color & 1, py = color >> 1;
+    const int ncx = (L.n - px + 1) / 2, ncy = (L.n - py + 1) / 2;
+    const int X0 = 3 * (px + 2 * TI * (int)blockIdx.x) - 3;
+    const int Y0 = 3 * (py + 2 * TJ * (int)blockIdx.y) - 3;
+    for (int idx = threadIdx.x; idx < T::WX * T::WY; idx += T::NT) {
+        const int u = idx % T::WX, v = idx / T::WX;
+        const int gi = X0 + u, gj = Y0 + v;
+        const bool in = gi >= 0 && gi < L.nd && gj >= 0 && gj < L.nd;
+        cp_async8(xt + idx, in ? x + gi + (int64_t)L.nd * gj : x, in);
+    }
+    const int el = threadIdx.x / 16, a = threadIdx.x % 16;
+    const int ti = el % TI, tj = el / TI;
+    const int i = blockIdx.x * TI + ti, j = blockIdx.y * TJ + tj;
+    const bool valid = i < ncx && j < ncy;
+    const int ex = px + 2 * i, ey = py + 2 * j;
+    const int ai = a % 4, aj = a / 4;
+    const int gi = 3 * ex + ai, gj = 3 * ey + aj;
+    const double bv = valid ? b[gi + (int64_t)L.nd * gj] : 0.0;
+    const double ridge = valid ? L.lam_eps * L.rho[gi] * L.rho[gj] : 0.0;
+    cp_async_wait_all();
+    __syncthreads();
+    if (valid) {
+        // element origin at tile (6 ti + 3, 6 tj + 3); the dof at (+ai, +aj)
+        const int u = 6 * ti + 3 + ai, v = 6 * tj + 3 + aj;
+        double s = ridge * xt[v * T::WX + u];
+        const int dx0 = (ai == 0 && ex > 0) ? -1 : 0, dx1 = (ai == 3 && ex < L.n - 1) ? 1 : 0;
+        const int dy0 = (aj == 0 && ey > 0) ? -1 : 0, dy1 = (aj == 3 && ey < L.n - 1) ? 1 : 0;
+        for (int dy = dy0; dy <= dy1; ++dy)
+            for (int dx = dx0; dx <= dx1; ++dx) {
+                const int ar = (ai - 3 * dx) + 4 * (aj - 3 * dy);  // the dof's row in that element
+                const double *xe = xt + (6 * tj + 3 + 3 * dy) * T::WX + 6 * ti + 3 + 3 * dx;
+#pragma unroll
+                for (int k = 0; k < 16; ++k) s += Ks[16 * k + ar] * xe[(k / 4) * T::WX + k % 4];
+            }
+        rs[el * 17 + a] = bv - s;
+    }
+    __syncthreads();
+    if (valid) {
+        const int cls = elem_class(ex, L.n) + 3 * elem_class(ey, L.n);
+        const double *Bi = L.binv + cls * 256 + a;
+        const double *re = rs + el * 17;
+        double z = 0.0;
+#pragma unroll
+        for (int k = 0; k < 16; ++k) z += Bi[16 * k] * re[k];
+        zc[((int64_t)i + (int64_t)ncx * j) * 16 + a] = z;
+    }
+}
+
+__global__ void __launch_bounds__(BS) bz_color_update_kernel(LevelDev L, int color,
+                                                             const double *__restrict__ zc,
+                                                             double *__restrict__ x) {
+    const int px = color & 1, py = color >> 1;
+    const int ncx = (L.n - px + 1) / 2, ncy = (L.n - py + 1) / 2;
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= (int64_t)ncx * ncy * 16) return;
+    const int ce = (int)(t / 16), a = (int)(t % 16);
+    const int ex = px + 2 * (ce % ncx), ey = py + 2 * (ce / ncx);
+    x[(3 * ex + a % 4) + (int64_t)L.nd * (3 * ey + a / 4)] += zc[t];
+}
+
+// ---------------------------------------------------------------- coarse V-cycle, one CTA
+// Levels 0..top of the hierarchy (the coarsest few, n <= COARSE_CTA_MAX_N elements per
+// direction) in one launch, their x, b, r resident in shared memory: smoothing, residual,
+// restriction, the dense coarsest solve and prolongation, phase after phase with block-wide
+// barriers. Operators, ridge factors, block inverses and transfer tables are read-only and
+// come through L1. b of level top is read from global memory at the start and x of level top
+// written back at the end.
+constexpr int COARSE_MAX_LEVELS = 8;
+constexpr int COARSE_THREADS = 1024;
+constexpr int COARSE_CTA_MAX_N = 16;
+constexpr size_t COARSE_SMEM_MAX = 200 * 1024;
+
+struct CoarseStack {
+    int top, pre, post, nc2;
+    LevelDev L[COARSE_MAX_LEVELS];
+    TransferDev T[COARSE_MAX_LEVELS];  // T[l]: between levels l - 1 and l
+    int off[COARSE_MAX_LEVELS];        // shared offset (doubles) of x_l; b_l, r_l follow
+    const double *bin;                 // b of level top
+    double *xout;                      // x of level top
+    const double *Cinv;
+};
+
+// shared doubles of the coarse stack for levels 0..top: K staging + x, b, r per level
+inline size_t coarse_smem_doubles(const std::vector<int> &nd, int top) {
+    size_t t = 256;
+    for (int l = 0; l <= top; ++l) t += 3 * (size_t)nd[l] * nd[l];
+    return t;
+}
+
+__device__ void coarse_smooth(const LevelDev &L, const double *K, double *x, const double *b,
+                              double *r, bool forward) {
+    for (int s = 0; s < 4; ++s) {
+        const int color = forward ? s : 3 - s;
+        const int px = color & 1, py = color >> 1;
+        const int64_t work = (int64_t)((L.n - px + 1) / 2) * ((L.n - py + 1) / 2) * 16;
+        for (int64_t t = threadIdx.x; t < work; t += blockDim.x) schwarz_res_item(L, K, color, x, b, r, t);
+        __syncthreads();
+        for (int64_t t = threadIdx.x; t < work; t += blockDim.x) schwarz_upd_item(L, color, r, x, t);
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(COARSE_THREADS) bz_coarse_vcycle_kernel(CoarseStack S) {
+    extern __shared__ __align__(16) double sm[];
+    double *K = sm;
+    auto X = [&](int l) { return sm + S.off[l]; };
+    auto B = [&](int l) { return sm + S.off[l] + S.L[l].nd * S.L[l].nd; };
+    auto R = [&](int l) { return sm + S.off[l] + 2 * S.L[l].nd * S.L[l].nd; };
+    {
+        const int n2 = S.L[S.top].nd * S.L[S.top].nd;
+        double *xt = X(S.top), *bt = B(S.top);
+        for (int i = threadIdx.x; i < n2; i += blockDim.x) {
+            bt[i] = S.bin[i];
+            xt[i] = 0.0;
+        }
+        __syncthreads();
+    }
+    for (int l = S.top; l >= 1; --l) {
+        const LevelDev &L = S.L[l];
+        for (int i = threadIdx.x; i < 256; i += blockDim.x) K[i] = L.K[i];
+        __syncthreads();
+        for (int it = 0; it < S.pre; ++it) coarse_smooth(L, K, X(l), B(l), R(l), true);
+        const int nd2 = L.nd * L.nd;
+        double *xl = X(l), *bl = B(l), *rl = R(l);
+        for (int t = threadIdx.x; t < nd2; t += blockDim.x)
+            rl[t] = bl[t] - row_apply(L, K, xl, t % L.nd, t / L.nd);
+        __syncthreads();
+        const LevelDev &C = S.L[l - 1];
+        const int ndc2 = C.nd * C.nd;
+        for (int t = threadIdx.x; t < ndc2; t += blockDim.x) restrict_item(S.T[l], C.nd, L.nd, rl, B(l - 1), X(l - 1), t);
+        __syncthreads();
+    }
+    {
+        const double *b0 = B(0);
+        double *x0 = X(0);
+        for (int i = threadIdx.x; i < S.nc2; i += blockDim.x) {
+            double s = 0.0;
+            for (int k = 0; k < S.nc2; ++k) s += S.Cinv[(int64_t)i * S.nc2 + k] * b0[k];
+            x0[i] = s;
+        }
+        __syncthreads();
+    }
+    for (int l = 1; l <= S.top; ++l) {
+        const LevelDev &L = S.L[l];
+        const LevelDev &C = S.L[l - 1];
+        for (int i = threadIdx.x; i < 256; i += blockDim.x) K[i] = L.K[i];
+        const int nd2 = L.nd * L.nd;
+        for (int t = threadIdx.x; t < nd2; t += blockDim.x) prolong_item(S.T[l], C.nd, L.nd, X(l - 1), X(l), t);
+        __syncthreads();
+        for (int it = 0; it < S.post; ++it) coarse_smooth(L, K, X(l), B(l), R(l), false);
+    }
+    {
+        const int n2 = S.L[S.top].nd * S.L[S.top].nd;
+        const double *xt = X(S.top);
+        for (int i = threadIdx.x; i < n2; i += blockDim.x) S.xout[i] = xt[i];
     }
 }
 
@@ -463,6 +899,8 @@ struct drf_bz {
     DevBuf<int> ctl;
     struct Lv {
         DevBuf<double> K, rho, binv, x, b, r;
+        DevBuf<int> fc0, cf0;     // transfer tables from the next coarser level (TransferDev)
+        DevBuf<double> fw, cw;
         int n = 0, nd = 0;
     };
     std::vector<Lv> lv;
@@ -483,11 +921,29 @@ struct drf_bz {
         return L;
     }
     int finest() const { return (int)lv.size() - 1; }
+    // transfer tables between level l - 1 and level l
+    TransferDev tdev(int l) const {
+        TransferDev T;
+        T.fc0 = lv[l].fc0.p; T.cf0 = lv[l].cf0.p; T.fw = lv[l].fw.p; T.cw = lv[l].cw.p;
+        return T;
+    }
     unsigned nparts() const { return 1024; }
     PcgCtl pctl() {
         PcgCtl c;
         c.sc = scal.p; c.stop = ctl.p; c.iters = ctl.p + 1; c.maxit = ctl.p + 2; c.part = part.p;
         return c;
+    }
+
+    // y = Q x (mode 0, per-tile partials of x.y in pt) or y = b - Q x (mode 1) on level l;
+    // returns the number of partials written
+    int apply(int l, const double *xin, const double *bin, double *yout, int mode, double *pt,
+              const int *stop) {
+        constexpr int TI = 32, TJ = 8;
+        const LevelDev L = levdev(l);
+        const dim3 grid((unsigned)((L.n + TI - 1) / TI), (unsigned)((L.n + TJ - 1) / TJ));
+        bz_apply_tile_kernel<TI, TJ><<<grid, TI * TJ, 0, stream>>>(L, xin, bin, yout, mode, pt, stop);
+        DRF_LAUNCHED();
+        return (int)(grid.x * grid.y);
     }
 
     // z = M r for the given preconditioner kind (enqueued on stream)
@@ -512,17 +968,49 @@ struct drf_bz {
         }
     }
 
+    // one color step of the Schwarz smoother on a grid-wide level: z of every element of the
+    // color into the level's residual buffer (free while smoothing), then x += z
+    template <int TI, int TJ>
+    void color_solve(int l, int color, int ncx, int ncy, const double *xl, const double *bl, double *zc) {
+        const dim3 grid((unsigned)((ncx + TI - 1) / TI), (unsigned)((ncy + TJ - 1) / TJ));
+        bz_color_solve_kernel<TI, TJ><<<grid, TI * TJ, SchwarzTile<TI, TJ>::smem_bytes(), stream>>>(
+            levdev(l), color, xl, bl, zc);
+        DRF_LAUNCHED();
+    }
+
+    template <int TI, int TJ>
+    void color_solve_dof(int l, int color, int ncx, int ncy, const double *xl, const double *bl, double *zc) {
+        const dim3 grid((unsigned)((ncx + TI - 1) / TI), (unsigned)((ncy + TJ - 1) / TJ));
+        bz_color_solve_dof_kernel<TI, TJ><<<grid, TI * TJ * 16, SchwarzDofTile<TI, TJ>::smem_bytes(), stream>>>(
+            levdev(l), color, xl, bl, zc);
+        DRF_LAUNCHED();
+    }
+
     void smooth(int l, double *xl, const double *bl, double *rl, bool forward) {
         const LevelDev L = levdev(l);
         for (int s = 0; s < 4; ++s) {
             const int color = forward ? s : 3 - s;
             const int px = color & 1, py = color >> 1;
-            const int64_t work = (int64_t)((L.n - px + 1) / 2) * ((L.n - py + 1) / 2) * 16;
-            bz_smooth_res_kernel<<<nblk(work), BS, 0, stream>>>(L, color, xl, bl, rl);
-            DRF_LAUNCHED();
-            bz_smooth_upd_kernel<<<nblk(work), BS, 0, stream>>>(L, color, rl, xl);
+            const int ncx = (L.n - px + 1) / 2, ncy = (L.n - py + 1) / 2;
+            const int64_t nce = (int64_t)ncx * ncy;
+            if (nce >= ELEM_THREAD_MIN_ELEMS)
+                color_solve<16, 4>(l, color, ncx, ncy, xl, bl, rl);
+            else
+                color_solve_dof<8, 2>(l, color, ncx, ncy, xl, bl, rl);
+            bz_color_update_kernel<<<nblk(nce * 16), BS, 0, stream>>>(L, color, rl, xl);
             DRF_LAUNCHED();
         }
+    }
+
+    // highest level run by the single-CTA coarse V-cycle (level 0 at least)
+    int coarse_top() const {
+        std::vector<int> nd(lv.size());
+        for (size_t l = 0; l < lv.size(); ++l) nd[l] = lv[l].nd;
+        int top = 0;
+        while (top + 1 < (int)lv.size() && top + 1 < COARSE_MAX_LEVELS && lv[top + 1].n <= COARSE_CTA_MAX_N &&
+               coarse_smem_doubles(nd, top + 1) * sizeof(double) <= COARSE_SMEM_MAX)
+            ++top;
+        return top;
     }
 
     // one V-cycle z = M r (z overwritten), finest level uses rin/zout directly
@@ -533,23 +1021,36 @@ struct drf_bz {
         X[Lf] = zout; B[Lf] = const_cast<double *>(rin); R[Lf] = lv[Lf].r.p;
         zero_kernel<<<nblk(ndof), BS, 0, stream>>>(ndof, zout, nullptr);
         DRF_LAUNCHED();
-        for (int l = Lf; l >= 1; --l) {
+        const int top = coarse_top();
+        for (int l = Lf; l > top; --l) {
             for (int it = 0; it < H.pre; ++it) smooth(l, X[l], B[l], R[l], true);
             const int64_t nd2 = (int64_t)lv[l].nd * lv[l].nd;
-            bz_apply_kernel<<<nblk(nd2), BS, 0, stream>>>(levdev(l), X[l], B[l], R[l], 1, nullptr, nullptr);
-            DRF_LAUNCHED();
+            apply(l, X[l], B[l], R[l], 1, nullptr, nullptr);
             const int64_t ndc2 = (int64_t)lv[l - 1].nd * lv[l - 1].nd;
-            bz_restrict_kernel<<<nblk(ndc2), BS, 0, stream>>>(lv[l - 1].n, lv[l - 1].nd, lv[l].nd,
-                                                              R[l], B[l - 1], X[l - 1]);
+            bz_restrict_kernel<<<nblk(ndc2), BS, 0, stream>>>(tdev(l), lv[l - 1].nd, lv[l].nd, R[l],
+                                                              B[l - 1], X[l - 1]);
             DRF_LAUNCHED();
         }
-        const int nc2 = lv[0].nd * lv[0].nd;
-        bz_coarse_kernel<<<1, 256, nc2 * sizeof(double), stream>>>(nc2, coarse.p, B[0], X[0]);
+        CoarseStack S;
+        std::memset(&S, 0, sizeof(S));
+        S.top = top; S.pre = H.pre; S.post = H.post;
+        S.nc2 = lv[0].nd * lv[0].nd;
+        S.Cinv = coarse.p;
+        S.bin = B[top];
+        S.xout = X[top];
+        int off = 256;
+        for (int l = 0; l <= top; ++l) {
+            S.L[l] = levdev(l);
+            if (l > 0) S.T[l] = tdev(l);
+            S.off[l] = off;
+            off += 3 * lv[l].nd * lv[l].nd;
+        }
+        bz_coarse_vcycle_kernel<<<1, COARSE_THREADS, (size_t)off * sizeof(double), stream>>>(S);
         DRF_LAUNCHED();
-        for (int l = 1; l <= Lf; ++l) {
+        for (int l = top + 1; l <= Lf; ++l) {
             const int64_t nd2 = (int64_t)lv[l].nd * lv[l].nd;
-            bz_prolong_kernel<<<nblk(nd2), BS, 0, stream>>>(lv[l - 1].n, lv[l - 1].nd, lv[l].nd,
-                                                            X[l - 1], X[l]);
+            bz_prolong_kernel<<<nblk(nd2), BS, 0, stream>>>(tdev(l), lv[l - 1].nd, lv[l].nd, X[l - 1],
+                                                            X[l]);
             DRF_LAUNCHED();
             for (int it = 0; it < H.post; ++it) smooth(l, X[l], B[l], R[l], false);
         }
@@ -558,13 +1059,10 @@ struct drf_bz {
     // one PCG iteration (assumes r, z, p, rz set)
     void pcg_iteration(int kind) {
         const int Lf = finest();
-        const LevelDev L = levdev(Lf);
         PcgCtl c = pctl();
-        const unsigned nb = nblk(ndof);
         // q = Q p with partial p.q
-        bz_apply_kernel<<<nb, BS, 0, stream>>>(L, p.p, nullptr, q.p, 0, part.p, c.stop);
-        DRF_LAUNCHED();
-        alpha_kernel<<<1, BS, 0, stream>>>(c, (int)nb);
+        const int na = apply(Lf, p.p, nullptr, q.p, 0, part.p, c.stop);
+        alpha_kernel<<<1, BS, 0, stream>>>(c, na);
         DRF_LAUNCHED();
         xr_update_kernel<<<nparts(), BS, 0, stream>>>(ndof, c, p.p, q.p, x.p, r.p);
         DRF_LAUNCHED();
@@ -590,21 +1088,64 @@ struct drf_bz {
 namespace drf {
 namespace {
 
-void upload_sub() {
-    static bool done[64] = {false};
-    int dev = 0;
-    DRF_CUDA(cudaGetDevice(&dev));
-    if (dev < 64 && done[dev]) return;
-    double S[2][16];
-    bz_subdivision_1d(S);
-    DRF_CUDA(cudaMemcpyToSymbol(cSub, S, sizeof(S)));
-    if (dev < 64) done[dev] = true;
+// dynamic shared memory above the default 48 KB for the Schwarz tile kernels (per device, set
+// outside any stream capture)
+template <int TI, int TJ>
+void allow_smem() {
+    DRF_CUDA(cudaFuncSetAttribute(bz_color_solve_kernel<TI, TJ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)SchwarzTile<TI, TJ>::smem_bytes()));
 }
 
-template <class V>
-void up(DevBuf<double> &d, const V &v) {
+// 1D transfer tables between nc and 2 nc elements (layout of TransferDev): prolongation rows
+// from the Bezier subdivision, fine index f in coarse element min(f / 6, nc - 1); restriction
+// rows are their transpose
+void transfer_tables(int nc, std::vector<int> &fc0, std::vector<double> &fw, std::vector<int> &cf0,
+                     std::vector<double> &cw) {
+    double S[2][16];
+    bz_subdivision_1d(S);
+    const int ndc = 3 * nc + 1, ndf = 6 * nc + 1;
+    fc0.assign(ndf, 0);
+    fw.assign((size_t)4 * ndf, 0.0);
+    std::vector<int> lo(ndc, ndf), hi(ndc, -1);
+    for (int f = 0; f < ndf; ++f) {
+        const int E = std::min(f / 6, nc - 1), k = f - 6 * E;
+        const double *row = k <= 3 ? &S[0][k * 4] : &S[1][(k - 3) * 4];
+        fc0[f] = 3 * E;
+        for (int a = 0; a < 4; ++a) {
+            fw[4 * f + a] = row[a];
+            if (row[a] != 0.0) {
+                lo[3 * E + a] = std::min(lo[3 * E + a], f);
+                hi[3 * E + a] = std::max(hi[3 * E + a], f);
+            }
+        }
+    }
+    cf0.assign(ndc, 0);
+    cw.assign((size_t)8 * ndc, 0.0);
+    for (int c = 0; c < ndc; ++c) {
+        DRF_CHECK(hi[c] >= lo[c] && hi[c] - lo[c] < 8, DRF_E_INVALID, "restriction row wider than 8");
+        cf0[c] = lo[c];
+    }
+    for (int f = 0; f < ndf; ++f)
+        for (int a = 0; a < 4; ++a)
+            if (fw[4 * f + a] != 0.0) {
+                const int c = fc0[f] + a;
+                cw[8 * c + (f - cf0[c])] = fw[4 * f + a];
+            }
+}
+
+// count 16x16 blocks, each transposed (the device layout of K and of the block inverses)
+std::vector<double> transposed16(const double *A, int count) {
+    std::vector<double> T((size_t)count * 256);
+    for (int c = 0; c < count; ++c)
+        for (int a = 0; a < 16; ++a)
+            for (int k = 0; k < 16; ++k) T[c * 256 + k * 16 + a] = A[c * 256 + a * 16 + k];
+    return T;
+}
+
+template <class T, class V>
+void up(DevBuf<T> &d, const V &v) {
     d.alloc(v.size());
-    DRF_CUDA(cudaMemcpy(d.p, v.data(), v.size() * 8, cudaMemcpyHostToDevice));
+    DRF_CUDA(cudaMemcpy(d.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
 }
 
 void check_bz(drf_bz *h) { DRF_CHECK(h != nullptr, DRF_E_INVALID, "null smoother handle"); }
@@ -628,14 +1169,13 @@ int drf_bz_create(const drf_bz_grid_desc *g, const double *dgauss, drf_bz **out)
         bz_setup_fine(h->H, *g);
         DRF_CUDA(cudaStreamCreateWithFlags(&h->own, cudaStreamNonBlocking));
         h->stream = h->own;
-        upload_sub();
         h->ndof = (int64_t)(3 * g->nx + 1) * (3 * g->ny + 1);
         // finest level only until drf_mg_setup
         h->lv.resize(1);
         auto &F = h->lv[0];
         F.n = g->nx;
         F.nd = 3 * g->nx + 1;
-        up(F.K, std::vector<double>(h->H.levels.back().K, h->H.levels.back().K + 256));
+        up(F.K, transposed16(h->H.levels.back().K, 1));
         up(F.rho, h->H.levels.back().rho);
         F.binv.alloc(9 * 256);
         DRF_CUDA(cudaMemset(F.binv.p, 0, 9 * 256 * 8));
@@ -694,9 +1234,7 @@ int drf_bz_apply_Q(drf_bz *h, const double *xh, double *yh) {
         check_bz(h);
         DRF_CHECK(xh && yh, DRF_E_INVALID, "null argument");
         DRF_CUDA(cudaMemcpyAsync(h->z.p, xh, h->ndof * 8, cudaMemcpyHostToDevice, h->stream));
-        bz_apply_kernel<<<nblk(h->ndof), BS, 0, h->stream>>>(h->levdev(h->finest()), h->z.p, nullptr,
-                                                             h->q.p, 0, nullptr, nullptr);
-        DRF_LAUNCHED();
+        h->apply(h->finest(), h->z.p, nullptr, h->q.p, 0, nullptr, nullptr);
         DRF_CUDA(cudaMemcpyAsync(yh, h->q.p, h->ndof * 8, cudaMemcpyDeviceToHost, h->stream));
         DRF_CUDA(cudaStreamSynchronize(h->stream));
     });
@@ -713,11 +1251,18 @@ int drf_mg_setup(drf_bz *h, int coarsest_n, int pre, int post) {
             const BzLevelHost &Lh = h->H.levels[l];
             lv[l].n = Lh.n;
             lv[l].nd = Lh.nd;
-            up(lv[l].K, std::vector<double>(Lh.K, Lh.K + 256));
+            const std::vector<double> kt = transposed16(Lh.K, 1);
+            up(lv[l].K, kt);
             up(lv[l].rho, Lh.rho);
-            std::vector<double> bi = Lh.binv;
-            if (bi.empty()) bi.assign(9 * 256, 0.0);
+            std::vector<double> bi =
+                Lh.binv.empty() ? std::vector<double>(9 * 256, 0.0) : transposed16(Lh.binv.data(), 9);
             up(lv[l].binv, bi);
+            if (l > 0) {
+                std::vector<int> fc0, cf0;
+                std::vector<double> fw, cw;
+                transfer_tables(h->H.levels[l - 1].n, fc0, fw, cf0, cw);
+                up(lv[l].fc0, fc0); up(lv[l].fw, fw); up(lv[l].cf0, cf0); up(lv[l].cw, cw);
+            }
             if (l < nl - 1) {
                 const size_t n2 = (size_t)Lh.nd * Lh.nd;
                 lv[l].x.alloc(n2); lv[l].b.alloc(n2); lv[l].r.alloc(n2);
@@ -727,8 +1272,11 @@ int drf_mg_setup(drf_bz *h, int coarsest_n, int pre, int post) {
         }
         h->lv = std::move(lv);
         up(h->coarse, h->H.coarse_inv);
-        const int nc2 = h->lv[0].nd * h->lv[0].nd;
-        DRF_CHECK((size_t)nc2 * 8 <= 48 * 1024, DRF_E_UNSUPPORTED, "coarsest level too large");
+        DRF_CHECK(coarse_smem_doubles({h->lv[0].nd}, 0) * sizeof(double) <= COARSE_SMEM_MAX, DRF_E_UNSUPPORTED,
+                  "coarsest level too large");
+        DRF_CUDA(cudaFuncSetAttribute(bz_coarse_vcycle_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)COARSE_SMEM_MAX));
+        allow_smem<16, 4>();
         h->mg_ready = true;
         if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; h->graph_kind = -1; }
     });
@@ -802,9 +1350,7 @@ int drf_pcg_solve(drf_bz *h, const double *bh, double *xh, double tol, int maxit
         const double tol2 = tol * tol;
         DRF_CUDA(cudaMemcpyAsync(h->scal.p + S_TOL2, &tol2, 8, cudaMemcpyHostToDevice, h->stream));
         // r = b - Q x ; bb = b.b ; z = M r ; rz = r.z ; p = z
-        const LevelDev L = h->levdev(h->finest());
-        bz_apply_kernel<<<nblk(n), BS, 0, h->stream>>>(L, h->x.p, h->bs.p, h->r.p, 1, nullptr, nullptr);
-        DRF_LAUNCHED();
+        h->apply(h->finest(), h->x.p, h->bs.p, h->r.p, 1, nullptr, nullptr);
         dot_kernel<<<h->nparts(), BS, 0, h->stream>>>(n, h->bs.p, h->bs.p, h->part.p, nullptr);
         DRF_LAUNCHED();
         reduce_kernel<<<1, BS, 0, h->stream>>>(h->part.p, (int)h->nparts(), h->scal.p + S_BB);
@@ -906,9 +1452,10 @@ int drf_bz_jacobi_pcg_noalloc(const drf_bz_grid_desc *g, const double *d_b, doub
         double *part = q + NOALLOC_MAX_DOF, *scal = part + NOALLOC_PARTS;
         int *ctl = reinterpret_cast<int *>(scal + 16);
         cudaStream_t st = (cudaStream_t)stream;
-        upload_sub();
-        double Kh[256], alpha = 0.0;
-        bz_fine_operator(*g, Kh, &alpha);
+        double Kr[256], Kh[256], alpha = 0.0;
+        bz_fine_operator(*g, Kr, &alpha);
+        for (int a = 0; a < 16; ++a)
+            for (int k = 0; k < 16; ++k) Kh[k * 16 + a] = Kr[a * 16 + k];
         // every value the solve reads is written here first (the array keeps the last call's data)
         DRF_CUDA(cudaMemcpyAsync(K, Kh, sizeof(Kh), cudaMemcpyHostToDevice, st));
         fill_kernel<<<nblk(nd), BS, 0, st>>>(nd, 1.0, rho);
