@@ -32,6 +32,9 @@ def _setup_sigs():
         "drf_mg_setup": [vp, C.c_int, C.c_int, C.c_int], "drf_mg_apply": [vp, dp, dp],
         "drf_bz_precondition": [vp, C.c_int, dp, dp],
         "drf_pcg_solve": [vp, dp, dp, C.c_double, C.c_int, C.c_int, C.POINTER(C.c_int), dp, dp],
+        "drf_bz_constraints_apply": [vp, C.c_int, dp, dp],
+        "drf_bz_constrained_solve": [vp, C.c_int, C.c_int, C.c_double, C.c_int, C.c_double, dp,
+                                     C.POINTER(C.c_int), dp, dp],
     }
     for k, a in sigs.items():
         getattr(L, k).argtypes = a
@@ -100,6 +103,24 @@ class BezierSmoother:
         check(lib().drf_pcg_solve(self.h, dptr(bb) if bb is not None else None, dptr(x), tol,
                                   maxit, PRECOND[precond], C.byref(it), C.byref(rr), C.byref(ms)))
         return x, dict(iters=it.value, relres=rr.value, ms=ms.value)
+
+    def constraints_apply(self, x, edge_ngauss=4):
+        """C1 edge-constraint rows A x (2 n (n - 1) edge_ngauss values, vertical edges first)."""
+        n = self.desc.nx
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.empty(2 * n * (n - 1) * edge_ngauss)
+        check(lib().drf_bz_constraints_apply(self.h, edge_ngauss, dptr(x), dptr(y)))
+        return y
+
+    def solve_constrained(self, edge_ngauss=4, tol=1e-10, maxit=5000, inner="mg", inner_tol=1e-12):
+        """Constrained minimiser (CGCubicBezierBathymetrySmoother::solve with C1 edge
+        constraints): CG on the Schur complement A Q^-1 A^T, each Q^-1 a PCG solve."""
+        x = np.empty(self.ndof)
+        it, rr, ms = C.c_int(), C.c_double(), C.c_double()
+        check(lib().drf_bz_constrained_solve(self.h, edge_ngauss, PRECOND[inner], tol, maxit,
+                                             inner_tol, dptr(x), C.byref(it), C.byref(rr),
+                                             C.byref(ms)))
+        return x, dict(outer_iters=it.value, relres=rr.value, ms=ms.value)
 
 
 class BezierMultigridPreconditioner:

@@ -10,6 +10,7 @@
 // local dof k = i + 4 j (the reference's cubic dof order, include/bathymetry/cubic_bezier_basis_2d.hpp).
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <string>
 #include <cstring>
 #include <memory>
@@ -873,6 +874,110 @@ __global__ void fill_kernel(int64_t n, double v, double *a) {
     if (t < n) a[t] = v;
 }
 
+// ---------------------------------------------------------------- C1 edge constraints
+// Row (edge, q) of A: continuity of the normal derivative at Gauss point t_q of an interior
+// edge, the derivative of each element at the shared edge taken from its Bernstein form and
+// scaled by 1 / h: (3 / h) sum_j B_j(t_q) (2 x_line - x_line-1 - x_line+1) over the 4 control
+// points along the edge (CGCubicBezierDofManager::build_edge_derivative_constraints,
+// src/bathymetry/cg_cubic_bezier_dof_manager.cpp:319; coefficients / scale as in
+// assemble_A_edge_free, src/bathymetry/cg_cubic_bezier_bathymetry_smoother.cpp:798).
+// Row order: edges between (ex, ey) and (ex + 1, ey) first, ((ey (n - 1) + ex) ng + q), then
+// edges between (ex, ey) and (ex, ey + 1), n (n - 1) ng + ((ey n + ex) ng + q).
+constexpr int CONS_MAX_NG = 8;
+struct ConsDev {
+    int n, nd, ng;
+    double sx, sy;                 // 3 / dx, 3 / dy
+    double Bw[CONS_MAX_NG][4];     // B_j(t_q)
+};
+
+__global__ void __launch_bounds__(BS) bz_cons_apply_kernel(ConsDev C, const double *__restrict__ x,
+                                                           double *__restrict__ y) {
+    const int64_t nv = (int64_t)C.n * (C.n - 1) * C.ng;
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= 2 * nv) return;
+    double s = 0.0;
+    if (t < nv) {
+        const int q = (int)(t % C.ng), e = (int)(t / C.ng);
+        const int ex = e % (C.n - 1), ey = e / (C.n - 1);
+        const double *g = x + (3 * ex + 2) + (int64_t)C.nd * (3 * ey);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const double *r = g + (int64_t)C.nd * j;
+            s += C.Bw[q][j] * (2.0 * r[1] - r[0] - r[2]);
+        }
+        y[t] = C.sx * s;
+    } else {
+        const int64_t u = t - nv;
+        const int q = (int)(u % C.ng), e = (int)(u / C.ng);
+        const int ex = e % C.n, ey = e / C.n;
+        const double *g = x + 3 * ex + (int64_t)C.nd * (3 * ey + 2);
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+            s += C.Bw[q][i] * (2.0 * g[i + C.nd] - g[i] - g[i + 2 * (int64_t)C.nd]);
+        y[t] = C.sy * s;
+    }
+}
+
+// out = A^T lam (base == nullptr) or out = base - A^T lam, gathered per control point
+__global__ void __launch_bounds__(BS) bz_cons_applyT_kernel(ConsDev C, const double *__restrict__ lam,
+                                                            const double *__restrict__ base,
+                                                            double *__restrict__ out) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= (int64_t)C.nd * C.nd) return;
+    const int gi = (int)(t % C.nd), gj = (int)(t / C.nd);
+    const int64_t nv = (int64_t)C.n * (C.n - 1) * C.ng;
+    // the edge line (interior) whose 3-point stencil covers index g, and the stencil weight
+    auto line = [&](int g, int &w) {
+        const int r = g % 3;
+        int e;
+        if (r == 2) { e = (g - 2) / 3; w = -1; }
+        else if (r == 0) { e = g / 3 - 1; w = 2; }
+        else { e = g >= 4 ? (g - 4) / 3 : -1; w = -1; }
+        return (e >= 0 && e <= C.n - 2) ? e : -1;
+    };
+    double s = 0.0;
+    int w;
+    const int lx = line(gi, w);
+    if (lx >= 0) {
+        const int ey1 = min(gj / 3, C.n - 1), ey0 = (gj % 3 == 0 && gj > 0) ? gj / 3 - 1 : ey1;
+        double a = 0.0;
+        for (int ey = ey0; ey <= ey1; ++ey) {
+            const int j = gj - 3 * ey;
+            const double *l = lam + ((int64_t)ey * (C.n - 1) + lx) * C.ng;
+            for (int q = 0; q < C.ng; ++q) a += C.Bw[q][j] * l[q];
+        }
+        s += C.sx * w * a;
+    }
+    const int ly = line(gj, w);
+    if (ly >= 0) {
+        const int ex1 = min(gi / 3, C.n - 1), ex0 = (gi % 3 == 0 && gi > 0) ? gi / 3 - 1 : ex1;
+        double a = 0.0;
+        for (int ex = ex0; ex <= ex1; ++ex) {
+            const int i = gi - 3 * ex;
+            const double *l = lam + nv + ((int64_t)ly * C.n + ex) * C.ng;
+            for (int q = 0; q < C.ng; ++q) a += C.Bw[q][i] * l[q];
+        }
+        s += C.sy * w * a;
+    }
+    out[t] = base ? base[t] - s : s;
+}
+
+// lam += a p ; r -= a q
+__global__ void __launch_bounds__(BS) cg_update_kernel(int64_t n, double a, const double *__restrict__ p,
+                                                       const double *__restrict__ q, double *lam, double *r) {
+    for (int64_t t = blockIdx.x * (int64_t)BS + threadIdx.x; t < n; t += (int64_t)gridDim.x * BS) {
+        lam[t] += a * p[t];
+        r[t] -= a * q[t];
+    }
+}
+
+// p = r + beta p
+__global__ void __launch_bounds__(BS) xpay_kernel(int64_t n, double beta, const double *__restrict__ r,
+                                                  double *p) {
+    for (int64_t t = blockIdx.x * (int64_t)BS + threadIdx.x; t < n; t += (int64_t)gridDim.x * BS)
+        p[t] = r[t] + beta * p[t];
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------- allocation-free solve
@@ -905,6 +1010,9 @@ struct drf_bz {
     };
     std::vector<Lv> lv;
     bool mg_ready = false;
+    // color steps with at least this many elements use the element-per-thread Schwarz kernel
+    // (environment DRF_BZ_ELEM_SMOOTHER_MIN overrides, read at drf_mg_setup)
+    int64_t elem_min = ELEM_THREAD_MIN_ELEMS;
     drf_cnn *cnn = nullptr;
     double cnn_scale = 1.0;
     cudaGraphExec_t graph = nullptr;
@@ -993,7 +1101,7 @@ struct drf_bz {
             const int px = color & 1, py = color >> 1;
             const int ncx = (L.n - px + 1) / 2, ncy = (L.n - py + 1) / 2;
             const int64_t nce = (int64_t)ncx * ncy;
-            if (nce >= ELEM_THREAD_MIN_ELEMS)
+            if (nce >= elem_min)
                 color_solve<16, 4>(l, color, ncx, ncy, xl, bl, rl);
             else
                 color_solve_dof<8, 2>(l, color, ncx, ncy, xl, bl, rl);
@@ -1153,6 +1261,135 @@ void check_bz(drf_bz *h) { DRF_CHECK(h != nullptr, DRF_E_INVALID, "null smoother
 }  // namespace
 }  // namespace drf
 
+namespace drf {
+namespace {
+
+// PCG on Q x = bs from the x already on the device (bs, x set by the caller); returns the
+// iterations done. Scalars (rr, bb) are left in scal.
+int pcg_run(drf_bz *h, int kind, double tol, int maxit) {
+    const int64_t n = h->ndof;
+    PcgCtl c = h->pctl();
+    const int ctl0[3] = {0, 0, maxit};
+    DRF_CUDA(cudaMemcpyAsync(h->ctl.p, ctl0, sizeof(ctl0), cudaMemcpyHostToDevice, h->stream));
+    const double tol2 = tol * tol;
+    DRF_CUDA(cudaMemcpyAsync(h->scal.p + S_TOL2, &tol2, 8, cudaMemcpyHostToDevice, h->stream));
+    // r = b - Q x ; bb = b.b ; z = M r ; rz = r.z ; p = z
+    h->apply(h->finest(), h->x.p, h->bs.p, h->r.p, 1, nullptr, nullptr);
+    dot_kernel<<<h->nparts(), BS, 0, h->stream>>>(n, h->bs.p, h->bs.p, h->part.p, nullptr);
+    DRF_LAUNCHED();
+    reduce_kernel<<<1, BS, 0, h->stream>>>(h->part.p, (int)h->nparts(), h->scal.p + S_BB);
+    DRF_LAUNCHED();
+    // converged at start (r = 0) handled through the convergence kernel on r.r
+    dot_kernel<<<h->nparts(), BS, 0, h->stream>>>(n, h->r.p, h->r.p, h->part.p, nullptr);
+    DRF_LAUNCHED();
+    reduce_kernel<<<1, BS, 0, h->stream>>>(h->part.p, (int)h->nparts(), h->scal.p + S_RR);
+    DRF_LAUNCHED();
+    h->precondition(kind, h->r.p, h->z.p, nullptr);
+    dot_kernel<<<h->nparts(), BS, 0, h->stream>>>(n, h->r.p, h->z.p, h->part.p, nullptr);
+    DRF_LAUNCHED();
+    reduce_kernel<<<1, BS, 0, h->stream>>>(h->part.p, (int)h->nparts(), h->scal.p + S_RZ);
+    DRF_LAUNCHED();
+    p_update_kernel<<<h->nparts(), BS, 0, h->stream>>>(n, c, h->z.p, h->p.p, 1);
+    DRF_LAUNCHED();
+    double sc[S_NSLOT];
+    DRF_CUDA(cudaMemcpyAsync(sc, h->scal.p, sizeof(sc), cudaMemcpyDeviceToHost, h->stream));
+    DRF_CUDA(cudaStreamSynchronize(h->stream));
+    int done = 0, it = 0;
+    if (!(sc[S_RR] > tol2 * sc[S_BB])) done = 1;
+    // iterations in graph-captured chunks; converged iterations return early on the device
+    const int chunk = 8;
+    if (!done && maxit > 0) {
+        if (!h->graph || h->graph_kind != kind || h->graph_chunk != chunk) {
+            if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }
+            cudaGraph_t g = nullptr;
+            DRF_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+            try {
+                for (int k = 0; k < chunk; ++k) h->pcg_iteration(kind);
+            } catch (...) {
+                cudaStreamEndCapture(h->stream, &g);
+                if (g) cudaGraphDestroy(g);
+                throw;
+            }
+            DRF_CUDA(cudaStreamEndCapture(h->stream, &g));
+            cudaError_t e = cudaGraphInstantiate(&h->graph, g, 0);
+            cudaGraphDestroy(g);
+            DRF_CUDA(e);
+            h->graph_kind = kind;
+            h->graph_chunk = chunk;
+        }
+        int ctl[2] = {0, 0};
+        while (true) {
+            DRF_CUDA(cudaGraphLaunch(h->graph, h->stream));
+            launch_counter().fetch_add(1);
+            DRF_CUDA(cudaMemcpyAsync(ctl, h->ctl.p, sizeof(ctl), cudaMemcpyDeviceToHost, h->stream));
+            DRF_CUDA(cudaStreamSynchronize(h->stream));
+            if (ctl[0] || ctl[1] >= maxit) break;
+        }
+        it = ctl[1];
+    }
+    return it;
+}
+
+// n-point Gauss-Legendre nodes on [0, 1], ascending (Newton on P_n from cosine guesses)
+void gauss01(int n, double *t) {
+    for (int i = 0; i < n; ++i) {
+        double x = std::cos(3.14159265358979323846 * (i + 0.75) / (n + 0.5));
+        for (int it = 0; it < 100; ++it) {
+            double p0 = 1.0, p1 = x;
+            for (int k = 2; k <= n; ++k) {
+                const double p2 = ((2.0 * k - 1.0) * x * p1 - (k - 1.0) * p0) / k;
+                p0 = p1;
+                p1 = p2;
+            }
+            const double dp = n * (x * p1 - p0) / (x * x - 1.0);
+            const double d = p1 / dp;
+            x -= d;
+            if (std::abs(d) < 1e-16) break;
+        }
+        t[n - 1 - i] = 0.5 * (x + 1.0);
+    }
+}
+
+ConsDev make_cons(const drf_bz *h, int ng) {
+    DRF_CHECK(ng >= 1 && ng <= CONS_MAX_NG, DRF_E_INVALID, "edge_ngauss must be in 1..8");
+    DRF_CHECK(h->H.g.nx == h->H.g.ny && h->H.g.nx >= 2, DRF_E_UNSUPPORTED,
+              "edge constraints need a square grid of at least 2 x 2 elements");
+    ConsDev C;
+    std::memset(&C, 0, sizeof(C));
+    C.n = h->H.g.nx;
+    C.nd = 3 * C.n + 1;
+    C.ng = ng;
+    C.sx = 3.0 / h->H.dx;
+    C.sy = 3.0 / h->H.dy;
+    double t[CONS_MAX_NG];
+    gauss01(ng, t);
+    for (int q = 0; q < ng; ++q) {
+        const double u = t[q], v = 1.0 - u;
+        C.Bw[q][0] = v * v * v;
+        C.Bw[q][1] = 3.0 * u * v * v;
+        C.Bw[q][2] = 3.0 * u * u * v;
+        C.Bw[q][3] = u * u * u;
+    }
+    return C;
+}
+
+inline int64_t cons_rows(const ConsDev &C) { return 2 * (int64_t)C.n * (C.n - 1) * C.ng; }
+
+// a.b over n entries on the device, returned to the host (synchronous)
+double dev_dot(drf_bz *h, int64_t n, const double *a, const double *b, double *slot) {
+    dot_kernel<<<h->nparts(), BS, 0, h->stream>>>(n, a, b, h->part.p, nullptr);
+    DRF_LAUNCHED();
+    reduce_kernel<<<1, BS, 0, h->stream>>>(h->part.p, (int)h->nparts(), slot);
+    DRF_LAUNCHED();
+    double v = 0.0;
+    DRF_CUDA(cudaMemcpyAsync(&v, slot, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    DRF_CUDA(cudaStreamSynchronize(h->stream));
+    return v;
+}
+
+}  // namespace
+}  // namespace drf
+
 extern "C" {
 
 int drf_bz_create(const drf_bz_grid_desc *g, const double *dgauss, drf_bz **out) {
@@ -1277,6 +1514,8 @@ int drf_mg_setup(drf_bz *h, int coarsest_n, int pre, int post) {
         DRF_CUDA(cudaFuncSetAttribute(bz_coarse_vcycle_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)COARSE_SMEM_MAX));
         allow_smem<16, 4>();
+        const char *em = std::getenv("DRF_BZ_ELEM_SMOOTHER_MIN");
+        h->elem_min = em ? std::max<int64_t>(0, std::atoll(em)) : ELEM_THREAD_MIN_ELEMS;
         h->mg_ready = true;
         if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; h->graph_kind = -1; }
     });
@@ -1328,6 +1567,93 @@ int drf_mg_apply(drf_bz *h, const double *rh, double *zh) {
     });
 }
 
+int drf_bz_constraints_apply(drf_bz *h, int edge_ngauss, const double *xh, double *yh) {
+    return guard([&] {
+        check_bz(h);
+        DRF_CHECK(xh && yh, DRF_E_INVALID, "null argument");
+        const ConsDev C = make_cons(h, edge_ngauss);
+        const int64_t m = cons_rows(C);
+        DevBuf<double> y(m);
+        DRF_CUDA(cudaMemcpyAsync(h->z.p, xh, h->ndof * 8, cudaMemcpyHostToDevice, h->stream));
+        bz_cons_apply_kernel<<<nblk(m), BS, 0, h->stream>>>(C, h->z.p, y.p);
+        DRF_LAUNCHED();
+        DRF_CUDA(cudaMemcpyAsync(yh, y.p, m * 8, cudaMemcpyDeviceToHost, h->stream));
+        DRF_CUDA(cudaStreamSynchronize(h->stream));
+    });
+}
+
+int drf_bz_constrained_solve(drf_bz *h, int edge_ngauss, int inner_kind, double tol, int maxit,
+                             double inner_tol, double *xh, int *outer_iters, double *relres, double *ms) {
+    return guard([&] {
+        check_bz(h);
+        DRF_CHECK(xh && tol > 0 && maxit >= 0 && inner_tol > 0, DRF_E_INVALID, "bad arguments");
+        DRF_CHECK(inner_kind >= 0 && inner_kind <= 3, DRF_E_INVALID, "unknown preconditioner kind");
+        DRF_CHECK(inner_kind != 2 || h->mg_ready, DRF_E_INVALID, "multigrid preconditioner not set up");
+        DRF_CHECK(inner_kind != 3 || h->cnn, DRF_E_INVALID, "no learned preconditioner attached");
+        const ConsDev C = make_cons(h, edge_ngauss);
+        const int64_t m = cons_rows(C), n = h->ndof;
+        DevBuf<double> lam(m), rs(m), ps(m), qs(m), slot(1);
+        cudaEvent_t e0, e1;
+        DRF_CUDA(cudaEventCreate(&e0));
+        DRF_CUDA(cudaEventCreate(&e1));
+        DRF_CUDA(cudaEventRecord(e0, h->stream));
+        // x = Q^-1 bs from x = 0 (the apply_Qinv seam)
+        auto qinv = [&] {
+            zero_kernel<<<nblk(n), BS, 0, h->stream>>>(n, h->x.p, nullptr);
+            DRF_LAUNCHED();
+            pcg_run(h, inner_kind, inner_tol, 100000);
+        };
+        const unsigned gm = nblk(m), gn = nblk(n);
+        // rhs = A Q^-1 b ; lambda = 0 ; r = rhs ; p = r
+        DRF_CUDA(cudaMemcpyAsync(h->bs.p, h->b.p, n * 8, cudaMemcpyDeviceToDevice, h->stream));
+        qinv();
+        bz_cons_apply_kernel<<<gm, BS, 0, h->stream>>>(C, h->x.p, rs.p);
+        DRF_LAUNCHED();
+        DRF_CUDA(cudaMemsetAsync(lam.p, 0, m * 8, h->stream));
+        DRF_CUDA(cudaMemcpyAsync(ps.p, rs.p, m * 8, cudaMemcpyDeviceToDevice, h->stream));
+        const double rz_init = dev_dot(h, m, rs.p, rs.p, slot.p);
+        double rz = rz_init;
+        int it = 0;
+        if (rz_init > 1e-30) {
+            while (it < maxit) {
+                bz_cons_applyT_kernel<<<gn, BS, 0, h->stream>>>(C, ps.p, nullptr, h->bs.p);
+                DRF_LAUNCHED();
+                qinv();
+                bz_cons_apply_kernel<<<gm, BS, 0, h->stream>>>(C, h->x.p, qs.p);
+                DRF_LAUNCHED();
+                const double pSp = dev_dot(h, m, ps.p, qs.p, slot.p);
+                if (!(std::abs(pSp) >= 1e-30)) break;
+                cg_update_kernel<<<1024, BS, 0, h->stream>>>(m, rz / pSp, ps.p, qs.p, lam.p, rs.p);
+                DRF_LAUNCHED();
+                const double rz_new = dev_dot(h, m, rs.p, rs.p, slot.p);
+                ++it;
+                if (rz_new / rz_init < tol * tol) {
+                    rz = rz_new;
+                    break;
+                }
+                xpay_kernel<<<1024, BS, 0, h->stream>>>(m, rz_new / rz, rs.p, ps.p);
+                DRF_LAUNCHED();
+                rz = rz_new;
+            }
+        }
+        // x = Q^-1 (b - A^T lambda)
+        bz_cons_applyT_kernel<<<gn, BS, 0, h->stream>>>(C, lam.p, h->b.p, h->bs.p);
+        DRF_LAUNCHED();
+        qinv();
+        DRF_CUDA(cudaEventRecord(e1, h->stream));
+        DRF_CUDA(cudaMemcpyAsync(xh, h->x.p, n * 8, cudaMemcpyDeviceToHost, h->stream));
+        DRF_CUDA(cudaStreamSynchronize(h->stream));
+        float t = 0.f;
+        DRF_CUDA(cudaEventElapsedTime(&t, e0, e1));
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (outer_iters) *outer_iters = it;
+        if (relres) *relres = rz_init > 0 ? std::sqrt(rz / rz_init) : 0.0;
+        if (ms) *ms = t;
+        DRF_CHECK(std::isfinite(rz), DRF_E_NONFINITE, "Schur CG diverged (non-finite residual)");
+    });
+}
+
 int drf_pcg_solve(drf_bz *h, const double *bh, double *xh, double tol, int maxit, int kind,
                   int *iters, double *relres, double *ms) {
     return guard([&] {
@@ -1344,66 +1670,9 @@ int drf_pcg_solve(drf_bz *h, const double *bh, double *xh, double tol, int maxit
         else DRF_CUDA(cudaMemcpyAsync(h->bs.p, h->b.p, n * 8, cudaMemcpyDeviceToDevice, h->stream));
         DRF_CUDA(cudaMemcpyAsync(h->x.p, xh, n * 8, cudaMemcpyHostToDevice, h->stream));
         DRF_CUDA(cudaEventRecord(e0, h->stream));
-        PcgCtl c = h->pctl();
-        const int ctl0[3] = {0, 0, maxit};
-        DRF_CUDA(cudaMemcpyAsync(h->ctl.p, ctl0, sizeof(ctl0), cudaMemcpyHostToDevice, h->stream));
-        const double tol2 = tol * tol;
-        DRF_CUDA(cudaMemcpyAsync(h->scal.p + S_TOL2, &tol2, 8, cudaMemcpyHostToDevice, h->stream));
-        // r = b - Q x ; bb = b.b ; z = M r ; rz = r.z ; p = z
-        h->apply(h->finest(), h->x.p, h->bs.p, h->r.p, 1, nullptr, nullptr);
-        dot_kernel<<<h->nparts(), BS, 0, h->stream>>>(n, h->bs.p, h->bs.p, h->part.p, nullptr);
-        DRF_LAUNCHED();
-        reduce_kernel<<<1, BS, 0, h->stream>>>(h->part.p, (int)h->nparts(), h->scal.p + S_BB);
-        DRF_LAUNCHED();
-        // converged at start (r = 0) handled through the convergence kernel on r.r
-        dot_kernel<<<h->nparts(), BS, 0, h->stream>>>(n, h->r.p, h->r.p, h->part.p, nullptr);
-        DRF_LAUNCHED();
-        reduce_kernel<<<1, BS, 0, h->stream>>>(h->part.p, (int)h->nparts(), h->scal.p + S_RR);
-        DRF_LAUNCHED();
-        h->precondition(kind, h->r.p, h->z.p, nullptr);
-        dot_kernel<<<h->nparts(), BS, 0, h->stream>>>(n, h->r.p, h->z.p, h->part.p, nullptr);
-        DRF_LAUNCHED();
-        reduce_kernel<<<1, BS, 0, h->stream>>>(h->part.p, (int)h->nparts(), h->scal.p + S_RZ);
-        DRF_LAUNCHED();
-        p_update_kernel<<<h->nparts(), BS, 0, h->stream>>>(n, c, h->z.p, h->p.p, 1);
-        DRF_LAUNCHED();
-        double sc[S_NSLOT];
-        DRF_CUDA(cudaMemcpyAsync(sc, h->scal.p, sizeof(sc), cudaMemcpyDeviceToHost, h->stream));
-        DRF_CUDA(cudaStreamSynchronize(h->stream));
-        int done = 0, it = 0;
-        if (!(sc[S_RR] > tol2 * sc[S_BB])) done = 1;
-        // iterations in graph-captured chunks; converged iterations return early on the device
-        const int chunk = 8;
-        if (!done && maxit > 0) {
-            if (!h->graph || h->graph_kind != kind || h->graph_chunk != chunk) {
-                if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }
-                cudaGraph_t g = nullptr;
-                DRF_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-                try {
-                    for (int k = 0; k < chunk; ++k) h->pcg_iteration(kind);
-                } catch (...) {
-                    cudaStreamEndCapture(h->stream, &g);
-                    if (g) cudaGraphDestroy(g);
-                    throw;
-                }
-                DRF_CUDA(cudaStreamEndCapture(h->stream, &g));
-                cudaError_t e = cudaGraphInstantiate(&h->graph, g, 0);
-                cudaGraphDestroy(g);
-                DRF_CUDA(e);
-                h->graph_kind = kind;
-                h->graph_chunk = chunk;
-            }
-            int ctl[2] = {0, 0};
-            while (true) {
-                DRF_CUDA(cudaGraphLaunch(h->graph, h->stream));
-                launch_counter().fetch_add(1);
-                DRF_CUDA(cudaMemcpyAsync(ctl, h->ctl.p, sizeof(ctl), cudaMemcpyDeviceToHost, h->stream));
-                DRF_CUDA(cudaStreamSynchronize(h->stream));
-                if (ctl[0] || ctl[1] >= maxit) break;
-            }
-            it = ctl[1];
-        }
+        const int it = pcg_run(h, kind, tol, maxit);
         DRF_CUDA(cudaEventRecord(e1, h->stream));
+        double sc[S_NSLOT];
         DRF_CUDA(cudaMemcpyAsync(sc, h->scal.p, sizeof(sc), cudaMemcpyDeviceToHost, h->stream));
         DRF_CUDA(cudaMemcpyAsync(xh, h->x.p, n * 8, cudaMemcpyDeviceToHost, h->stream));
         DRF_CUDA(cudaStreamSynchronize(h->stream));

@@ -185,6 +185,25 @@ int drf_bz_precondition(drf_bz *h, int kind, const double *r, double *z);
 int drf_pcg_solve(drf_bz *h, const double *b, double *x, double tol, int maxit, int kind,
                   int *iters, double *relres, double *ms);
 
+/* C1 continuity rows y = A x: the normal derivative matched at edge_ngauss (1..8) Gauss points
+ * of every interior edge (CGCubicBezierDofManager::build_edge_derivative_constraints,
+ * src/bathymetry/cg_cubic_bezier_dof_manager.cpp:319, scaled by 1/h as assemble_A_edge_free,
+ * src/bathymetry/cg_cubic_bezier_bathymetry_smoother.cpp:798). Square grids. y has
+ * 2 n (n - 1) edge_ngauss rows: edges between (ex, ey) and (ex + 1, ey) first, row
+ * (ey (n - 1) + ex) edge_ngauss + q, then edges between (ex, ey) and (ex, ey + 1), row
+ * n (n - 1) edge_ngauss + (ey n + ex) edge_ngauss + q. Host buffers. */
+int drf_bz_constraints_apply(drf_bz *h, int edge_ngauss, const double *x, double *y);
+
+/* Constrained minimiser under the C1 rows: CG on the Schur complement S = A Q^-1 A^T with
+ * rhs A Q^-1 b, then x = Q^-1 (b - A^T lambda)
+ * (CGCubicBezierBathymetrySmoother::solve_with_constraints_iterative,
+ * src/bathymetry/cg_cubic_bezier_bathymetry_smoother.cpp:305, Schur preconditioner None:
+ * stop when r.r / r0.r0 < tol^2). Every Q^-1 is a PCG solve from zero to inner_tol with
+ * preconditioner inner_kind (as drf_pcg_solve). b is the assembled right-hand side. x: host
+ * output; *outer_iters, *relres = sqrt(r.r / r0.r0), *ms = device time. */
+int drf_bz_constrained_solve(drf_bz *h, int edge_ngauss, int inner_kind, double tol, int maxit,
+                             double inner_tol, double *x, int *outer_iters, double *relres, double *ms);
+
 /* ------------------------------------------------------------------ learned preconditioner
  * No counterpart in the reference. A 4-layer conv3x3 network (BF16, FP32 accumulation) on
  * 3x3 superpixels of the control-point grid, trained on the GPU on (residual, error) pairs

@@ -66,3 +66,60 @@ def test_pcg_zero_rhs_and_maxit():
     assert info["iters"] == 0 and np.all(x == 0)
     x, info = g.solve("none", tol=1e-14, maxit=3)
     assert info["iters"] == 3
+
+
+def test_vcycle_element_thread_smoother_matches_oracle(monkeypatch):
+    # the element-per-thread Schwarz kernel (large levels) on every grid-wide level
+    monkeypatch.setenv("DRF_BZ_ELEM_SMOOTHER_MIN", "1")
+    g, o = pair(32)
+    g.mg_setup(2)
+    o.mg_setup(2)
+    r = np.random.default_rng(4).standard_normal(g.ndof)
+    assert rel(g.mg_apply(r), o.vcycle(r)) < 1e-11
+
+
+def _oracle_row_order(n, ng):
+    """GPU row index of each oracle constraint row (oracle: per element, right edge then top)."""
+    nv = n * (n - 1) * ng
+    out = []
+    for ey in range(n):
+        for ex in range(n):
+            if ex + 1 < n:
+                out += [(ey * (n - 1) + ex) * ng + q for q in range(ng)]
+            if ey + 1 < n:
+                out += [nv + (ey * n + ex) * ng + q for q in range(ng)]
+    return np.array(out)
+
+
+@pytest.mark.parametrize("ng", [2, 4])
+def test_constraint_rows_match_oracle(ng):
+    n = 8
+    g, o = pair(n)
+    A = o.constraints(ng)
+    x = np.random.default_rng(5).standard_normal(g.ndof)
+    y = g.constraints_apply(x, ng)
+    assert y.shape[0] == A.shape[0]
+    assert rel(y[_oracle_row_order(n, ng)], A @ x) < 1e-12
+
+
+@pytest.mark.parametrize("inner", ["mg", "jacobi"])
+def test_constrained_solve_doc_known_answer(inner):
+    # docs/cg_bezier_solver_verification.md:32-39: objective 25.235, ||x|| 61.715, data
+    # residual 0.1398 for the 16 x 16 sin-exp case, against the oracle's direct Schur solve
+    from test_oracle_bz import GOLD, doc_case, schur_solve
+    k = GOLD["bezier_doc_16x16"]
+    o = doc_case()
+    X, Y = O.gauss_points(16, 16, 0, 0, 1000.0, 1000.0)
+    d = np.exp(np.sin(2 * np.pi * X / 1000.0) * np.sin(2 * np.pi * Y / 1000.0))
+    g = BezierSmoother(16, 16, 1000.0, 1000.0, d, lam=1.0, ridge_epsilon=1e-4)
+    if inner == "mg":
+        g.mg_setup(2)
+    x, info = g.solve_constrained(4, tol=1e-10, inner=inner, inner_tol=1e-13)
+    xo, A = schur_solve(o)
+    assert info["relres"] < 1e-10 and info["outer_iters"] > 0
+    assert rel(x, xo) < 1e-7
+    obj, reg, dat = o.objective(x)
+    assert abs(obj - k["objective"]) < 6e-4
+    assert abs(np.linalg.norm(x) - k["x_norm"]) < 6e-4
+    assert abs(dat - k["data_residual"]) < 6e-5
+    assert np.abs(A @ x).max() < 1e-7
