@@ -241,6 +241,53 @@ int drf_bz_set_cnn(drf_bz *h, drf_cnn *net, double out_scale);
 int drf_bz_jacobi_pcg_noalloc(const drf_bz_grid_desc *grid, const double *d_b, double *d_x,
                               double tol, int maxit, void *stream, int *iters, double *relres);
 
+/* ------------------------------------------------------------------ mortars (non-conforming faces)
+ * MortarSpace (src/dg/mortar.cpp:13; include/dg/mortar.hpp:29) and the non-conforming face flux
+ * of DG3DIntegration (compute_interface_flux_nonconforming, src/dg/operators_3d.cpp:345) for
+ * hexahedral LGL elements of one order p (1..5): mortar order p, (2p+1)^2 Gauss-Legendre
+ * mortar points on the coarse face, P = M^-1 B and L = B^T for the coarse face and each fine
+ * face (fine coupling over the mortar points inside the closed sub-face), scalar flux at the
+ * mortar nodes, lifts L_c M^-1 F to the coarse face and -L_f M^-1 F to the fine faces.
+ * Connection types are FaceConnectionType (include/dg/face_connection.hpp:15); face f has its
+ * normal along axis f / 2, positive when f is odd; face node (it, jt) is the volume node with
+ * the normal index on the face and the two tangential indices in axis order. */
+enum {
+    DRF_MORTAR_SAME_LEVEL = 0,
+    DRF_MORTAR_FINE_2X1 = 1,
+    DRF_MORTAR_FINE_1X2 = 2,
+    DRF_MORTAR_FINE_3_2PLUS1 = 3,
+    DRF_MORTAR_FINE_3_1PLUS2 = 4,
+    DRF_MORTAR_FINE_2X2 = 5
+};
+/* scalar numerical fluxes for u_t + div(a u) = 0 (include/flux/numerical_flux.hpp):
+ * CentralFlux (:244), UpwindFlux (:264), LaxFriedrichsFlux (:222) with speed |a.n| */
+enum { DRF_MORTAR_FLUX_CENTRAL = 0, DRF_MORTAR_FLUX_UPWIND = 1, DRF_MORTAR_FLUX_LF = 2 };
+
+typedef struct drf_mortar drf_mortar;
+
+/* Operators of one connection type (MortarSpace::build_projection_operators,
+ * src/dg/mortar.cpp:80), row-major, nm = (p+1)^2: M, Minv, Pc (nm x nm), Lc (nm x nm), Pf and Lf
+ * (nfine x nm x nm). Any output may be NULL. */
+int drf_mortar_ops(int order, int type, double *M, double *Minv, double *Pc, double *Lc, double *Pf,
+                   double *Lf, int *nfine);
+
+/* n_if interfaces: type[i], coarse_elem[i], coarse_face[i], and 4 slots per interface of
+ * fine_elem / fine_face (the type's first 1..4 are used, in sub-face order of
+ * compute_subface_bounds, src/dg/mortar.cpp:27). Elements index a state of n_elem x (p+1)^3
+ * values (element-major, node i + (p+1)(j + (p+1)k)). */
+int drf_mortar_create(int order, int64_t n_if, const int *type, const int64_t *coarse_elem,
+                      const int *coarse_face, const int64_t *fine_elem, const int *fine_face,
+                      int64_t n_elem, drf_mortar **out);
+int drf_mortar_destroy(drf_mortar *h);
+int drf_mortar_set_stream(drf_mortar *h, void *stream);
+
+/* rhs += the mortar flux lifts of every interface, accumulated in interface order (coarse face,
+ * then the fine faces), for the scalar field U and advection velocity a[3]. Host buffers. */
+int drf_mortar_apply(drf_mortar *h, int flux_kind, const double *a, const double *U, double *rhs);
+/* The same on device buffers, enqueued on the handle's stream. */
+int drf_mortar_apply_device(drf_mortar *h, int flux_kind, const double *a, const double *d_U,
+                            double *d_rhs);
+
 #ifdef __cplusplus
 }
 #endif

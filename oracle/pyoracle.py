@@ -314,3 +314,51 @@ def cnn_forward_backward(params, X, T=None, round_bf16=True):
                                       _p(_c(T)) if T is not None else None, _p(out),
                                       _p(grad) if grad is not None else None, int(round_bf16))
     return out, grad, loss
+
+
+# ----------------------------------------------------------------------------- mortars
+MORTAR_NUM_FINE = {0: 1, 1: 2, 2: 2, 3: 3, 4: 3, 5: 4}  # FaceConnectionType 0..5
+
+
+def mortar_ops(order, ctype):
+    """Mortar operators of one connection type (MortarSpace, src/dg/mortar.cpp:80)."""
+    L = lib()
+    L.orc_mortar_ops.argtypes = [C.c_int, C.c_int] + [_dp] * 6
+    nm = (order + 1) ** 2
+    nfine = MORTAR_NUM_FINE[ctype]
+    M, Minv, Pc, Lc = (np.empty((nm, nm)) for _ in range(4))
+    Pf, Lf = np.empty((nfine, nm, nm)), np.empty((nfine, nm, nm))
+    r = L.orc_mortar_ops(order, ctype, _p(M), _p(Minv), _p(Pc), _p(Lc), _p(Pf), _p(Lf))
+    if r < 0:
+        raise ValueError("oracle: bad mortar arguments")
+    return dict(M=M, Minv=Minv, Pc=Pc, Lc=Lc, Pf=Pf, Lf=Lf)
+
+
+def mortar_apply(order, ifaces, flux_kind, a, U, rhs=None):
+    """rhs + the non-conforming face fluxes of the interfaces (list of (type, coarse_elem,
+    coarse_face, [fine_elems], [fine_faces])) for the scalar field U (n_elem x (order+1)^3)."""
+    L = lib()
+    L.orc_mortar_apply.argtypes = [C.c_int, C.c_long, C.c_void_p, C.c_void_p, C.c_void_p,
+                                   C.c_void_p, C.c_void_p, C.c_int, _dp, C.c_long, _dp, _dp]
+    arr = mortar_arrays(ifaces)
+    U = _c(U)
+    out = np.zeros_like(U) if rhs is None else _c(rhs).copy()
+    ptr = lambda x: x.ctypes.data_as(C.c_void_p)
+    r = L.orc_mortar_apply(order, len(ifaces), ptr(arr["type"]), ptr(arr["ce"]), ptr(arr["cf"]),
+                           ptr(arr["fe"]), ptr(arr["ff"]), flux_kind, _p(_c(a)), U.shape[0],
+                           _p(U), _p(out))
+    if r < 0:
+        raise ValueError("oracle: bad mortar arguments")
+    return out
+
+
+def mortar_arrays(ifaces):
+    """Flat arrays (type, coarse elem/face, 4 fine elems/faces per interface, -1 padded)."""
+    n = len(ifaces)
+    out = dict(type=np.zeros(n, np.int32), ce=np.zeros(n, np.int64), cf=np.zeros(n, np.int32),
+               fe=-np.ones((n, 4), np.int64), ff=-np.ones((n, 4), np.int32))
+    for i, (t, ce, cf, fe, ff) in enumerate(ifaces):
+        out["type"][i], out["ce"][i], out["cf"][i] = t, ce, cf
+        out["fe"][i, :len(fe)] = fe
+        out["ff"][i, :len(ff)] = ff
+    return out
