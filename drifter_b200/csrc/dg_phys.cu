@@ -114,25 +114,74 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t phase) {
     return false;
 }
 
+// Threads per stage CTA at most (pencils are strided over the block); two CTAs of this size
+// share an SM (the register budget the kernel is compiled for: 65536 / (2 * 448) = 73).
+constexpr int STAGE_MAX_THREADS = 448;
+
+// Two prognostic variables of one node processed together ((Hu, Hv) and (HT, HS) share every
+// 1D operator entry and every face speed). FP32 pairs use Blackwell's packed FP32x2
+// instructions (one instruction for both lanes, IEEE single rounding per lane, as the scalar
+// form); FP64 pairs are two scalar operations.
 template <typename T>
-__device__ __forceinline__ T sel4(const T (&x)[4], int v) {
-    return v == 0 ? x[0] : (v == 1 ? x[1] : (v == 2 ? x[2] : x[3]));
+struct P2 {
+    T x, y;
+};
+template <typename T>
+__device__ __forceinline__ P2<T> bc(T s) { return {s, s}; }
+
+__device__ __forceinline__ P2<float> p2fma(P2<float> a, P2<float> b, P2<float> c) {
+    P2<float> r;
+    asm("{ .reg .b64 ra, rb, rc, rd; mov.b64 ra, {%2, %3}; mov.b64 rb, {%4, %5}; mov.b64 rc, {%6, %7};"
+        " fma.rn.f32x2 rd, ra, rb, rc; mov.b64 {%0, %1}, rd; }"
+        : "=f"(r.x), "=f"(r.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
+    return r;
 }
+__device__ __forceinline__ P2<float> p2mul(P2<float> a, P2<float> b) {
+    P2<float> r;
+    asm("{ .reg .b64 ra, rb, rd; mov.b64 ra, {%2, %3}; mov.b64 rb, {%4, %5};"
+        " mul.rn.f32x2 rd, ra, rb; mov.b64 {%0, %1}, rd; }"
+        : "=f"(r.x), "=f"(r.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return r;
+}
+__device__ __forceinline__ P2<float> p2add(P2<float> a, P2<float> b) {
+    P2<float> r;
+    asm("{ .reg .b64 ra, rb, rd; mov.b64 ra, {%2, %3}; mov.b64 rb, {%4, %5};"
+        " add.rn.f32x2 rd, ra, rb; mov.b64 {%0, %1}, rd; }"
+        : "=f"(r.x), "=f"(r.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return r;
+}
+__device__ __forceinline__ P2<float> p2sub(P2<float> a, P2<float> b) {
+    P2<float> r;
+    asm("{ .reg .b64 ra, rb, rd; mov.b64 ra, {%2, %3}; mov.b64 rb, {%4, %5};"
+        " sub.rn.f32x2 rd, ra, rb; mov.b64 {%0, %1}, rd; }"
+        : "=f"(r.x), "=f"(r.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return r;
+}
+__device__ __forceinline__ P2<double> p2fma(P2<double> a, P2<double> b, P2<double> c) {
+    return {fma(a.x, b.x, c.x), fma(a.y, b.y, c.y)};
+}
+__device__ __forceinline__ P2<double> p2mul(P2<double> a, P2<double> b) { return {a.x * b.x, a.y * b.y}; }
+__device__ __forceinline__ P2<double> p2add(P2<double> a, P2<double> b) { return {a.x + b.x, a.y + b.y}; }
+__device__ __forceinline__ P2<double> p2sub(P2<double> a, P2<double> b) { return {a.x - b.x, a.y - b.y}; }
 
 // Shared-memory plan of the stage kernel for one water column (ncn = nz*(N+1)^3 nodes):
 //   two mbarriers (16 B), sQ[4][ncn] state, sRes[4][ncn] LSRK 2N register, sR[4][ncn]
-//   right-hand side (sR[0] first holds the horizontal divergence and the layer integrals),
-//   sOm[ncn] omega, per layer x 2D-node scratch, and the column's 2D fields.
+//   right-hand side, sD[ncn] horizontal divergence -> layer integrals (in place), per layer x
+//   2D-node increments, the column's 2D fields (1/H, H, eta) and its pressure-gradient rows.
 inline size_t stage_smem_bytes(int nz, int np, size_t tsz) {
     const int np2 = np * np, ncn = nz * np2 * np;
-    return 16 + ((size_t)13 * ncn + (size_t)2 * nz * np2 + 4 * np2) * tsz;
+    return 16 + ((size_t)13 * ncn + (size_t)2 * nz * np2 + 5 * np2) * tsz;
 }
 
 // One CTA per water column; work is organised in pencils (lines of N+1 nodes) so every
 // thread applies the 1D operators to registers, with the operator entries read as
 // warp-uniform constants: x pencils (j,k,layer), y pencils (i,k,layer), z pencils (i,j,layer).
 template <typename T, int NP>
-__global__ void __launch_bounds__(512) dg3d_stage_kernel(StageArgs<T> a) {
+__global__ void __launch_bounds__(STAGE_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) dg3d_stage_kernel(StageArgs<T> a) {
     constexpr int NP2 = NP * NP, NP3 = NP2 * NP, N = NP - 1;
     using B = BT<T>;
     const Geo &G = a.G;
@@ -144,11 +193,11 @@ __global__ void __launch_bounds__(512) dg3d_stage_kernel(StageArgs<T> a) {
     T *sQ = reinterpret_cast<T *>(smem_raw + 16);  // [4][ncn]
     T *sRes = sQ + 4 * ncn;                        // [4][ncn]
     T *sR = sRes + 4 * ncn;                        // [4][ncn]
-    T *sOm = sR + 4 * ncn;                         // [ncn]
-    T *sL1 = sOm + ncn;                            // [nz][NP2]
-    T *sL2 = sL1 + nz * NP2;                       // [nz][NP2]
-    T *sIH = sL2 + nz * NP2, *sHt = sIH + NP2, *sEt = sHt + NP2, *sItot = sEt + NP2;
-    T *sD = sR;                                    // divergence / layer integrals
+    T *sD = sR + 4 * ncn;                          // [ncn] divergence -> layer integrals
+    T *sL1 = sD + ncn;                             // [nz][NP2] column increments (Hu)
+    T *sL2 = sL1 + nz * NP2;                       // [nz][NP2] column increments (Hv)
+    T *sIH = sL2 + nz * NP2, *sHt = sIH + NP2, *sEt = sHt + NP2;
+    T *sPx = sEt + NP2, *sPy = sPx + NP2;          // g H d(eta)/dx, g H d(eta)/dy per 2D node
     __shared__ int s_ok;
 
     const double tnow = a.tdev[0] + a.toff;
@@ -183,11 +232,22 @@ __global__ void __launch_bounds__(512) dg3d_stage_kernel(StageArgs<T> a) {
         }
     }
     for (int t = threadIdx.x; t < NP2; t += blockDim.x) {
-        const double e = a.eta[(size_t)c * NP2 + t];
+        const double *ec = a.eta + (size_t)c * NP2;
+        const double e = ec[t];
         const double H = e + a.h[(size_t)c * NP2 + t];
         sEt[t] = (T)e;
         sHt[t] = (T)H;
         sIH[t] = (T)(1.0 / H);
+        // the column's pressure-gradient rows g H d(eta)/dx, g H d(eta)/dy (shared by its layers)
+        const int i = t % NP, j = t / NP;
+        T gex = 0, gey = 0;
+#pragma unroll
+        for (int m = 0; m < NP; ++m) {
+            gex += B::D(i * NP + m) * (T)ec[m + NP * j];
+            gey += B::D(j * NP + m) * (T)ec[i + NP * m];
+        }
+        sPx[t] = g * (T)H * cx * gex;
+        sPy[t] = g * (T)H * cy * gey;
     }
     if (threadIdx.x == 0) s_ok = a.bulk ? (int)mbar_wait(&bars[0], 0) : 1;
     __syncthreads();
@@ -201,11 +261,15 @@ __global__ void __launch_bounds__(512) dg3d_stage_kernel(StageArgs<T> a) {
             sQ[n] += (T)a.corrU[(size_t)c * NP2 + an];
             sQ[ncn + n] += (T)a.corrV[(size_t)c * NP2 + an];
         }
+        __syncthreads();
     }
-    __syncthreads();
 
     // state across horizontal side s at own node (ez,i,j,k): q+ (4), eta+, H+
-    auto outside = [&](int s, int ez, int i, int j, int k, int n, T qp[4], T &etap, T &Hp) {
+    struct Side {
+        T q[4], e, H;
+    };
+    auto outside = [&](int s, int ez, int i, int j, int k, int n) -> Side {
+        Side o;
         int nc = -1, ni = i, nj = j;
         if (s == 0 && ex > 0) { nc = c - 1; ni = N; }
         if (s == 1 && ex < G.nx - 1) { nc = c + 1; ni = 0; }
@@ -216,74 +280,150 @@ __global__ void __launch_bounds__(512) dg3d_stage_kernel(StageArgs<T> a) {
             const size_t nb = (size_t)nc * ncn + (size_t)ez * NP3 + ni + NP * (nj + NP * k);
             const size_t n2 = (size_t)nc * NP2 + ni + NP * nj;
 #pragma unroll
-            for (int v = 0; v < 4; ++v) qp[v] = a.qin[v][nb];
+            for (int v = 0; v < 4; ++v) o.q[v] = a.qin[v][nb];
             if (a.corrU) {
-                qp[0] += (T)a.corrU[n2];
-                qp[1] += (T)a.corrV[n2];
+                o.q[0] += (T)a.corrU[n2];
+                o.q[1] += (T)a.corrV[n2];
             }
             const double e = a.eta[n2];
-            etap = (T)e;
-            Hp = (T)(e + a.h[n2]);
-            return;
+            o.e = (T)e;
+            o.H = (T)(e + a.h[n2]);
+            return o;
         }
-        if (G.bc[s] == DRF_BC_TIDE) {
-            etap = etide;
-            Hp = etide + (T)a.h[(size_t)c * NP2 + an];
-            const T r = Hp * sIH[an];
+        const int bcs = s == 0 ? G.bc[0] : (s == 1 ? G.bc[1] : (s == 2 ? G.bc[2] : G.bc[3]));
+        if (bcs == DRF_BC_TIDE) {
+            o.e = etide;
+            o.H = etide + (T)a.h[(size_t)c * NP2 + an];
+            const T r = o.H * sIH[an];
 #pragma unroll
-            for (int v = 0; v < 4; ++v) qp[v] = sQ[v * ncn + n] * r;
+            for (int v = 0; v < 4; ++v) o.q[v] = sQ[v * ncn + n] * r;
         } else {
-            etap = sEt[an];
-            Hp = sHt[an];
+            o.e = sEt[an];
+            o.H = sHt[an];
 #pragma unroll
-            for (int v = 0; v < 4; ++v) qp[v] = sQ[v * ncn + n];
-            if (s <= 1) qp[0] = -qp[0]; else qp[1] = -qp[1];
+            for (int v = 0; v < 4; ++v) o.q[v] = sQ[v * ncn + n];
+            if (s <= 1) o.q[0] = -o.q[0]; else o.q[1] = -o.q[1];
         }
+        return o;
     };
 
-    // ---- horizontal divergence of (Hu, Hv) with central face flux: x pencils (both face
-    // neighbours fetched up front so their latencies overlap)
+    // ---- horizontal passes. Each pencil (a line of N+1 nodes) gives its direction's part of
+    // (1) the horizontal divergence of (Hu, Hv) with a central face flux, which feeds omega, and
+    // (2) the right-hand side: advection, pressure, horizontal diffusion and the LF face terms,
+    // with the variables processed in pairs (Hu, Hv), (HT, HS). Both face neighbours are
+    // fetched up front so their latencies overlap.
+    const T nh = (T)G.nu_h;
+    const bool hdiff = G.nu_h > 0.0;
+    // one horizontal pencil: axis 0 (x, sides 0/1) or 1 (y, sides 2/3), a compile-time
+    // constant of each instance; nodes e0 + st*m
+    auto hpass = [&](auto AX, int ez, int e0, int st, int iy, int jx) {
+        constexpr int axis = decltype(AX)::value;
+        const T cd = axis == 0 ? cx : cy, Ld = axis == 0 ? Lx : Ly;
+        // own-node indices (i, j, k) of the pencil's two end nodes
+        const int k = (e0 % NP3) / NP2;
+        const Side o0 = axis == 0 ? outside(0, ez, 0, iy, k, e0) : outside(2, ez, jx, 0, k, e0);
+        const Side oN = axis == 0 ? outside(1, ez, N, iy, k, e0 + N) : outside(3, ez, jx, N, k, e0 + NP * N);
+        const T ep0 = o0.e, epN = oN.e, Hp0 = o0.H, HpN = oN.H;
+        // the neighbours' momentum normal to this pencil's faces and the two variable pairs
+        const T qn0 = axis == 0 ? o0.q[0] : o0.q[1], qnN = axis == 0 ? oN.q[0] : oN.q[1];
+        const P2<T> p0a = {o0.q[0], o0.q[1]}, p0b = {o0.q[2], o0.q[3]};
+        const P2<T> pNa = {oN.q[0], oN.q[1]}, pNb = {oN.q[2], oN.q[3]};
+        // 2D node of pencil node m: x pencil (m, iy), y pencil (jx, m)
+        auto an2 = [&](int m) { return axis == 0 ? m + NP * iy : jx + NP * m; };
+        P2<T> q01[NP];
+        T ih[NP], un[NP];
+#pragma unroll
+        for (int m = 0; m < NP; ++m) {
+            q01[m] = {sQ[e0 + st * m], sQ[ncn + e0 + st * m]};
+            ih[m] = sIH[an2(m)];
+            un[m] = (axis == 0 ? q01[m].x : q01[m].y) * ih[m];  // velocity along the pencil
+        }
+        // (1) divergence part, central face flux on the normal momentum
+        {
+            const T qa = qn0, qb = qnN;
+#pragma unroll
+            for (int i = 0; i < NP; ++i) {
+                const T q0 = axis == 0 ? q01[0].x : q01[0].y, qN = axis == 0 ? q01[N].x : q01[N].y;
+                T s = 0;
+#pragma unroll
+                for (int m = 0; m < NP; ++m) s += B::D(i * NP + m) * (axis == 0 ? q01[m].x : q01[m].y);
+                T d = cd * s;
+                if (i == 0) d += Ld * (T(0.5) * (q0 + qa) * T(-1) - q0 * T(-1));
+                if (i == N) d += Ld * (T(0.5) * (qN + qb) - qN);
+                if (axis == 0) sD[e0 + st * i] = d;
+                else sD[e0 + st * i] += d;
+            }
+        }
+        // normal velocities and LF speeds at both ends
+        const T unm0 = -un[0], unp0 = -qn0 / Hp0;
+        const T lam0 = fmax(fabs(unm0), fabs(unp0));
+        const T unmN = un[N], unpN = qnN / HpN;
+        const T lamN = fmax(fabs(unmN), fabs(unpN));
+        // (2) right-hand side, one variable pair at a time
+#pragma unroll 1
+        for (int pr = 0; pr < 2; ++pr) {
+            P2<T> q[NP], f[NP];
+#pragma unroll
+            for (int m = 0; m < NP; ++m) {
+                q[m] = {sQ[2 * pr * ncn + e0 + st * m], sQ[(2 * pr + 1) * ncn + e0 + st * m]};
+                f[m] = p2mul(q[m], bc(un[m]));
+            }
+            const P2<T> qp0v = pr == 0 ? p0a : p0b;
+            const P2<T> qpNv = pr == 0 ? pNa : pNb;
+#pragma unroll
+            for (int i = 0; i < NP; ++i) {
+                P2<T> s = bc(T(0));
+#pragma unroll
+                for (int m = 0; m < NP; ++m) s = p2fma(bc(B::D(i * NP + m)), f[m], s);
+                P2<T> r = p2mul(bc(-cd), s);
+                const int a2 = an2(i);
+                const T Hh = sHt[a2];
+                if (pr == 0) {
+                    if (axis == 0) r.x -= sPx[a2];
+                    else r.y -= sPy[a2];
+                    if (hdiff) {
+                        P2<T> dd = bc(T(0));
+#pragma unroll
+                        for (int m = 0; m < NP; ++m) dd = p2fma(bc(B::D2(i * NP + m)), p2mul(q[m], bc(ih[m])), dd);
+                        r = p2fma(bc(nh * Hh), p2mul(bc(cd * cd), dd), r);
+                    }
+                }
+                if (i == 0 || i == N) {
+                    const P2<T> qm = q[i], qpv = i == 0 ? qp0v : qpNv;
+                    const T unm = i == 0 ? unm0 : unmN, unp = i == 0 ? unp0 : unpN;
+                    const T lam = i == 0 ? lam0 : lamN;
+                    const P2<T> fs = p2sub(p2mul(bc(T(0.5)), p2add(p2mul(qm, bc(unm)), p2mul(qpv, bc(unp)))),
+                                           p2mul(bc(T(0.5) * lam), p2sub(qpv, qm)));
+                    r = p2fma(bc(-Ld), p2sub(fs, p2mul(qm, bc(unm))), r);
+                    if (pr == 0) {
+                        const T nn = i == 0 ? T(-1) : T(1);
+                        const T ep = i == 0 ? ep0 : epN;
+                        const T pf = Ld * (g * Hh * T(0.5) * (ep - sEt[a2])) * nn;
+                        if (axis == 0) r.x -= pf;
+                        else r.y -= pf;
+                    }
+                }
+                const int n = e0 + st * i, v0 = 2 * pr;
+                if (axis == 0) {
+                    sR[v0 * ncn + n] = r.x;
+                    sR[(v0 + 1) * ncn + n] = r.y;
+                } else {
+                    sR[v0 * ncn + n] += r.x;
+                    sR[(v0 + 1) * ncn + n] += r.y;
+                }
+            }
+        }
+    };
+    // x pencils (j, k, layer)
     for (int p = threadIdx.x; p < npen; p += blockDim.x) {
         const int ez = p / NP2, j = p % NP, k = (p / NP) % NP;
-        const int e0 = ez * NP3 + NP * (j + NP * k);
-        T qa[4], qb[4], ea, eb, Ha, Hb;
-        outside(0, ez, 0, j, k, e0, qa, ea, Ha);
-        outside(1, ez, N, j, k, e0 + N, qb, eb, Hb);
-        T q[NP];
-#pragma unroll
-        for (int m = 0; m < NP; ++m) q[m] = sQ[e0 + m];
-#pragma unroll
-        for (int i = 0; i < NP; ++i) {
-            T s = 0;
-#pragma unroll
-            for (int m = 0; m < NP; ++m) s += B::D(i * NP + m) * q[m];
-            T d = cx * s;
-            if (i == 0) d += Lx * (T(0.5) * (q[0] + qa[0]) * T(-1) - q[0] * T(-1));
-            if (i == N) d += Lx * (T(0.5) * (q[N] + qb[0]) - q[N]);
-            sD[e0 + i] = d;
-        }
+        hpass(std::integral_constant<int, 0>{}, ez, ez * NP3 + NP * (j + NP * k), 1, j, 0);
     }
     __syncthreads();
-    // y pencils
+    // y pencils (i, k, layer)
     for (int p = threadIdx.x; p < npen; p += blockDim.x) {
         const int ez = p / NP2, i = p % NP, k = (p / NP) % NP;
-        const int e0 = ez * NP3 + i + NP2 * k;
-        T qa[4], qb[4], ea, eb, Ha, Hb;
-        outside(2, ez, i, 0, k, e0, qa, ea, Ha);
-        outside(3, ez, i, N, k, e0 + NP * N, qb, eb, Hb);
-        T q[NP];
-#pragma unroll
-        for (int m = 0; m < NP; ++m) q[m] = sQ[ncn + e0 + NP * m];
-#pragma unroll
-        for (int j = 0; j < NP; ++j) {
-            T s = 0;
-#pragma unroll
-            for (int m = 0; m < NP; ++m) s += B::D(j * NP + m) * q[m];
-            T d = cy * s;
-            if (j == 0) d += Ly * (T(0.5) * (q[0] + qa[1]) * T(-1) - q[0] * T(-1));
-            if (j == N) d += Ly * (T(0.5) * (q[N] + qb[1]) - q[N]);
-            sD[e0 + NP * j] += d;
-        }
+        hpass(std::integral_constant<int, 1>{}, ez, ez * NP3 + i + NP2 * k, NP, 0, i);
     }
     __syncthreads();
     // ---- layer integrals J_k = (dsig/2) sum_m S[k][m] delta_m: z pencils
@@ -303,146 +443,7 @@ __global__ void __launch_bounds__(512) dg3d_stage_kernel(StageArgs<T> a) {
         }
     }
     __syncthreads();
-    for (int an = threadIdx.x; an < NP2; an += blockDim.x) {
-        T Ib = 0;
-        for (int ez = 0; ez < nz; ++ez) {
-            sL1[ez * NP2 + an] = Ib;
-            Ib = Ib + sD[ez * NP3 + an + NP2 * N];
-        }
-        sItot[an] = Ib;
-        if (a.mode == 1 && a.deta_out) a.deta_out[(size_t)c * NP2 + an] = -(double)Ib;
-    }
-    __syncthreads();
-    for (int p = threadIdx.x; p < npen; p += blockDim.x) {
-        const int ez = p / NP2, an = p % NP2;
-        const int e0 = ez * NP3 + an;
-        const T Ib = sL1[ez * NP2 + an], It = sItot[an], iH = sIH[an];
-#pragma unroll
-        for (int k = 0; k < NP; ++k) {
-            const T I = Ib + sD[e0 + NP2 * k];
-            T s1 = (T)(G.dsig * (ez + 0.5 * ((double)B::x(k) + 1.0)));
-            if (ez == nz - 1 && k == N) s1 = T(1);
-            const T om = (-I + s1 * It) * iH;
-            sOm[e0 + NP2 * k] = om;
-            if (a.mode == 1 && a.omega_out) a.omega_out[base + e0 + NP2 * k] = om;
-        }
-    }
-    __syncthreads();
 
-    // ---- right-hand side, x pencils: advection d/dx, pressure, horizontal diffusion xx, x faces.
-    // Variables are processed one at a time to keep few values live per thread.
-    const T nh = (T)G.nu_h;
-    const bool hdiff = G.nu_h > 0.0;
-    for (int p = threadIdx.x; p < npen; p += blockDim.x) {
-        const int ez = p / NP2, j = p % NP, k = (p / NP) % NP;
-        const int e0 = ez * NP3 + NP * (j + NP * k);
-        T u[NP];
-#pragma unroll
-        for (int m = 0; m < NP; ++m) u[m] = sQ[e0 + m] * sIH[m + NP * j];
-        // both end faces: outside state, normal velocities and LF speed
-        T qp0[4], qpN[4], ep0, epN, Hp0, HpN;
-        outside(0, ez, 0, j, k, e0, qp0, ep0, Hp0);
-        outside(1, ez, N, j, k, e0 + N, qpN, epN, HpN);
-        const T unm0 = -u[0], unp0 = -qp0[0] / Hp0, lam0 = fmax(fabs(unm0), fabs(unp0));
-        const T unmN = u[N], unpN = qpN[0] / HpN, lamN = fmax(fabs(unmN), fabs(unpN));
-#pragma unroll 1
-        for (int v = 0; v < 4; ++v) {
-            T q[NP];
-#pragma unroll
-            for (int m = 0; m < NP; ++m) q[m] = sQ[v * ncn + e0 + m];
-#pragma unroll
-            for (int i = 0; i < NP; ++i) {
-                T s = 0;
-#pragma unroll
-                for (int m = 0; m < NP; ++m) s += B::D(i * NP + m) * (q[m] * u[m]);
-                T r = -cx * s;
-                const T Hh = sHt[i + NP * j];
-                if (v == 0) {
-                    T ge = 0;
-#pragma unroll
-                    for (int m = 0; m < NP; ++m) ge += B::D(i * NP + m) * sEt[m + NP * j];
-                    r -= g * Hh * cx * ge;
-                }
-                if (v <= 1 && hdiff) {
-                    T xx = 0;
-#pragma unroll
-                    for (int m = 0; m < NP; ++m)
-                        xx += B::D2(i * NP + m) * (v == 0 ? u[m] : q[m] * sIH[m + NP * j]);
-                    r += nh * Hh * (cx * cx * xx);
-                }
-                if (i == 0 || i == N) {
-                    const T qm = q[i];
-                    const T qpv = i == 0 ? sel4(qp0, v) : sel4(qpN, v);
-                    const T unm = i == 0 ? unm0 : unmN, unp = i == 0 ? unp0 : unpN;
-                    const T lam = i == 0 ? lam0 : lamN;
-                    const T fs = T(0.5) * (qm * unm + qpv * unp) - T(0.5) * lam * (qpv - qm);
-                    r -= Lx * (fs - qm * unm);
-                    if (v == 0) {
-                        const T nx = i == 0 ? T(-1) : T(1);
-                        const T ep = i == 0 ? ep0 : epN;
-                        r -= Lx * (g * Hh * T(0.5) * (ep - sEt[i + NP * j])) * nx;
-                    }
-                }
-                sR[v * ncn + e0 + i] = r;
-            }
-        }
-    }
-    __syncthreads();
-    // ---- y pencils: advection d/dy, pressure, horizontal diffusion yy, y faces
-    for (int p = threadIdx.x; p < npen; p += blockDim.x) {
-        const int ez = p / NP2, i = p % NP, k = (p / NP) % NP;
-        const int e0 = ez * NP3 + i + NP2 * k;
-        T w[NP];
-#pragma unroll
-        for (int m = 0; m < NP; ++m) w[m] = sQ[ncn + e0 + NP * m] * sIH[i + NP * m];
-        T qp0[4], qpN[4], ep0, epN, Hp0, HpN;
-        outside(2, ez, i, 0, k, e0, qp0, ep0, Hp0);
-        outside(3, ez, i, N, k, e0 + NP * N, qpN, epN, HpN);
-        const T unm0 = -w[0], unp0 = -qp0[1] / Hp0, lam0 = fmax(fabs(unm0), fabs(unp0));
-        const T unmN = w[N], unpN = qpN[1] / HpN, lamN = fmax(fabs(unmN), fabs(unpN));
-#pragma unroll 1
-        for (int v = 0; v < 4; ++v) {
-            T q[NP];
-#pragma unroll
-            for (int m = 0; m < NP; ++m) q[m] = sQ[v * ncn + e0 + NP * m];
-#pragma unroll
-            for (int j = 0; j < NP; ++j) {
-                T s = 0;
-#pragma unroll
-                for (int m = 0; m < NP; ++m) s += B::D(j * NP + m) * (q[m] * w[m]);
-                T r = -cy * s;
-                const T Hh = sHt[i + NP * j];
-                if (v == 1) {
-                    T ge = 0;
-#pragma unroll
-                    for (int m = 0; m < NP; ++m) ge += B::D(j * NP + m) * sEt[i + NP * m];
-                    r -= g * Hh * cy * ge;
-                }
-                if (v <= 1 && hdiff) {
-                    T yy = 0;
-#pragma unroll
-                    for (int m = 0; m < NP; ++m)
-                        yy += B::D2(j * NP + m) * (v == 1 ? w[m] : q[m] * sIH[i + NP * m]);
-                    r += nh * Hh * (cy * cy * yy);
-                }
-                if (j == 0 || j == N) {
-                    const T qm = q[j];
-                    const T qpv = j == 0 ? sel4(qp0, v) : sel4(qpN, v);
-                    const T unm = j == 0 ? unm0 : unmN, unp = j == 0 ? unp0 : unpN;
-                    const T lam = j == 0 ? lam0 : lamN;
-                    const T fs = T(0.5) * (qm * unm + qpv * unp) - T(0.5) * lam * (qpv - qm);
-                    r -= Ly * (fs - qm * unm);
-                    if (v == 1) {
-                        const T ny = j == 0 ? T(-1) : T(1);
-                        const T ep = j == 0 ? ep0 : epN;
-                        r -= Ly * (g * Hh * T(0.5) * (ep - sEt[i + NP * j])) * ny;
-                    }
-                }
-                sR[v * ncn + e0 + NP * j] += r;
-            }
-        }
-    }
-    __syncthreads();
     // ---- z pencils: advection d/dsigma, Coriolis, vertical diffusion, sigma faces, surface
     // and bed stresses, then the LSRK update and the FP64 column increments
     if (a.bulk && need_res) {
@@ -458,9 +459,22 @@ __global__ void __launch_bounds__(512) dg3d_stage_kernel(StageArgs<T> a) {
         const int e0 = ez * NP3 + an;
         const T iH = sIH[an], fa = (T)a.f[(size_t)c * NP2 + an];
         const bool bed = ez == 0, top = ez == nz - 1;
+        // omega of this pencil: H omega(sigma) = -I(sigma) + (1 + sigma) I(top), with I the
+        // cumulative layer integral (the layer totals summed bottom-up, as a sequential scan)
+        T Ib = 0;
+        for (int e = 0; e < ez; ++e) Ib = Ib + sD[e * NP3 + an + NP2 * N];
+        T It = Ib;
+        for (int e = ez; e < nz; ++e) It = It + sD[e * NP3 + an + NP2 * N];
+        if (a.mode == 1 && a.deta_out && bed) a.deta_out[(size_t)c * NP2 + an] = -(double)It;
         T om[NP];
 #pragma unroll
-        for (int m = 0; m < NP; ++m) om[m] = sOm[e0 + NP2 * m];
+        for (int k = 0; k < NP; ++k) {
+            const T I = Ib + sD[e0 + NP2 * k];
+            T s1 = (T)(G.dsig * (ez + 0.5 * ((double)B::x(k) + 1.0)));
+            if (top && k == N) s1 = T(1);
+            om[k] = (-I + s1 * It) * iH;
+            if (a.mode == 1 && a.omega_out) a.omega_out[base + e0 + NP2 * k] = om[k];
+        }
         // bed stress (only the bottom layer's k = 0 node) and surface stress
         T fbx = 0, fby = 0;
         if (bed) {
@@ -476,67 +490,93 @@ __global__ void __launch_bounds__(512) dg3d_stage_kernel(StageArgs<T> a) {
         }
         const T w0 = om[0] * T(-1), wN = om[N];
         const int nb0 = (ez - 1) * NP3 + an + NP2 * N, nbN = (ez + 1) * NP3 + an;
-        const T wp0 = bed ? T(0) : sOm[nb0] * T(-1), wpN = top ? T(0) : sOm[nbN];
+        // omega is continuous across layer faces by construction (the neighbour's end value
+        // is computed from the same prefix and sigma), so the neighbour's value is this one's
+        const T wp0 = bed ? T(0) : w0, wpN = top ? T(0) : wN;
         const T lam0 = fmax(fabs(w0), fabs(wp0)), lamN = fmax(fabs(wN), fabs(wpN));
-        T incU = 0, incV = 0;
+        P2<T> inc = bc(T(0));
+        // vertical diffusion kappa / H d2(q / H)/dsigma2 with the 1/H of q / H taken out of the sum
+        const T ihc = iH * cs * cs * iH;
 #pragma unroll 1
-        for (int v = 0; v < 4; ++v) {
-            const T kp = v <= 1 ? (T)G.nu_v : (v == 2 ? (T)G.kT : (T)G.kS);
-            T q[NP];
+        for (int pr = 0; pr < 2; ++pr) {
+            const int v0 = 2 * pr, v1 = v0 + 1;
+            // the pair's output arrays, selected without indexing the parameter arrays
+            T *const res0 = pr == 0 ? a.res[0] : a.res[2], *const res1 = pr == 0 ? a.res[1] : a.res[3];
+            T *const out0 = pr == 0 ? a.qout[0] : a.qout[2], *const out1 = pr == 0 ? a.qout[1] : a.qout[3];
+            // vertical diffusivities of the pair (a zero one contributes exactly nothing)
+            const T k0 = pr == 0 ? (T)G.nu_v : (T)G.kT, k1 = pr == 0 ? (T)G.nu_v : (T)G.kS;
+            const P2<T> kc = {k0 > T(0) ? k0 * ihc : T(0), k1 > T(0) ? k1 * ihc : T(0)};
+            P2<T> q[NP], fo[NP];
 #pragma unroll
-            for (int m = 0; m < NP; ++m) q[m] = sQ[v * ncn + e0 + NP2 * m];
+            for (int m = 0; m < NP; ++m) {
+                q[m] = {sQ[v0 * ncn + e0 + NP2 * m], sQ[v1 * ncn + e0 + NP2 * m]};
+                fo[m] = p2mul(q[m], bc(om[m]));
+            }
 #pragma unroll
             for (int k = 0; k < NP; ++k) {
                 const int n = e0 + NP2 * k;
-                T s = 0, z2 = 0;
+                P2<T> s = bc(T(0)), z2 = bc(T(0));
 #pragma unroll
                 for (int m = 0; m < NP; ++m) {
-                    s += B::D(k * NP + m) * (q[m] * om[m]);
-                    z2 += B::D2(k * NP + m) * (q[m] * iH);
+                    s = p2fma(bc(B::D(k * NP + m)), fo[m], s);
+                    z2 = p2fma(bc(B::D2(k * NP + m)), q[m], z2);
                 }
-                T r = sR[v * ncn + n] - cs * s;
-                if (kp > T(0)) r += kp * iH * cs * cs * z2;
-                if (v == 0) r += fa * sQ[ncn + n];
-                if (v == 1) r += -fa * sQ[n];
+                P2<T> r = p2fma(bc(-cs), s, P2<T>{sR[v0 * ncn + n], sR[v1 * ncn + n]});
+                r = p2fma(kc, z2, r);
+                if (pr == 0) {  // Coriolis
+                    r.x += fa * q[k].y;
+                    r.y += -fa * q[k].x;
+                }
                 if (k == 0) {
                     const T wm = w0;
                     if (!bed) {
-                        const T qpp = sQ[v * ncn + nb0];
-                        const T fs = T(0.5) * (q[0] * wm + qpp * wp0) - T(0.5) * lam0 * (qpp - q[0]);
-                        r -= Ls * (fs - q[0] * wm);
+                        const P2<T> qpp = {sQ[v0 * ncn + nb0], sQ[v1 * ncn + nb0]};
+                        const P2<T> fs = p2sub(p2mul(bc(T(0.5)), p2add(p2mul(q[0], bc(wm)), p2mul(qpp, bc(wp0)))),
+                                               p2mul(bc(T(0.5) * lam0), p2sub(qpp, q[0])));
+                        r = p2fma(bc(-Ls), p2sub(fs, p2mul(q[0], bc(wm))), r);
                     } else {
-                        r -= Ls * (T(0) - q[0] * wm);
-                        if (v == 0) r += fbx;
-                        if (v == 1) r += fby;
+                        r = p2fma(bc(-Ls), p2sub(bc(T(0)), p2mul(q[0], bc(wm))), r);
+                        if (pr == 0) {
+                            r.x += fbx;
+                            r.y += fby;
+                        }
                     }
                 }
                 if (k == N) {
                     const T wm = wN;
                     if (!top) {
-                        const T qpp = sQ[v * ncn + nbN];
-                        const T fs = T(0.5) * (q[N] * wm + qpp * wpN) - T(0.5) * lamN * (qpp - q[N]);
-                        r -= Ls * (fs - q[N] * wm);
+                        const P2<T> qpp = {sQ[v0 * ncn + nbN], sQ[v1 * ncn + nbN]};
+                        const P2<T> fs = p2sub(p2mul(bc(T(0.5)), p2add(p2mul(q[N], bc(wm)), p2mul(qpp, bc(wpN)))),
+                                               p2mul(bc(T(0.5) * lamN), p2sub(qpp, q[N])));
+                        r = p2fma(bc(-Ls), p2sub(fs, p2mul(q[N], bc(wm))), r);
                     } else {
-                        r -= Ls * (T(0) - q[N] * wm);
-                        if (v == 0) r += fsx;
-                        if (v == 1) r += fsy;
+                        r = p2fma(bc(-Ls), p2sub(bc(T(0)), p2mul(q[N], bc(wm))), r);
+                        if (pr == 0) {
+                            r.x += fsx;
+                            r.y += fsy;
+                        }
                     }
                 }
                 const size_t gi = base + n;
                 if (a.mode == 1) {
-                    a.res[v][gi] = r;
+                    res0[gi] = r.x;
+                    res1[gi] = r.y;
                 } else {
-                    const T rn = (a.first ? T(0) : a.A * sRes[v * ncn + n]) + a.dt * r;
-                    a.res[v][gi] = rn;
-                    a.qout[v][gi] = q[k] + a.B * rn;
-                    if (v == 0) incU += B::w(k) * (a.B * rn);
-                    if (v == 1) incV += B::w(k) * (a.B * rn);
+                    const P2<T> r0 = a.first ? bc(T(0))
+                                             : p2mul(bc(a.A), P2<T>{sRes[v0 * ncn + n], sRes[v1 * ncn + n]});
+                    const P2<T> rn = p2fma(bc(a.dt), r, r0);
+                    res0[gi] = rn.x;
+                    res1[gi] = rn.y;
+                    const P2<T> qn = p2fma(bc(a.B), rn, q[k]);
+                    out0[gi] = qn.x;
+                    out1[gi] = qn.y;
+                    if (pr == 0) inc = p2fma(bc(B::w(k)), p2mul(bc(a.B), rn), inc);
                 }
             }
         }
         if (a.mode == 0) {
-            sL1[ez * NP2 + an] = incU;
-            sL2[ez * NP2 + an] = incV;
+            sL1[ez * NP2 + an] = inc.x;
+            sL2[ez * NP2 + an] = inc.y;
         }
     }
     if (a.mode == 0) {
@@ -568,7 +608,37 @@ struct BaroArgs {
     int64_t ncol;
 };
 
-template <int NP>
+// F*(U-, U+) - F(U-) for the Lax-Friedrichs flux (sw_flux_lf minus sw_phys_flux of U-) with
+// the interior side's 1/h and sqrt(g h) supplied: one division and one square root per face
+// (the exterior side's). Same formulas, reciprocals in place of divisions.
+__device__ __forceinline__ void lf_minus_phys(const double UL[3], double ihL, double cL, const double UR[3],
+                                              double nx, double ny, double g, double d[3]) {
+    const double hLc = UL[0] < 1e-10 ? 1e-10 : UL[0], hRc = UR[0] < 1e-10 ? 1e-10 : UR[0];
+    const double iL = UL[0] < 1e-10 ? 1e10 : ihL, iR = 1.0 / hRc;
+    const double cLc = UL[0] < 1e-10 ? sqrt(g * hLc) : cL, cR = sqrt(g * hRc);
+    const double uL = UL[1] * iL, vL = UL[2] * iL, uR = UR[1] * iR, vR = UR[2] * iR;
+    const double FxL[3] = {UL[1], UL[1] * uL + 0.5 * g * hLc * hLc, UL[1] * vL};
+    const double FyL[3] = {UL[2], UL[2] * uL, UL[2] * vL + 0.5 * g * hLc * hLc};
+    const double FxR[3] = {UR[1], UR[1] * uR + 0.5 * g * hRc * hRc, UR[1] * vR};
+    const double FyR[3] = {UR[2], UR[2] * uR, UR[2] * vR + 0.5 * g * hRc * hRc};
+    const double unL = uL * nx + vL * ny, unR = uR * nx + vR * ny;
+    const double lam = fmax(fabs(unL) + cLc, fabs(unR) + cR);
+    const double Fm[3] = {hLc * unL, hLc * uL * unL + 0.5 * g * hLc * hLc * nx,
+                          hLc * vL * unL + 0.5 * g * hLc * hLc * ny};
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        const double FnL = FxL[q] * nx + FyL[q] * ny, FnR = FxR[q] * nx + FyR[q] * ny;
+        d[q] = (0.5 * (FnL + FnR) - 0.5 * lam * (UR[q] - UL[q])) - Fm[q];
+    }
+}
+
+// Register budget of the subcycle kernels: four tiles per SM for up to 5 x 5 nodes per column.
+#define BARO_BOUNDS __launch_bounds__(BARO_CPB * NP * NP, NP <= 5 ? 4 : 2)
+
+// One tile of BARO_CPB columns: the barotropic right-hand side Phi(U) at this thread's 2D node.
+// FK is the face flux (the model's flux2d). Every global load, the neighbours' face values
+// included, is issued before the tile barrier.
+template <int NP, int FK>
 __device__ __forceinline__ bool baro_tile_phi(const BaroArgs &a, double &re, double &ru,
                                               double &rv, int64_t &t) {
     constexpr int NP2 = NP * NP, N = NP - 1;
@@ -580,13 +650,26 @@ __device__ __forceinline__ bool baro_tile_phi(const BaroArgs &a, double &re, dou
     const bool valid = c < a.ncol;
     if (threadIdx.x < NP2) sD[threadIdx.x] = cB.D[threadIdx.x];
     t = c * NP2 + an;
-    double H = 1.0;
+    const int ex = (int)(c % G.nx), ey = (int)(c / G.nx);
+    // the neighbour node across this node's x face (i = 0 or N) and y face (j = 0 or N)
+    int64_t qx = -1, qy = -1;
+    if (valid && i == 0 && ex > 0) qx = (c - 1) * NP2 + N + NP * j;
+    if (valid && i == N && ex < G.nx - 1) qx = (c + 1) * NP2 + NP * j;
+    if (valid && j == 0 && ey > 0) qy = (c - G.nx) * NP2 + i + NP * N;
+    if (valid && j == N && ey < G.ny - 1) qy = (c + G.nx) * NP2 + i;
+    double e = 0.0, hb = 0.0, hu0 = 0.0, hv0 = 0.0, fc = 0.0, fx = 0.0, fy = 0.0;
+    double xR[4] = {0.0, 0.0, 0.0, 0.0}, yR[4] = {0.0, 0.0, 0.0, 0.0};
     if (valid) {
-        const double e = a.e[t];
-        H = e + a.h[t];
+        e = a.e[t]; hb = a.h[t]; hu0 = a.hu[t]; hv0 = a.hv[t]; fc = a.f[t];
+        if (a.Fx) { fx = a.Fx[t]; fy = a.Fy[t]; }
+    }
+    if (qx >= 0) { xR[0] = a.e[qx]; xR[1] = a.h[qx]; xR[2] = a.hu[qx]; xR[3] = a.hv[qx]; }
+    if (qy >= 0) { yR[0] = a.e[qy]; yR[1] = a.h[qy]; yR[2] = a.hu[qy]; yR[3] = a.hv[qy]; }
+    const double H = valid ? e + hb : 1.0;
+    if (valid) {
         sE[threadIdx.x] = e;
-        sU[threadIdx.x] = a.hu[t];
-        sV[threadIdx.x] = a.hv[t];
+        sU[threadIdx.x] = hu0;
+        sV[threadIdx.x] = hv0;
         sI[threadIdx.x] = 1.0 / H;
     }
     __syncthreads();
@@ -608,89 +691,91 @@ __device__ __forceinline__ bool baro_tile_phi(const BaroArgs &a, double &re, dou
         gex += dxm * sE[px];
         gey += dym * sE[py];
     }
-    const double hu0 = sU[threadIdx.x], hv0 = sV[threadIdx.x];
     re = -(G.cx * dhu + G.cy * dhv);
-    ru = -(G.cx * auu + G.cy * auv) - G.g * H * G.cx * gex + a.f[t] * hv0 + (a.Fx ? a.Fx[t] : 0.0);
-    rv = -(G.cx * avu + G.cy * avv) - G.g * H * G.cy * gey - a.f[t] * hu0 + (a.Fy ? a.Fy[t] : 0.0);
-    if (!(i == 0 || i == N || j == 0 || j == N)) return true;
-    const int ex = (int)(c % G.nx), ey = (int)(c / G.nx);
+    ru = -(G.cx * auu + G.cy * auv) - G.g * H * G.cx * gex + fc * hv0 + fx;
+    rv = -(G.cx * avu + G.cy * avv) - G.g * H * G.cy * gey - fc * hu0 + fy;
+    const bool bxf = i == 0 || i == N, byf = j == 0 || j == N;
+    if (!(bxf || byf)) return true;
     const double etide = tide_at(G, a.tdev[0] + a.toff);
+    const double UL[3] = {H, hu0, hv0};
+    const double ihL = sI[threadIdx.x], cL = FK == DRF_FLUX_LF ? sqrt(G.g * (H < 1e-10 ? 1e-10 : H)) : 0.0;
+    // x face first, then y face (a corner node has both)
 #pragma unroll
-    for (int s = 0; s < 4; ++s) {
-        const bool on = (s == 0 && i == 0) || (s == 1 && i == N) || (s == 2 && j == 0) ||
-                        (s == 3 && j == N);
-        if (!on) continue;
+    for (int f = 0; f < 2; ++f) {
+        if (f == 0 ? !bxf : !byf) continue;
+        const int s = f == 0 ? (i == 0 ? 0 : 1) : (j == 0 ? 2 : 3);
         const double nx = s == 0 ? -1.0 : (s == 1 ? 1.0 : 0.0);
         const double ny = s == 2 ? -1.0 : (s == 3 ? 1.0 : 0.0);
         const double L = s <= 1 ? G.Lx : G.Ly;
-        int64_t nc = -1;
-        int ni = i, nj = j;
-        if (s == 0 && ex > 0) { nc = c - 1; ni = N; }
-        if (s == 1 && ex < G.nx - 1) { nc = c + 1; ni = 0; }
-        if (s == 2 && ey > 0) { nc = c - G.nx; nj = N; }
-        if (s == 3 && ey < G.ny - 1) { nc = c + G.nx; nj = 0; }
-        double UL[3] = {H, hu0, hv0}, UR[3];
-        if (nc >= 0) {
-            const int64_t q = nc * NP2 + ni + NP * nj;
-            UR[0] = a.e[q] + a.h[q]; UR[1] = a.hu[q]; UR[2] = a.hv[q];
-        } else if (G.bc[s] == DRF_BC_TIDE) {
-            UR[0] = etide + a.h[t];
+        const int64_t q = f == 0 ? qx : qy;
+        const double *nb = f == 0 ? xR : yR;
+        double UR[3];
+        if (q >= 0) {
+            UR[0] = nb[0] + nb[1]; UR[1] = nb[2]; UR[2] = nb[3];
+        } else if ((s == 0 ? G.bc[0] : (s == 1 ? G.bc[1] : (s == 2 ? G.bc[2] : G.bc[3]))) == DRF_BC_TIDE) {
+            UR[0] = etide + hb;
             const double r = UR[0] / H;
             UR[1] = UL[1] * r; UR[2] = UL[2] * r;
         } else {
             UR[0] = H; UR[1] = UL[1]; UR[2] = UL[2];
             if (s <= 1) UR[1] = -UL[1]; else UR[2] = -UL[2];
         }
-        double Fs[3], Fm[3];
-        sw_flux(G.flux2d, UL, UR, nx, ny, G.g, Fs);
-        sw_phys_flux(UL, nx, ny, G.g, Fm);
-        re -= L * (Fs[0] - Fm[0]);
-        ru -= L * (Fs[1] - Fm[1]);
-        rv -= L * (Fs[2] - Fm[2]);
+        double d[3];
+        if (FK == DRF_FLUX_LF) {
+            lf_minus_phys(UL, ihL, cL, UR, nx, ny, G.g, d);
+        } else {
+            double Fs[3], Fm[3];
+            sw_flux(FK, UL, UR, nx, ny, G.g, Fs);
+            sw_phys_flux(UL, nx, ny, G.g, Fm);
+            d[0] = Fs[0] - Fm[0]; d[1] = Fs[1] - Fm[1]; d[2] = Fs[2] - Fm[2];
+        }
+        re -= L * d[0];
+        ru -= L * d[1];
+        rv -= L * d[2];
     }
     return true;
 }
 
-template <int NP>
+template <int NP, int FK>
 __global__ void baro_rhs_kernel(BaroArgs a, double *ke, double *ku, double *kv) {
     double re, ru, rv;
     int64_t t;
-    if (!baro_tile_phi<NP>(a, re, ru, rv, t)) return;
+    if (!baro_tile_phi<NP, FK>(a, re, ru, rv, t)) return;
     ke[t] = re; ku[t] = ru; kv[t] = rv;
 }
 
 // F = (3D-integrated increment)/dt - Phi(U^n); keeps HU^n, HV^n for the transport correction.
-template <int NP>
+template <int NP, int FK>
 __global__ void baro_force_kernel(BaroArgs a, double dt, const double *dHU3, const double *dHV3,
                                   double *Fx, double *Fy, double *HUo, double *HVo) {
     double re, ru, rv;
     int64_t t;
-    if (!baro_tile_phi<NP>(a, re, ru, rv, t)) return;
+    if (!baro_tile_phi<NP, FK>(a, re, ru, rv, t)) return;
     Fx[t] = dHU3[t] / dt - ru;
     Fy[t] = dHV3[t] / dt - rv;
     HUo[t] = a.hu[t];
     HVo[t] = a.hv[t];
 }
 
-template <int NP>
-__global__ void baro_pred_kernel(BaroArgs a, double dtb, double *k1e, double *k1u, double *k1v,
+template <int NP, int FK>
+__global__ void BARO_BOUNDS baro_pred_kernel(BaroArgs a, double dtb, double *k1e, double *k1u, double *k1v,
                                  double *es, double *us, double *vs) {
     double re, ru, rv;
     int64_t t;
-    if (!baro_tile_phi<NP>(a, re, ru, rv, t)) return;
+    if (!baro_tile_phi<NP, FK>(a, re, ru, rv, t)) return;
     k1e[t] = re; k1u[t] = ru; k1v[t] = rv;
     es[t] = a.e[t] + dtb * re;
     us[t] = a.hu[t] + dtb * ru;
     vs[t] = a.hv[t] + dtb * rv;
 }
 
-template <int NP>
-__global__ void baro_corr_kernel(BaroArgs a, double dtb, const double *k1e, const double *k1u,
+template <int NP, int FK>
+__global__ void BARO_BOUNDS baro_corr_kernel(BaroArgs a, double dtb, const double *k1e, const double *k1u,
                                  const double *k1v, double *e, double *hu, double *hv,
                                  double *esum, int first) {
     double re, ru, rv;
     int64_t t;
-    if (!baro_tile_phi<NP>(a, re, ru, rv, t)) return;
+    if (!baro_tile_phi<NP, FK>(a, re, ru, rv, t)) return;
     const double hd = 0.5 * dtb;
     const double en = e[t] + hd * (k1e[t] + re);
     e[t] = en;
@@ -875,6 +960,14 @@ void dispatch_np(int np, F &&f) {
     }
 }
 
+// the 2D face flux as a compile-time constant of the barotropic kernels
+template <class F>
+void dispatch_flux(int kind, F &&f) {
+    if (kind == DRF_FLUX_HLLC) f(std::integral_constant<int, DRF_FLUX_HLLC>{});
+    else if (kind == DRF_FLUX_ROE) f(std::integral_constant<int, DRF_FLUX_ROE>{});
+    else f(std::integral_constant<int, DRF_FLUX_LF>{});
+}
+
 const double LSRK_A[5] = {0.0, -0.4178904745, -1.192151694643, -1.697784692471, -1.514183444257};
 const double LSRK_B[5] = {0.1496590219993, 0.3792103129999, 0.8229550293869, 0.6994504559488,
                           0.1530572479681};
@@ -930,7 +1023,7 @@ struct drf_dg {
     int stage_threads() const {
         const int npen = G.nz * np2;
         int bs = ((npen + 31) / 32) * 32;
-        return bs < 64 ? 64 : (bs > 512 ? 512 : bs);
+        return bs < 64 ? 64 : (bs > STAGE_MAX_THREADS ? STAGE_MAX_THREADS : bs);
     }
 
     template <typename T, int NP>
@@ -999,19 +1092,22 @@ struct drf_dg {
         // after 5 stages the state is in `out`
         const unsigned nbt = (unsigned)((ncol + BARO_CPB - 1) / BARO_CPB);
         const int bt = BARO_CPB * NP * NP;
-        baro_force_kernel<NP><<<nbt, bt, 0, stream>>>(baro<NP>(eta, HU, HV, false, 0.0), dt, dHU3,
-                                                      dHV3, Fx, Fy, HUo, HVo);
-        DRF_LAUNCHED();
-        const double dtb = dt / nsub;
-        for (int m = 0; m < nsub; ++m) {
-            baro_pred_kernel<NP><<<nbt, bt, 0, stream>>>(baro<NP>(eta, HU, HV, true, m * dtb), dtb,
-                                                         k1[0], k1[1], k1[2], us[0], us[1], us[2]);
+        dispatch_flux(G.flux2d, [&](auto fk) {
+            constexpr int FK = decltype(fk)::value;
+            baro_force_kernel<NP, FK><<<nbt, bt, 0, stream>>>(baro<NP>(eta, HU, HV, false, 0.0), dt, dHU3,
+                                                              dHV3, Fx, Fy, HUo, HVo);
             DRF_LAUNCHED();
-            baro_corr_kernel<NP><<<nbt, bt, 0, stream>>>(
-                baro<NP>(us[0], us[1], us[2], true, m * dtb + dtb), dtb, k1[0], k1[1], k1[2], eta,
-                HU, HV, esum, m == 0);
-            DRF_LAUNCHED();
-        }
+            const double dtb = dt / nsub;
+            for (int m = 0; m < nsub; ++m) {
+                baro_pred_kernel<NP, FK><<<nbt, bt, 0, stream>>>(baro<NP>(eta, HU, HV, true, m * dtb), dtb,
+                                                                 k1[0], k1[1], k1[2], us[0], us[1], us[2]);
+                DRF_LAUNCHED();
+                baro_corr_kernel<NP, FK><<<nbt, bt, 0, stream>>>(
+                    baro<NP>(us[0], us[1], us[2], true, m * dtb + dtb), dtb, k1[0], k1[1], k1[2], eta,
+                    HU, HV, esum, m == 0);
+                DRF_LAUNCHED();
+            }
+        });
         baro_finish_kernel<<<blocks_for(n2), 256, 0, stream>>>(n2, nsub, dt, esum, eta_avg, HU, HV,
                                                                HUo, HVo, dHU3, dHV3, corrU, corrV,
                                                                tdev);
@@ -1292,9 +1388,12 @@ int drf_dg_compute_rhs2d(drf_dg *m, const double *Fx, const double *Fy, double t
         DRF_CUDA(cudaStreamSynchronize(m->stream));
         dispatch_np(m->np, [&](auto npc) {
             constexpr int NP = decltype(npc)::value;
-            baro_rhs_kernel<NP><<<(unsigned)((m->ncol + BARO_CPB - 1) / BARO_CPB), BARO_CPB * NP * NP,
-                                  0, m->stream>>>(m->baro<NP>(m->eta, m->HU, m->HV, true, time - tcur),
-                                                  m->k1[0], m->k1[1], m->k1[2]);
+            dispatch_flux(m->G.flux2d, [&](auto fk) {
+                constexpr int FK = decltype(fk)::value;
+                baro_rhs_kernel<NP, FK><<<(unsigned)((m->ncol + BARO_CPB - 1) / BARO_CPB), BARO_CPB * NP * NP,
+                                          0, m->stream>>>(m->baro<NP>(m->eta, m->HU, m->HV, true, time - tcur),
+                                                          m->k1[0], m->k1[1], m->k1[2]);
+            });
         });
         DRF_LAUNCHED();
         DRF_CUDA(cudaStreamSynchronize(m->stream));
