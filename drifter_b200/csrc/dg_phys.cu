@@ -161,6 +161,12 @@ __device__ __forceinline__ P2<float> p2sub(P2<float> a, P2<float> b) {
         : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
     return r;
 }
+// k * x + c with a scalar k (an operator entry from constant memory): two scalar FMAs, which
+// take the constant as an operand (a packed FMA would first need it duplicated in registers)
+template <typename T>
+__device__ __forceinline__ P2<T> p2fma_k(T k, P2<T> x, P2<T> c) {
+    return {fma(k, x.x, c.x), fma(k, x.y, c.y)};
+}
 __device__ __forceinline__ P2<double> p2fma(P2<double> a, P2<double> b, P2<double> c) {
     return {fma(a.x, b.x, c.x), fma(a.y, b.y, c.y)};
 }
@@ -171,10 +177,11 @@ __device__ __forceinline__ P2<double> p2sub(P2<double> a, P2<double> b) { return
 // Shared-memory plan of the stage kernel for one water column (ncn = nz*(N+1)^3 nodes):
 //   two mbarriers (16 B), sQ[4][ncn] state, sRes[4][ncn] LSRK 2N register, sR[4][ncn]
 //   right-hand side, sD[ncn] horizontal divergence -> layer integrals (in place), per layer x
-//   2D-node increments, the column's 2D fields (1/H, H, eta) and its pressure-gradient rows.
+//   2D-node increments, the column's 2D fields (1/H, H, eta), its pressure-gradient rows and
+//   1 + sigma per z node.
 inline size_t stage_smem_bytes(int nz, int np, size_t tsz) {
     const int np2 = np * np, ncn = nz * np2 * np;
-    return 16 + ((size_t)13 * ncn + (size_t)2 * nz * np2 + 5 * np2) * tsz;
+    return 16 + ((size_t)13 * ncn + (size_t)2 * nz * np2 + 5 * np2 + (size_t)nz * np) * tsz;
 }
 
 // One CTA per water column; work is organised in pencils (lines of N+1 nodes) so every
@@ -198,10 +205,17 @@ __global__ void __launch_bounds__(STAGE_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) dg3
     T *sL2 = sL1 + nz * NP2;                       // [nz][NP2] column increments (Hv)
     T *sIH = sL2 + nz * NP2, *sHt = sIH + NP2, *sEt = sHt + NP2;
     T *sPx = sEt + NP2, *sPy = sPx + NP2;          // g H d(eta)/dx, g H d(eta)/dy per 2D node
+    T *sS1 = sPy + NP2;                            // [nz][NP] 1 + sigma at the column's z nodes
     __shared__ int s_ok;
 
-    const double tnow = a.tdev[0] + a.toff;
-    const T etide = (T)tide_at(G, tnow);
+    // tidal elevation: evaluated once per CTA, and only by a column on a tidal side
+    __shared__ T s_etide;
+    if (threadIdx.x == 0) {
+        const bool tidal = (ex == 0 && G.bc[0] == DRF_BC_TIDE) || (ex == G.nx - 1 && G.bc[1] == DRF_BC_TIDE) ||
+                           (ey == 0 && G.bc[2] == DRF_BC_TIDE) || (ey == G.ny - 1 && G.bc[3] == DRF_BC_TIDE);
+        s_etide = tidal ? (T)tide_at(G, a.tdev[0] + a.toff) : T(0);
+    }
+    T etide = 0;  // read after the first barrier
     const T cx = (T)G.cx, cy = (T)G.cy, cs = (T)G.cs;
     const T Lx = (T)G.Lx, Ly = (T)G.Ly, Ls = (T)G.Ls;
     const T g = (T)G.g;
@@ -249,12 +263,17 @@ __global__ void __launch_bounds__(STAGE_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) dg3
         sPx[t] = g * (T)H * cx * gex;
         sPy[t] = g * (T)H * cy * gey;
     }
+    for (int t = threadIdx.x; t < nz * NP; t += blockDim.x) {
+        const int ez = t / NP, k = t % NP;
+        sS1[t] = (ez == nz - 1 && k == N) ? T(1) : (T)(G.dsig * (ez + 0.5 * ((double)B::x(k) + 1.0)));
+    }
     if (threadIdx.x == 0) s_ok = a.bulk ? (int)mbar_wait(&bars[0], 0) : 1;
     __syncthreads();
     if (!s_ok) {
         if (threadIdx.x == 0) atomicExch(a.err, DRF_E_TIMEOUT);
         return;
     }
+    etide = s_etide;
     if (a.corrU) {  // pending transport correction of the previous step
         for (int n = threadIdx.x; n < ncn; n += blockDim.x) {
             const int an = n % NP2;
@@ -362,11 +381,12 @@ __global__ void __launch_bounds__(STAGE_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) dg3
         // (2) right-hand side, one variable pair at a time
 #pragma unroll 1
         for (int pr = 0; pr < 2; ++pr) {
-            P2<T> q[NP], f[NP];
+            P2<T> q[NP], f[NP], vel[NP];
 #pragma unroll
             for (int m = 0; m < NP; ++m) {
                 q[m] = {sQ[2 * pr * ncn + e0 + st * m], sQ[(2 * pr + 1) * ncn + e0 + st * m]};
                 f[m] = p2mul(q[m], bc(un[m]));
+                vel[m] = p2mul(q[m], bc(ih[m]));  // (u, v) for the diffusion of (Hu, Hv)
             }
             const P2<T> qp0v = pr == 0 ? p0a : p0b;
             const P2<T> qpNv = pr == 0 ? pNa : pNb;
@@ -374,7 +394,7 @@ __global__ void __launch_bounds__(STAGE_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) dg3
             for (int i = 0; i < NP; ++i) {
                 P2<T> s = bc(T(0));
 #pragma unroll
-                for (int m = 0; m < NP; ++m) s = p2fma(bc(B::D(i * NP + m)), f[m], s);
+                for (int m = 0; m < NP; ++m) s = p2fma_k(B::D(i * NP + m), f[m], s);
                 P2<T> r = p2mul(bc(-cd), s);
                 const int a2 = an2(i);
                 const T Hh = sHt[a2];
@@ -384,7 +404,7 @@ __global__ void __launch_bounds__(STAGE_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) dg3
                     if (hdiff) {
                         P2<T> dd = bc(T(0));
 #pragma unroll
-                        for (int m = 0; m < NP; ++m) dd = p2fma(bc(B::D2(i * NP + m)), p2mul(q[m], bc(ih[m])), dd);
+                        for (int m = 0; m < NP; ++m) dd = p2fma_k(B::D2(i * NP + m), vel[m], dd);
                         r = p2fma(bc(nh * Hh), p2mul(bc(cd * cd), dd), r);
                     }
                 }
@@ -470,8 +490,7 @@ __global__ void __launch_bounds__(STAGE_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) dg3
 #pragma unroll
         for (int k = 0; k < NP; ++k) {
             const T I = Ib + sD[e0 + NP2 * k];
-            T s1 = (T)(G.dsig * (ez + 0.5 * ((double)B::x(k) + 1.0)));
-            if (top && k == N) s1 = T(1);
+            const T s1 = sS1[ez * NP + k];
             om[k] = (-I + s1 * It) * iH;
             if (a.mode == 1 && a.omega_out) a.omega_out[base + e0 + NP2 * k] = om[k];
         }
@@ -518,8 +537,8 @@ __global__ void __launch_bounds__(STAGE_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) dg3
                 P2<T> s = bc(T(0)), z2 = bc(T(0));
 #pragma unroll
                 for (int m = 0; m < NP; ++m) {
-                    s = p2fma(bc(B::D(k * NP + m)), fo[m], s);
-                    z2 = p2fma(bc(B::D2(k * NP + m)), q[m], z2);
+                    s = p2fma_k(B::D(k * NP + m), fo[m], s);
+                    z2 = p2fma_k(B::D2(k * NP + m), q[m], z2);
                 }
                 P2<T> r = p2fma(bc(-cs), s, P2<T>{sR[v0 * ncn + n], sR[v1 * ncn + n]});
                 r = p2fma(kc, z2, r);
