@@ -41,6 +41,7 @@ def parse():
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 GPU comparison run")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-cg", action="store_true", help="skip the C4 Bezier CG comparison")
+    ap.add_argument("--no-ens", action="store_true", help="skip the C5 ensemble measurement")
     return ap.parse_args()
 
 
@@ -221,6 +222,60 @@ def run_cg(stream, reps=3):
     return out
 
 
+def run_ensemble(stream, steps=5, warmup=3):
+    """C5: 64 independent N=3 runs of uneven size stepped together (one persistent stage launch
+    per LSRK stage for all members, one graph per baroclinic step), against the same members
+    stepped one model after another on the same stream. Device time with CUDA events."""
+    import torch
+    from drifter_b200 import configs
+    from drifter_b200.dg import Ensemble, OceanModel
+    cases = configs.c5()
+    nsub = cases[0]["nsub"]
+    dts = [c["dt"] for c in cases]
+    ndof = sum(4 * c["cfg"].n3 for c in cases)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ens = Ensemble(cases)
+    ens.set_stream(stream.cuda_stream)
+    for m, c in zip(ens.members, cases):
+        m.upload_state(c["q"], c["eta"])
+    ens.step(dts, nsub, warmup)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    ens.step(dts, nsub, steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    info = ens.info()
+    diag = ens.members[0].diagnostics()
+    ens.close()
+    del ens
+    # the same members one after another (each model's own step graph)
+    models = []
+    for c in cases:
+        m = OceanModel(c["cfg"], c["h"], c["f"], c["taux"], c["tauy"])
+        m.set_stream(stream.cuda_stream)
+        m.upload_state(c["q"], c["eta"])
+        models.append(m)
+    for m, c in zip(models, cases):
+        m.step(c["dt"], nsub, warmup)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(steps):
+        for m, c in zip(models, cases):
+            m.step(c["dt"], nsub, 1)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_seq = e0.elapsed_time(e1) / steps
+    for m in models:
+        m.close()
+    return {"workload": f"C5 {len(cases)} members N=3, meshes 16..64 x 16..64 x 4..8, mixed precision, "
+                        f"{nsub} barotropic subcycles",
+            "dofs": ndof, "columns": info["items"], "stage_grid": info["grid"],
+            "value": ndof * 5 / (ms / 1e3), "unit": UNIT, "ms_per_step": ms,
+            "sequential_ms_per_step": ms_seq, "speedup_vs_sequential": ms_seq / ms,
+            "member0_max_eta": diag["max_eta"]}
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -348,6 +403,10 @@ def run_ours(args, rank, world, local):
     if not args.no_cg:
         cg = run_cg(stream)
 
+    ens = None
+    if not args.no_ens:
+        ens = run_ensemble(stream)
+
     cpu = None
     if rank == 0 and not args.no_cpu:
         v, meta = cpu_baseline(seconds=12.0, threads=1)
@@ -372,6 +431,7 @@ def run_ours(args, rank, world, local):
             "e2e": e2e,
             "fp64_gpu": fp64,
             "cg": cg,
+            "ensemble": ens,
             "gpu_launches": int(launches),
             "clocks": ck,
         }

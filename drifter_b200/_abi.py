@@ -73,6 +73,16 @@ _SIGS = {
     "drf_dg_download_surface": (C.c_int, [C.c_void_p, _dp]),
     "drf_dg_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64),
                               C.POINTER(C.c_int)]),
+    "drf_ens_create": (C.c_int, [C.c_int, C.POINTER(MeshDesc), C.POINTER(DGParams),
+                                 C.POINTER(_dp), C.POINTER(_dp), C.POINTER(_dp), C.POINTER(_dp),
+                                 C.POINTER(C.c_void_p)]),
+    "drf_ens_destroy": (C.c_int, [C.c_void_p]),
+    "drf_ens_member": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
+    "drf_ens_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "drf_ens_sync": (C.c_int, [C.c_void_p]),
+    "drf_ens_step": (C.c_int, [C.c_void_p, _dp, C.c_int, C.c_int]),
+    "drf_ens_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int),
+                               C.POINTER(C.c_int)]),
 }
 
 

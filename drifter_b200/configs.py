@@ -5,6 +5,9 @@ C1  plain FP64 DG, CPU-runnable: 100x100 km closed basin, 16x16x4 hexes, N=3, Ga
 C2  uniform large DG: 200x200 km, 128x128x16 hexes, N=4, depth 20 m + 32 random Gaussians
     clipped to [20, 2000] m, M2 tide (1 m, 44714 s) on the west boundary, linear T
     stratification (20 C surface to 4 C bottom), S = 35.
+C5  uneven ensemble: 64 independent runs, N=3, meshes 16..64 x 16..64 x 4..8 hexes, per-member
+    seeded bathymetry (Gaussian bumps over a sloping shelf) and wind stress 0-0.2 N/m^2, mixed
+    precision.
 Any config can be shrunk (nx, ny, nz overrides) for parity tests: the generator keeps the
 physics and the seeded bathymetry law.
 """
@@ -165,3 +168,41 @@ def c4(n: int = 512, L: float = 51200.0, seed: int = SEED, lam: float = 1.0, eps
     d = ((1 - fu) * (1 - fv) * f[j0, i0] + fu * (1 - fv) * f[j0, i1] + (1 - fu) * fv * f[j1, i0]
          + fu * fv * f[j1, i1])
     return dict(n=n, L=L, lam=lam, eps=eps, d=d.copy(), name=f"C4 Bezier {n}x{n}")
+
+
+def c5_member(i: int, nx: int, ny: int, nz: int, order: int = 3, precision: str = "mixed",
+              seed: int = SEED) -> dict:
+    """Member i of the C5 ensemble: a closed 2 km-per-element basin with its own seeded
+    bathymetry (20-1000 m: a sloping shelf plus 8 Gaussian bumps) and uniform wind stress."""
+    rng = np.random.default_rng(seed + 1000 + i)
+    L = 2e3
+    cfg = DGConfig(nx=nx, ny=ny, nz=nz, order=order, Lx=nx * L, Ly=ny * L, precision=precision)
+    X, Y, Sg = node_coords(cfg)
+    h = 20.0 + 480.0 * X / cfg.Lx
+    for _ in range(8):
+        a, w = rng.uniform(0.0, 400.0), rng.uniform(0.03, 0.12) * min(cfg.Lx, cfg.Ly)
+        x0, y0 = rng.uniform(0.0, cfg.Lx), rng.uniform(0.0, cfg.Ly)
+        h += a * np.exp(-((X - x0) ** 2 + (Y - y0) ** 2) / (2 * w * w))
+    h = np.clip(h, 20.0, 1000.0)
+    tau = rng.uniform(0.0, 0.2)
+    ang = rng.uniform(0.0, 2 * np.pi)
+    f = np.full(cfg.n2, 1e-4)
+    taux = np.full(cfg.n2, tau * np.cos(ang))
+    tauy = np.full(cfg.n2, tau * np.sin(ang))
+    eta = np.zeros(cfg.n2)
+    H3 = expand_2d_to_3d(cfg, h + eta)
+    T = 8.0 + 8.0 * (1.0 + Sg)
+    q = [np.zeros(cfg.n3), np.zeros(cfg.n3), T * H3, 35.0 * H3]
+    nsub = 20
+    dt = _cfl_dt(cfg, h.max(), nsub)
+    return dict(cfg=cfg, h=h, f=f, taux=taux, tauy=tauy, q=q, eta=eta, dt=dt, nsub=nsub,
+                name=f"C5 member {i} {nx}x{ny}x{nz} N={order}")
+
+
+def c5(members: int = 64, nmin: int = 16, nmax: int = 64, zmin: int = 4, zmax: int = 8,
+       order: int = 3, precision: str = "mixed", seed: int = SEED) -> list:
+    """C5: an uneven ensemble; member sizes uniform in {nmin..nmax}^2 x {zmin..zmax}."""
+    rng = np.random.default_rng(seed + 5)
+    sizes = [(int(rng.integers(nmin, nmax + 1)), int(rng.integers(nmin, nmax + 1)),
+              int(rng.integers(zmin, zmax + 1))) for _ in range(members)]
+    return [c5_member(i, nx, ny, nz, order, precision, seed) for i, (nx, ny, nz) in enumerate(sizes)]

@@ -25,25 +25,27 @@
 namespace drf {
 namespace {
 
-__constant__ DevBasis cB;
+// Basis tables per node count NP (orders 1..MAXNP-1 each keep their own entry, so models of
+// different orders can live in one process).
+__constant__ DevBasis cBs[MAXNP + 1];
 
-template <typename T>
+template <typename T, int NP>
 struct BT;
-template <>
-struct BT<double> {
-    __device__ static double D(int i) { return cB.D[i]; }
-    __device__ static double D2(int i) { return cB.D2[i]; }
-    __device__ static double S(int i) { return cB.S[i]; }
-    __device__ static double w(int i) { return cB.w[i]; }
-    __device__ static double x(int i) { return cB.x[i]; }
+template <int NP>
+struct BT<double, NP> {
+    __device__ static double D(int i) { return cBs[NP].D[i]; }
+    __device__ static double D2(int i) { return cBs[NP].D2[i]; }
+    __device__ static double S(int i) { return cBs[NP].S[i]; }
+    __device__ static double w(int i) { return cBs[NP].w[i]; }
+    __device__ static double x(int i) { return cBs[NP].x[i]; }
 };
-template <>
-struct BT<float> {
-    __device__ static float D(int i) { return cB.Df[i]; }
-    __device__ static float D2(int i) { return cB.D2f[i]; }
-    __device__ static float S(int i) { return cB.Sf[i]; }
-    __device__ static float w(int i) { return cB.wf[i]; }
-    __device__ static float x(int i) { return cB.xf[i]; }
+template <int NP>
+struct BT<float, NP> {
+    __device__ static float D(int i) { return cBs[NP].Df[i]; }
+    __device__ static float D2(int i) { return cBs[NP].D2f[i]; }
+    __device__ static float S(int i) { return cBs[NP].Sf[i]; }
+    __device__ static float w(int i) { return cBs[NP].wf[i]; }
+    __device__ static float x(int i) { return cBs[NP].xf[i]; }
 };
 
 struct Geo {
@@ -187,13 +189,18 @@ inline size_t stage_smem_bytes(int nz, int np, size_t tsz) {
 // One CTA per water column; work is organised in pencils (lines of N+1 nodes) so every
 // thread applies the 1D operators to registers, with the operator entries read as
 // warp-uniform constants: x pencils (j,k,layer), y pencils (i,k,layer), z pencils (i,j,layer).
+//
+// stage_column is the work of one CTA on column c. `ph` is the phase parity the column's
+// mbarrier waits expect and `init` says whether this CTA still has to initialise the two
+// mbarriers (the first column a CTA processes). Returns false when a bounded wait gave up
+// (the status word is set); the CTA must then stop.
 template <typename T, int NP>
-__global__ void __launch_bounds__(STAGE_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) dg3d_stage_kernel(StageArgs<T> a) {
+__device__ __forceinline__ bool stage_column(const StageArgs<T> &a, int c, uint32_t ph, bool init) {
     constexpr int NP2 = NP * NP, NP3 = NP2 * NP, N = NP - 1;
-    using B = BT<T>;
+    using B = BT<T, NP>;
     const Geo &G = a.G;
     const int nz = G.nz, ncn = nz * NP3, npen = nz * NP2;
-    const int c = blockIdx.x, ex = c % G.nx, ey = c / G.nx;
+    const int ex = c % G.nx, ey = c / G.nx;
     const size_t base = (size_t)c * ncn;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw);
@@ -224,8 +231,14 @@ __global__ void __launch_bounds__(STAGE_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) dg3
     // ---- stage the column: state (and the 2N register) by TMA bulk copies when aligned
     if (a.bulk) {
         if (threadIdx.x == 0) {
-            mbar_init(&bars[0], 1);
-            mbar_init(&bars[1], 1);
+            if (init) {
+                mbar_init(&bars[0], 1);
+                mbar_init(&bars[1], 1);
+            } else {
+                // shared memory of the previous column was read and written by this CTA's
+                // threads: order those accesses before the bulk copies overwrite it
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            }
             const uint32_t bytes = (uint32_t)(ncn * sizeof(T));
             mbar_expect_tx(&bars[0], 4 * bytes);
 #pragma unroll
@@ -267,11 +280,11 @@ __global__ void __launch_bounds__(STAGE_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) dg3
         const int ez = t / NP, k = t % NP;
         sS1[t] = (ez == nz - 1 && k == N) ? T(1) : (T)(G.dsig * (ez + 0.5 * ((double)B::x(k) + 1.0)));
     }
-    if (threadIdx.x == 0) s_ok = a.bulk ? (int)mbar_wait(&bars[0], 0) : 1;
+    if (threadIdx.x == 0) s_ok = a.bulk ? (int)mbar_wait(&bars[0], ph) : 1;
     __syncthreads();
     if (!s_ok) {
         if (threadIdx.x == 0) atomicExch(a.err, DRF_E_TIMEOUT);
-        return;
+        return false;
     }
     etide = s_etide;
     if (a.corrU) {  // pending transport correction of the previous step
@@ -467,11 +480,11 @@ __global__ void __launch_bounds__(STAGE_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) dg3
     // ---- z pencils: advection d/dsigma, Coriolis, vertical diffusion, sigma faces, surface
     // and bed stresses, then the LSRK update and the FP64 column increments
     if (a.bulk && need_res) {
-        if (threadIdx.x == 0) s_ok = (int)mbar_wait(&bars[1], 0);
+        if (threadIdx.x == 0) s_ok = (int)mbar_wait(&bars[1], ph);
         __syncthreads();
         if (!s_ok) {
             if (threadIdx.x == 0) atomicExch(a.err, DRF_E_TIMEOUT);
-            return;
+            return false;
         }
     }
     for (int p = threadIdx.x; p < npen; p += blockDim.x) {
@@ -612,6 +625,13 @@ __global__ void __launch_bounds__(STAGE_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) dg3
             a.dHV3[i2] = (a.first ? 0.0 : a.dHV3[i2]) + hd * sv;
         }
     }
+    return true;
+}
+
+// One model: one CTA per water column.
+template <typename T, int NP>
+__global__ void __launch_bounds__(STAGE_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) dg3d_stage_kernel(StageArgs<T> a) {
+    stage_column<T, NP>(a, blockIdx.x, 0u, true);
 }
 
 // ------------------------------------------------------------------------- barotropic (FP64)
@@ -658,16 +678,16 @@ __device__ __forceinline__ void lf_minus_phys(const double UL[3], double ihL, do
 // FK is the face flux (the model's flux2d). Every global load, the neighbours' face values
 // included, is issued before the tile barrier.
 template <int NP, int FK>
-__device__ __forceinline__ bool baro_tile_phi(const BaroArgs &a, double &re, double &ru,
+__device__ __forceinline__ bool baro_tile_phi(const BaroArgs &a, int64_t tile, double &re, double &ru,
                                               double &rv, int64_t &t) {
     constexpr int NP2 = NP * NP, N = NP - 1;
     __shared__ double sE[BARO_CPB * NP2], sU[BARO_CPB * NP2], sV[BARO_CPB * NP2],
         sI[BARO_CPB * NP2], sD[NP2];
     const Geo &G = a.G;
     const int lc = threadIdx.x / NP2, an = threadIdx.x % NP2, i = an % NP, j = an / NP;
-    const int64_t c = (int64_t)blockIdx.x * BARO_CPB + lc;
+    const int64_t c = tile * BARO_CPB + lc;
     const bool valid = c < a.ncol;
-    if (threadIdx.x < NP2) sD[threadIdx.x] = cB.D[threadIdx.x];
+    if (threadIdx.x < NP2) sD[threadIdx.x] = cBs[NP].D[threadIdx.x];
     t = c * NP2 + an;
     const int ex = (int)(c % G.nx), ey = (int)(c / G.nx);
     // the neighbour node across this node's x face (i = 0 or N) and y face (j = 0 or N)
@@ -759,48 +779,67 @@ template <int NP, int FK>
 __global__ void baro_rhs_kernel(BaroArgs a, double *ke, double *ku, double *kv) {
     double re, ru, rv;
     int64_t t;
-    if (!baro_tile_phi<NP, FK>(a, re, ru, rv, t)) return;
+    if (!baro_tile_phi<NP, FK>(a, blockIdx.x, re, ru, rv, t)) return;
     ke[t] = re; ku[t] = ru; kv[t] = rv;
 }
 
 // F = (3D-integrated increment)/dt - Phi(U^n); keeps HU^n, HV^n for the transport correction.
 template <int NP, int FK>
-__global__ void baro_force_kernel(BaroArgs a, double dt, const double *dHU3, const double *dHV3,
-                                  double *Fx, double *Fy, double *HUo, double *HVo) {
+__device__ __forceinline__ void baro_force_body(const BaroArgs &a, int64_t tile, double dt, const double *dHU3,
+                                                const double *dHV3, double *Fx, double *Fy, double *HUo,
+                                                double *HVo) {
     double re, ru, rv;
     int64_t t;
-    if (!baro_tile_phi<NP, FK>(a, re, ru, rv, t)) return;
+    if (!baro_tile_phi<NP, FK>(a, tile, re, ru, rv, t)) return;
     Fx[t] = dHU3[t] / dt - ru;
     Fy[t] = dHV3[t] / dt - rv;
     HUo[t] = a.hu[t];
     HVo[t] = a.hv[t];
 }
-
 template <int NP, int FK>
-__global__ void BARO_BOUNDS baro_pred_kernel(BaroArgs a, double dtb, double *k1e, double *k1u, double *k1v,
-                                 double *es, double *us, double *vs) {
+__global__ void baro_force_kernel(BaroArgs a, double dt, const double *dHU3, const double *dHV3,
+                                  double *Fx, double *Fy, double *HUo, double *HVo) {
+    baro_force_body<NP, FK>(a, blockIdx.x, dt, dHU3, dHV3, Fx, Fy, HUo, HVo);
+}
+
+// Heun predictor: k1 = Phi(U^m), U* = U^m + dtb k1
+template <int NP, int FK>
+__device__ __forceinline__ void baro_pred_body(const BaroArgs &a, int64_t tile, double dtb, double *k1e,
+                                               double *k1u, double *k1v, double *es, double *us, double *vs) {
     double re, ru, rv;
     int64_t t;
-    if (!baro_tile_phi<NP, FK>(a, re, ru, rv, t)) return;
+    if (!baro_tile_phi<NP, FK>(a, tile, re, ru, rv, t)) return;
     k1e[t] = re; k1u[t] = ru; k1v[t] = rv;
     es[t] = a.e[t] + dtb * re;
     us[t] = a.hu[t] + dtb * ru;
     vs[t] = a.hv[t] + dtb * rv;
 }
-
 template <int NP, int FK>
-__global__ void BARO_BOUNDS baro_corr_kernel(BaroArgs a, double dtb, const double *k1e, const double *k1u,
-                                 const double *k1v, double *e, double *hu, double *hv,
-                                 double *esum, int first) {
+__global__ void BARO_BOUNDS baro_pred_kernel(BaroArgs a, double dtb, double *k1e, double *k1u, double *k1v,
+                                 double *es, double *us, double *vs) {
+    baro_pred_body<NP, FK>(a, blockIdx.x, dtb, k1e, k1u, k1v, es, us, vs);
+}
+
+// Heun corrector: U^{m+1} = U^m + dtb/2 (k1 + Phi(U*)); accumulates eta for its time mean
+template <int NP, int FK>
+__device__ __forceinline__ void baro_corr_body(const BaroArgs &a, int64_t tile, double dtb, const double *k1e,
+                                               const double *k1u, const double *k1v, double *e, double *hu,
+                                               double *hv, double *esum, int first) {
     double re, ru, rv;
     int64_t t;
-    if (!baro_tile_phi<NP, FK>(a, re, ru, rv, t)) return;
+    if (!baro_tile_phi<NP, FK>(a, tile, re, ru, rv, t)) return;
     const double hd = 0.5 * dtb;
     const double en = e[t] + hd * (k1e[t] + re);
     e[t] = en;
     hu[t] = hu[t] + hd * (k1u[t] + ru);
     hv[t] = hv[t] + hd * (k1v[t] + rv);
     esum[t] = (first ? 0.0 : esum[t]) + en;
+}
+template <int NP, int FK>
+__global__ void BARO_BOUNDS baro_corr_kernel(BaroArgs a, double dtb, const double *k1e, const double *k1u,
+                                 const double *k1v, double *e, double *hu, double *hv,
+                                 double *esum, int first) {
+    baro_corr_body<NP, FK>(a, blockIdx.x, dtb, k1e, k1u, k1v, e, hu, hv, esum, first);
 }
 
 __global__ void baro_finish_kernel(int64_t n2, int nsub, double dt, const double *esum,
@@ -809,6 +848,130 @@ __global__ void baro_finish_kernel(int64_t n2, int nsub, double dt, const double
                                    const double *dHV3, double *corrU, double *corrV, double *tdev) {
     const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (t == 0) tdev[0] = tdev[0] + dt;
+    if (t >= n2) return;
+    eta_avg[t] = esum[t] / nsub;
+    corrU[t] = HU[t] - (HUo[t] + dHU3[t]);
+    corrV[t] = HV[t] - (HVo[t] + dHV3[t]);
+}
+
+// ------------------------------------------------------------------------- ensembles
+// An ensemble keeps every array of its members in pools laid out array-major: member m's slice
+// of a 3D array starts at element off3, of a 2D array at off2, and its model time is tdev[m].
+// The launches below are built from the pool bases (member 0's pointers) and shift them per
+// CTA to the member the CTA works on.
+struct EnsMember {
+    int64_t off3, off2;
+    Geo G;
+    double dt;  // baroclinic step of this member
+    int ncol, bulk;
+};
+
+template <typename T>
+__device__ __forceinline__ void shift_stage(StageArgs<T> &a, const EnsMember &m, int idx) {
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+        a.qin[v] += m.off3;
+        a.qout[v] += m.off3;
+        a.res[v] += m.off3;
+    }
+    a.eta += m.off2; a.h += m.off2; a.f += m.off2; a.taux += m.off2; a.tauy += m.off2;
+    if (a.corrU) { a.corrU += m.off2; a.corrV += m.off2; }
+    a.dHU3 += m.off2; a.dHV3 += m.off2;
+    a.tdev += idx;
+    a.dt = (T)m.dt;
+    a.bulk = m.bulk;
+    a.G = m.G;
+}
+
+// Persistent stage launch over all members: CTA b takes work items b, b + gridDim.x, ...;
+// an item is (member, column), ordered tallest columns first so the tail of the launch is
+// made of the cheapest columns. Shared memory is sized for the tallest member.
+template <typename T, int NP>
+__global__ void __launch_bounds__(STAGE_MAX_THREADS, sizeof(T) == 4 ? 2 : 1)
+    dg3d_stage_ens_kernel(StageArgs<T> a, const EnsMember *mem, const int2 *items, int nitems) {
+    __shared__ StageArgs<T> sa;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    if (threadIdx.x == 0) {  // the column's two mbarriers, initialised once per CTA
+        uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw);
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+    }
+    // each column staged by bulk copies completes one phase of both barriers (the register
+    // barrier only in stages that read the register, which is the same for every item)
+    uint32_t ph = 0;
+    for (int w = blockIdx.x; w < nitems; w += gridDim.x) {
+        const int2 wi = items[w];
+        if (threadIdx.x == 0) {
+            StageArgs<T> b = a;
+            shift_stage(b, mem[wi.x], wi.x);
+            sa = b;
+        }
+        __syncthreads();
+        if (!stage_column<T, NP>(sa, wi.y, ph, false)) return;
+        if (sa.bulk) ph ^= 1u;
+        __syncthreads();  // the next item overwrites the column's shared memory and sa
+    }
+}
+
+__device__ __forceinline__ void shift_baro(BaroArgs &a, const EnsMember &m, int idx) {
+    a.e += m.off2; a.hu += m.off2; a.hv += m.off2; a.h += m.off2; a.f += m.off2;
+    if (a.Fx) { a.Fx += m.off2; a.Fy += m.off2; }
+    a.tdev += idx;
+    a.G = m.G;
+    a.ncol = m.ncol;
+}
+
+// Barotropic launches of an ensemble: block b is tile tiles[b].y of member tiles[b].x. The
+// substep's time offset is sub * (dt_m / nsub) as in the single-model step.
+struct BaroEns {
+    const EnsMember *mem;
+    const int2 *tiles;
+    int nsub, sub;
+};
+
+template <int NP, int FK>
+__global__ void baro_force_ens_kernel(BaroArgs a, BaroEns E, const double *dHU3, const double *dHV3,
+                                      double *Fx, double *Fy, double *HUo, double *HVo) {
+    const int2 w = E.tiles[blockIdx.x];
+    const EnsMember &m = E.mem[w.x];
+    shift_baro(a, m, w.x);
+    a.toff = 0.0;
+    const int64_t o = m.off2;
+    baro_force_body<NP, FK>(a, w.y, m.dt, dHU3 + o, dHV3 + o, Fx + o, Fy + o, HUo + o, HVo + o);
+}
+template <int NP, int FK>
+__global__ void BARO_BOUNDS baro_pred_ens_kernel(BaroArgs a, BaroEns E, double *k1e, double *k1u,
+                                                 double *k1v, double *es, double *us, double *vs) {
+    const int2 w = E.tiles[blockIdx.x];
+    const EnsMember &m = E.mem[w.x];
+    shift_baro(a, m, w.x);
+    const double dtb = m.dt / E.nsub;
+    a.toff = __dmul_rn((double)E.sub, dtb);
+    const int64_t o = m.off2;
+    baro_pred_body<NP, FK>(a, w.y, dtb, k1e + o, k1u + o, k1v + o, es + o, us + o, vs + o);
+}
+template <int NP, int FK>
+__global__ void BARO_BOUNDS baro_corr_ens_kernel(BaroArgs a, BaroEns E, const double *k1e, const double *k1u,
+                                                 const double *k1v, double *e, double *hu, double *hv,
+                                                 double *esum) {
+    const int2 w = E.tiles[blockIdx.x];
+    const EnsMember &m = E.mem[w.x];
+    shift_baro(a, m, w.x);
+    const double dtb = m.dt / E.nsub;
+    a.toff = __dadd_rn(__dmul_rn((double)E.sub, dtb), dtb);  // unfused, as the host computes it
+    const int64_t o = m.off2;
+    baro_corr_body<NP, FK>(a, w.y, dtb, k1e + o, k1u + o, k1v + o, e + o, hu + o, hv + o, esum + o,
+                           E.sub == 0);
+}
+
+// baro_finish_kernel over the pooled 2D arrays; each member's clock advances by its own dt.
+__global__ void baro_finish_ens_kernel(int64_t n2, int nsub, const EnsMember *mem, int nmem,
+                                       const double *esum, double *eta_avg, const double *HU,
+                                       const double *HV, const double *HUo, const double *HVo,
+                                       const double *dHU3, const double *dHV3, double *corrU,
+                                       double *corrV, double *tdev) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t < nmem) tdev[t] = tdev[t] + mem[t].dt;
     if (t >= n2) return;
     eta_avg[t] = esum[t] / nsub;
     corrU[t] = HU[t] - (HUo[t] + dHU3[t]);
@@ -840,7 +1003,7 @@ __global__ void column_integral_kernel(int64_t n2, int nz, double dsig, const T 
     for (int ez = 0; ez < nz; ++ez)
 #pragma unroll
         for (int k = 0; k < NP; ++k)
-            s += 0.5 * dsig * cB.w[k] * (double)q[(c * nz + ez) * NP3 + an + NP2 * k];
+            s += 0.5 * dsig * cBs[NP].w[k] * (double)q[(c * nz + ez) * NP3 + an + NP2 * k];
     out[t] = s;
 }
 
@@ -875,7 +1038,7 @@ __global__ void diag3d_kernel(int64_t n3, int nz, const T *Hu, const T *Hv, cons
         const int ln = (int)(t % NP3), an = ln % NP2, i = an % NP, j = an / NP, k = ln / NP2;
         const int64_t i2 = c * NP2 + an;
         const double H = eta[i2] + h[i2];
-        const double wv = wvol * cB.w[i] * cB.w[j] * cB.w[k];
+        const double wv = wvol * cBs[NP].w[i] * cBs[NP].w[j] * cBs[NP].w[k];
         const double hu = Hu[t], hv = Hv[t];
         en = wv * 0.5 * (hu * hu + hv * hv) / H;
         heat = wv * (double)HT[t];
@@ -910,7 +1073,7 @@ __global__ void diag2d_kernel(int64_t n2, int nz, const double *eta, const doubl
     double mw = 0, mu = 0, pe = 0, emax = -1e300, emin = 1e300;
     if (t < n2) {
         const int an = (int)(t % NP2), i = an % NP, j = an / NP;
-        const double H = eta[t] + h[t], wa = warea * cB.w[i] * cB.w[j];
+        const double H = eta[t] + h[t], wa = warea * cBs[NP].w[i] * cBs[NP].w[j];
         mw = wa * H;
         mu = (double)nz * NP * H;
         pe = wa * 0.5 * g * eta[t] * eta[t];
@@ -1012,6 +1175,12 @@ struct drf_dg {
     DevBuf<unsigned char> q3;  // [2 ping-pong][4 vars] + [4 res] + [4 tmp] of n3 values each
     DevBuf<double> d2;         // 2D FP64 arrays
     DevBuf<int> errbuf;        // device status word written by bounded waits
+    int *err = nullptr;        // the status word in use (errbuf, or the ensemble's)
+    // 3D arrays: q3p + (array * n3s + node) * tsz; n3s = n3 for a model that owns its memory,
+    // the pool length for an ensemble member (a view into the ensemble's pools)
+    unsigned char *q3p = nullptr;
+    int64_t n3s = 0;
+    bool view = false;
     DevBuf<double> diag;       // diagnostics partials
     double *h = nullptr, *f = nullptr, *taux = nullptr, *tauy = nullptr, *eta = nullptr,
            *HU = nullptr, *HV = nullptr, *eta_avg = nullptr, *esum = nullptr, *Fx = nullptr,
@@ -1025,9 +1194,32 @@ struct drf_dg {
     int graph_nsub = 0;
     size_t smem = 0;
 
-    void *q(int buf, int v) { return q3.p + ((size_t)buf * 4 + v) * n3 * tsz; }
-    void *res(int v) { return q3.p + ((size_t)8 + v) * n3 * tsz; }
-    void *tmp(int v) { return q3.p + ((size_t)12 + v) * n3 * tsz; }
+    void *q(int buf, int v) { return q3p + ((size_t)buf * 4 + v) * n3s * tsz; }
+    void *res(int v) { return q3p + ((size_t)8 + v) * n3s * tsz; }
+    void *tmp(int v) { return q3p + ((size_t)12 + v) * n3s * tsz; }
+
+    // 2D arrays per model (26 named arrays, then the model time)
+    static constexpr int N2ARRAYS = 27;
+    // Points the model at its device memory: 16 3D arrays of stride3 values from q3base and
+    // 26 2D arrays of stride2 values from d2base; tdev_ is its clock and err_ its status word.
+    void bind(unsigned char *q3base, int64_t stride3, double *d2base, int64_t stride2, double *tdev_,
+              int *err_) {
+        q3p = q3base;
+        n3s = stride3;
+        double *p = d2base;
+        auto take = [&]() { double *r = p; p += stride2; return r; };
+        h = take(); f = take(); taux = take(); tauy = take(); eta = take();
+        HU = take(); HV = take(); eta_avg = take(); esum = take(); Fx = take();
+        Fy = take(); HUo = take(); HVo = take();
+        for (int i = 0; i < 3; ++i) k1[i] = take();
+        for (int i = 0; i < 3; ++i) us[i] = take();
+        dHU3 = take(); dHV3 = take(); scratch2 = take();
+        corrU = take(); corrV = take();
+        tdev = tdev_;
+        err = err_;
+    }
+    void setup(const drf_mesh_desc *mesh, const drf_dg_params *params, const double *h_,
+               const double *f_, const double *taux_, const double *tauy_);
 
     void drop_graphs() {
         for (auto &g : graph)
@@ -1049,6 +1241,15 @@ struct drf_dg {
     void launch_stage(int in, int out, int s, double dt, int mode, void *const *rout,
                       T *omega_out, double *deta_out, const double *eta_use, double toff,
                       bool with_corr = false) {
+        const StageArgs<T> a = stage_args<T>(in, out, s, dt, mode, rout, omega_out, deta_out, eta_use, toff,
+                                             with_corr);
+        dg3d_stage_kernel<T, NP><<<ncol, stage_threads(), smem, stream>>>(a);
+        DRF_LAUNCHED();
+    }
+    template <typename T>
+    StageArgs<T> stage_args(int in, int out, int s, double dt, int mode, void *const *rout,
+                            T *omega_out, double *deta_out, const double *eta_use, double toff,
+                            bool with_corr) {
         StageArgs<T> a{};
         for (int v = 0; v < 4; ++v) {
             a.qin[v] = (const T *)q(in, v);
@@ -1064,10 +1265,9 @@ struct drf_dg {
         a.corrU = with_corr ? corrU : nullptr;
         a.corrV = with_corr ? corrV : nullptr;
         a.bulk = ((size_t)G.nz * np3 * sizeof(T)) % 16 == 0;
-        a.err = errbuf.p;
+        a.err = err;
         a.G = G;
-        dg3d_stage_kernel<T, NP><<<ncol, stage_threads(), smem, stream>>>(a);
-        DRF_LAUNCHED();
+        return a;
     }
 
     // folds a pending transport correction into the current state buffer
@@ -1147,13 +1347,23 @@ struct drf_dg {
 namespace drf {
 namespace {
 
+// Raises a kernel's dynamic shared-memory limit to what the device allows next to the kernel's
+// static shared memory.
+void allow_max_dynamic_smem(const void *fn, int optin_max) {
+    cudaFuncAttributes fa{};
+    DRF_CUDA(cudaFuncGetAttributes(&fa, fn));
+    DRF_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  optin_max - (int)fa.sharedSizeBytes));
+}
+
 void upload_phys_basis(const HostBasis &b) {
     static std::mutex mu;
-    static int cur_order[64] = {0};
+    static bool done[64][MAXNP + 1] = {};
     int dev = 0;
     DRF_CUDA(cudaGetDevice(&dev));
+    DRF_CHECK(b.np >= 2 && b.np <= MAXNP, DRF_E_UNSUPPORTED, "polynomial order out of range");
     std::lock_guard<std::mutex> lk(mu);
-    if (dev < 64 && cur_order[dev] == b.order) return;
+    if (dev < 64 && done[dev][b.np]) return;
     DevBasis db;
     std::memset(&db, 0, sizeof(db));
     for (int i = 0; i < b.np * b.np; ++i) {
@@ -1164,8 +1374,8 @@ void upload_phys_basis(const HostBasis &b) {
         db.w[i] = b.w[i]; db.x[i] = b.x[i];
         db.wf[i] = (float)b.w[i]; db.xf[i] = (float)b.x[i];
     }
-    DRF_CUDA(cudaMemcpyToSymbol(cB, &db, sizeof(db)));
-    if (dev < 64) cur_order[dev] = b.order;
+    DRF_CUDA(cudaMemcpyToSymbol(cBs, &db, sizeof(db), (size_t)b.np * sizeof(DevBasis)));
+    if (dev < 64) done[dev][b.np] = true;
 }
 
 template <typename T>
@@ -1198,16 +1408,69 @@ void check_model(drf_dg *m) { DRF_CHECK(m != nullptr, DRF_E_INVALID, "null model
 // surfaces a status word set on the device (a bounded wait that gave up)
 void check_device_status(drf_dg *m) {
     int st = 0;
-    DRF_CUDA(cudaMemcpyAsync(&st, m->errbuf.p, sizeof(int), cudaMemcpyDeviceToHost, m->stream));
+    DRF_CUDA(cudaMemcpyAsync(&st, m->err, sizeof(int), cudaMemcpyDeviceToHost, m->stream));
     DRF_CUDA(cudaStreamSynchronize(m->stream));
     if (st != 0) {
-        DRF_CUDA(cudaMemsetAsync(m->errbuf.p, 0, sizeof(int), m->stream));
+        DRF_CUDA(cudaMemsetAsync(m->err, 0, sizeof(int), m->stream));
         throw Error(st, "a device-side wait gave up (status " + std::to_string(st) + ")");
     }
 }
 
 }  // namespace
 }  // namespace drf
+
+// Host-side set-up shared by a model and an ensemble member: argument checks, basis tables,
+// geometry constants and the stage kernel's shared-memory size. No device memory is touched.
+void drf_dg::setup(const drf_mesh_desc *mesh, const drf_dg_params *params, const double *h_,
+                   const double *f_, const double *taux_, const double *tauy_) {
+    DRF_CHECK(mesh->nx >= 1 && mesh->ny >= 1 && mesh->nz >= 1, DRF_E_INVALID,
+              "mesh must have at least one element per direction");
+    DRF_CHECK(mesh->Lx > 0 && mesh->Ly > 0, DRF_E_INVALID, "basin extent must be positive");
+    DRF_CHECK(params->flux2d >= 0 && params->flux2d <= 2, DRF_E_INVALID, "unknown flux kind");
+    DRF_CHECK(params->precision == DRF_PREC_FP64 || params->precision == DRF_PREC_MIXED,
+              DRF_E_INVALID, "unknown precision");
+    for (int s = 0; s < 4; ++s)
+        DRF_CHECK(params->bc[s] == DRF_BC_WALL || params->bc[s] == DRF_BC_TIDE, DRF_E_INVALID,
+                  "unknown boundary type");
+    this->mesh = *mesh;  // (the parameters shadow the members of the same name)
+    this->prm = *params;
+    basis = make_lgl_basis(mesh->order);
+    np = basis.np; np2 = np * np; np3 = np2 * np;
+    ncol = mesh->nx * mesh->ny;
+    n2 = (int64_t)ncol * np2;
+    n3 = n2 * mesh->nz * np;
+    mixed = params->precision == DRF_PREC_MIXED;
+    tsz = mixed ? 4 : 8;
+    for (const double *a : {h_, f_, taux_, tauy_})
+        DRF_CHECK(all_finite(a, n2), DRF_E_NONFINITE, "non-finite value in a 2D field");
+    for (int64_t i = 0; i < n2; ++i)
+        DRF_CHECK(h_[i] > 0.0, DRF_E_INVALID, "bathymetry must be positive (no dry nodes)");
+    const double dx = mesh->Lx / mesh->nx, dy = mesh->Ly / mesh->ny, ds = 1.0 / mesh->nz;
+    const double wend = basis.w[0];
+    G.nx = mesh->nx; G.ny = mesh->ny; G.nz = mesh->nz; G.flux2d = params->flux2d;
+    for (int s = 0; s < 4; ++s) G.bc[s] = params->bc[s];
+    G.cx = 2.0 / dx; G.cy = 2.0 / dy; G.cs = 2.0 / ds;
+    G.Lx = G.cx / wend; G.Ly = G.cy / wend; G.Ls = G.cs / wend; G.dsig = ds;
+    G.g = params->g; G.rho0 = params->rho0; G.nu_h = params->nu_h; G.nu_v = params->nu_v;
+    G.kT = params->kappa_v_T; G.kS = params->kappa_v_S; G.cd = params->cd;
+    G.tide_amp = params->tide_amp;
+    G.tide_w = params->tide_period != 0.0 ? 2.0 * M_PI / params->tide_period : 0.0;
+    upload_phys_basis(basis);
+    // shared memory of the stage kernel: 9 column arrays + per-layer bases + 2D scalars
+    smem = stage_smem_bytes(mesh->nz, np, tsz);
+    int dev = 0, maxsm = 0;
+    DRF_CUDA(cudaGetDevice(&dev));
+    DRF_CUDA(cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    DRF_CHECK(smem + 512 <= (size_t)maxsm, DRF_E_UNSUPPORTED,
+              "water column too tall for one CTA: nz*(N+1)^3 too large");
+    // the limit is a property of the kernel, shared by every model in the process: allow the
+    // device maximum (the shared memory a launch actually asks for sets its occupancy)
+    with_types([&](auto tv, auto npc) {
+        using T = decltype(tv);
+        constexpr int NP = decltype(npc)::value;
+        allow_max_dynamic_smem(reinterpret_cast<const void *>(dg3d_stage_kernel<T, NP>), maxsm);
+    });
+}
 
 extern "C" {
 
@@ -1216,74 +1479,18 @@ int drf_dg_create(const drf_mesh_desc *mesh, const drf_dg_params *params, const 
     return guard([&] {
         DRF_CHECK(mesh && params && h && f && taux && tauy && out, DRF_E_INVALID, "null argument");
         *out = nullptr;
-        DRF_CHECK(mesh->nx >= 1 && mesh->ny >= 1 && mesh->nz >= 1, DRF_E_INVALID,
-                  "mesh must have at least one element per direction");
-        DRF_CHECK(mesh->Lx > 0 && mesh->Ly > 0, DRF_E_INVALID, "basin extent must be positive");
-        DRF_CHECK(params->flux2d >= 0 && params->flux2d <= 2, DRF_E_INVALID, "unknown flux kind");
-        DRF_CHECK(params->precision == DRF_PREC_FP64 || params->precision == DRF_PREC_MIXED,
-                  DRF_E_INVALID, "unknown precision");
-        for (int s = 0; s < 4; ++s)
-            DRF_CHECK(params->bc[s] == DRF_BC_WALL || params->bc[s] == DRF_BC_TIDE, DRF_E_INVALID,
-                      "unknown boundary type");
         auto m = std::make_unique<drf_dg>();
-        m->mesh = *mesh;
-        m->prm = *params;
-        m->basis = make_lgl_basis(mesh->order);
-        m->np = m->basis.np; m->np2 = m->np * m->np; m->np3 = m->np2 * m->np;
-        m->ncol = mesh->nx * mesh->ny;
-        m->n2 = (int64_t)m->ncol * m->np2;
-        m->n3 = m->n2 * mesh->nz * m->np;
-        m->mixed = params->precision == DRF_PREC_MIXED;
-        m->tsz = m->mixed ? 4 : 8;
-        for (const double *a : {h, f, taux, tauy})
-            DRF_CHECK(all_finite(a, m->n2), DRF_E_NONFINITE, "non-finite value in a 2D field");
-        for (int64_t i = 0; i < m->n2; ++i)
-            DRF_CHECK(h[i] > 0.0, DRF_E_INVALID, "bathymetry must be positive (no dry nodes)");
-        Geo &G = m->G;
-        const double dx = mesh->Lx / mesh->nx, dy = mesh->Ly / mesh->ny, ds = 1.0 / mesh->nz;
-        const double wend = m->basis.w[0];
-        G.nx = mesh->nx; G.ny = mesh->ny; G.nz = mesh->nz; G.flux2d = params->flux2d;
-        for (int s = 0; s < 4; ++s) G.bc[s] = params->bc[s];
-        G.cx = 2.0 / dx; G.cy = 2.0 / dy; G.cs = 2.0 / ds;
-        G.Lx = G.cx / wend; G.Ly = G.cy / wend; G.Ls = G.cs / wend; G.dsig = ds;
-        G.g = params->g; G.rho0 = params->rho0; G.nu_h = params->nu_h; G.nu_v = params->nu_v;
-        G.kT = params->kappa_v_T; G.kS = params->kappa_v_S; G.cd = params->cd;
-        G.tide_amp = params->tide_amp;
-        G.tide_w = params->tide_period != 0.0 ? 2.0 * M_PI / params->tide_period : 0.0;
-        upload_phys_basis(m->basis);
+        m->setup(mesh, params, h, f, taux, tauy);
         DRF_CUDA(cudaStreamCreateWithFlags(&m->own, cudaStreamNonBlocking));
         m->stream = m->own;
-        // shared memory of the stage kernel: 9 column arrays + per-layer bases + 2D scalars
-        const int ncn = mesh->nz * m->np3;
-        m->smem = stage_smem_bytes(mesh->nz, m->np, m->tsz);
-        int dev = 0, maxsm = 0;
-        DRF_CUDA(cudaGetDevice(&dev));
-        DRF_CUDA(cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-        DRF_CHECK(m->smem <= (size_t)maxsm, DRF_E_UNSUPPORTED,
-                  "water column too tall for one CTA: nz*(N+1)^3 too large");
-        m->with_types([&](auto tv, auto npc) {
-            using T = decltype(tv);
-            constexpr int NP = decltype(npc)::value;
-            DRF_CUDA(cudaFuncSetAttribute(dg3d_stage_kernel<T, NP>,
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)m->smem));
-        });
         m->errbuf.alloc(1);
         DRF_CUDA(cudaMemset(m->errbuf.p, 0, sizeof(int)));
         m->q3.alloc((size_t)16 * m->n3 * m->tsz);
         DRF_CUDA(cudaMemset(m->q3.p, 0, m->q3.n));
-        const int n2arrays = 27;
-        m->d2.alloc((size_t)n2arrays * m->n2 + 8);
+        m->d2.alloc((size_t)drf_dg::N2ARRAYS * m->n2 + 8);
         DRF_CUDA(cudaMemset(m->d2.p, 0, m->d2.n * 8));
-        double *p = m->d2.p;
-        auto take = [&]() { double *r = p; p += m->n2; return r; };
-        m->h = take(); m->f = take(); m->taux = take(); m->tauy = take(); m->eta = take();
-        m->HU = take(); m->HV = take(); m->eta_avg = take(); m->esum = take(); m->Fx = take();
-        m->Fy = take(); m->HUo = take(); m->HVo = take();
-        for (int i = 0; i < 3; ++i) m->k1[i] = take();
-        for (int i = 0; i < 3; ++i) m->us[i] = take();
-        m->dHU3 = take(); m->dHV3 = take(); m->scratch2 = take();
-        m->corrU = take(); m->corrV = take();
-        m->tdev = p;
+        m->bind(m->q3.p, m->n3, m->d2.p, m->n2, m->d2.p + (size_t)(drf_dg::N2ARRAYS - 1) * m->n2,
+                m->errbuf.p);
         DRF_CUDA(cudaMemcpy(m->h, h, m->n2 * 8, cudaMemcpyHostToDevice));
         DRF_CUDA(cudaMemcpy(m->f, f, m->n2 * 8, cudaMemcpyHostToDevice));
         DRF_CUDA(cudaMemcpy(m->taux, taux, m->n2 * 8, cudaMemcpyHostToDevice));
@@ -1295,6 +1502,7 @@ int drf_dg_create(const drf_mesh_desc *mesh, const drf_dg_params *params, const 
 int drf_dg_destroy(drf_dg *m) {
     return guard([&] {
         if (!m) return;
+        DRF_CHECK(!m->view, DRF_E_INVALID, "an ensemble member is destroyed with its ensemble");
         if (m->stream) cudaStreamSynchronize(m->stream);
         delete m;
     });
@@ -1303,6 +1511,7 @@ int drf_dg_destroy(drf_dg *m) {
 int drf_dg_set_stream(drf_dg *m, void *s) {
     return guard([&] {
         check_model(m);
+        DRF_CHECK(!m->view, DRF_E_INVALID, "set the stream of the ensemble, not of a member");
         DRF_CUDA(cudaStreamSynchronize(m->stream));
         m->drop_graphs();
         m->stream = s ? (cudaStream_t)s : m->own;
@@ -1324,10 +1533,10 @@ int drf_dg_upload_state(drf_dg *m, const double *const *q4, const double *eta, d
         for (int v = 0; v < 4; ++v)
             DRF_CHECK(q4[v] && all_finite(q4[v], m->n3), DRF_E_NONFINITE, "non-finite state value");
         DRF_CHECK(all_finite(eta, m->n2), DRF_E_NONFINITE, "non-finite eta");
-        m->cur = 0;
+        if (!m->view) m->cur = 0;  // an ensemble member keeps the ensemble's buffer parity
         for (int v = 0; v < 4; ++v) {
-            if (m->mixed) to_device<float>(m, m->q(0, v), q4[v]);
-            else to_device<double>(m, m->q(0, v), q4[v]);
+            if (m->mixed) to_device<float>(m, m->q(m->cur, v), q4[v]);
+            else to_device<double>(m, m->q(m->cur, v), q4[v]);
         }
         DRF_CUDA(cudaMemcpyAsync(m->eta, eta, m->n2 * 8, cudaMemcpyHostToDevice, m->stream));
         DRF_CUDA(cudaMemcpyAsync(m->eta_avg, eta, m->n2 * 8, cudaMemcpyHostToDevice, m->stream));
@@ -1425,6 +1634,7 @@ int drf_dg_compute_rhs2d(drf_dg *m, const double *Fx, const double *Fy, double t
 int drf_dg_step_modesplit(drf_dg *m, double dt, int nsub, int nsteps) {
     return guard([&] {
         check_model(m);
+        DRF_CHECK(!m->view, DRF_E_INVALID, "ensemble members are stepped together (drf_ens_step)");
         DRF_CHECK(nsub >= 1, DRF_E_INVALID, "nsub must be >= 1");
         DRF_CHECK(dt > 0.0 && std::isfinite(dt), DRF_E_INVALID, "dt must be positive");
         DRF_CHECK(nsteps >= 0, DRF_E_INVALID, "nsteps must be >= 0");
@@ -1692,6 +1902,277 @@ int drf_dg_info(drf_dg *m, int64_t *n3d, int64_t *n2d, int *precision) {
         if (n3d) *n3d = m->n3;
         if (n2d) *n2d = m->n2;
         if (precision) *precision = m->prm.precision;
+    });
+}
+
+}  // extern "C"
+
+// ----------------------------------------------------------------------------- ensembles
+struct drf_ens {
+    std::vector<std::unique_ptr<drf_dg>> mem;  // member views into the pools below
+    DevBuf<unsigned char> q3;                  // 16 pooled 3D arrays
+    DevBuf<double> d2;                         // 26 pooled 2D arrays + one clock per member
+    DevBuf<int> errbuf;
+    DevBuf<EnsMember> table;
+    DevBuf<int2> items, tiles;
+    std::vector<EnsMember> htab;
+    int nitems = 0, ntiles = 0, grid = 0, threads = 0;
+    size_t smem = 0;
+    int64_t n3tot = 0, n2tot = 0;
+    cudaStream_t stream = nullptr, own = nullptr;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    int graph_nsub = 0;
+    int cur = 0;
+
+    void drop_graphs() {
+        for (auto &g : graph)
+            if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+        graph_nsub = 0;
+    }
+    ~drf_ens() {
+        drop_graphs();
+        if (own) cudaStreamDestroy(own);
+    }
+
+    // one baroclinic step of every member from ping-pong buffer `in`, as drf_dg::enqueue_step
+    template <typename T, int NP>
+    void enqueue(int in, int nsub) {
+        drf_dg *m0 = mem[0].get();  // its arrays start the pools
+        const int out = 1 - in;
+        int src = in;
+        for (int s = 0; s < 5; ++s) {
+            const int dst = (s % 2 == 0) ? out : in;
+            const StageArgs<T> a = m0->template stage_args<T>(src, dst, s, 0.0, 0, nullptr, nullptr, nullptr,
+                                                              m0->eta, 0.0, s == 0);
+            dg3d_stage_ens_kernel<T, NP><<<grid, threads, smem, stream>>>(a, table.p, items.p, nitems);
+            DRF_LAUNCHED();
+            src = dst;
+        }
+        const int bt = BARO_CPB * NP * NP;
+        dispatch_flux(m0->G.flux2d, [&](auto fk) {
+            constexpr int FK = decltype(fk)::value;
+            baro_force_ens_kernel<NP, FK><<<ntiles, bt, 0, stream>>>(
+                m0->template baro<NP>(m0->eta, m0->HU, m0->HV, false, 0.0), BaroEns{table.p, tiles.p, nsub, 0},
+                m0->dHU3, m0->dHV3, m0->Fx, m0->Fy, m0->HUo, m0->HVo);
+            DRF_LAUNCHED();
+            for (int sub = 0; sub < nsub; ++sub) {
+                const BaroEns E{table.p, tiles.p, nsub, sub};
+                baro_pred_ens_kernel<NP, FK><<<ntiles, bt, 0, stream>>>(
+                    m0->template baro<NP>(m0->eta, m0->HU, m0->HV, true, 0.0), E, m0->k1[0], m0->k1[1],
+                    m0->k1[2], m0->us[0], m0->us[1], m0->us[2]);
+                DRF_LAUNCHED();
+                baro_corr_ens_kernel<NP, FK><<<ntiles, bt, 0, stream>>>(
+                    m0->template baro<NP>(m0->us[0], m0->us[1], m0->us[2], true, 0.0), E, m0->k1[0], m0->k1[1],
+                    m0->k1[2], m0->eta, m0->HU, m0->HV, m0->esum);
+                DRF_LAUNCHED();
+            }
+        });
+        const int64_t nfin = n2tot > (int64_t)mem.size() ? n2tot : (int64_t)mem.size();
+        baro_finish_ens_kernel<<<blocks_for(nfin), 256, 0, stream>>>(
+            n2tot, nsub, table.p, (int)mem.size(), m0->esum, m0->eta_avg, m0->HU, m0->HV, m0->HUo, m0->HVo,
+            m0->dHU3, m0->dHV3, m0->corrU, m0->corrV, m0->tdev);
+        DRF_LAUNCHED();
+    }
+};
+
+namespace {
+void check_ens(drf_ens *e) { DRF_CHECK(e != nullptr, DRF_E_INVALID, "null ensemble handle"); }
+}  // namespace
+
+extern "C" {
+
+int drf_ens_create(int nmembers, const drf_mesh_desc *meshes, const drf_dg_params *params,
+                   const double *const *h, const double *const *f, const double *const *taux,
+                   const double *const *tauy, drf_ens **out) {
+    return guard([&] {
+        DRF_CHECK(out && meshes && params && h && f && taux && tauy, DRF_E_INVALID, "null argument");
+        *out = nullptr;
+        DRF_CHECK(nmembers >= 1, DRF_E_INVALID, "an ensemble needs at least one member");
+        auto e = std::make_unique<drf_ens>();
+        // members: host set-up and pool offsets (3D slices padded to 64 values, 256 B in FP32,
+        // so every member's column blocks keep the 16-byte alignment of the bulk copies)
+        std::vector<int64_t> off3(nmembers), off2(nmembers);
+        for (int i = 0; i < nmembers; ++i) {
+            DRF_CHECK(h[i] && f[i] && taux[i] && tauy[i], DRF_E_INVALID, "null member field");
+            auto m = std::make_unique<drf_dg>();
+            m->setup(&meshes[i], &params[i], h[i], f[i], taux[i], tauy[i]);
+            if (i > 0) {
+                const drf_dg &m0 = *e->mem[0];
+                DRF_CHECK(m->np == m0.np && m->mixed == m0.mixed && m->G.flux2d == m0.G.flux2d,
+                          DRF_E_INVALID, "ensemble members must share order, precision and 2D flux");
+            }
+            m->view = true;
+            off3[i] = e->n3tot;
+            off2[i] = e->n2tot;
+            e->n3tot += (m->n3 + 63) / 64 * 64;
+            e->n2tot += m->n2;
+            e->threads = std::max(e->threads, m->stage_threads());
+            e->smem = std::max(e->smem, m->smem);
+            e->mem.push_back(std::move(m));
+        }
+        drf_dg &m0 = *e->mem[0];
+        DRF_CUDA(cudaStreamCreateWithFlags(&e->own, cudaStreamNonBlocking));
+        e->stream = e->own;
+        e->errbuf.alloc(1);
+        DRF_CUDA(cudaMemset(e->errbuf.p, 0, sizeof(int)));
+        e->q3.alloc((size_t)16 * e->n3tot * m0.tsz);
+        DRF_CUDA(cudaMemset(e->q3.p, 0, e->q3.n));
+        e->d2.alloc((size_t)(drf_dg::N2ARRAYS - 1) * e->n2tot + nmembers);
+        DRF_CUDA(cudaMemset(e->d2.p, 0, e->d2.n * 8));
+        double *tdev = e->d2.p + (size_t)(drf_dg::N2ARRAYS - 1) * e->n2tot;
+        // work lists: stage items (member, column), tallest columns first; barotropic tiles
+        std::vector<int2> items, tiles;
+        for (int i = 0; i < nmembers; ++i) {
+            drf_dg &m = *e->mem[i];
+            m.bind(e->q3.p + (size_t)off3[i] * m.tsz, e->n3tot, e->d2.p + off2[i], e->n2tot, tdev + i, e->errbuf.p);
+            m.stream = e->stream;
+            DRF_CUDA(cudaMemcpy(m.h, h[i], m.n2 * 8, cudaMemcpyHostToDevice));
+            DRF_CUDA(cudaMemcpy(m.f, f[i], m.n2 * 8, cudaMemcpyHostToDevice));
+            DRF_CUDA(cudaMemcpy(m.taux, taux[i], m.n2 * 8, cudaMemcpyHostToDevice));
+            DRF_CUDA(cudaMemcpy(m.tauy, tauy[i], m.n2 * 8, cudaMemcpyHostToDevice));
+            EnsMember t{};
+            t.off3 = off3[i];
+            t.off2 = off2[i];
+            t.G = m.G;
+            t.dt = 0.0;
+            t.ncol = m.ncol;
+            t.bulk = ((size_t)m.G.nz * m.np3 * m.tsz) % 16 == 0 && ((size_t)off3[i] * m.tsz) % 16 == 0 &&
+                     ((size_t)e->n3tot * m.tsz) % 16 == 0;
+            e->htab.push_back(t);
+            for (int c = 0; c < m.ncol; ++c) items.push_back(make_int2(i, c));
+            for (int b = 0; b < (m.ncol + BARO_CPB - 1) / BARO_CPB; ++b) tiles.push_back(make_int2(i, b));
+        }
+        std::stable_sort(items.begin(), items.end(), [&](int2 a, int2 b) {
+            return e->mem[a.x]->G.nz > e->mem[b.x]->G.nz;
+        });
+        e->nitems = (int)items.size();
+        e->ntiles = (int)tiles.size();
+        e->table.alloc(nmembers);
+        DRF_CUDA(cudaMemcpy(e->table.p, e->htab.data(), nmembers * sizeof(EnsMember), cudaMemcpyHostToDevice));
+        e->items.alloc(items.size());
+        DRF_CUDA(cudaMemcpy(e->items.p, items.data(), items.size() * sizeof(int2), cudaMemcpyHostToDevice));
+        e->tiles.alloc(tiles.size());
+        DRF_CUDA(cudaMemcpy(e->tiles.p, tiles.data(), tiles.size() * sizeof(int2), cudaMemcpyHostToDevice));
+        // persistent grid: as many stage CTAs as fit on the device at once
+        int dev = 0, nsm = 0, per_sm = 0;
+        DRF_CUDA(cudaGetDevice(&dev));
+        DRF_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+        m0.with_types([&](auto tv, auto npc) {
+            using T = decltype(tv);
+            constexpr int NP = decltype(npc)::value;
+            int maxsm = 0;
+            DRF_CUDA(cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+            allow_max_dynamic_smem(reinterpret_cast<const void *>(dg3d_stage_ens_kernel<T, NP>), maxsm);
+            DRF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dg3d_stage_ens_kernel<T, NP>,
+                                                                   e->threads, e->smem));
+        });
+        DRF_CHECK(per_sm >= 1, DRF_E_UNSUPPORTED, "ensemble stage kernel does not fit on an SM");
+        e->grid = std::min(e->nitems, per_sm * nsm);
+        *out = e.release();
+    });
+}
+
+int drf_ens_destroy(drf_ens *e) {
+    return guard([&] {
+        if (!e) return;
+        if (e->stream) cudaStreamSynchronize(e->stream);
+        delete e;
+    });
+}
+
+int drf_ens_member(drf_ens *e, int i, drf_dg **member) {
+    return guard([&] {
+        check_ens(e);
+        DRF_CHECK(member, DRF_E_INVALID, "null output");
+        DRF_CHECK(i >= 0 && i < (int)e->mem.size(), DRF_E_INVALID, "member index out of range");
+        *member = e->mem[i].get();
+    });
+}
+
+int drf_ens_set_stream(drf_ens *e, void *s) {
+    return guard([&] {
+        check_ens(e);
+        DRF_CUDA(cudaStreamSynchronize(e->stream));
+        e->drop_graphs();
+        e->stream = s ? (cudaStream_t)s : e->own;
+        for (auto &m : e->mem) {
+            m->drop_graphs();
+            m->stream = e->stream;
+        }
+    });
+}
+
+int drf_ens_sync(drf_ens *e) {
+    return guard([&] {
+        check_ens(e);
+        DRF_CUDA(cudaStreamSynchronize(e->stream));
+        check_device_status(e->mem[0].get());
+    });
+}
+
+int drf_ens_step(drf_ens *e, const double *dt, int nsub, int nsteps) {
+    return guard([&] {
+        check_ens(e);
+        DRF_CHECK(dt, DRF_E_INVALID, "null argument");
+        DRF_CHECK(nsub >= 1, DRF_E_INVALID, "nsub must be >= 1");
+        DRF_CHECK(nsteps >= 0, DRF_E_INVALID, "nsteps must be >= 0");
+        bool changed = false;
+        for (size_t i = 0; i < e->mem.size(); ++i) {
+            DRF_CHECK(dt[i] > 0.0 && std::isfinite(dt[i]), DRF_E_INVALID, "dt must be positive");
+            DRF_CHECK(e->mem[i]->cur == e->cur, DRF_E_INVALID, "ensemble member out of step");
+            if (e->htab[i].dt != dt[i]) {
+                e->htab[i].dt = dt[i];
+                changed = true;
+            }
+        }
+        if (changed)  // step sizes live in the member table the graphs read
+            DRF_CUDA(cudaMemcpyAsync(e->table.p, e->htab.data(), e->htab.size() * sizeof(EnsMember),
+                                     cudaMemcpyHostToDevice, e->stream));
+        if (e->graph_nsub != nsub) {
+            e->drop_graphs();
+            for (int in = 0; in < 2; ++in) {
+                cudaGraph_t g = nullptr;
+                DRF_CUDA(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+                try {
+                    e->mem[0]->with_types([&](auto tv, auto npc) {
+                        using T = decltype(tv);
+                        constexpr int NP = decltype(npc)::value;
+                        e->template enqueue<T, NP>(in, nsub);
+                    });
+                } catch (...) {
+                    cudaStreamEndCapture(e->stream, &g);
+                    if (g) cudaGraphDestroy(g);
+                    throw;
+                }
+                DRF_CUDA(cudaStreamEndCapture(e->stream, &g));
+                cudaError_t st = cudaGraphInstantiate(&e->graph[in], g, 0);
+                cudaGraphDestroy(g);
+                DRF_CUDA(st);
+            }
+            e->graph_nsub = nsub;
+        }
+        for (int s = 0; s < nsteps; ++s) {
+            DRF_CUDA(cudaGraphLaunch(e->graph[e->cur], e->stream));
+            launch_counter().fetch_add(5 + 2 + 2 * (uint64_t)nsub);
+            e->cur = 1 - e->cur;
+        }
+        for (auto &m : e->mem) {
+            m->cur = e->cur;
+            if (nsteps > 0) m->pending = true;
+        }
+    });
+}
+
+int drf_ens_info(drf_ens *e, int64_t *n3d, int *items, int *grid) {
+    return guard([&] {
+        check_ens(e);
+        if (n3d) {
+            int64_t s = 0;
+            for (auto &m : e->mem) s += m->n3;
+            *n3d = s;
+        }
+        if (items) *items = e->nitems;
+        if (grid) *grid = e->grid;
     });
 }
 

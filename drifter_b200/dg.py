@@ -124,29 +124,43 @@ class DGConfig:
         return self.nx * self.ny * self.np_ ** 2
 
 
+def _mesh_params(cfg: DGConfig):
+    mesh = _abi.MeshDesc(cfg.nx, cfg.ny, cfg.nz, cfg.order, cfg.Lx, cfg.Ly)
+    prm = _abi.DGParams()
+    prm.g, prm.rho0, prm.nu_h, prm.nu_v = cfg.g, cfg.rho0, cfg.nu_h, cfg.nu_v
+    prm.kappa_v_T, prm.kappa_v_S, prm.cd = cfg.kappa_v_T, cfg.kappa_v_S, cfg.cd
+    prm.flux2d = _abi.FLUX[cfg.flux2d]
+    prm.precision = _abi.PREC[cfg.precision]
+    for s in range(4):
+        prm.bc[s] = _abi.BC[cfg.bc[s]]
+    prm.tide_amp, prm.tide_period = cfg.tide_amp, cfg.tide_period
+    return mesh, prm
+
+
 class OceanModel:
     """Coupled sigma-coordinate DG model resident on the GPU (one CUDA stream)."""
 
     def __init__(self, cfg: DGConfig, h, f, taux, tauy):
         self.cfg = cfg
-        mesh = _abi.MeshDesc(cfg.nx, cfg.ny, cfg.nz, cfg.order, cfg.Lx, cfg.Ly)
-        prm = _abi.DGParams()
-        prm.g, prm.rho0, prm.nu_h, prm.nu_v = cfg.g, cfg.rho0, cfg.nu_h, cfg.nu_v
-        prm.kappa_v_T, prm.kappa_v_S, prm.cd = cfg.kappa_v_T, cfg.kappa_v_S, cfg.cd
-        prm.flux2d = _abi.FLUX[cfg.flux2d]
-        prm.precision = _abi.PREC[cfg.precision]
-        for s in range(4):
-            prm.bc[s] = _abi.BC[cfg.bc[s]]
-        prm.tide_amp, prm.tide_period = cfg.tide_amp, cfg.tide_period
+        mesh, prm = _mesh_params(cfg)
         self._keep = [_c(h), _c(f), _c(taux), _c(tauy)]
         hd = C.c_void_p()
         check(lib().drf_dg_create(C.byref(mesh), C.byref(prm), *[dptr(a) for a in self._keep],
                                   C.byref(hd)))
         self.handle = hd
+        self._owner = None
+
+    @classmethod
+    def _member(cls, cfg: DGConfig, handle, owner) -> "OceanModel":
+        """A member of an Ensemble: shares the ensemble's memory and stream, stepped by it."""
+        m = cls.__new__(cls)
+        m.cfg, m.handle, m._owner = cfg, handle, owner
+        return m
 
     def close(self):
         if getattr(self, "handle", None):
-            lib().drf_dg_destroy(self.handle)
+            if self._owner is None:
+                lib().drf_dg_destroy(self.handle)
             self.handle = None
 
     def __del__(self):
@@ -216,3 +230,61 @@ class OceanModel:
         ms, ab, nd = C.c_double(), C.c_double(), C.c_double()
         check(lib().drf_dg_time_stage(self.handle, nrep, C.byref(ms), C.byref(ab), C.byref(nd)))
         return dict(ms=ms.value, alg_bytes=ab.value, ndof=nd.value)
+
+
+class Ensemble:
+    """Independent coupled DG runs stepped together (one persistent launch per LSRK stage of
+    all members, one launch per barotropic substep, one CUDA graph per baroclinic step).
+
+    `members[i]` is an OceanModel view of member i (upload/download/diagnostics); the members
+    are stepped only through `step`. Each member's result equals OceanModel.step on it alone.
+    """
+
+    def __init__(self, cases: list):
+        """cases: dicts with cfg (DGConfig), h, f, taux, tauy (the configs generators' form)."""
+        n = len(cases)
+        meshes = (_abi.MeshDesc * n)()
+        prms = (_abi.DGParams * n)()
+        for i, c in enumerate(cases):
+            meshes[i], prms[i] = _mesh_params(c["cfg"])
+        self._keep = [[_c(c[k]) for c in cases] for k in ("h", "f", "taux", "tauy")]
+        arrs = [dptr_array(a) for a in self._keep]
+        hd = C.c_void_p()
+        check(lib().drf_ens_create(n, meshes, prms, *arrs, C.byref(hd)))
+        self.handle = hd
+        self.members = []
+        for i, c in enumerate(cases):
+            mh = C.c_void_p()
+            check(lib().drf_ens_member(self.handle, i, C.byref(mh)))
+            self.members.append(OceanModel._member(c["cfg"], mh, self))
+
+    def close(self):
+        if getattr(self, "handle", None):
+            for m in self.members:
+                m.handle = None
+            lib().drf_ens_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_ptr: int | None):
+        check(lib().drf_ens_set_stream(self.handle, C.c_void_p(stream_ptr or 0)))
+
+    def sync(self):
+        check(lib().drf_ens_sync(self.handle))
+
+    def step(self, dts, nsub: int, nsteps: int = 1):
+        """nsteps baroclinic steps; member i advances by dts[i] per step."""
+        d = _c(dts)
+        if len(d) != len(self.members):
+            raise ValueError("one step size per member")
+        check(lib().drf_ens_step(self.handle, dptr(d), nsub, nsteps))
+
+    def info(self) -> dict:
+        n3, it, gr = C.c_int64(), C.c_int(), C.c_int()
+        check(lib().drf_ens_info(self.handle, C.byref(n3), C.byref(it), C.byref(gr)))
+        return dict(n3=n3.value, items=it.value, grid=gr.value)

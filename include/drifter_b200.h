@@ -147,6 +147,33 @@ int drf_dg_download_surface(drf_dg *m, double *eta);
 /* Size and pointer introspection for the bench (device-resident timing). */
 int drf_dg_info(drf_dg *m, int64_t *n3d_nodes, int64_t *n2d_nodes, int *precision);
 
+/* ------------------------------------------------------------------ ensembles
+ * An ensemble of independent coupled DG runs with their own meshes (nx, ny, nz), bathymetry,
+ * forcing, parameters and step sizes, stepped together: each LSRK stage of all members is ONE
+ * persistent kernel launch over every member's water columns, each barotropic substep one
+ * launch over every member's 2D tiles, and each baroclinic step one CUDA graph. Per member
+ * the result is that of ModeSplittingSolver::step (include/physics/mode_splitting.hpp:241)
+ * as computed by drf_dg_step_modesplit. The reference runs members one after the other. */
+typedef struct drf_ens drf_ens;
+
+/* All members share the order, precision and 2D flux kind; the arrays are indexed by member
+ * (h[i], f[i], taux[i], tauy[i] are member i's 2D fields, as for drf_dg_create). */
+int drf_ens_create(int nmembers, const drf_mesh_desc *meshes, const drf_dg_params *params,
+                   const double *const *h, const double *const *f, const double *const *taux,
+                   const double *const *tauy, drf_ens **out);
+int drf_ens_destroy(drf_ens *e);
+/* Handle of member i for drf_dg_upload_state, drf_dg_download_state, drf_dg_diagnostics,
+ * drf_dg_compute_rhs, drf_dg_set_forcing and drf_dg_download_surface. It is owned by the
+ * ensemble: drf_dg_destroy, drf_dg_set_stream and drf_dg_step_modesplit reject it. */
+int drf_ens_member(drf_ens *e, int i, drf_dg **member);
+int drf_ens_set_stream(drf_ens *e, void *cuda_stream);
+int drf_ens_sync(drf_ens *e);
+/* nsteps baroclinic steps of every member, member i with step dt[i] and nsub subcycles. */
+int drf_ens_step(drf_ens *e, const double *dt, int nsub, int nsteps);
+/* Totals for the bench: 3D nodes over all members, stage work items (water columns) and the
+ * persistent stage grid. */
+int drf_ens_info(drf_ens *e, int64_t *n3d_nodes, int *items, int *grid);
+
 /* ------------------------------------------------------------------ Bezier smoother
  * Uniform-grid cubic Bezier bathymetry smoother: Q = alpha H + lambda (B^T W B + eps I),
  * control points (3 nx + 1) x (3 ny + 1), point (gi, gj) at gi + (3 nx + 1) gj. */
