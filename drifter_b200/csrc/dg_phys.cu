@@ -177,13 +177,15 @@ __device__ __forceinline__ P2<double> p2add(P2<double> a, P2<double> b) { return
 __device__ __forceinline__ P2<double> p2sub(P2<double> a, P2<double> b) { return {a.x - b.x, a.y - b.y}; }
 
 // Shared-memory plan of the stage kernel for one water column (ncn = nz*(N+1)^3 nodes):
-//   two mbarriers (16 B), sQ[4][ncn] state, sRes[4][ncn] LSRK 2N register, sR[4][ncn]
+//   two mbarriers (16 B), the FP64 column increments of the earlier stages [2][(N+1)^2],
+//   sQ[4][ncn] state, sRes[4][ncn] LSRK 2N register, sR[4][ncn]
 //   right-hand side, sD[ncn] horizontal divergence -> layer integrals (in place), per layer x
 //   2D-node increments, the column's 2D fields (1/H, H, eta), its pressure-gradient rows and
 //   1 + sigma per z node.
 inline size_t stage_smem_bytes(int nz, int np, size_t tsz) {
     const int np2 = np * np, ncn = nz * np2 * np;
-    return 16 + ((size_t)13 * ncn + (size_t)2 * nz * np2 + 5 * np2 + (size_t)nz * np) * tsz;
+    return 16 + (size_t)2 * np2 * 8 +
+           ((size_t)13 * ncn + (size_t)2 * nz * np2 + 5 * np2 + (size_t)nz * np) * tsz;
 }
 
 // One CTA per water column; work is organised in pencils (lines of N+1 nodes) so every
@@ -204,7 +206,8 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, int c, uint3
     const size_t base = (size_t)c * ncn;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw);
-    T *sQ = reinterpret_cast<T *>(smem_raw + 16);  // [4][ncn]
+    double *sOld = reinterpret_cast<double *>(smem_raw + 16);  // [2][NP2] column increments so far
+    T *sQ = reinterpret_cast<T *>(smem_raw + 16 + 2 * NP2 * sizeof(double));  // [4][ncn]
     T *sRes = sQ + 4 * ncn;                        // [4][ncn]
     T *sR = sRes + 4 * ncn;                        // [4][ncn]
     T *sD = sR + 4 * ncn;                          // [ncn] divergence -> layer integrals
@@ -227,6 +230,12 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, int c, uint3
     const T Lx = (T)G.Lx, Ly = (T)G.Ly, Ls = (T)G.Ls;
     const T g = (T)G.g;
     const bool need_res = a.mode == 0 && !a.first;
+    // the column increments of the earlier stages, read while the column is being staged
+    if (a.mode == 0 && !a.first)
+        for (int t = threadIdx.x; t < NP2; t += blockDim.x) {
+            sOld[t] = a.dHU3[(size_t)c * NP2 + t];
+            sOld[NP2 + t] = a.dHV3[(size_t)c * NP2 + t];
+        }
 
     // ---- stage the column: state (and the 2N register) by TMA bulk copies when aligned
     if (a.bulk) {
@@ -280,6 +289,58 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, int c, uint3
         const int ez = t / NP, k = t % NP;
         sS1[t] = (ez == nz - 1 && k == N) ? T(1) : (T)(G.dsig * (ez + 0.5 * ((double)B::x(k) + 1.0)));
     }
+    // state across horizontal side s at own node (ez,i,j,k): q+ (4), eta+, H+
+    struct Side {
+        T q[4], e, H;
+    };
+    // the neighbouring column's values across side s (global loads); false on a basin side
+    auto fetch_side = [&](int s, int ez, int i, int j, int k, Side &o) -> bool {
+        int nc = -1, ni = i, nj = j;
+        if (s == 0 && ex > 0) { nc = c - 1; ni = N; }
+        if (s == 1 && ex < G.nx - 1) { nc = c + 1; ni = 0; }
+        if (s == 2 && ey > 0) { nc = c - G.nx; nj = N; }
+        if (s == 3 && ey < G.ny - 1) { nc = c + G.nx; nj = 0; }
+        if (nc < 0) return false;
+        const size_t nb = (size_t)nc * ncn + (size_t)ez * NP3 + ni + NP * (nj + NP * k);
+        const size_t n2 = (size_t)nc * NP2 + ni + NP * nj;
+#pragma unroll
+        for (int v = 0; v < 4; ++v) o.q[v] = a.qin[v][nb];
+        if (a.corrU) {
+            o.q[0] += (T)a.corrU[n2];
+            o.q[1] += (T)a.corrV[n2];
+        }
+        const double e = a.eta[n2];
+        o.e = (T)e;
+        o.H = (T)(e + a.h[n2]);
+        return true;
+    };
+    // the exterior state on a basin side (wall mirror or tidal elevation) at own node n
+    auto basin_side = [&](int s, int i, int j, int n, Side &o) {
+        const int an = i + NP * j;
+        const int bcs = s == 0 ? G.bc[0] : (s == 1 ? G.bc[1] : (s == 2 ? G.bc[2] : G.bc[3]));
+        if (bcs == DRF_BC_TIDE) {
+            o.e = etide;
+            o.H = etide + (T)a.h[(size_t)c * NP2 + an];
+            const T r = o.H * sIH[an];
+#pragma unroll
+            for (int v = 0; v < 4; ++v) o.q[v] = sQ[v * ncn + n] * r;
+        } else {
+            o.e = sEt[an];
+            o.H = sHt[an];
+#pragma unroll
+            for (int v = 0; v < 4; ++v) o.q[v] = sQ[v * ncn + n];
+            if (s <= 1) o.q[0] = -o.q[0]; else o.q[1] = -o.q[1];
+        }
+    };
+    // the neighbour faces of this thread's first x pencil are loaded while the column's bulk
+    // copies are in flight (the x pass then starts without a global-load wait)
+    Side fx0, fxN;
+    bool hx0 = false, hxN = false;
+    if (threadIdx.x < npen) {
+        const int p = threadIdx.x, ez = p / NP2, j = p % NP, k = (p / NP) % NP;
+        hx0 = fetch_side(0, ez, 0, j, k, fx0);
+        hxN = fetch_side(1, ez, N, j, k, fxN);
+    }
     if (threadIdx.x == 0) s_ok = a.bulk ? (int)mbar_wait(&bars[0], ph) : 1;
     __syncthreads();
     if (!s_ok) {
@@ -296,49 +357,6 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, int c, uint3
         __syncthreads();
     }
 
-    // state across horizontal side s at own node (ez,i,j,k): q+ (4), eta+, H+
-    struct Side {
-        T q[4], e, H;
-    };
-    auto outside = [&](int s, int ez, int i, int j, int k, int n) -> Side {
-        Side o;
-        int nc = -1, ni = i, nj = j;
-        if (s == 0 && ex > 0) { nc = c - 1; ni = N; }
-        if (s == 1 && ex < G.nx - 1) { nc = c + 1; ni = 0; }
-        if (s == 2 && ey > 0) { nc = c - G.nx; nj = N; }
-        if (s == 3 && ey < G.ny - 1) { nc = c + G.nx; nj = 0; }
-        const int an = i + NP * j;
-        if (nc >= 0) {
-            const size_t nb = (size_t)nc * ncn + (size_t)ez * NP3 + ni + NP * (nj + NP * k);
-            const size_t n2 = (size_t)nc * NP2 + ni + NP * nj;
-#pragma unroll
-            for (int v = 0; v < 4; ++v) o.q[v] = a.qin[v][nb];
-            if (a.corrU) {
-                o.q[0] += (T)a.corrU[n2];
-                o.q[1] += (T)a.corrV[n2];
-            }
-            const double e = a.eta[n2];
-            o.e = (T)e;
-            o.H = (T)(e + a.h[n2]);
-            return o;
-        }
-        const int bcs = s == 0 ? G.bc[0] : (s == 1 ? G.bc[1] : (s == 2 ? G.bc[2] : G.bc[3]));
-        if (bcs == DRF_BC_TIDE) {
-            o.e = etide;
-            o.H = etide + (T)a.h[(size_t)c * NP2 + an];
-            const T r = o.H * sIH[an];
-#pragma unroll
-            for (int v = 0; v < 4; ++v) o.q[v] = sQ[v * ncn + n] * r;
-        } else {
-            o.e = sEt[an];
-            o.H = sHt[an];
-#pragma unroll
-            for (int v = 0; v < 4; ++v) o.q[v] = sQ[v * ncn + n];
-            if (s <= 1) o.q[0] = -o.q[0]; else o.q[1] = -o.q[1];
-        }
-        return o;
-    };
-
     // ---- horizontal passes. Each pencil (a line of N+1 nodes) gives its direction's part of
     // (1) the horizontal divergence of (Hu, Hv) with a central face flux, which feeds omega, and
     // (2) the right-hand side: advection, pressure, horizontal diffusion and the LF face terms,
@@ -348,13 +366,9 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, int c, uint3
     const bool hdiff = G.nu_h > 0.0;
     // one horizontal pencil: axis 0 (x, sides 0/1) or 1 (y, sides 2/3), a compile-time
     // constant of each instance; nodes e0 + st*m
-    auto hpass = [&](auto AX, int ez, int e0, int st, int iy, int jx) {
+    auto hpass = [&](auto AX, int e0, int st, int iy, int jx, const Side &o0, const Side &oN) {
         constexpr int axis = decltype(AX)::value;
         const T cd = axis == 0 ? cx : cy, Ld = axis == 0 ? Lx : Ly;
-        // own-node indices (i, j, k) of the pencil's two end nodes
-        const int k = (e0 % NP3) / NP2;
-        const Side o0 = axis == 0 ? outside(0, ez, 0, iy, k, e0) : outside(2, ez, jx, 0, k, e0);
-        const Side oN = axis == 0 ? outside(1, ez, N, iy, k, e0 + N) : outside(3, ez, jx, N, k, e0 + NP * N);
         const T ep0 = o0.e, epN = oN.e, Hp0 = o0.H, HpN = oN.H;
         // the neighbours' momentum normal to this pencil's faces and the two variable pairs
         const T qn0 = axis == 0 ? o0.q[0] : o0.q[1], qnN = axis == 0 ? oN.q[0] : oN.q[1];
@@ -447,16 +461,44 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, int c, uint3
             }
         }
     };
-    // x pencils (j, k, layer)
-    for (int p = threadIdx.x; p < npen; p += blockDim.x) {
+    // x pencils (j, k, layer); the first one's neighbour faces were prefetched
+    auto xpencil = [&](int p, Side &o0, Side &oN, bool h0, bool hN) {
         const int ez = p / NP2, j = p % NP, k = (p / NP) % NP;
-        hpass(std::integral_constant<int, 0>{}, ez, ez * NP3 + NP * (j + NP * k), 1, j, 0);
+        const int e0 = ez * NP3 + NP * (j + NP * k);
+        if (!h0) basin_side(0, 0, j, e0, o0);
+        if (!hN) basin_side(1, N, j, e0 + N, oN);
+        hpass(std::integral_constant<int, 0>{}, e0, 1, j, 0, o0, oN);
+    };
+    if (threadIdx.x < npen) xpencil(threadIdx.x, fx0, fxN, hx0, hxN);
+    for (int p = threadIdx.x + blockDim.x; p < npen; p += blockDim.x) {
+        const int ez = p / NP2, j = p % NP, k = (p / NP) % NP;
+        Side o0, oN;
+        const bool h0 = fetch_side(0, ez, 0, j, k, o0), hN = fetch_side(1, ez, N, j, k, oN);
+        xpencil(p, o0, oN, h0, hN);
+    }
+    // the first y pencil's neighbour faces are loaded across the barrier
+    Side fy0, fyN;
+    bool hy0 = false, hyN = false;
+    if (threadIdx.x < npen) {
+        const int p = threadIdx.x, ez = p / NP2, i = p % NP, k = (p / NP) % NP;
+        hy0 = fetch_side(2, ez, i, 0, k, fy0);
+        hyN = fetch_side(3, ez, i, N, k, fyN);
     }
     __syncthreads();
     // y pencils (i, k, layer)
-    for (int p = threadIdx.x; p < npen; p += blockDim.x) {
+    auto ypencil = [&](int p, Side &o0, Side &oN, bool h0, bool hN) {
         const int ez = p / NP2, i = p % NP, k = (p / NP) % NP;
-        hpass(std::integral_constant<int, 1>{}, ez, ez * NP3 + i + NP2 * k, NP, 0, i);
+        const int e0 = ez * NP3 + i + NP2 * k;
+        if (!h0) basin_side(2, i, 0, e0, o0);
+        if (!hN) basin_side(3, i, N, e0 + NP * N, oN);
+        hpass(std::integral_constant<int, 1>{}, e0, NP, 0, i, o0, oN);
+    };
+    if (threadIdx.x < npen) ypencil(threadIdx.x, fy0, fyN, hy0, hyN);
+    for (int p = threadIdx.x + blockDim.x; p < npen; p += blockDim.x) {
+        const int ez = p / NP2, i = p % NP, k = (p / NP) % NP;
+        Side o0, oN;
+        const bool h0 = fetch_side(2, ez, i, 0, k, o0), hN = fetch_side(3, ez, i, N, k, oN);
+        ypencil(p, o0, oN, h0, hN);
     }
     __syncthreads();
     // ---- layer integrals J_k = (dsig/2) sum_m S[k][m] delta_m: z pencils
@@ -613,16 +655,23 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, int c, uint3
     }
     if (a.mode == 0) {
         __syncthreads();
-        for (int an = threadIdx.x; an < NP2; an += blockDim.x) {
-            double su = 0.0, sv = 0.0;
-            for (int ez = 0; ez < nz; ++ez) {
-                su += (double)sL1[ez * NP2 + an];
-                sv += (double)sL2[ez * NP2 + an];
+        // one thread per (2D node, component): FP64 sum over the layers in four partial sums
+        for (int t = threadIdx.x; t < 2 * NP2; t += blockDim.x) {
+            const int v = t / NP2, an = t % NP2;
+            const T *L = (v == 0 ? sL1 : sL2) + an;
+            double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+            int ez = 0;
+            for (; ez + 4 <= nz; ez += 4) {
+                s0 += (double)L[ez * NP2];
+                s1 += (double)L[(ez + 1) * NP2];
+                s2 += (double)L[(ez + 2) * NP2];
+                s3 += (double)L[(ez + 3) * NP2];
             }
+            for (; ez < nz; ++ez) s0 += (double)L[ez * NP2];
+            const double sum = (s0 + s1) + (s2 + s3);
             const size_t i2 = (size_t)c * NP2 + an;
-            const double hd = 0.5 * G.dsig;
-            a.dHU3[i2] = (a.first ? 0.0 : a.dHU3[i2]) + hd * su;
-            a.dHV3[i2] = (a.first ? 0.0 : a.dHV3[i2]) + hd * sv;
+            double *out = v == 0 ? a.dHU3 : a.dHV3;
+            out[i2] = (a.first ? 0.0 : sOld[t]) + 0.5 * G.dsig * sum;
         }
     }
     return true;
