@@ -13,7 +13,11 @@
 //   baro_force, (baro_pred, baro_corr) x nsub, baro_finish; the transport correction the
 //   barotropic step leaves is folded into the next step's first stage.
 #include <algorithm>
+#include <array>
 #include <cmath>
+#include <cstdlib>
+#include <map>
+#include <tuple>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -687,7 +691,9 @@ __global__ void __launch_bounds__(STAGE_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) dg3
 // One CTA per tile of BARO_CPB water columns (one thread per 2D node): the column's state is
 // staged in shared memory with 1/H computed once per node; element-local derivatives read the
 // tile, face fluxes read the neighbouring column's face node from global memory.
-constexpr int BARO_CPB = 8;
+constexpr int BARO_CPB = 8;  // tile of the ensemble launches and the default of a single model
+// Columns per CTA the autotuner tries for a single model's barotropic kernels.
+constexpr int BARO_TILES[4] = {2, 4, 8, 16};
 
 struct BaroArgs {
     const double *e, *hu, *hv, *h, *f, *Fx, *Fy, *tdev;
@@ -720,21 +726,24 @@ __device__ __forceinline__ void lf_minus_phys(const double UL[3], double ihL, do
     }
 }
 
-// Register budget of the subcycle kernels: four tiles per SM for up to 5 x 5 nodes per column.
-#define BARO_BOUNDS __launch_bounds__(BARO_CPB * NP * NP, NP <= 5 ? 4 : 2)
+// Register budget of the subcycle kernels: 800 resident threads per SM (80 registers) for up to
+// 5 x 5 nodes per column, 576 (112 registers) for 6 x 6, whatever the tile.
+constexpr int baro_min_blocks(int threads, int np) {
+    return (np <= 5 ? 800 : 576) / threads < 1 ? 1 : (np <= 5 ? 800 : 576) / threads;
+}
+#define BARO_BOUNDS __launch_bounds__(CPB * NP * NP, baro_min_blocks(CPB * NP * NP, NP))
 
 // One tile of BARO_CPB columns: the barotropic right-hand side Phi(U) at this thread's 2D node.
 // FK is the face flux (the model's flux2d). Every global load, the neighbours' face values
 // included, is issued before the tile barrier.
-template <int NP, int FK>
+template <int NP, int FK, int CPB>
 __device__ __forceinline__ bool baro_tile_phi(const BaroArgs &a, int64_t tile, double &re, double &ru,
                                               double &rv, int64_t &t) {
     constexpr int NP2 = NP * NP, N = NP - 1;
-    __shared__ double sE[BARO_CPB * NP2], sU[BARO_CPB * NP2], sV[BARO_CPB * NP2],
-        sI[BARO_CPB * NP2], sD[NP2];
+    __shared__ double sE[CPB * NP2], sU[CPB * NP2], sV[CPB * NP2], sI[CPB * NP2], sD[NP2];
     const Geo &G = a.G;
     const int lc = threadIdx.x / NP2, an = threadIdx.x % NP2, i = an % NP, j = an / NP;
-    const int64_t c = tile * BARO_CPB + lc;
+    const int64_t c = tile * CPB + lc;
     const bool valid = c < a.ncol;
     if (threadIdx.x < NP2) sD[threadIdx.x] = cBs[NP].D[threadIdx.x];
     t = c * NP2 + an;
@@ -824,59 +833,59 @@ __device__ __forceinline__ bool baro_tile_phi(const BaroArgs &a, int64_t tile, d
     return true;
 }
 
-template <int NP, int FK>
+template <int NP, int FK, int CPB>
 __global__ void baro_rhs_kernel(BaroArgs a, double *ke, double *ku, double *kv) {
     double re, ru, rv;
     int64_t t;
-    if (!baro_tile_phi<NP, FK>(a, blockIdx.x, re, ru, rv, t)) return;
+    if (!baro_tile_phi<NP, FK, CPB>(a, blockIdx.x, re, ru, rv, t)) return;
     ke[t] = re; ku[t] = ru; kv[t] = rv;
 }
 
 // F = (3D-integrated increment)/dt - Phi(U^n); keeps HU^n, HV^n for the transport correction.
-template <int NP, int FK>
+template <int NP, int FK, int CPB>
 __device__ __forceinline__ void baro_force_body(const BaroArgs &a, int64_t tile, double dt, const double *dHU3,
                                                 const double *dHV3, double *Fx, double *Fy, double *HUo,
                                                 double *HVo) {
     double re, ru, rv;
     int64_t t;
-    if (!baro_tile_phi<NP, FK>(a, tile, re, ru, rv, t)) return;
+    if (!baro_tile_phi<NP, FK, CPB>(a, tile, re, ru, rv, t)) return;
     Fx[t] = dHU3[t] / dt - ru;
     Fy[t] = dHV3[t] / dt - rv;
     HUo[t] = a.hu[t];
     HVo[t] = a.hv[t];
 }
-template <int NP, int FK>
+template <int NP, int FK, int CPB>
 __global__ void baro_force_kernel(BaroArgs a, double dt, const double *dHU3, const double *dHV3,
                                   double *Fx, double *Fy, double *HUo, double *HVo) {
-    baro_force_body<NP, FK>(a, blockIdx.x, dt, dHU3, dHV3, Fx, Fy, HUo, HVo);
+    baro_force_body<NP, FK, CPB>(a, blockIdx.x, dt, dHU3, dHV3, Fx, Fy, HUo, HVo);
 }
 
 // Heun predictor: k1 = Phi(U^m), U* = U^m + dtb k1
-template <int NP, int FK>
+template <int NP, int FK, int CPB>
 __device__ __forceinline__ void baro_pred_body(const BaroArgs &a, int64_t tile, double dtb, double *k1e,
                                                double *k1u, double *k1v, double *es, double *us, double *vs) {
     double re, ru, rv;
     int64_t t;
-    if (!baro_tile_phi<NP, FK>(a, tile, re, ru, rv, t)) return;
+    if (!baro_tile_phi<NP, FK, CPB>(a, tile, re, ru, rv, t)) return;
     k1e[t] = re; k1u[t] = ru; k1v[t] = rv;
     es[t] = a.e[t] + dtb * re;
     us[t] = a.hu[t] + dtb * ru;
     vs[t] = a.hv[t] + dtb * rv;
 }
-template <int NP, int FK>
+template <int NP, int FK, int CPB>
 __global__ void BARO_BOUNDS baro_pred_kernel(BaroArgs a, double dtb, double *k1e, double *k1u, double *k1v,
                                  double *es, double *us, double *vs) {
-    baro_pred_body<NP, FK>(a, blockIdx.x, dtb, k1e, k1u, k1v, es, us, vs);
+    baro_pred_body<NP, FK, CPB>(a, blockIdx.x, dtb, k1e, k1u, k1v, es, us, vs);
 }
 
 // Heun corrector: U^{m+1} = U^m + dtb/2 (k1 + Phi(U*)); accumulates eta for its time mean
-template <int NP, int FK>
+template <int NP, int FK, int CPB>
 __device__ __forceinline__ void baro_corr_body(const BaroArgs &a, int64_t tile, double dtb, const double *k1e,
                                                const double *k1u, const double *k1v, double *e, double *hu,
                                                double *hv, double *esum, int first) {
     double re, ru, rv;
     int64_t t;
-    if (!baro_tile_phi<NP, FK>(a, tile, re, ru, rv, t)) return;
+    if (!baro_tile_phi<NP, FK, CPB>(a, tile, re, ru, rv, t)) return;
     const double hd = 0.5 * dtb;
     const double en = e[t] + hd * (k1e[t] + re);
     e[t] = en;
@@ -884,11 +893,11 @@ __device__ __forceinline__ void baro_corr_body(const BaroArgs &a, int64_t tile, 
     hv[t] = hv[t] + hd * (k1v[t] + rv);
     esum[t] = (first ? 0.0 : esum[t]) + en;
 }
-template <int NP, int FK>
+template <int NP, int FK, int CPB>
 __global__ void BARO_BOUNDS baro_corr_kernel(BaroArgs a, double dtb, const double *k1e, const double *k1u,
                                  const double *k1v, double *e, double *hu, double *hv,
                                  double *esum, int first) {
-    baro_corr_body<NP, FK>(a, blockIdx.x, dtb, k1e, k1u, k1v, e, hu, hv, esum, first);
+    baro_corr_body<NP, FK, CPB>(a, blockIdx.x, dtb, k1e, k1u, k1v, e, hu, hv, esum, first);
 }
 
 __global__ void baro_finish_kernel(int64_t n2, int nsub, double dt, const double *esum,
@@ -986,9 +995,9 @@ __global__ void baro_force_ens_kernel(BaroArgs a, BaroEns E, const double *dHU3,
     shift_baro(a, m, w.x);
     a.toff = 0.0;
     const int64_t o = m.off2;
-    baro_force_body<NP, FK>(a, w.y, m.dt, dHU3 + o, dHV3 + o, Fx + o, Fy + o, HUo + o, HVo + o);
+    baro_force_body<NP, FK, BARO_CPB>(a, w.y, m.dt, dHU3 + o, dHV3 + o, Fx + o, Fy + o, HUo + o, HVo + o);
 }
-template <int NP, int FK>
+template <int NP, int FK, int CPB = BARO_CPB>
 __global__ void BARO_BOUNDS baro_pred_ens_kernel(BaroArgs a, BaroEns E, double *k1e, double *k1u,
                                                  double *k1v, double *es, double *us, double *vs) {
     const int2 w = E.tiles[blockIdx.x];
@@ -997,9 +1006,9 @@ __global__ void BARO_BOUNDS baro_pred_ens_kernel(BaroArgs a, BaroEns E, double *
     const double dtb = m.dt / E.nsub;
     a.toff = __dmul_rn((double)E.sub, dtb);
     const int64_t o = m.off2;
-    baro_pred_body<NP, FK>(a, w.y, dtb, k1e + o, k1u + o, k1v + o, es + o, us + o, vs + o);
+    baro_pred_body<NP, FK, BARO_CPB>(a, w.y, dtb, k1e + o, k1u + o, k1v + o, es + o, us + o, vs + o);
 }
-template <int NP, int FK>
+template <int NP, int FK, int CPB = BARO_CPB>
 __global__ void BARO_BOUNDS baro_corr_ens_kernel(BaroArgs a, BaroEns E, const double *k1e, const double *k1u,
                                                  const double *k1v, double *e, double *hu, double *hv,
                                                  double *esum) {
@@ -1009,7 +1018,7 @@ __global__ void BARO_BOUNDS baro_corr_ens_kernel(BaroArgs a, BaroEns E, const do
     const double dtb = m.dt / E.nsub;
     a.toff = __dadd_rn(__dmul_rn((double)E.sub, dtb), dtb);  // unfused, as the host computes it
     const int64_t o = m.off2;
-    baro_corr_body<NP, FK>(a, w.y, dtb, k1e + o, k1u + o, k1v + o, e + o, hu + o, hv + o, esum + o,
+    baro_corr_body<NP, FK, BARO_CPB>(a, w.y, dtb, k1e + o, k1u + o, k1v + o, e + o, hu + o, hv + o, esum + o,
                            E.sub == 0);
 }
 
@@ -1206,6 +1215,17 @@ const double LSRK_C[5] = {0.0, 0.1496590219993, 0.3704009573644, 0.6222557631345
 
 inline unsigned blocks_for(int64_t n, int bs = 256) { return (unsigned)((n + bs - 1) / bs); }
 
+// the barotropic tile (columns per CTA) as a compile-time constant
+template <class F>
+void dispatch_cpb(int cpb, F &&f) {
+    switch (cpb) {
+    case 2: f(std::integral_constant<int, 2>{}); break;
+    case 4: f(std::integral_constant<int, 4>{}); break;
+    case 16: f(std::integral_constant<int, 16>{}); break;
+    default: f(std::integral_constant<int, 8>{}); break;
+    }
+}
+
 }  // namespace
 }  // namespace drf
 
@@ -1240,6 +1260,9 @@ struct drf_dg {
     bool pending = false;  // a transport correction in corrU/corrV is not yet in q(cur)
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     double graph_dt = 0.0;
+    // barotropic tile chosen by the autotuner (0 = not tuned yet) and the candidates' times
+    int baro_cpb = 0;
+    double baro_ms[4] = {0.0, 0.0, 0.0, 0.0};
     int graph_nsub = 0;
     size_t smem = 0;
 
@@ -1269,6 +1292,7 @@ struct drf_dg {
     }
     void setup(const drf_mesh_desc *mesh, const drf_dg_params *params, const double *h_,
                const double *f_, const double *taux_, const double *tauy_);
+    void tune_baro();
 
     void drop_graphs() {
         for (auto &g : graph)
@@ -1357,24 +1381,27 @@ struct drf_dg {
             launch_stage<T, NP>(src, dst, s, dt, 0, nullptr, nullptr, nullptr, eta, 0.0, s == 0);
             src = dst;
         }
-        // after 5 stages the state is in `out`
-        const unsigned nbt = (unsigned)((ncol + BARO_CPB - 1) / BARO_CPB);
-        const int bt = BARO_CPB * NP * NP;
-        dispatch_flux(G.flux2d, [&](auto fk) {
-            constexpr int FK = decltype(fk)::value;
-            baro_force_kernel<NP, FK><<<nbt, bt, 0, stream>>>(baro<NP>(eta, HU, HV, false, 0.0), dt, dHU3,
-                                                              dHV3, Fx, Fy, HUo, HVo);
-            DRF_LAUNCHED();
-            const double dtb = dt / nsub;
-            for (int m = 0; m < nsub; ++m) {
-                baro_pred_kernel<NP, FK><<<nbt, bt, 0, stream>>>(baro<NP>(eta, HU, HV, true, m * dtb), dtb,
-                                                                 k1[0], k1[1], k1[2], us[0], us[1], us[2]);
+        // after 5 stages the state is in `out`; the barotropic tile is the tuned one
+        dispatch_cpb(baro_cpb, [&](auto cpbc) {
+            constexpr int CPB = decltype(cpbc)::value;
+            const unsigned nbt = (unsigned)((ncol + CPB - 1) / CPB);
+            const int bt = CPB * NP * NP;
+            dispatch_flux(G.flux2d, [&](auto fk) {
+                constexpr int FK = decltype(fk)::value;
+                baro_force_kernel<NP, FK, CPB><<<nbt, bt, 0, stream>>>(baro<NP>(eta, HU, HV, false, 0.0), dt,
+                                                                       dHU3, dHV3, Fx, Fy, HUo, HVo);
                 DRF_LAUNCHED();
-                baro_corr_kernel<NP, FK><<<nbt, bt, 0, stream>>>(
-                    baro<NP>(us[0], us[1], us[2], true, m * dtb + dtb), dtb, k1[0], k1[1], k1[2], eta,
-                    HU, HV, esum, m == 0);
-                DRF_LAUNCHED();
-            }
+                const double dtb = dt / nsub;
+                for (int m = 0; m < nsub; ++m) {
+                    baro_pred_kernel<NP, FK, CPB><<<nbt, bt, 0, stream>>>(
+                        baro<NP>(eta, HU, HV, true, m * dtb), dtb, k1[0], k1[1], k1[2], us[0], us[1], us[2]);
+                    DRF_LAUNCHED();
+                    baro_corr_kernel<NP, FK, CPB><<<nbt, bt, 0, stream>>>(
+                        baro<NP>(us[0], us[1], us[2], true, m * dtb + dtb), dtb, k1[0], k1[1], k1[2], eta,
+                        HU, HV, esum, m == 0);
+                    DRF_LAUNCHED();
+                }
+            });
         });
         baro_finish_kernel<<<blocks_for(n2), 256, 0, stream>>>(n2, nsub, dt, esum, eta_avg, HU, HV,
                                                                HUo, HVo, dHU3, dHV3, corrU, corrV,
@@ -1519,6 +1546,73 @@ void drf_dg::setup(const drf_mesh_desc *mesh, const drf_dg_params *params, const
         constexpr int NP = decltype(npc)::value;
         allow_max_dynamic_smem(reinterpret_cast<const void *>(dg3d_stage_kernel<T, NP>), maxsm);
     });
+}
+
+// Autotuner of the barotropic tile (water columns per CTA of the subcycle kernels): times the
+// predictor kernel, which writes only scratch arrays, at every candidate tile on the model's
+// stream (two warm-up launches, then ten between CUDA events) and keeps the fastest. Choices
+// are cached per (device, order, flux, number of columns) for the life of the process.
+// DRIFTER_B200_TUNE=0 in the environment keeps the default tile.
+void drf_dg::tune_baro() {
+    if (baro_cpb) return;
+    const char *env = std::getenv("DRIFTER_B200_TUNE");
+    if (env && env[0] == '0') {
+        baro_cpb = BARO_CPB;
+        return;
+    }
+    static std::mutex mu;
+    static std::map<std::tuple<int, int, int, int>, std::pair<int, std::array<double, 4>>> cache;
+    int dev = 0;
+    DRF_CUDA(cudaGetDevice(&dev));
+    const auto key = std::make_tuple(dev, np, G.flux2d, ncol);
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = cache.find(key);
+        if (it != cache.end()) {
+            baro_cpb = it->second.first;
+            for (int i = 0; i < 4; ++i) baro_ms[i] = it->second.second[i];
+            return;
+        }
+    }
+    cudaEvent_t e0, e1;
+    DRF_CUDA(cudaEventCreate(&e0));
+    DRF_CUDA(cudaEventCreate(&e1));
+    int best = BARO_CPB;
+    double best_ms = 1e300;
+    dispatch_np(np, [&](auto npc) {
+        constexpr int NP = decltype(npc)::value;
+        dispatch_flux(G.flux2d, [&](auto fk) {
+            constexpr int FK = decltype(fk)::value;
+            for (int i = 0; i < 4; ++i)
+                dispatch_cpb(BARO_TILES[i], [&](auto cpbc) {
+                    constexpr int CPB = decltype(cpbc)::value;
+                    const unsigned nbt = (unsigned)((ncol + CPB - 1) / CPB);
+                    auto launch = [&]() {
+                        baro_pred_kernel<NP, FK, CPB><<<nbt, CPB * NP * NP, 0, stream>>>(
+                            baro<NP>(eta, HU, HV, true, 0.0), 1.0, k1[0], k1[1], k1[2], us[0], us[1], us[2]);
+                        DRF_LAUNCHED();
+                    };
+                    launch();
+                    launch();
+                    DRF_CUDA(cudaEventRecord(e0, stream));
+                    for (int r = 0; r < 10; ++r) launch();
+                    DRF_CUDA(cudaEventRecord(e1, stream));
+                    DRF_CUDA(cudaEventSynchronize(e1));
+                    float ms = 0.f;
+                    DRF_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+                    baro_ms[i] = ms / 10.0;
+                    if (baro_ms[i] < best_ms) {
+                        best_ms = baro_ms[i];
+                        best = CPB;
+                    }
+                });
+        });
+    });
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    baro_cpb = best;
+    std::lock_guard<std::mutex> lk(mu);
+    cache[key] = {best, {baro_ms[0], baro_ms[1], baro_ms[2], baro_ms[3]}};
 }
 
 extern "C" {
@@ -1667,7 +1761,7 @@ int drf_dg_compute_rhs2d(drf_dg *m, const double *Fx, const double *Fy, double t
             constexpr int NP = decltype(npc)::value;
             dispatch_flux(m->G.flux2d, [&](auto fk) {
                 constexpr int FK = decltype(fk)::value;
-                baro_rhs_kernel<NP, FK><<<(unsigned)((m->ncol + BARO_CPB - 1) / BARO_CPB), BARO_CPB * NP * NP,
+                baro_rhs_kernel<NP, FK, BARO_CPB><<<(unsigned)((m->ncol + BARO_CPB - 1) / BARO_CPB), BARO_CPB * NP * NP,
                                           0, m->stream>>>(m->baro<NP>(m->eta, m->HU, m->HV, true, time - tcur),
                                                           m->k1[0], m->k1[1], m->k1[2]);
             });
@@ -1687,6 +1781,7 @@ int drf_dg_step_modesplit(drf_dg *m, double dt, int nsub, int nsteps) {
         DRF_CHECK(nsub >= 1, DRF_E_INVALID, "nsub must be >= 1");
         DRF_CHECK(dt > 0.0 && std::isfinite(dt), DRF_E_INVALID, "dt must be positive");
         DRF_CHECK(nsteps >= 0, DRF_E_INVALID, "nsteps must be >= 0");
+        m->tune_baro();  // first step only: outside any capture
         if (m->graph_nsub != nsub || m->graph_dt != dt) {
             m->drop_graphs();
             for (int in = 0; in < 2; ++in) {
@@ -1942,6 +2037,16 @@ int drf_dg_download_surface(drf_dg *m, double *eta) {
         DRF_CHECK(eta, DRF_E_INVALID, "null argument");
         DRF_CUDA(cudaMemcpyAsync(eta, m->eta, m->n2 * 8, cudaMemcpyDeviceToHost, m->stream));
         DRF_CUDA(cudaStreamSynchronize(m->stream));
+    });
+}
+
+int drf_dg_tuning(drf_dg *m, int *baro_cols_per_cta, double *baro_ms4) {
+    return guard([&] {
+        check_model(m);
+        m->tune_baro();
+        if (baro_cols_per_cta) *baro_cols_per_cta = m->baro_cpb;
+        if (baro_ms4)
+            for (int i = 0; i < 4; ++i) baro_ms4[i] = m->baro_ms[i];
     });
 }
 

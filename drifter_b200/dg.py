@@ -226,6 +226,13 @@ class OceanModel:
                 "min_eta", "max_T", "min_T")
         return dict(zip(keys, out.tolist()))
 
+    def tuning(self) -> dict:
+        """The autotuned barotropic tile (columns per CTA) and each candidate's time (ms)."""
+        cpb, ms = C.c_int(), np.zeros(4)
+        check(lib().drf_dg_tuning(self.handle, C.byref(cpb), dptr(ms)))
+        return dict(baro_cols_per_cta=cpb.value,
+                    candidates_ms={str(c): round(float(t), 5) for c, t in zip((2, 4, 8, 16), ms)})
+
     def time_stage(self, nrep: int = 20) -> dict:
         ms, ab, nd = C.c_double(), C.c_double(), C.c_double()
         check(lib().drf_dg_time_stage(self.handle, nrep, C.byref(ms), C.byref(ab), C.byref(nd)))

@@ -144,6 +144,12 @@ int drf_dg_set_forcing(drf_dg *m, const double *taux, const double *tauy);
 /* Copies the 2D surface elevation to the host (synchronous). */
 int drf_dg_download_surface(drf_dg *m, double *eta);
 
+/* Autotuned launch shape: the barotropic subcycle kernels' tile (water columns per CTA) chosen
+ * by timing the candidates 2, 4, 8, 16 on this model (done at the first step, or here), and
+ * the candidates' times in ms (baro_ms4 may be NULL). No counterpart in the reference, which
+ * has no kernels; DRIFTER_B200_TUNE=0 keeps the default tile of 8. */
+int drf_dg_tuning(drf_dg *m, int *baro_cols_per_cta, double *baro_ms4);
+
 /* Size and pointer introspection for the bench (device-resident timing). */
 int drf_dg_info(drf_dg *m, int64_t *n3d_nodes, int64_t *n2d_nodes, int *precision);
 

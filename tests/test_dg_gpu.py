@@ -207,3 +207,23 @@ def test_time_stage_reports_positive_rate():
     gpu.upload_state(case["q"], case["eta"])
     r = gpu.time_stage(5)
     assert r["ms"] > 0 and r["alg_bytes"] > 0 and r["ndof"] == 4 * case["cfg"].n3
+
+
+def test_autotuned_barotropic_tile_matches_default_tile(monkeypatch):
+    """The autotuner picks one of the candidate tiles by timing; every tile does the same
+    arithmetic per 2D node, so the tuned step equals the default-tile step exactly."""
+    case = _tidal_small("fp64", nx=9, ny=7)
+    tuned = OceanModel(case["cfg"], case["h"], case["f"], case["taux"], case["tauy"])
+    tuned.upload_state(case["q"], case["eta"])
+    tuned.step(case["dt"], case["nsub"], 2)
+    t = tuned.tuning()
+    assert t["baro_cols_per_cta"] in (2, 4, 8, 16)
+    assert all(v > 0 for v in t["candidates_ms"].values())
+    monkeypatch.setenv("DRIFTER_B200_TUNE", "0")
+    fixed = OceanModel(case["cfg"], case["h"], case["f"], case["taux"], case["tauy"])
+    fixed.upload_state(case["q"], case["eta"])
+    fixed.step(case["dt"], case["nsub"], 2)
+    assert fixed.tuning()["baro_cols_per_cta"] == 8
+    a, b = tuned.download_state(), fixed.download_state()
+    for k in ("eta", "HU", "HV", "Hu", "HT"):
+        assert relerr(a[k], b[k]) <= 1e-15, k
