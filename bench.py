@@ -42,6 +42,7 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-cg", action="store_true", help="skip the C4 Bezier CG comparison")
     ap.add_argument("--no-ens", action="store_true", help="skip the C5 ensemble measurement")
+    ap.add_argument("--no-amr", action="store_true", help="skip the C3 AMR measurement")
     return ap.parse_args()
 
 
@@ -276,6 +277,39 @@ def run_ensemble(stream, steps=5, warmup=3):
             "member0_max_eta": diag["max_eta"]}
 
 
+def run_amr(stream, steps=5, warmup=3):
+    """C3: DG3DIntegration::compute_rhs on the directionally refined mesh of the seeded fBm
+    coastline (about 2.6e5 hexes, N=3), complete mode (conforming, boundary and mortar faces),
+    LF flux: the right-hand side alone and the LSRK45 step (one graph per step), device time."""
+    import torch
+    from drifter_b200 import configs
+    from drifter_b200.amr import DG3DIntegration
+    c = configs.c3()
+    m = c["mesh"]
+    gpu = DG3DIntegration(c["order"], m)
+    gpu.set_stream(stream.cuda_stream)
+    gpu.upload(c["U"])
+    rhs = gpu.time_rhs(c["a"], nrep=20, flux="lf", mode="complete")
+    dt = 1e-4
+    gpu.step(c["a"], dt, warmup, flux="lf", mode="complete")
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    gpu.step(c["a"], dt, steps, flux="lf", mode="complete")
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    ndof = m["n_elem"] * (c["order"] + 1) ** 3
+    gpu.close()
+    types = np.bincount([f[0] for f in m["ifaces"]], minlength=6)
+    return {"workload": c["name"] + ", complete mode, LF flux, LSRK45",
+            "hexes": int(m["n_elem"]), "dofs": int(ndof),
+            "faces": {"conforming": int(len(m["conf"])), "boundary": int(len(m["bnd"])),
+                      "mortar_2x1": int(types[1]), "mortar_1x2": int(types[2]), "mortar_2x2": int(types[5])},
+            "value": ndof * 5 / (ms / 1e3), "unit": UNIT, "ms_per_step": ms,
+            "rhs_ms": rhs["ms"], "rhs_gbs": rhs["alg_bytes"] / (rhs["ms"] / 1e3) / 1e9}
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -408,6 +442,9 @@ def run_ours(args, rank, world, local):
     ens = None
     if not args.no_ens:
         ens = run_ensemble(stream)
+    amr = None
+    if not args.no_amr:
+        amr = run_amr(stream)
 
     cpu = None
     if rank == 0 and not args.no_cpu:
@@ -434,6 +471,7 @@ def run_ours(args, rank, world, local):
             "fp64_gpu": fp64,
             "cg": cg,
             "ensemble": ens,
+            "amr": amr,
             "gpu_launches": int(launches),
             "clocks": ck,
         }

@@ -1,0 +1,105 @@
+"""DG3DIntegration (include/dg/operators_3d.hpp:153) on directionally refined hexahedral meshes
+over the C ABI: compute_rhs (src/dg/operators_3d.cpp:228) of the scalar conservation law
+u_t + div(a u) = 0, with the non-conforming faces coupled by mortars, and an LSRK45 stepper
+whose steps are CUDA graphs. All compute runs in libdrifter_b200.so on the GPU."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from ._abi import check, dptr, lib
+from .mortar import FLUX
+
+MODES = {"reference": 0, "complete": 1}
+
+
+def _sigs():
+    L = lib()
+    vp, dp, i64 = C.c_void_p, C.POINTER(C.c_double), C.c_int64
+    sigs = {
+        "drf_amr_create": [C.c_int, i64, i64, vp, i64, vp, i64, vp, vp, vp, vp, vp, C.POINTER(vp)],
+        "drf_amr_destroy": [vp], "drf_amr_set_stream": [vp, vp], "drf_amr_sync": [vp],
+        "drf_amr_compute_rhs": [vp, C.c_int, C.c_int, dp, dp, dp],
+        "drf_amr_upload": [vp, dp], "drf_amr_download": [vp, dp],
+        "drf_amr_step": [vp, C.c_int, C.c_int, dp, C.c_double, C.c_int],
+        "drf_amr_time_rhs": [vp, C.c_int, C.c_int, dp, C.c_int, dp, dp],
+    }
+    for k, a in sigs.items():
+        getattr(L, k).argtypes = a
+        getattr(L, k).restype = C.c_int
+    return L
+
+
+class DG3DIntegration:
+    """The reference class's compute_rhs for one mesh (the dict of configs.amr_mesh: elements,
+    conforming pairs, boundary faces and non-conforming interfaces) at polynomial order N."""
+
+    def __init__(self, order: int, mesh: dict):
+        L = _sigs()
+        self.order, self.n_elem = order, int(mesh["n_elem"])
+        self.nd = (order + 1) ** 3
+        conf = np.ascontiguousarray(mesh["conf"], np.int64).reshape(-1, 4)
+        bnd = np.ascontiguousarray(mesh["bnd"], np.int64).reshape(-1, 2)
+        ifs = mesh["ifaces"]
+        n = len(ifs)
+        t = np.zeros(n, np.int32)
+        ce = np.zeros(n, np.int64)
+        cf = np.zeros(n, np.int32)
+        fe = -np.ones((n, 4), np.int64)
+        ff = -np.ones((n, 4), np.int32)
+        for i, (ty, e, f, fes, ffs) in enumerate(ifs):
+            t[i], ce[i], cf[i] = ty, e, f
+            fe[i, :len(fes)] = fes
+            ff[i, :len(ffs)] = ffs
+        self._keep = (conf, bnd, t, ce, cf, fe, ff)
+        ptr = lambda a: a.ctypes.data_as(C.c_void_p)
+        h = C.c_void_p()
+        check(L.drf_amr_create(order, self.n_elem, len(conf), ptr(conf), len(bnd), ptr(bnd), n, ptr(t),
+                               ptr(ce), ptr(cf), ptr(fe), ptr(ff), C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().drf_amr_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_ptr: int | None):
+        check(lib().drf_amr_set_stream(self.h, C.c_void_p(stream_ptr or 0)))
+
+    def sync(self):
+        check(lib().drf_amr_sync(self.h))
+
+    def compute_rhs(self, U, a, flux: str = "lf", mode: str = "reference") -> np.ndarray:
+        U = np.ascontiguousarray(U, dtype=np.float64).reshape(self.n_elem, self.nd)
+        out = np.empty_like(U)
+        av = np.ascontiguousarray(a, dtype=np.float64)
+        check(lib().drf_amr_compute_rhs(self.h, MODES[mode], FLUX[flux], dptr(av), dptr(U), dptr(out)))
+        return out
+
+    def upload(self, U):
+        U = np.ascontiguousarray(U, dtype=np.float64).reshape(self.n_elem, self.nd)
+        check(lib().drf_amr_upload(self.h, dptr(U)))
+
+    def download(self) -> np.ndarray:
+        out = np.empty((self.n_elem, self.nd))
+        check(lib().drf_amr_download(self.h, dptr(out)))
+        return out
+
+    def step(self, a, dt: float, nsteps: int = 1, flux: str = "lf", mode: str = "reference"):
+        """nsteps LSRK45 steps of du/dt = -compute_rhs(u), each one CUDA graph."""
+        av = np.ascontiguousarray(a, dtype=np.float64)
+        check(lib().drf_amr_step(self.h, MODES[mode], FLUX[flux], dptr(av), dt, nsteps))
+
+    def time_rhs(self, a, nrep: int = 20, flux: str = "lf", mode: str = "reference") -> dict:
+        av = np.ascontiguousarray(a, dtype=np.float64)
+        ms, ab = C.c_double(), C.c_double()
+        check(lib().drf_amr_time_rhs(self.h, MODES[mode], FLUX[flux], dptr(av), nrep, C.byref(ms),
+                                     C.byref(ab)))
+        return dict(ms=ms.value, alg_bytes=ab.value)

@@ -206,3 +206,167 @@ def c5(members: int = 64, nmin: int = 16, nmax: int = 64, zmin: int = 4, zmax: i
     sizes = [(int(rng.integers(nmin, nmax + 1)), int(rng.integers(nmin, nmax + 1)),
               int(rng.integers(zmin, zmax + 1))) for _ in range(members)]
     return [c5_member(i, nx, ny, nz, order, precision, seed) for i, (nx, ny, nz) in enumerate(sizes)]
+
+
+# ----------------------------------------------------------------------------- C3 AMR mesh
+FINE_TYPE = {(0, 0): 0, (1, 0): 1, (0, 1): 2, (1, 1): 5}  # (split t1, split t2) -> FaceConnectionType
+
+
+def fbm_hurst(m: int, hurst: float, seed: int) -> np.ndarray:
+    """Periodic fractional-Brownian surface with Hurst exponent H (spectrum 1/f^(2H+2))."""
+    return fbm_field(m, seed, beta=2.0 * hurst + 2.0)
+
+
+def c3_levels(nb: int = 256, hurst: float = 0.7, seed: int = SEED, lmax: int = 3):
+    """Directional refinement levels (lx, ly, lz) per base column of an nb x nb grid, refined
+    towards the zero line of a seeded fBm field (the coastline: wet columns, mean below the
+    median, with a dry column across a face): level lmax on coastal columns,
+    one less per column of Chebyshev distance; on the coast the direction along the coastline
+    is refined one level less (anisotropy); 2:1 balance in every tangential direction; a
+    vertical split where both horizontal levels are lmax."""
+    sub = 4
+    phi = fbm_hurst(nb * sub, hurst, seed)
+    phi = phi - np.median(phi)
+    pm = phi.reshape(nb, sub, nb, sub).mean(axis=(1, 3))  # [iy, ix] column means
+    wet = pm < 0
+    coast = np.zeros_like(wet)  # wet columns with a dry column across a face
+    coast[:, :-1] |= wet[:, :-1] & ~wet[:, 1:]
+    coast[:, 1:] |= wet[:, 1:] & ~wet[:, :-1]
+    coast[:-1, :] |= wet[:-1, :] & ~wet[1:, :]
+    coast[1:, :] |= wet[1:, :] & ~wet[:-1, :]
+    # Chebyshev distance to the coast (in columns), capped at lmax + 1
+    dist = np.where(coast, 0, lmax + 1).astype(np.int64)
+    for d in range(1, lmax + 1):
+        near = np.zeros_like(coast)
+        src = dist == d - 1
+        for dy in (-1, 0, 1):
+            for dx in (-1, 0, 1):
+                near |= np.roll(np.roll(src, dy, 0), dx, 1)
+        dist = np.where((dist > d) & near, d, dist)
+    L = np.maximum(0, lmax - dist)
+    gy, gx = np.gradient(pm)
+    lx, ly = L.copy(), L.copy()
+    along_y = coast & (np.abs(gx) >= 2.0 * np.abs(gy))  # coastline runs along y: refine x more
+    along_x = coast & (np.abs(gy) >= 2.0 * np.abs(gx))
+    ly[along_y] = np.maximum(0, ly[along_y] - 1)
+    lx[along_x] = np.maximum(0, lx[along_x] - 1)
+    # 2:1 balance of the tangential levels across faces (raise the coarser side)
+    for _ in range(2 * lmax + 2):
+        ly_n = np.maximum(np.roll(ly, 1, 1), np.roll(ly, -1, 1))  # x neighbours (periodic rolls
+        lx_n = np.maximum(np.roll(lx, 1, 0), np.roll(lx, -1, 0))  # are harmless: only raise)
+        ly2, lx2 = np.maximum(ly, ly_n - 1), np.maximum(lx, lx_n - 1)
+        if (ly2 == ly).all() and (lx2 == lx).all():
+            break
+        ly, lx = ly2, lx2
+    lz = ((lx == lmax) & (ly == lmax)).astype(np.int64)
+    return lx, ly, lz
+
+
+def amr_mesh(lx, ly, lz, L: float = 1.0):
+    """Hexahedra and face connections of a column-wise directionally refined grid.
+
+    Returns elements (grouped by level tuple), conforming face pairs, boundary faces and the
+    non-conforming interfaces (type, coarse element and face, fine elements and faces in the
+    sub-face order of MortarSpace::compute_subface_bounds, src/dg/mortar.cpp:27), sorted by
+    connection type. Face f has its normal along axis f // 2, positive when f is odd; the
+    tangential axes of a face are the other two in axis order (t1 < t2)."""
+    ny, nx = lx.shape
+    lv = np.stack([lx.ravel(), ly.ravel(), lz.ravel()], 1)  # column c = ix + nx * iy
+    ncol = nx * ny
+    order = np.lexsort((np.arange(ncol), lv[:, 2], lv[:, 1], lv[:, 0]))
+    ncell = (1 << lv[:, 0]) * (1 << lv[:, 1]) * (1 << lv[:, 2])
+    off = np.zeros(ncol, np.int64)
+    off[order] = np.concatenate([[0], np.cumsum(ncell[order])[:-1]])
+    n_elem = int(ncell.sum())
+
+    def eid(c, sx, sy, sz):
+        nxc, nyc = 1 << lv[c, 0], 1 << lv[c, 1]
+        return off[c] + sx + nxc * (sy + nyc * sz)
+
+    elem_level = np.zeros((n_elem, 3), np.int64)
+    elem_box = np.zeros((n_elem, 6))
+    conf, bnd, ifs = [], [], []
+    dxb = L / nx
+    for c in range(ncol):
+        ix, iy = c % nx, c // nx
+        nxc, nyc, nzc = 1 << lv[c, 0], 1 << lv[c, 1], 1 << lv[c, 2]
+        for sz in range(nzc):
+            for sy in range(nyc):
+                for sx in range(nxc):
+                    e = eid(c, sx, sy, sz)
+                    elem_level[e] = lv[c]
+                    elem_box[e] = [(ix + sx / nxc) * dxb, (iy + sy / nyc) * dxb, sz / nzc,
+                                   (ix + (sx + 1) / nxc) * dxb, (iy + (sy + 1) / nyc) * dxb, (sz + 1) / nzc]
+                    # faces inside the column, and the column's bottom/top/basin sides
+                    if sx + 1 < nxc: conf.append((e, 1, eid(c, sx + 1, sy, sz), 0))
+                    if sy + 1 < nyc: conf.append((e, 3, eid(c, sx, sy + 1, sz), 2))
+                    if sz + 1 < nzc: conf.append((e, 5, eid(c, sx, sy, sz + 1), 4))
+                    if sz == 0: bnd.append((e, 4))
+                    if sz == nzc - 1: bnd.append((e, 5))
+                    if sx == 0 and ix == 0: bnd.append((e, 0))
+                    if sx == nxc - 1 and ix == nx - 1: bnd.append((e, 1))
+                    if sy == 0 and iy == 0: bnd.append((e, 2))
+                    if sy == nyc - 1 and iy == ny - 1: bnd.append((e, 3))
+        # faces with the next column in x (normal axis 0: tangents y, z) and in y (axis 1: x, z)
+        for axis, nbc in ((0, c + 1 if ix + 1 < nx else -1), (1, c + nx if iy + 1 < ny else -1)):
+            if nbc < 0:
+                continue
+            t1 = 1 if axis == 0 else 0
+            la, lb = lv[c], lv[nbc]
+            da = (la[t1] - lb[t1], la[2] - lb[2])
+            fa, fb = 2 * axis + 1, 2 * axis  # face of this column / of the neighbour
+            if da[0] >= 0 and da[1] >= 0:
+                coarse, fine, cf, ff, d = nbc, c, fb, fa, da
+            else:
+                coarse, fine, cf, ff, d = c, nbc, fa, fb, (-da[0], -da[1])
+            assert d[0] in (0, 1) and d[1] in (0, 1), "2:1 balance violated"
+            lc, lf = lv[coarse], lv[fine]
+            n1c, nzc_ = 1 << lc[t1], 1 << lc[2]
+            # the layer of cells of each column that touches the shared face
+            def cell(col, lvl, a1, a2, at_max):
+                nxc, nyc = 1 << lvl[0], 1 << lvl[1]
+                s_norm = ((nxc if axis == 0 else nyc) - 1) if at_max else 0
+                if axis == 0:
+                    return eid(col, s_norm, a1, a2)
+                return eid(col, a1, s_norm, a2)
+            coarse_is_low = (coarse == c)  # the lower column holds the +normal face
+            for p2 in range(nzc_):
+                for p1 in range(n1c):
+                    ce = cell(coarse, lc, p1, p2, coarse_is_low)
+                    fines = []
+                    for b2 in range(1 + d[1]):
+                        for b1 in range(1 + d[0]):
+                            fines.append(cell(fine, lf, p1 * (1 + d[0]) + b1, p2 * (1 + d[1]) + b2,
+                                              not coarse_is_low))
+                    t = FINE_TYPE[d]
+                    if t == 0:
+                        conf.append((ce, cf, fines[0], ff))
+                    else:
+                        ifs.append((t, ce, cf, fines, [ff] * len(fines)))
+    ifs.sort(key=lambda r: r[0])  # interfaces grouped by connection type
+    conf = np.array(conf, np.int64).reshape(-1, 4)
+    bnd = np.array(bnd, np.int64).reshape(-1, 2)
+    return dict(n_elem=n_elem, level=elem_level, box=elem_box, conf=conf, bnd=bnd, ifaces=ifs,
+                col_levels=lv)
+
+
+def c3(nb: int = 256, order: int = 3, seed: int = SEED, hurst: float = 0.7):
+    """C3: directional AMR (4 levels per horizontal direction, 2 vertically) refined towards a
+    seeded fBm (Hurst 0.7) coastline on an nb x nb base grid, N=3; a scalar field advected
+    with a constant velocity (the scalar conservation law of DG3DIntegration::compute_rhs)."""
+    lx, ly, lz = c3_levels(nb, hurst, seed)
+    mesh = amr_mesh(lx, ly, lz)
+    npn = order + 1
+    rng = np.random.default_rng(seed + 3)
+    box = mesh["box"]
+    x = lgl_nodes(order)
+    # a smooth seeded field sampled at every element's nodes
+    kx, ky, kz = rng.uniform(1, 4, 3)
+    X = box[:, None, 0] + 0.5 * (x[None, :] + 1) * (box[:, None, 3] - box[:, None, 0])
+    Y = box[:, None, 1] + 0.5 * (x[None, :] + 1) * (box[:, None, 4] - box[:, None, 1])
+    Z = box[:, None, 2] + 0.5 * (x[None, :] + 1) * (box[:, None, 5] - box[:, None, 2])
+    U = (np.sin(2 * np.pi * kx * X)[:, None, None, :] * np.cos(2 * np.pi * ky * Y)[:, None, :, None]
+         * (1.0 + 0.5 * Z)[:, :, None, None]).reshape(mesh["n_elem"], npn ** 3)
+    a = np.array([1.0, 0.6, 0.2])
+    return dict(order=order, mesh=mesh, U=np.ascontiguousarray(U), a=a,
+                name=f"C3 AMR {nb}x{nb} base, {mesh['n_elem']} hexes N={order}")

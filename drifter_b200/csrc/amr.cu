@@ -1,0 +1,511 @@
+// DG3DIntegration::compute_rhs (src/dg/operators_3d.cpp:228-282) on a directionally refined
+// (AMR) hexahedral mesh, for the scalar conservation law u_t + div(a u) = 0 with a constant
+// velocity a, plus a low-storage RK45 step replayed as one CUDA graph.
+//
+// Semantics, as the reference computes them (reference coordinates: identity Jacobian):
+//   R_e = M^-1 ( -sum_q w_q grad(phi)(x_q) . a u(x_q)          volume_integral (:81), N-point
+//                                                              Gauss-Legendre per direction
+//                + conforming / boundary face lifts            mode 1 only (TODO in the reference)
+//                + mortar lifts of the non-conforming faces )  compute_interface_flux_nonconforming (:345)
+// and the step integrates du/dt = -R (R is the weak divergence of a u: volume -grad(phi), faces +F).
+//
+// Kernel design. The volume term is a tensor product: with B (N x (N+1)) the LGL basis at the
+// Gauss-Legendre points, B' its derivative and W the weights, the quadrature equals
+//   -(a_x K x M x M + a_y M x K x M + a_z M x M x K) u,  K = B'^T W B,  M = B^T W B,
+// applied sum-factorized (six small passes over an element's (N+1)^3 nodes in shared memory).
+// One thread per node, several elements per CTA; each node then adds the flux of every face
+// it lies on (faces 0..5 in order, own outward normal, the neighbour's face node read from
+// global memory), so the result needs no atomics. The mortar kernels (mortar.cu) add the
+// non-conforming lifts in interface order; the mass inverse is fused into the output or the
+// LSRK update.
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <vector>
+
+#include "common.cuh"
+
+namespace drf {
+namespace {
+
+struct AmrBasis {
+    double K[MAXNP * MAXNP], M[MAXNP * MAXNP], w[MAXNP];
+};
+__constant__ AmrBasis cAmr[MAXNP + 1];  // per node count
+
+const double AMR_LSRK_A[5] = {0.0, -0.4178904745, -1.192151694643, -1.697784692471, -1.514183444257};
+const double AMR_LSRK_B[5] = {0.1496590219993, 0.3792103129999, 0.8229550293869, 0.6994504559488,
+                              0.1530572479681};
+
+struct AmrArgs {
+    const double *U;
+    double *R;              // weak right-hand side (before the mass inverse)
+    const int64_t *nbe;     // [elem][6] conforming neighbour element (or -1)
+    const int8_t *nbk;      // [elem][6] 0 none, 1 conforming, 2 boundary
+    const int8_t *nbf;      // [elem][6] neighbour face
+    int64_t n_elem;
+    double ax, ay, az;
+    int flux;               // 0 central, 1 upwind, 2 Lax-Friedrichs
+};
+
+__device__ __forceinline__ double amr_flux(int kind, double uL, double uR, double vn) {
+    if (kind == 0) return 0.5 * (vn * uL + vn * uR);
+    if (kind == 1) return vn * (vn >= 0 ? uL : uR);
+    return 0.5 * (vn * uL + vn * uR) - 0.5 * fabs(vn) * (uR - uL);
+}
+
+// volume node of face node (it, jt) of face f: normal index at the boundary, tangents in axis order
+template <int NP>
+__device__ __forceinline__ int face_node(int f, int it, int jt) {
+    const int axis = f / 2, b = (f % 2) ? NP - 1 : 0;
+    if (axis == 0) return b + NP * (it + NP * jt);
+    if (axis == 1) return it + NP * (b + NP * jt);
+    return it + NP * (jt + NP * b);
+}
+
+template <int NP>
+constexpr int amr_epb() {  // elements per CTA: about 256 threads
+    return (256 / (NP * NP * NP)) < 1 ? 1 : 256 / (NP * NP * NP);
+}
+
+// R = volume term + conforming/boundary face lifts, one thread per node.
+template <int NP>
+__global__ void __launch_bounds__(amr_epb<NP>() * NP * NP * NP) amr_rhs_kernel(AmrArgs a) {
+    constexpr int NP3 = NP * NP * NP, EPB = amr_epb<NP>();
+    __shared__ double sU[EPB * NP3], sP[EPB * NP3], sQ[EPB * NP3], s1[EPB * NP3], s2[EPB * NP3];
+    const AmrBasis &Bs = cAmr[NP];
+    const int le = threadIdx.x / NP3, n = threadIdx.x % NP3;
+    const int i = n % NP, j = (n / NP) % NP, k = n / (NP * NP);
+    const int64_t e = (int64_t)blockIdx.x * EPB + le;
+    const bool valid = e < a.n_elem;
+    double *U = sU + le * NP3, *P = sP + le * NP3, *Q = sQ + le * NP3, *T1 = s1 + le * NP3, *T2 = s2 + le * NP3;
+    const double u = valid ? a.U[e * NP3 + n] : 0.0;
+    U[n] = u;
+    __syncthreads();
+    // z: P = (I x I x M) u, Q = (I x I x K) u
+    double p = 0.0, q = 0.0;
+#pragma unroll
+    for (int m = 0; m < NP; ++m) {
+        const double um = U[i + NP * (j + NP * m)];
+        p += Bs.M[k * NP + m] * um;
+        q += Bs.K[k * NP + m] * um;
+    }
+    P[n] = p;
+    Q[n] = q;
+    __syncthreads();
+    // y: T1 = (I x M x I) P, T2 = (I x K x I) P, U <- (I x M x I) Q
+    double t1 = 0.0, t2 = 0.0, t3 = 0.0;
+#pragma unroll
+    for (int m = 0; m < NP; ++m) {
+        const int nm = i + NP * (m + NP * k);
+        t1 += Bs.M[j * NP + m] * P[nm];
+        t2 += Bs.K[j * NP + m] * P[nm];
+        t3 += Bs.M[j * NP + m] * Q[nm];
+    }
+    __syncthreads();  // every thread has read U (its own node) and P, Q
+    T1[n] = t1;
+    T2[n] = t2;
+    U[n] = t3;
+    __syncthreads();
+    // x: r = -(a_x (K x I x I) T1 + a_y (M x I x I) T2 + a_z (M x I x I) T3)
+    double vx = 0.0, vy = 0.0, vz = 0.0;
+#pragma unroll
+    for (int m = 0; m < NP; ++m) {
+        const int nm = m + NP * (j + NP * k);
+        vx += Bs.K[i * NP + m] * T1[nm];
+        vy += Bs.M[i * NP + m] * T2[nm];
+        vz += Bs.M[i * NP + m] * U[nm];
+    }
+    if (!valid) return;
+    double r = -(a.ax * vx + a.ay * vy + a.az * vz);
+    // faces this node lies on, in face order
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+        const int axis = f / 2;
+        const int idx = axis == 0 ? i : (axis == 1 ? j : k);
+        if (idx != ((f % 2) ? NP - 1 : 0)) continue;
+        const int kd = a.nbk[e * 6 + f];
+        if (kd == 0) continue;
+        const int it = axis == 0 ? j : i, jt = axis == 2 ? j : k;
+        const double vn = ((f % 2) ? 1.0 : -1.0) * (axis == 0 ? a.ax : (axis == 1 ? a.ay : a.az));
+        double uR = u;
+        if (kd == 1) uR = a.U[a.nbe[e * 6 + f] * NP3 + face_node<NP>(a.nbf[e * 6 + f], it, jt)];
+        r += Bs.w[it] * Bs.w[jt] * amr_flux(a.flux, u, uR, vn);
+    }
+    a.R[e * NP3 + n] = r;
+}
+
+// out = M^-1 R (the right-hand side the caller sees)
+template <int NP>
+__global__ void amr_massinv_kernel(int64_t n, const double *R, double *out) {
+    constexpr int NP3 = NP * NP * NP;
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const int nn = (int)(t % NP3), i = nn % NP, j = (nn / NP) % NP, k = nn / (NP * NP);
+    const AmrBasis &Bs = cAmr[NP];
+    out[t] = R[t] * (1.0 / (Bs.w[i] * Bs.w[j] * Bs.w[k]));
+}
+
+// LSRK45 stage: res = A res + dt (-M^-1 R); U += B res
+template <int NP>
+__global__ void amr_lsrk_kernel(int64_t n, const double *R, double *res, double *U, double A, double B,
+                                double dt, int first) {
+    constexpr int NP3 = NP * NP * NP;
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const int nn = (int)(t % NP3), i = nn % NP, j = (nn / NP) % NP, k = nn / (NP * NP);
+    const AmrBasis &Bs = cAmr[NP];
+    const double rhs = R[t] * (1.0 / (Bs.w[i] * Bs.w[j] * Bs.w[k]));
+    const double rn = (first ? 0.0 : A * res[t]) + dt * (-rhs);
+    res[t] = rn;
+    U[t] = U[t] + B * rn;
+}
+
+template <class F>
+void amr_dispatch(int np, F &&f) {
+    switch (np) {
+    case 2: f(std::integral_constant<int, 2>{}); break;
+    case 3: f(std::integral_constant<int, 3>{}); break;
+    case 4: f(std::integral_constant<int, 4>{}); break;
+    case 5: f(std::integral_constant<int, 5>{}); break;
+    case 6: f(std::integral_constant<int, 6>{}); break;
+    default: throw Error(DRF_E_UNSUPPORTED, "AMR: order must be 1..5");
+    }
+}
+
+}  // namespace
+}  // namespace drf
+
+using namespace drf;
+
+struct drf_amr {
+    int order = 0, np = 0, nd = 0;
+    int64_t n_elem = 0, n_conf = 0, n_bnd = 0, n_if = 0;
+    cudaStream_t stream = nullptr, own = nullptr;
+    DevBuf<int64_t> nbe;
+    DevBuf<int8_t> nbk, nbf;
+    DevBuf<double> U, R, res, out;  // device state, weak rhs, LSRK register, caller-visible rhs
+    drf_mortar *mortar = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    int g_mode = -1, g_flux = -1;
+    double g_a[3] = {0, 0, 0}, g_dt = 0.0;
+
+    ~drf_amr() {
+        if (graph) cudaGraphExecDestroy(graph);
+        if (mortar) drf_mortar_destroy(mortar);
+        if (own) cudaStreamDestroy(own);
+    }
+    void drop_graph() {
+        if (graph) cudaGraphExecDestroy(graph);
+        graph = nullptr;
+        g_mode = -1;
+    }
+    // R = weak right-hand side of U (volume + faces of the mode + mortar lifts)
+    void enqueue_rhs(int mode, int flux, const double a[3]) {
+        AmrArgs A{};
+        A.U = U.p; A.R = R.p; A.nbe = nbe.p; A.nbf = nbf.p; A.n_elem = n_elem;
+        A.ax = a[0]; A.ay = a[1]; A.az = a[2]; A.flux = flux;
+        // mode 0 reads an all-zero face table: the reference's TODO branches
+        A.nbk = mode == 1 ? nbk.p : nbk.p + (size_t)6 * n_elem;
+        amr_dispatch(np, [&](auto npc) {
+            constexpr int NP = decltype(npc)::value;
+            constexpr int EPB = amr_epb<NP>();
+            amr_rhs_kernel<NP><<<(unsigned)((n_elem + EPB - 1) / EPB), EPB * NP * NP * NP, 0, stream>>>(A);
+            DRF_LAUNCHED();
+        });
+        if (mortar) {
+            const int rc = drf_mortar_apply_device(mortar, flux, a, U.p, R.p);
+            DRF_CHECK(rc == DRF_OK, rc, "mortar apply failed");
+        }
+    }
+    void enqueue_step(int mode, int flux, const double a[3], double dt) {
+        const int64_t n = n_elem * nd;
+        for (int s = 0; s < 5; ++s) {
+            enqueue_rhs(mode, flux, a);
+            amr_dispatch(np, [&](auto npc) {
+                constexpr int NP = decltype(npc)::value;
+                amr_lsrk_kernel<NP><<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(
+                    n, R.p, res.p, U.p, AMR_LSRK_A[s], AMR_LSRK_B[s], dt, s == 0);
+                DRF_LAUNCHED();
+            });
+        }
+    }
+};
+
+namespace {
+
+void amr_check(drf_amr *h) { DRF_CHECK(h != nullptr, DRF_E_INVALID, "null AMR handle"); }
+
+void amr_check_args(int mode, int flux, const double *a) {
+    DRF_CHECK(mode == 0 || mode == 1, DRF_E_INVALID, "mode must be 0 (reference) or 1 (complete)");
+    DRF_CHECK(flux >= 0 && flux <= 2, DRF_E_INVALID, "flux kind must be 0 (central), 1 (upwind) or 2 (LF)");
+    DRF_CHECK(a && std::isfinite(a[0]) && std::isfinite(a[1]) && std::isfinite(a[2]), DRF_E_INVALID,
+              "advection velocity must be finite");
+}
+
+// Gauss-Legendre nodes and weights (n points) by Newton on the Legendre recurrence
+void gl_rule(int n, std::vector<double> &x, std::vector<double> &w) {
+    x.assign(n, 0.0);
+    w.assign(n, 0.0);
+    for (int i = 0; i < n; ++i) {
+        double z = std::cos(M_PI * (i + 0.75) / (n + 0.5)), dp = 1.0;
+        for (int it = 0; it < 100; ++it) {
+            double p0 = 1.0, p1 = z;
+            for (int k = 2; k <= n; ++k) {
+                const double p2 = ((2.0 * k - 1.0) * z * p1 - (k - 1.0) * p0) / k;
+                p0 = p1;
+                p1 = p2;
+            }
+            if (n == 1) p1 = z, p0 = 1.0;
+            dp = n * (z * p1 - p0) / (z * z - 1.0);
+            const double dz = p1 / dp;
+            z -= dz;
+            if (std::abs(dz) < 1e-16) break;
+        }
+        x[n - 1 - i] = z;  // ascending
+        w[n - 1 - i] = 2.0 / ((1.0 - z * z) * dp * dp);
+    }
+}
+
+// K = B'^T W B and M = B^T W B of the reference's volume quadrature (N Gauss-Legendre points)
+void upload_amr_basis(int order) {
+    static std::mutex mu;
+    static bool done[64][MAXNP + 1] = {};
+    int dev = 0;
+    DRF_CUDA(cudaGetDevice(&dev));
+    const HostBasis b = make_lgl_basis(order);
+    const int np = b.np, nq = order;
+    std::lock_guard<std::mutex> lk(mu);
+    if (dev < 64 && done[dev][np]) return;
+    std::vector<double> gx, gw;
+    gl_rule(nq, gx, gw);
+    // barycentric Lagrange interpolation of the LGL basis at the GL points
+    std::vector<double> bw(np, 1.0), B((size_t)nq * np, 0.0), Bd((size_t)nq * np, 0.0);
+    for (int j = 0; j < np; ++j)
+        for (int k = 0; k < np; ++k)
+            if (k != j) bw[j] /= (b.x[j] - b.x[k]);
+    for (int q = 0; q < nq; ++q) {
+        double den = 0.0;
+        for (int j = 0; j < np; ++j) den += bw[j] / (gx[q] - b.x[j]);
+        for (int j = 0; j < np; ++j) B[q * np + j] = bw[j] / (gx[q] - b.x[j]) / den;
+    }
+    for (int q = 0; q < nq; ++q)  // phi_m'(x_q) = sum_i phi_i(x_q) D[i][m]
+        for (int m = 0; m < np; ++m)
+            for (int i = 0; i < np; ++i) Bd[q * np + m] += B[q * np + i] * b.D[i * np + m];
+    AmrBasis ab;
+    std::memset(&ab, 0, sizeof(ab));
+    for (int i = 0; i < np; ++i) {
+        ab.w[i] = b.w[i];
+        for (int m = 0; m < np; ++m) {
+            double k = 0.0, mm = 0.0;
+            for (int q = 0; q < nq; ++q) {
+                k += Bd[q * np + i] * gw[q] * B[q * np + m];
+                mm += B[q * np + i] * gw[q] * B[q * np + m];
+            }
+            ab.K[i * np + m] = k;
+            ab.M[i * np + m] = mm;
+        }
+    }
+    DRF_CUDA(cudaMemcpyToSymbol(cAmr, &ab, sizeof(ab), (size_t)np * sizeof(AmrBasis)));
+    if (dev < 64) done[dev][np] = true;
+}
+
+}  // namespace
+
+extern "C" {
+
+int drf_amr_create(int order, int64_t n_elem, int64_t n_conf, const int64_t *conf, int64_t n_bnd,
+                   const int64_t *bnd, int64_t n_if, const int *type, const int64_t *coarse_elem,
+                   const int *coarse_face, const int64_t *fine_elem, const int *fine_face, drf_amr **out) {
+    return guard([&] {
+        DRF_CHECK(out, DRF_E_INVALID, "null output");
+        *out = nullptr;
+        DRF_CHECK(order >= 1 && order < MAXNP, DRF_E_UNSUPPORTED, "AMR: order must be 1..5");
+        DRF_CHECK(n_elem >= 1 && n_conf >= 0 && n_bnd >= 0 && n_if >= 0, DRF_E_INVALID, "bad sizes");
+        DRF_CHECK((n_conf == 0 || conf) && (n_bnd == 0 || bnd), DRF_E_INVALID, "null face list");
+        auto h = std::make_unique<drf_amr>();
+        h->order = order;
+        h->np = order + 1;
+        h->nd = h->np * h->np * h->np;
+        h->n_elem = n_elem;
+        h->n_conf = n_conf;
+        h->n_bnd = n_bnd;
+        h->n_if = n_if;
+        // face table: the second half stays zero (the reference-semantics launches read it)
+        std::vector<int64_t> nbe((size_t)6 * n_elem, -1);
+        std::vector<int8_t> nbk((size_t)12 * n_elem, 0), nbf((size_t)6 * n_elem, 0);
+        auto set = [&](int64_t e, int64_t f, int8_t kd, int64_t e2, int64_t f2) {
+            DRF_CHECK(e >= 0 && e < n_elem && f >= 0 && f < 6, DRF_E_INVALID, "face list entry out of range");
+            DRF_CHECK(nbk[e * 6 + f] == 0, DRF_E_INVALID, "face listed twice");
+            nbk[e * 6 + f] = kd;
+            nbe[e * 6 + f] = e2;
+            nbf[e * 6 + f] = (int8_t)f2;
+        };
+        for (int64_t i = 0; i < n_conf; ++i) {
+            const int64_t *c = conf + 4 * i;
+            DRF_CHECK(c[2] >= 0 && c[2] < n_elem && c[3] >= 0 && c[3] < 6 && c[1] / 2 == c[3] / 2 &&
+                          c[1] != c[3],
+                      DRF_E_INVALID, "conforming pair must join opposite faces of one axis");
+            set(c[0], c[1], 1, c[2], c[3]);
+            set(c[2], c[3], 1, c[0], c[1]);
+        }
+        for (int64_t i = 0; i < n_bnd; ++i) set(bnd[2 * i], bnd[2 * i + 1], 2, -1, 0);
+        upload_amr_basis(order);
+        DRF_CUDA(cudaStreamCreateWithFlags(&h->own, cudaStreamNonBlocking));
+        h->stream = h->own;
+        h->nbe.alloc(nbe.size());
+        h->nbk.alloc(nbk.size());
+        h->nbf.alloc(nbf.size());
+        DRF_CUDA(cudaMemcpy(h->nbe.p, nbe.data(), nbe.size() * 8, cudaMemcpyHostToDevice));
+        DRF_CUDA(cudaMemcpy(h->nbk.p, nbk.data(), nbk.size(), cudaMemcpyHostToDevice));
+        DRF_CUDA(cudaMemcpy(h->nbf.p, nbf.data(), nbf.size(), cudaMemcpyHostToDevice));
+        const size_t n = (size_t)n_elem * h->nd;
+        h->U.alloc(n);
+        h->R.alloc(n);
+        h->res.alloc(n);
+        h->out.alloc(n);
+        DRF_CUDA(cudaMemset(h->U.p, 0, n * 8));
+        DRF_CUDA(cudaMemset(h->res.p, 0, n * 8));
+        if (n_if > 0) {
+            const int rc = drf_mortar_create(order, n_if, type, coarse_elem, coarse_face, fine_elem, fine_face,
+                                             n_elem, &h->mortar);
+            DRF_CHECK(rc == DRF_OK, rc, "mortar interfaces rejected");
+            DRF_CHECK(drf_mortar_set_stream(h->mortar, h->stream) == DRF_OK, DRF_E_CUDA, "mortar stream");
+        }
+        *out = h.release();
+    });
+}
+
+int drf_amr_destroy(drf_amr *h) {
+    return guard([&] {
+        if (!h) return;
+        if (h->stream) cudaStreamSynchronize(h->stream);
+        delete h;
+    });
+}
+
+int drf_amr_set_stream(drf_amr *h, void *s) {
+    return guard([&] {
+        amr_check(h);
+        DRF_CUDA(cudaStreamSynchronize(h->stream));
+        h->drop_graph();
+        h->stream = s ? (cudaStream_t)s : h->own;
+        if (h->mortar) DRF_CHECK(drf_mortar_set_stream(h->mortar, h->stream) == DRF_OK, DRF_E_CUDA, "mortar stream");
+    });
+}
+
+int drf_amr_upload(drf_amr *h, const double *U) {
+    return guard([&] {
+        amr_check(h);
+        DRF_CHECK(U, DRF_E_INVALID, "null argument");
+        const size_t n = (size_t)h->n_elem * h->nd;
+        DRF_CHECK(all_finite(U, n), DRF_E_NONFINITE, "non-finite state");
+        DRF_CUDA(cudaMemcpyAsync(h->U.p, U, n * 8, cudaMemcpyHostToDevice, h->stream));
+        DRF_CUDA(cudaStreamSynchronize(h->stream));
+    });
+}
+
+int drf_amr_download(drf_amr *h, double *U) {
+    return guard([&] {
+        amr_check(h);
+        DRF_CHECK(U, DRF_E_INVALID, "null argument");
+        const size_t n = (size_t)h->n_elem * h->nd;
+        DRF_CUDA(cudaMemcpyAsync(U, h->U.p, n * 8, cudaMemcpyDeviceToHost, h->stream));
+        DRF_CUDA(cudaStreamSynchronize(h->stream));
+        DRF_CHECK(all_finite(U, n), DRF_E_NONFINITE, "non-finite state (the run blew up)");
+    });
+}
+
+int drf_amr_compute_rhs(drf_amr *h, int mode, int flux_kind, const double *a, const double *U, double *rhs) {
+    return guard([&] {
+        amr_check(h);
+        amr_check_args(mode, flux_kind, a);
+        DRF_CHECK(rhs, DRF_E_INVALID, "null output");
+        const int64_t n = h->n_elem * h->nd;
+        if (U) {
+            DRF_CHECK(all_finite(U, (size_t)n), DRF_E_NONFINITE, "non-finite state");
+            DRF_CUDA(cudaMemcpyAsync(h->U.p, U, n * 8, cudaMemcpyHostToDevice, h->stream));
+        }
+        h->enqueue_rhs(mode, flux_kind, a);
+        amr_dispatch(h->np, [&](auto npc) {
+            constexpr int NP = decltype(npc)::value;
+            amr_massinv_kernel<NP><<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(n, h->R.p, h->out.p);
+            DRF_LAUNCHED();
+        });
+        DRF_CUDA(cudaMemcpyAsync(rhs, h->out.p, n * 8, cudaMemcpyDeviceToHost, h->stream));
+        DRF_CUDA(cudaStreamSynchronize(h->stream));
+    });
+}
+
+int drf_amr_step(drf_amr *h, int mode, int flux_kind, const double *a, double dt, int nsteps) {
+    return guard([&] {
+        amr_check(h);
+        amr_check_args(mode, flux_kind, a);
+        DRF_CHECK(dt > 0.0 && std::isfinite(dt), DRF_E_INVALID, "dt must be positive");
+        DRF_CHECK(nsteps >= 0, DRF_E_INVALID, "nsteps must be >= 0");
+        if (!h->graph || h->g_mode != mode || h->g_flux != flux_kind || h->g_dt != dt ||
+            std::memcmp(h->g_a, a, sizeof(h->g_a)) != 0) {
+            h->drop_graph();
+            cudaGraph_t g = nullptr;
+            DRF_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+            try {
+                h->enqueue_step(mode, flux_kind, a, dt);
+            } catch (...) {
+                cudaStreamEndCapture(h->stream, &g);
+                if (g) cudaGraphDestroy(g);
+                throw;
+            }
+            DRF_CUDA(cudaStreamEndCapture(h->stream, &g));
+            cudaError_t e = cudaGraphInstantiate(&h->graph, g, 0);
+            cudaGraphDestroy(g);
+            DRF_CUDA(e);
+            h->g_mode = mode;
+            h->g_flux = flux_kind;
+            h->g_dt = dt;
+            std::memcpy(h->g_a, a, sizeof(h->g_a));
+        }
+        const uint64_t per_step = 5 * (2 + (h->mortar ? 2 : 0));
+        for (int s = 0; s < nsteps; ++s) {
+            DRF_CUDA(cudaGraphLaunch(h->graph, h->stream));
+            launch_counter().fetch_add(per_step);
+        }
+    });
+}
+
+int drf_amr_sync(drf_amr *h) {
+    return guard([&] {
+        amr_check(h);
+        DRF_CUDA(cudaStreamSynchronize(h->stream));
+    });
+}
+
+int drf_amr_time_rhs(drf_amr *h, int mode, int flux_kind, const double *a, int nrep, double *ms,
+                     double *alg_bytes) {
+    return guard([&] {
+        amr_check(h);
+        amr_check_args(mode, flux_kind, a);
+        DRF_CHECK(nrep >= 1 && ms, DRF_E_INVALID, "bad arguments");
+        cudaEvent_t e0, e1;
+        DRF_CUDA(cudaEventCreate(&e0));
+        DRF_CUDA(cudaEventCreate(&e1));
+        h->enqueue_rhs(mode, flux_kind, a);  // warm-up
+        DRF_CUDA(cudaEventRecord(e0, h->stream));
+        for (int r = 0; r < nrep; ++r) h->enqueue_rhs(mode, flux_kind, a);
+        DRF_CUDA(cudaEventRecord(e1, h->stream));
+        DRF_CUDA(cudaEventSynchronize(e1));
+        float t = 0.f;
+        DRF_CUDA(cudaEventElapsedTime(&t, e0, e1));
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        *ms = (double)t / nrep;
+        // algorithmic bytes of one right-hand side: u read and R written once per node, the
+        // neighbours' face traces of the conforming faces (mode 1) and the mortars' face traces
+        // read once, and the mortar lifts read-modify-written on the touched face nodes.
+        const double npf = (double)h->np * h->np;
+        const double faces = (mode == 1 ? 2.0 * h->n_conf : 0.0) + 3.0 * h->n_if;
+        if (alg_bytes) *alg_bytes = 16.0 * h->n_elem * h->nd + 8.0 * faces * npf + 16.0 * 3.0 * h->n_if * npf;
+    });
+}
+
+}  // extern "C"

@@ -321,6 +321,37 @@ int drf_mortar_apply(drf_mortar *h, int flux_kind, const double *a, const double
 int drf_mortar_apply_device(drf_mortar *h, int flux_kind, const double *a, const double *d_U,
                             double *d_rhs);
 
+/* ------------------------------------------------------------------ AMR scalar DG
+ * DG3DIntegration::compute_rhs (src/dg/operators_3d.cpp:228) for u_t + div(a u) = 0 with a
+ * constant velocity a on a directionally refined hexahedral mesh of one order N (1..5), in the
+ * reference's reference-coordinate form (identity Jacobian, :249-250): volume_integral (:81)
+ * with N Gauss-Legendre points per direction, the mortar flux of every non-conforming face
+ * (:345, once per coarse face), then the diagonal LGL mass inverse (:279). mode 0 is exactly
+ * that (the reference leaves conforming and boundary faces as TODO, :262-268); mode 1 also
+ * applies ConformingInterface::compute_flux (src/dg/mortar.cpp:320) and compute_boundary_flux
+ * (:393, Outflow) with the collocated (N+1)-point LGL face weights.
+ * conf: n_conf x (elem1, face1, elem2, face2) conforming pairs; bnd: n_bnd x (elem, face);
+ * interfaces as drf_mortar_create (FaceConnection, include/dg/face_connection.hpp:51).
+ * U, rhs: n_elem x (N+1)^3 element-major host arrays. flux: 0 central, 1 upwind, 2 LF. */
+typedef struct drf_amr drf_amr;
+int drf_amr_create(int order, int64_t n_elem, int64_t n_conf, const int64_t *conf, int64_t n_bnd,
+                   const int64_t *bnd, int64_t n_if, const int *type, const int64_t *coarse_elem,
+                   const int *coarse_face, const int64_t *fine_elem, const int *fine_face, drf_amr **out);
+int drf_amr_destroy(drf_amr *h);
+int drf_amr_set_stream(drf_amr *h, void *cuda_stream);
+int drf_amr_sync(drf_amr *h);
+/* rhs = compute_rhs(U) (U NULL: the handle's device state). */
+int drf_amr_compute_rhs(drf_amr *h, int mode, int flux_kind, const double *a, const double *U, double *rhs);
+int drf_amr_upload(drf_amr *h, const double *U);
+int drf_amr_download(drf_amr *h, double *U);
+/* nsteps of LSRK45 (LSRK45::step, src/solver/time_stepper.cpp:126) on du/dt = -compute_rhs(u)
+ * of the device state, each step one CUDA graph (5 x (volume/face kernel, mortar kernels,
+ * update)). */
+int drf_amr_step(drf_amr *h, int mode, int flux_kind, const double *a, double dt, int nsteps);
+/* Device time of one right-hand side (mean of nrep, CUDA events) and its algorithmic bytes. */
+int drf_amr_time_rhs(drf_amr *h, int mode, int flux_kind, const double *a, int nrep, double *ms,
+                     double *alg_bytes);
+
 #ifdef __cplusplus
 }
 #endif

@@ -362,3 +362,43 @@ def mortar_arrays(ifaces):
         out["fe"][i, :len(fe)] = fe
         out["ff"][i, :len(ff)] = ff
     return out
+
+
+# ----------------------------------------------------------------------------- AMR scalar DG
+LSRK_A = (0.0, -0.4178904745, -1.192151694643, -1.697784692471, -1.514183444257)
+LSRK_B = (0.1496590219993, 0.3792103129999, 0.8229550293869, 0.6994504559488, 0.1530572479681)
+
+
+def amr_rhs(order, mesh, mode, flux_kind, a, U):
+    """DG3DIntegration::compute_rhs (src/dg/operators_3d.cpp:228) on an AMR mesh (the dict of
+    configs.amr_mesh): mode 0 the reference's semantics, 1 with conforming and boundary faces."""
+    L = lib()
+    vp = C.c_void_p
+    L.orc_amr_rhs.argtypes = [C.c_int, C.c_long, C.c_int, C.c_int, _dp, C.c_long, vp, C.c_long, vp,
+                              C.c_long, vp, vp, vp, vp, vp, _dp, _dp]
+    arr = mortar_arrays(mesh["ifaces"])
+    U = _c(U)
+    out = np.zeros_like(U)
+    conf = np.ascontiguousarray(mesh["conf"], np.int64)
+    bnd = np.ascontiguousarray(mesh["bnd"], np.int64)
+    ptr = lambda x: x.ctypes.data_as(C.c_void_p)
+    r = L.orc_amr_rhs(order, U.shape[0], mode, flux_kind, _p(_c(a)), len(conf), ptr(conf), len(bnd),
+                      ptr(bnd), len(mesh["ifaces"]), ptr(arr["type"]), ptr(arr["ce"]), ptr(arr["cf"]),
+                      ptr(arr["fe"]), ptr(arr["ff"]), _p(U), _p(out))
+    if r < 0:
+        raise ValueError("oracle: bad AMR arguments")
+    return out
+
+
+def amr_lsrk(order, mesh, mode, flux_kind, a, U, dt, nsteps):
+    """nsteps of the five-stage low-storage RK45 (LSRK45::step, src/solver/time_stepper.cpp:126)
+    on du/dt = -R(u), R = compute_rhs (the reference's right-hand side is the weak divergence
+    of a u: its volume term carries -grad(phi) and its face terms +F)."""
+    u = _c(U).copy()
+    res = np.zeros_like(u)
+    for _ in range(nsteps):
+        for s in range(5):
+            r = amr_rhs(order, mesh, mode, flux_kind, a, u)
+            res = LSRK_A[s] * res + dt * (-r)
+            u = u + LSRK_B[s] * res
+    return u
