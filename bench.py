@@ -43,6 +43,8 @@ def parse():
     ap.add_argument("--no-cg", action="store_true", help="skip the C4 Bezier CG comparison")
     ap.add_argument("--no-ens", action="store_true", help="skip the C5 ensemble measurement")
     ap.add_argument("--no-amr", action="store_true", help="skip the C3 AMR measurement")
+    ap.add_argument("--only", choices=["amr", "ens", "cg"], default=None,
+                    help="run one workload section alone and print its JSON (profiling aid)")
     return ap.parse_args()
 
 
@@ -334,6 +336,15 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def run_only(args, local):
+    import torch
+    torch.cuda.set_device(local)
+    stream = torch.cuda.Stream()
+    fn = {"amr": run_amr, "ens": run_ensemble, "cg": run_cg}[args.only]
+    out = fn(stream, steps=args.steps, warmup=args.warmup) if args.only != "cg" else fn(stream)
+    print(json.dumps({"only": args.only, **out}), flush=True)
+
+
 def run_ours(args, rank, world, local):
     import torch
     torch.cuda.set_device(local)
@@ -484,6 +495,8 @@ def main():
     try:
         if args.impl == "reference":
             run_reference(args, rank, world)
+        elif args.only:
+            run_only(args, local)
         else:
             run_ours(args, rank, world, local)
     finally:

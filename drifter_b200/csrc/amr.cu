@@ -74,7 +74,14 @@ template <int NP>
 __global__ void __launch_bounds__(amr_epb<NP>() * NP * NP * NP) amr_rhs_kernel(AmrArgs a) {
     constexpr int NP3 = NP * NP * NP, EPB = amr_epb<NP>();
     __shared__ double sU[EPB * NP3], sP[EPB * NP3], sQ[EPB * NP3], s1[EPB * NP3], s2[EPB * NP3];
-    const AmrBasis &Bs = cAmr[NP];
+    // the 1D operators in shared memory: lanes index them by their own node (a constant-memory
+    // read with different addresses across a warp is serialised)
+    __shared__ AmrBasis Bs;
+    for (int t = threadIdx.x; t < NP * NP; t += blockDim.x) {
+        Bs.K[t] = cAmr[NP].K[t];
+        Bs.M[t] = cAmr[NP].M[t];
+        if (t < NP) Bs.w[t] = cAmr[NP].w[t];
+    }
     const int le = threadIdx.x / NP3, n = threadIdx.x % NP3;
     const int i = n % NP, j = (n / NP) % NP, k = n / (NP * NP);
     const int64_t e = (int64_t)blockIdx.x * EPB + le;

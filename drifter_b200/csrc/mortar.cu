@@ -191,7 +191,8 @@ HostOps build_ops(int order, int t) {
     return o;
 }
 
-// device operator block of one type: Minv | Pc | Lc | Pf[4] | Lf[4], each nm * nm doubles
+// device operator block of one type: Minv | Pc | Lc | Pf[4] | Lf[4], each nm * nm doubles,
+// stored transposed (column-major)
 constexpr int OPS_MATS = 11;
 __host__ __device__ inline size_t ops_stride(int nm) { return (size_t)OPS_MATS * nm * nm; }
 
@@ -220,13 +221,16 @@ __device__ __forceinline__ double scalar_flux(int kind, double uL, double uR, do
     return 0.5 * (vn * uL + vn * uR) - 0.5 * fabs(vn) * (uR - uL);
 }
 
+// NP (nodes per direction) is a compile-time constant so the small dense products unroll and
+// their operator loads pipeline.
+template <int NP>
 __global__ void __launch_bounds__(32 * MW) mortar_face_kernel(MortarDev D, int kind, double a0, double a1,
                                                               double a2, const double *__restrict__ U,
                                                               double *__restrict__ contrib) {
-    __shared__ double sU[MW][SLOTS][MAXNM];
-    __shared__ double sF[MW][MAXNM], sG[MW][MAXNM];
+    constexpr int nm = NP * NP, nf = NP * NP, np = NP;
+    __shared__ double sU[MW][SLOTS][nm];
+    __shared__ double sF[MW][nm], sG[MW][nm];
     const int w = threadIdx.x / 32, lane = threadIdx.x % 32;
-    const int nm = D.nm, nf = D.nm, np = D.np;
     for (int64_t i = blockIdx.x * (int64_t)MW + w; i < D.n_if; i += (int64_t)gridDim.x * MW) {
         const int t = D.type[i], nfine = type_num_fine_dev(t);
         const double *op = D.ops + (size_t)t * ops_stride(nm);
@@ -243,11 +247,13 @@ __global__ void __launch_bounds__(32 * MW) mortar_face_kernel(MortarDev D, int k
         const double vn = ((cf & 1) ? 1.0 : -1.0) * (axis == 0 ? a0 : (axis == 1 ? a1 : a2));
         for (int m = lane; m < nm; m += 32) {
             double uc = 0.0, uf = 0.0;
-            for (int j = 0; j < nf; ++j) uc += Pc[m * nf + j] * sU[w][0][j];
+#pragma unroll
+            for (int j = 0; j < nf; ++j) uc += Pc[j * nm + m] * sU[w][0][j];
             for (int f = 0; f < nfine; ++f) {
                 double s = 0.0;
-                const double *P = Pf + (size_t)f * nm * nm + m * nf;
-                for (int j = 0; j < nf; ++j) s += P[j] * sU[w][1 + f][j];
+                const double *P = Pf + (size_t)f * nm * nm + m;
+#pragma unroll
+                for (int j = 0; j < nf; ++j) s += P[j * nm] * sU[w][1 + f][j];
                 uf += s;
             }
             sF[w][m] = scalar_flux(kind, uc, uf, vn);
@@ -255,19 +261,22 @@ __global__ void __launch_bounds__(32 * MW) mortar_face_kernel(MortarDev D, int k
         __syncwarp();
         for (int m = lane; m < nm; m += 32) {
             double g = 0.0;
-            for (int k = 0; k < nm; ++k) g += Minv[m * nm + k] * sF[w][k];
+#pragma unroll
+            for (int k = 0; k < nm; ++k) g += Minv[k * nm + m] * sF[w][k];
             sG[w][m] = g;
         }
         __syncwarp();
         double *out = contrib + (size_t)i * SLOTS * nf;
         for (int j = lane; j < nf; j += 32) {
             double s = 0.0;
-            for (int m = 0; m < nm; ++m) s += Lc[j * nm + m] * sG[w][m];
+#pragma unroll
+            for (int m = 0; m < nm; ++m) s += Lc[m * nf + j] * sG[w][m];
             out[j] = s;
             for (int f = 0; f < nfine; ++f) {
-                const double *L = Lf + (size_t)f * nm * nm + j * nm;
+                const double *L = Lf + (size_t)f * nm * nm + j;
                 double sf = 0.0;
-                for (int m = 0; m < nm; ++m) sf += L[m] * sG[w][m];
+#pragma unroll
+                for (int m = 0; m < nm; ++m) sf += L[m * nf] * sG[w][m];
                 out[(1 + f) * nf + j] = -sf;
             }
         }
@@ -330,7 +339,13 @@ struct drf_mortar {
     void run(int kind, const double a[3], const double *dU, double *drhs) {
         if (n_if == 0) return;
         const unsigned g = (unsigned)std::min<int64_t>((n_if + MW - 1) / MW, 148 * 16);
-        mortar_face_kernel<<<g, 32 * MW, 0, stream>>>(dev(), kind, a[0], a[1], a[2], dU, contrib.p);
+        switch (np) {
+        case 2: mortar_face_kernel<2><<<g, 32 * MW, 0, stream>>>(dev(), kind, a[0], a[1], a[2], dU, contrib.p); break;
+        case 3: mortar_face_kernel<3><<<g, 32 * MW, 0, stream>>>(dev(), kind, a[0], a[1], a[2], dU, contrib.p); break;
+        case 4: mortar_face_kernel<4><<<g, 32 * MW, 0, stream>>>(dev(), kind, a[0], a[1], a[2], dU, contrib.p); break;
+        case 5: mortar_face_kernel<5><<<g, 32 * MW, 0, stream>>>(dev(), kind, a[0], a[1], a[2], dU, contrib.p); break;
+        default: mortar_face_kernel<6><<<g, 32 * MW, 0, stream>>>(dev(), kind, a[0], a[1], a[2], dU, contrib.p); break;
+        }
         DRF_LAUNCHED();
         const int64_t nt = n_touched * nd;
         mortar_lift_kernel<<<(unsigned)((nt + 255) / 256), 256, 0, stream>>>(np, nd, n_touched, touched.p, ptr.p,
@@ -394,13 +409,20 @@ int drf_mortar_create(int order, int64_t n_if, const int *type, const int64_t *c
         for (int t = 0; t < MORTAR_TYPES; ++t) {
             const HostOps o = build_ops(order, t);
             double *dst = ops.data() + t * ops_stride(h->nm);
-            const size_t n2 = (size_t)h->nm * h->nm;
-            std::memcpy(dst, o.Minv.data(), n2 * 8);
-            std::memcpy(dst + n2, o.Pc.data(), n2 * 8);
-            std::memcpy(dst + 2 * n2, o.Lc.data(), n2 * 8);
+            const int nm = h->nm;
+            const size_t n2 = (size_t)nm * nm;
+            // stored transposed: in the face kernel lane m reads row m, so column-major storage
+            // makes a warp's reads of one column consecutive addresses
+            auto put_t = [&](double *d, const std::vector<double> &A) {
+                for (int r = 0; r < nm; ++r)
+                    for (int c = 0; c < nm; ++c) d[(size_t)c * nm + r] = A[(size_t)r * nm + c];
+            };
+            put_t(dst, o.Minv);
+            put_t(dst + n2, o.Pc);
+            put_t(dst + 2 * n2, o.Lc);
             for (int f = 0; f < o.nfine; ++f) {
-                std::memcpy(dst + (3 + f) * n2, o.Pf[f].data(), n2 * 8);
-                std::memcpy(dst + (7 + f) * n2, o.Lf[f].data(), n2 * 8);
+                put_t(dst + (3 + f) * n2, o.Pf[f]);
+                put_t(dst + (7 + f) * n2, o.Lf[f]);
             }
         }
         // interfaces, validated; per-element entries in interface order
