@@ -389,6 +389,7 @@ def run_ours(args, rank, world, local):
     peak, peak_kind = measured_peaks()
     achieved = st["alg_bytes"] / (st["ms"] / 1e3) / 1e9
     traffic = profile_traffic("dg3d_stage_c2_mixed.md")
+    copy = model.time_copy(nrep=5 * args.steps)  # the stage's access structure as a pure copy
 
     # end to end through the C ABI: per step upload the surface stress from pinned host memory,
     # run the step, read back the surface elevation and the diagnostics
@@ -476,6 +477,7 @@ def run_ours(args, rank, world, local):
                          "frac": achieved / peak, "traffic": traffic,
                          "kernel": "dg3d_stage_kernel<float,5>", "kernel_ms": st["ms"],
                          "alg_bytes_per_launch": st["alg_bytes"],
+                         "copy_ceiling_gbs": copy["gbs"], "copy_ceiling_frac": copy["gbs"] / peak,
                          "peak_source": f"{peak_kind} MEASURED_PEAKS.json hbm_gbs"},
             "cpu_baseline": cpu,
             "e2e": e2e,

@@ -69,27 +69,50 @@ constexpr int amr_epb() {  // elements per CTA: about 256 threads
     return (256 / (NP * NP * NP)) < 1 ? 1 : 256 / (NP * NP * NP);
 }
 
-// R = volume term + conforming/boundary face lifts, one thread per node.
+// R = volume term + conforming/boundary face lifts, one thread per node. The element's face
+// table and its conforming neighbours' face traces are loaded at the start (each thread takes
+// face-node slots n, n + NP^3, ...) so those global loads overlap the volume passes.
 template <int NP>
 __global__ void __launch_bounds__(amr_epb<NP>() * NP * NP * NP) amr_rhs_kernel(AmrArgs a) {
-    constexpr int NP3 = NP * NP * NP, EPB = amr_epb<NP>();
+    constexpr int NP2 = NP * NP, NP3 = NP2 * NP, EPB = amr_epb<NP>(), NFS = 6 * NP2;
+    constexpr int SLOTS = (NFS + NP3 - 1) / NP3;  // face-node slots per thread
     __shared__ double sU[EPB * NP3], sP[EPB * NP3], sQ[EPB * NP3], s1[EPB * NP3], s2[EPB * NP3];
+    __shared__ double sN[EPB * NFS];                // neighbour face traces [elem][face][node]
+    __shared__ int sNbe[EPB * 6];
+    __shared__ int8_t sK[EPB * 6], sNf[EPB * 6];
     // the 1D operators in shared memory: lanes index them by their own node (a constant-memory
     // read with different addresses across a warp is serialised)
     __shared__ AmrBasis Bs;
-    for (int t = threadIdx.x; t < NP * NP; t += blockDim.x) {
+    for (int t = threadIdx.x; t < NP2; t += blockDim.x) {
         Bs.K[t] = cAmr[NP].K[t];
         Bs.M[t] = cAmr[NP].M[t];
         if (t < NP) Bs.w[t] = cAmr[NP].w[t];
     }
     const int le = threadIdx.x / NP3, n = threadIdx.x % NP3;
-    const int i = n % NP, j = (n / NP) % NP, k = n / (NP * NP);
+    const int i = n % NP, j = (n / NP) % NP, k = n / NP2;
     const int64_t e = (int64_t)blockIdx.x * EPB + le;
     const bool valid = e < a.n_elem;
     double *U = sU + le * NP3, *P = sP + le * NP3, *Q = sQ + le * NP3, *T1 = s1 + le * NP3, *T2 = s2 + le * NP3;
     const double u = valid ? a.U[e * NP3 + n] : 0.0;
+    if (n < 6) {
+        sK[le * 6 + n] = valid ? a.nbk[e * 6 + n] : (int8_t)0;
+        sNbe[le * 6 + n] = valid ? (int)a.nbe[e * 6 + n] : -1;
+        sNf[le * 6 + n] = valid ? a.nbf[e * 6 + n] : (int8_t)0;
+    }
     U[n] = u;
     __syncthreads();
+    // neighbour face traces: loads issued now, stored to shared memory after the volume passes
+    double nv[SLOTS];
+#pragma unroll
+    for (int sl = 0; sl < SLOTS; ++sl) {
+        const int slot = n + sl * NP3;
+        nv[sl] = 0.0;
+        if (slot < NFS) {
+            const int f = slot / NP2, fn = slot % NP2;
+            if (sK[le * 6 + f] == 1)
+                nv[sl] = a.U[(int64_t)sNbe[le * 6 + f] * NP3 + face_node<NP>(sNf[le * 6 + f], fn % NP, fn / NP)];
+        }
+    }
     // z: P = (I x I x M) u, Q = (I x I x K) u
     double p = 0.0, q = 0.0;
 #pragma unroll
@@ -114,6 +137,9 @@ __global__ void __launch_bounds__(amr_epb<NP>() * NP * NP * NP) amr_rhs_kernel(A
     T1[n] = t1;
     T2[n] = t2;
     U[n] = t3;
+#pragma unroll
+    for (int sl = 0; sl < SLOTS; ++sl)
+        if (n + sl * NP3 < NFS) sN[le * NFS + n + sl * NP3] = nv[sl];
     __syncthreads();
     // x: r = -(a_x (K x I x I) T1 + a_y (M x I x I) T2 + a_z (M x I x I) T3)
     double vx = 0.0, vy = 0.0, vz = 0.0;
@@ -132,12 +158,11 @@ __global__ void __launch_bounds__(amr_epb<NP>() * NP * NP * NP) amr_rhs_kernel(A
         const int axis = f / 2;
         const int idx = axis == 0 ? i : (axis == 1 ? j : k);
         if (idx != ((f % 2) ? NP - 1 : 0)) continue;
-        const int kd = a.nbk[e * 6 + f];
+        const int kd = sK[le * 6 + f];
         if (kd == 0) continue;
         const int it = axis == 0 ? j : i, jt = axis == 2 ? j : k;
         const double vn = ((f % 2) ? 1.0 : -1.0) * (axis == 0 ? a.ax : (axis == 1 ? a.ay : a.az));
-        double uR = u;
-        if (kd == 1) uR = a.U[a.nbe[e * 6 + f] * NP3 + face_node<NP>(a.nbf[e * 6 + f], it, jt)];
+        const double uR = kd == 1 ? sN[le * NFS + f * NP2 + it + NP * jt] : u;
         r += Bs.w[it] * Bs.w[jt] * amr_flux(a.flux, u, uR, vn);
     }
     a.R[e * NP3 + n] = r;
@@ -330,6 +355,7 @@ int drf_amr_create(int order, int64_t n_elem, int64_t n_conf, const int64_t *con
         *out = nullptr;
         DRF_CHECK(order >= 1 && order < MAXNP, DRF_E_UNSUPPORTED, "AMR: order must be 1..5");
         DRF_CHECK(n_elem >= 1 && n_conf >= 0 && n_bnd >= 0 && n_if >= 0, DRF_E_INVALID, "bad sizes");
+        DRF_CHECK(n_elem < ((int64_t)1 << 31), DRF_E_UNSUPPORTED, "AMR: at most 2^31 - 1 elements");
         DRF_CHECK((n_conf == 0 || conf) && (n_bnd == 0 || bnd), DRF_E_INVALID, "null face list");
         auto h = std::make_unique<drf_amr>();
         h->order = order;

@@ -912,6 +912,48 @@ __global__ void baro_finish_kernel(int64_t n2, int nsub, double dt, const double
     corrV[t] = HV[t] - (HVo[t] + dHV3[t]);
 }
 
+// Memory-only counterpart of the stage kernel: the same CTA shape and dynamic shared memory
+// (so the same CTAs per SM), the column's state and LSRK register staged by the same bulk
+// copies, and the 8 arrays written back in the z-pencil pattern of the LSRK update, with no
+// arithmetic in between. Its bandwidth is the ceiling this access structure can reach.
+template <typename T, int NP>
+__global__ void __launch_bounds__(STAGE_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) dg3d_copy_kernel(StageArgs<T> a) {
+    constexpr int NP2 = NP * NP, NP3 = NP2 * NP;
+    const int nz = a.G.nz, ncn = nz * NP3, npen = nz * NP2;
+    const size_t base = (size_t)blockIdx.x * ncn;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw);
+    T *sQ = reinterpret_cast<T *>(smem_raw + 16 + 2 * NP2 * sizeof(double));
+    __shared__ int s_ok;
+    const uint32_t bytes = (uint32_t)(ncn * sizeof(T));
+    if (threadIdx.x == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_expect_tx(&bars[0], 8 * bytes);
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            bulk_g2s(sQ + v * ncn, a.qin[v] + base, bytes, &bars[0]);
+            bulk_g2s(sQ + (4 + v) * ncn, a.res[v] + base, bytes, &bars[0]);
+        }
+        s_ok = (int)mbar_wait(&bars[0], 0);
+    }
+    __syncthreads();
+    if (!s_ok) {
+        if (threadIdx.x == 0) atomicExch(a.err, DRF_E_TIMEOUT);
+        return;
+    }
+    for (int p = threadIdx.x; p < npen; p += blockDim.x) {
+        const int e0 = (p / NP2) * NP3 + p % NP2;
+#pragma unroll
+        for (int v = 0; v < 4; ++v)
+#pragma unroll
+            for (int k = 0; k < NP; ++k) {
+                const int n = e0 + NP2 * k;
+                a.qout[v][base + n] = sQ[v * ncn + n];
+                a.res[v][base + n] = sQ[(4 + v) * ncn + n];
+            }
+    }
+}
+
 // ------------------------------------------------------------------------- ensembles
 // An ensemble keeps every array of its members in pools laid out array-major: member m's slice
 // of a 3D array starts at element off3, of a 2D array at off2, and its model time is tdev[m].
@@ -1083,43 +1125,65 @@ __global__ void combine_kernel(int64_t n, Comb<T> cb) {
 }
 
 // diagnostics: per-block partials (fixed order -> deterministic)
-template <typename T, int NP>
-__global__ void diag3d_kernel(int64_t n3, int nz, const T *Hu, const T *Hv, const T *HT,
-                              const T *HS, const double *eta, const double *h, double wvol,
-                              double *part) {
-    constexpr int NP2 = NP * NP, NP3 = NP2 * NP;
-    __shared__ double red[6][256];
-    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    double en = 0, heat = 0, salt = 0, um = 0, Tmax = -1e300, Tmin = 1e300;
-    if (t < n3) {
-        const int64_t c = t / ((int64_t)nz * NP3);
-        const int ln = (int)(t % NP3), an = ln % NP2, i = an % NP, j = an / NP, k = ln / NP2;
-        const int64_t i2 = c * NP2 + an;
-        const double H = eta[i2] + h[i2];
-        const double wv = wvol * cBs[NP].w[i] * cBs[NP].w[j] * cBs[NP].w[k];
-        const double hu = Hu[t], hv = Hv[t];
-        en = wv * 0.5 * (hu * hu + hv * hv) / H;
-        heat = wv * (double)HT[t];
-        salt = wv * (double)HS[t];
-        um = sqrt(hu * hu + hv * hv) / H;
-        Tmax = Tmin = (double)HT[t] / H;
-    }
-    red[0][threadIdx.x] = en; red[1][threadIdx.x] = heat; red[2][threadIdx.x] = salt;
-    red[3][threadIdx.x] = um; red[4][threadIdx.x] = Tmax; red[5][threadIdx.x] = Tmin;
-    __syncthreads();
-    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-        if (threadIdx.x < s) {
-            red[0][threadIdx.x] += red[0][threadIdx.x + s];
-            red[1][threadIdx.x] += red[1][threadIdx.x + s];
-            red[2][threadIdx.x] += red[2][threadIdx.x + s];
-            red[3][threadIdx.x] = fmax(red[3][threadIdx.x], red[3][threadIdx.x + s]);
-            red[4][threadIdx.x] = fmax(red[4][threadIdx.x], red[4][threadIdx.x + s]);
-            red[5][threadIdx.x] = fmin(red[5][threadIdx.x], red[5][threadIdx.x + s]);
+// block sum / max / min of v[q] over the block, through warp shuffles (blockDim.x = 256)
+template <int Q>
+__device__ __forceinline__ void block_reduce(double (&v)[Q], const int (&op)[Q], double (*red)[8]) {
+    const int lane = threadIdx.x % 32, w = threadIdx.x / 32;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        for (int o = 16; o > 0; o >>= 1) {
+            const double x = __shfl_down_sync(0xffffffffu, v[q], o);
+            v[q] = op[q] == 0 ? v[q] + x : (op[q] == 1 ? fmax(v[q], x) : fmin(v[q], x));
         }
-        __syncthreads();
+        if (lane == 0) red[q][w] = v[q];
     }
+    __syncthreads();
     if (threadIdx.x == 0)
-        for (int q = 0; q < 6; ++q) part[blockIdx.x * 6 + q] = red[q][0];
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            double a = red[q][0];
+            for (int i = 1; i < 8; ++i) a = op[q] == 0 ? a + red[q][i] : (op[q] == 1 ? fmax(a, red[q][i]) : fmin(a, red[q][i]));
+            v[q] = a;
+        }
+}
+
+// 3D diagnostics, one block per column at a time (grid-stride over columns), 256 threads. A
+// pending transport correction (corrU, corrV non-null) is added on the fly with the same
+// arithmetic as folding it into the state, which is left untouched.
+template <typename T, int NP>
+__global__ void __launch_bounds__(256) diag3d_kernel(int ncol, int nz, const T *Hu, const T *Hv, const T *HT,
+                                                     const T *HS, const double *eta, const double *h,
+                                                     const double *corrU, const double *corrV, double wvol,
+                                                     double *part) {
+    constexpr int NP2 = NP * NP, NP3 = NP2 * NP;
+    __shared__ double red[6][8];
+    const int ncn = nz * NP3;
+    double v[6] = {0.0, 0.0, 0.0, 0.0, -1e300, 1e300};  // energy, heat, salt, max speed, max T, min T
+    for (int c = blockIdx.x; c < ncol; c += gridDim.x) {
+        const size_t base = (size_t)c * ncn;
+        for (int ln = threadIdx.x; ln < ncn; ln += blockDim.x) {
+            const int an = ln % NP2, i = an % NP, j = an / NP, k = (ln % NP3) / NP2;
+            const size_t i2 = (size_t)c * NP2 + an, t = base + ln;
+            const double H = eta[i2] + h[i2];
+            const double wv = wvol * cBs[NP].w[i] * cBs[NP].w[j] * cBs[NP].w[k];
+            T huT = Hu[t], hvT = Hv[t];
+            if (corrU) {
+                huT = huT + (T)corrU[i2];
+                hvT = hvT + (T)corrV[i2];
+            }
+            const double hu = huT, hv = hvT, ht = HT[t];
+            v[0] += wv * 0.5 * (hu * hu + hv * hv) / H;
+            v[1] += wv * ht;
+            v[2] += wv * (double)HS[t];
+            v[3] = fmax(v[3], sqrt(hu * hu + hv * hv) / H);
+            v[4] = fmax(v[4], ht / H);
+            v[5] = fmin(v[5], ht / H);
+        }
+    }
+    const int op[6] = {0, 0, 0, 1, 1, 2};
+    block_reduce<6>(v, op, red);
+    if (threadIdx.x == 0)
+        for (int q = 0; q < 6; ++q) part[blockIdx.x * 6 + q] = v[q];
 }
 
 template <int NP>
@@ -1955,8 +2019,10 @@ int drf_dg_diagnostics(drf_dg *m, double *out10) {
     return guard([&] {
         check_model(m);
         DRF_CHECK(out10, DRF_E_INVALID, "null output");
-        m->materialize();
-        const unsigned nb3 = blocks_for(m->n3), nb2 = blocks_for(m->n2);
+        int dev = 0, nsm = 0;
+        DRF_CUDA(cudaGetDevice(&dev));
+        DRF_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+        const unsigned nb3 = (unsigned)std::min<int64_t>(m->ncol, (int64_t)nsm * 8), nb2 = blocks_for(m->n2);
         if (m->diag.n < (size_t)nb3 * 6 + (size_t)nb2 * 5 + 10)
             m->diag.alloc((size_t)nb3 * 6 + (size_t)nb2 * 5 + 10);
         double *p3 = m->diag.p, *p2 = p3 + (size_t)nb3 * 6, *res10 = p2 + (size_t)nb2 * 5;
@@ -1966,8 +2032,9 @@ int drf_dg_diagnostics(drf_dg *m, double *out10) {
             constexpr int NP = decltype(npc)::value;
             const int c = m->cur;
             diag3d_kernel<T, NP><<<nb3, 256, 0, m->stream>>>(
-                m->n3, m->G.nz, (const T *)m->q(c, 0), (const T *)m->q(c, 1), (const T *)m->q(c, 2),
-                (const T *)m->q(c, 3), m->eta, m->h, 0.125 * dx * dy * m->G.dsig, p3);
+                m->ncol, m->G.nz, (const T *)m->q(c, 0), (const T *)m->q(c, 1), (const T *)m->q(c, 2),
+                (const T *)m->q(c, 3), m->eta, m->h, m->pending ? m->corrU : nullptr,
+                m->pending ? m->corrV : nullptr, 0.125 * dx * dy * m->G.dsig, p3);
             DRF_LAUNCHED();
             diag2d_kernel<NP><<<nb2, 256, 0, m->stream>>>(m->n2, m->G.nz, m->eta, m->h,
                                                          0.25 * dx * dy, m->G.g, p2);
@@ -1981,6 +2048,51 @@ int drf_dg_diagnostics(drf_dg *m, double *out10) {
         std::memcpy(out10, vals, sizeof(vals));
         for (int i = 0; i < 10; ++i)
             DRF_CHECK(std::isfinite(vals[i]), DRF_E_NONFINITE, "non-finite diagnostic (model blew up)");
+    });
+}
+
+int drf_dg_time_copy(drf_dg *m, int nrep, double *ms, double *bytes) {
+    return guard([&] {
+        check_model(m);
+        DRF_CHECK(nrep >= 1 && ms, DRF_E_INVALID, "bad arguments");
+        DRF_CHECK(((size_t)m->G.nz * m->np3 * m->tsz) % 16 == 0, DRF_E_UNSUPPORTED,
+                  "column blocks are not 16-byte multiples");
+        DRF_CHECK(m->smem >= 16 + (size_t)2 * m->np2 * 8 + (size_t)8 * m->G.nz * m->np3 * m->tsz,
+                  DRF_E_UNSUPPORTED, "shared memory plan too small for the copy");
+        m->materialize();
+        cudaEvent_t e0, e1;
+        DRF_CUDA(cudaEventCreate(&e0));
+        DRF_CUDA(cudaEventCreate(&e1));
+        m->with_types([&](auto tv, auto npc) {
+            using T = decltype(tv);
+            constexpr int NP = decltype(npc)::value;
+            // reads the current state and the register, writes the spare ping-pong buffer and
+            // the register back unchanged: the model state is not modified
+            const StageArgs<T> a = m->template stage_args<T>(m->cur, 1 - m->cur, 1, 0.0, 0, nullptr, nullptr,
+                                                             nullptr, m->eta, 0.0, false);
+            allow_max_dynamic_smem(reinterpret_cast<const void *>(dg3d_copy_kernel<T, NP>), [] {
+                int dev = 0, v = 0;
+                cudaGetDevice(&dev);
+                cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+                return v;
+            }());
+            dg3d_copy_kernel<T, NP><<<m->ncol, m->stage_threads(), m->smem, m->stream>>>(a);
+            DRF_LAUNCHED();
+            DRF_CUDA(cudaEventRecord(e0, m->stream));
+            for (int r = 0; r < nrep; ++r) {
+                dg3d_copy_kernel<T, NP><<<m->ncol, m->stage_threads(), m->smem, m->stream>>>(a);
+                DRF_LAUNCHED();
+            }
+            DRF_CUDA(cudaEventRecord(e1, m->stream));
+        });
+        DRF_CUDA(cudaEventSynchronize(e1));
+        float t = 0.f;
+        DRF_CUDA(cudaEventElapsedTime(&t, e0, e1));
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        *ms = (double)t / nrep;
+        if (bytes) *bytes = 16.0 * (double)m->n3 * m->tsz;
+        check_device_status(m);
     });
 }
 

@@ -233,6 +233,12 @@ class OceanModel:
         return dict(baro_cols_per_cta=cpb.value,
                     candidates_ms={str(c): round(float(t), 5) for c, t in zip((2, 4, 8, 16), ms)})
 
+    def time_copy(self, nrep: int = 20) -> dict:
+        """The stage kernel's access structure as a pure copy: time per launch and bytes."""
+        ms, b = C.c_double(), C.c_double()
+        check(lib().drf_dg_time_copy(self.handle, nrep, C.byref(ms), C.byref(b)))
+        return dict(ms=ms.value, bytes=b.value, gbs=b.value / (ms.value / 1e3) / 1e9)
+
     def time_stage(self, nrep: int = 20) -> dict:
         ms, ab, nd = C.c_double(), C.c_double(), C.c_double()
         check(lib().drf_dg_time_stage(self.handle, nrep, C.byref(ms), C.byref(ab), C.byref(nd)))

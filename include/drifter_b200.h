@@ -137,6 +137,13 @@ int drf_dg_diagnostics(drf_dg *m, double *out10);
  * stage moves by the algorithmic model (*alg_bytes) and the number of 3D DOFs (*ndof). */
 int drf_dg_time_stage(drf_dg *m, int nrep, double *ms, double *alg_bytes, double *ndof);
 
+/* Device time of the stage kernel's memory traffic alone: a copy kernel with the same CTA
+ * shape, shared memory and bulk-copy staging that reads the state and the LSRK register and
+ * writes 8 arrays back in the stage's store pattern (*bytes moved per launch). It is the
+ * bandwidth ceiling of the stage's access structure; the model state is not modified.
+ * No counterpart in the reference. */
+int drf_dg_time_copy(drf_dg *m, int nrep, double *ms, double *bytes);
+
 /* Replaces the surface stress fields (WindStress::compute, src/physics/primitive_equations.cpp:695)
  * for the following steps; asynchronous on the model's stream (pinned host memory recommended;
  * the caller keeps the buffers alive until the next drf_dg_sync). */

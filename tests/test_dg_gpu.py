@@ -227,3 +227,32 @@ def test_autotuned_barotropic_tile_matches_default_tile(monkeypatch):
     a, b = tuned.download_state(), fixed.download_state()
     for k in ("eta", "HU", "HV", "Hu", "HT"):
         assert relerr(a[k], b[k]) <= 1e-15, k
+
+
+def test_time_copy_leaves_the_state_unchanged():
+    case = _tidal_small("mixed", order=4, nx=6, ny=4, nz=4)
+    gpu = OceanModel(case["cfg"], case["h"], case["f"], case["taux"], case["tauy"])
+    gpu.upload_state(case["q"], case["eta"])
+    gpu.step(case["dt"], case["nsub"], 1)
+    before = gpu.download_state()
+    r = gpu.time_copy(3)
+    assert r["ms"] > 0 and r["bytes"] == 16 * 4 * case["cfg"].n3
+    after = gpu.download_state()
+    for k in ("Hu", "HT", "eta"):
+        assert np.array_equal(before[k], after[k]), k
+
+
+def test_diagnostics_with_pending_correction_equal_materialized():
+    """Diagnostics add a pending transport correction on the fly; downloading (which folds it
+    into the state) first must not change them."""
+    case = _tidal_small("mixed", order=3)
+    a = OceanModel(case["cfg"], case["h"], case["f"], case["taux"], case["tauy"])
+    b = OceanModel(case["cfg"], case["h"], case["f"], case["taux"], case["tauy"])
+    for m in (a, b):
+        m.upload_state(case["q"], case["eta"])
+        m.step(case["dt"], case["nsub"], 2)
+    da = a.diagnostics()
+    b.download_state()
+    db = b.diagnostics()
+    for k in da:
+        assert da[k] == db[k], k
