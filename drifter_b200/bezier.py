@@ -35,6 +35,7 @@ def _setup_sigs():
         "drf_bz_constraints_apply": [vp, C.c_int, dp, dp],
         "drf_bz_constrained_solve": [vp, C.c_int, C.c_int, C.c_double, C.c_int, C.c_double, dp,
                                      C.POINTER(C.c_int), dp, dp],
+        "drf_bz_element_errors": [vp, dp, dp, C.c_int, dp, dp],
     }
     for k, a in sigs.items():
         getattr(L, k).argtypes = a
@@ -103,6 +104,19 @@ class BezierSmoother:
         check(lib().drf_pcg_solve(self.h, dptr(bb) if bb is not None else None, dptr(x), tol,
                                   maxit, PRECOND[precond], C.byref(it), C.byref(rr), C.byref(ms)))
         return x, dict(iters=it.value, relres=rr.value, ms=ms.value)
+
+    def element_errors(self, x, zdata, ngauss=4):
+        """Per-element L2 misfit of the surface x to the data sampled at the ngauss x ngauss
+        Gauss points of every element (AdaptiveCGCubicBezierSmoother::compute_element_l2_error
+        and the normalized error of estimate_element_error): returns (l2, normalized)."""
+        xx = np.ascontiguousarray(x, dtype=np.float64)
+        zd = np.ascontiguousarray(zdata, dtype=np.float64)
+        ne = self.desc.nx * self.desc.ny
+        if zd.size != ne * ngauss * ngauss:
+            raise ValueError("zdata must hold ngauss^2 samples per element")
+        l2, nrm = np.empty(ne), np.empty(ne)
+        check(lib().drf_bz_element_errors(self.h, dptr(xx), dptr(zd), ngauss, dptr(l2), dptr(nrm)))
+        return l2, nrm
 
     def constraints_apply(self, x, edge_ngauss=4):
         """C1 edge-constraint rows A x (2 n (n - 1) edge_ngauss values, vertical edges first)."""

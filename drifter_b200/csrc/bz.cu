@@ -996,6 +996,56 @@ static __device__ __align__(256) double g_noalloc_scratch[NOALLOC_DOUBLES];
 
 using namespace drf;
 
+namespace drf {
+namespace {
+// AdaptiveCGCubicBezierSmoother::compute_element_l2_error
+// (src/bathymetry/adaptive_cg_cubic_bezier_smoother.cpp:100) for every element at once: one
+// warp per element evaluates the bicubic Bezier patch (Bernstein basis, the element's 16
+// control points, dof i + 4j) at the ng x ng Gauss-Legendre points of [0, 1]^2, squares the
+// misfit to the data sampled there, and reduces sqrt(sum w_i w_j diff^2 * dx dy).
+__global__ void __launch_bounds__(256) bz_elem_error_kernel(int nx, int ny, int ng, const double *__restrict__ x,
+                                                            const double *__restrict__ zd,
+                                                            const double *__restrict__ gq, double area,
+                                                            double *__restrict__ l2, double *__restrict__ nrm) {
+    const int64_t e = (int64_t)blockIdx.x * 8 + threadIdx.x / 32;
+    const int lane = threadIdx.x % 32;
+    if (e >= (int64_t)nx * ny) return;
+    const int ex = (int)(e % nx), ey = (int)(e / nx), stride = 3 * nx + 1;
+    double c[16];
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+        for (int i = 0; i < 4; ++i) c[i + 4 * j] = x[(size_t)(3 * ex + i) + (size_t)stride * (3 * ey + j)];
+    const int ng2 = ng * ng;
+    double acc = 0.0;
+    for (int q = lane; q < ng2; q += 32) {
+        const int qi = q % ng, qj = q / ng;
+        const double u = gq[qi], v = gq[qj], w = gq[ng + qi] * gq[ng + qj];
+        const double u1 = 1.0 - u, v1 = 1.0 - v;
+        const double bu[4] = {u1 * u1 * u1, 3.0 * u * u1 * u1, 3.0 * u * u * u1, u * u * u};
+        const double bv[4] = {v1 * v1 * v1, 3.0 * v * v1 * v1, 3.0 * v * v * v1, v * v * v};
+        double z = 0.0;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            double r = 0.0;
+#pragma unroll
+            for (int i = 0; i < 4; ++i) r += c[i + 4 * j] * bu[i];
+            z += r * bv[j];
+        }
+        const double diff = zd[e * ng2 + q] - z;
+        acc += w * diff * diff;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if (lane == 0) {
+        const double err = sqrt(acc * area);
+        l2[e] = err;
+        if (nrm) nrm[e] = err / sqrt(area);
+    }
+}
+}  // namespace
+}  // namespace drf
+
 struct drf_bz {
     BzSetup H;  // host-side setup (element matrices, levels, transfers)
     cudaStream_t stream = nullptr, own = nullptr;
@@ -1473,6 +1523,48 @@ int drf_bz_apply_Q(drf_bz *h, const double *xh, double *yh) {
         DRF_CUDA(cudaMemcpyAsync(h->z.p, xh, h->ndof * 8, cudaMemcpyHostToDevice, h->stream));
         h->apply(h->finest(), h->z.p, nullptr, h->q.p, 0, nullptr, nullptr);
         DRF_CUDA(cudaMemcpyAsync(yh, h->q.p, h->ndof * 8, cudaMemcpyDeviceToHost, h->stream));
+        DRF_CUDA(cudaStreamSynchronize(h->stream));
+    });
+}
+
+int drf_bz_element_errors(drf_bz *h, const double *xh, const double *zdata, int ngauss, double *l2,
+                          double *normalized) {
+    return guard([&] {
+        check_bz(h);
+        DRF_CHECK(xh && zdata && l2, DRF_E_INVALID, "null argument");
+        DRF_CHECK(ngauss >= 1 && ngauss <= 16, DRF_E_INVALID, "ngauss must be 1..16");
+        const drf_bz_grid_desc &g = h->H.g;
+        const int64_t ne = (int64_t)g.nx * g.ny, npt = ne * ngauss * ngauss;
+        DRF_CHECK(all_finite(zdata, (size_t)npt), DRF_E_NONFINITE, "non-finite data");
+        // Gauss-Legendre nodes and weights on [0, 1] (Newton on the Legendre recurrence)
+        std::vector<double> gq(2 * ngauss);
+        for (int i = 0; i < ngauss; ++i) {
+            double z = std::cos(M_PI * (i + 0.75) / (ngauss + 0.5)), dp = 1.0;
+            for (int it = 0; it < 100; ++it) {
+                double p0 = 1.0, p1 = z;
+                for (int k = 2; k <= ngauss; ++k) {
+                    const double p2 = ((2.0 * k - 1.0) * z * p1 - (k - 1.0) * p0) / k;
+                    p0 = p1;
+                    p1 = p2;
+                }
+                if (ngauss == 1) { p1 = z; p0 = 1.0; }
+                dp = ngauss * (z * p1 - p0) / (z * z - 1.0);
+                const double dz = p1 / dp;
+                z -= dz;
+                if (std::abs(dz) < 1e-16) break;
+            }
+            gq[ngauss - 1 - i] = 0.5 * (z + 1.0);
+            gq[ngauss + ngauss - 1 - i] = 1.0 / ((1.0 - z * z) * dp * dp);
+        }
+        DevBuf<double> dz((size_t)npt), dgq(gq.size()), dl2(ne), dnrm(normalized ? ne : 1);
+        DRF_CUDA(cudaMemcpyAsync(h->z.p, xh, h->ndof * 8, cudaMemcpyHostToDevice, h->stream));
+        DRF_CUDA(cudaMemcpyAsync(dz.p, zdata, npt * 8, cudaMemcpyHostToDevice, h->stream));
+        DRF_CUDA(cudaMemcpyAsync(dgq.p, gq.data(), gq.size() * 8, cudaMemcpyHostToDevice, h->stream));
+        bz_elem_error_kernel<<<(unsigned)((ne + 7) / 8), 256, 0, h->stream>>>(
+            g.nx, g.ny, ngauss, h->z.p, dz.p, dgq.p, h->H.dx * h->H.dy, dl2.p, normalized ? dnrm.p : nullptr);
+        DRF_LAUNCHED();
+        DRF_CUDA(cudaMemcpyAsync(l2, dl2.p, ne * 8, cudaMemcpyDeviceToHost, h->stream));
+        if (normalized) DRF_CUDA(cudaMemcpyAsync(normalized, dnrm.p, ne * 8, cudaMemcpyDeviceToHost, h->stream));
         DRF_CUDA(cudaStreamSynchronize(h->stream));
     });
 }

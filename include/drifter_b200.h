@@ -209,6 +209,15 @@ int drf_bz_info(drf_bz *h, int64_t *ndof, double *alpha, int *nlevels);
 int drf_bz_get_rhs(drf_bz *h, double *b);
 /* y = Q x, matrix-free (the SpMV L.Q * x of src/bathymetry/bezier_multigrid_preconditioner.cpp:776). */
 int drf_bz_apply_Q(drf_bz *h, const double *x, double *y);
+/* Per-element L2 misfit of the smoothed surface x (control points) to the data, for every
+ * element: AdaptiveCGCubicBezierSmoother::compute_element_l2_error / estimate_element_error
+ * (src/bathymetry/adaptive_cg_cubic_bezier_smoother.cpp:100,142), the error estimate of the
+ * adaptive smoother's refinement loop. zdata holds the data sampled at the ngauss x ngauss
+ * Gauss-Legendre points of each element ([ey][ex][qj][qi], points on [0,1]^2, the reference's
+ * ngauss_error, default 4). l2[e] = sqrt(sum_q w_q (z_data - z_bezier)^2 * dx dy);
+ * normalized[e] = l2[e] / sqrt(dx dy) (may be NULL). */
+int drf_bz_element_errors(drf_bz *h, const double *x, const double *zdata, int ngauss, double *l2,
+                          double *normalized);
 /* BezierMultigridPreconditioner::setup (include/bathymetry/bezier_multigrid_preconditioner.hpp:240):
  * levels down to coarsest_n elements per direction, pre/post colored-Schwarz sweeps. */
 int drf_mg_setup(drf_bz *h, int coarsest_n, int pre, int post);

@@ -1,5 +1,6 @@
 // ORACLE — test infrastructure only. Cubic Bezier smoother restatement (see bz_oracle.hpp).
 #include "bz_oracle.hpp"
+#include "oracle.hpp"
 
 #include <algorithm>
 #include <cmath>
@@ -558,3 +559,56 @@ int bz_pcg(const BzSystem &S, const BzMG *M, int precond, const double *b, doubl
 }
 
 }  // namespace orc
+
+// AdaptiveCGCubicBezierSmoother::compute_element_l2_error
+// (src/bathymetry/adaptive_cg_cubic_bezier_smoother.cpp:100-138) and the normalized error of
+// estimate_element_error (:142-150) for every element of a uniform nx x ny grid: the Gauss
+// point (u, v) on [0, 1]^2 is mapped to x = xmin + u dx and evaluated through
+// CGBezierSmootherBase::evaluate_in_element (src/bathymetry/cg_bezier_smoother_base.cpp:166:
+// u = (x - xmin) / dx, clamped), with the cubic Bernstein basis and the element's control
+// points (dof i + 4j). zdata: [ey][ex][qj][qi]. Returns 0, -1 on bad arguments.
+extern "C" int orc_bz_element_errors(int nx, int ny, double x0, double y0, double Lx, double Ly, int ng,
+                                     const double *x, const double *zdata, double *l2, double *nrm) {
+    if (nx < 1 || ny < 1 || ng < 1) return -1;
+    orc::Vec gx, gw;
+    orc::gauss_legendre(ng, gx, gw);
+    std::vector<double> gn(ng), gwt(ng);
+    for (int i = 0; i < ng; ++i) {
+        gn[i] = 0.5 * (gx[i] + 1.0);
+        gwt[i] = 0.5 * gw[i];
+    }
+    const double dx = Lx / nx, dy = Ly / ny;
+    const long stride = 3L * nx + 1;
+    auto bern = [](double t, double b[4]) {
+        const double s = 1.0 - t;
+        b[0] = s * s * s; b[1] = 3.0 * t * s * s; b[2] = 3.0 * t * t * s; b[3] = t * t * t;
+    };
+    for (int ey = 0; ey < ny; ++ey)
+        for (int ex = 0; ex < nx; ++ex) {
+            const double xmin = x0 + ex * dx, ymin = y0 + ey * dy;
+            double c[16];
+            for (int j = 0; j < 4; ++j)
+                for (int i = 0; i < 4; ++i) c[i + 4 * j] = x[(3L * ex + i) + stride * (3L * ey + j)];
+            double err2 = 0.0;
+            for (int j = 0; j < ng; ++j)
+                for (int i = 0; i < ng; ++i) {
+                    const double px = xmin + gn[i] * dx, py = ymin + gn[j] * dy;
+                    double u = (px - xmin) / dx, v = (py - ymin) / dy;
+                    u = u < 0.0 ? 0.0 : (u > 1.0 ? 1.0 : u);
+                    v = v < 0.0 ? 0.0 : (v > 1.0 ? 1.0 : v);
+                    double bu[4], bv[4];
+                    bern(u, bu);
+                    bern(v, bv);
+                    double z = 0.0;
+                    for (int b = 0; b < 4; ++b)
+                        for (int a = 0; a < 4; ++a) z += c[a + 4 * b] * bu[a] * bv[b];
+                    const long e = (long)ey * nx + ex;
+                    const double diff = zdata[(e * ng + j) * ng + i] - z;
+                    err2 += gwt[i] * gwt[j] * diff * diff;
+                }
+            const long e = (long)ey * nx + ex;
+            l2[e] = std::sqrt(err2 * dx * dy);
+            if (nrm) nrm[e] = l2[e] / std::sqrt(dx * dy);
+        }
+    return 0;
+}

@@ -402,3 +402,16 @@ def amr_lsrk(order, mesh, mode, flux_kind, a, U, dt, nsteps):
             res = LSRK_A[s] * res + dt * (-r)
             u = u + LSRK_B[s] * res
     return u
+
+
+def bz_element_errors(nx, ny, Lx, Ly, ngauss, x, zdata, x0=0.0, y0=0.0):
+    """Per-element L2 misfit and normalized error of the adaptive smoother's estimate
+    (AdaptiveCGCubicBezierSmoother::compute_element_l2_error)."""
+    L = lib()
+    L.orc_bz_element_errors.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
+                                        C.c_int, _dp, _dp, _dp, _dp]
+    l2, nrm = np.empty(nx * ny), np.empty(nx * ny)
+    r = L.orc_bz_element_errors(nx, ny, x0, y0, Lx, Ly, ngauss, _p(_c(x)), _p(_c(zdata)), _p(l2), _p(nrm))
+    if r < 0:
+        raise ValueError("oracle: bad element-error arguments")
+    return l2, nrm

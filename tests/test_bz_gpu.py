@@ -5,6 +5,7 @@ import numpy as np
 import pytest
 
 import pyoracle as O
+from drifter_b200 import configs
 from drifter_b200.bezier import BezierMultigridPreconditioner, BezierSmoother
 
 pytestmark = pytest.mark.gpu
@@ -123,3 +124,34 @@ def test_constrained_solve_doc_known_answer(inner):
     assert abs(np.linalg.norm(x) - k["x_norm"]) < 6e-4
     assert abs(dat - k["data_residual"]) < 6e-5
     assert np.abs(A @ x).max() < 1e-7
+
+
+@pytest.mark.parametrize("ng", [3, 4, 5])
+def test_element_errors_match_oracle(ng):
+    """AdaptiveCGCubicBezierSmoother::compute_element_l2_error for every element on the GPU
+    against the oracle, for the smoothed surface of a 16 x 16 grid."""
+    c = configs.c4(n=16, L=1600.0)
+    s = BezierSmoother(16, 16, c["L"], c["L"], c["d"], lam=c["lam"], ridge_epsilon=c["eps"])
+    s.mg_setup(2)
+    x, _ = s.solve("mg", tol=1e-10)
+    rng = np.random.default_rng(ng)
+    z = rng.uniform(0, 4000, 16 * 16 * ng * ng)
+    l2, nrm = s.element_errors(x, z, ngauss=ng)
+    r2, rn = O.bz_element_errors(16, 16, c["L"], c["L"], ng, x, z)
+    assert np.abs(l2 - r2).max() <= 1e-12 * np.abs(r2).max()
+    assert np.abs(nrm - rn).max() <= 1e-12 * np.abs(rn).max()
+    s.close()
+
+
+def test_element_errors_c4_full_size():
+    """C4 (512 x 512): the misfit of the MG-PCG solution to the data at the 4 x 4 Gauss points,
+    GPU against the oracle."""
+    c = configs.c4()
+    s = BezierSmoother(c["n"], c["n"], c["L"], c["L"], c["d"], lam=c["lam"], ridge_epsilon=c["eps"])
+    s.mg_setup(2)
+    x, inf = s.solve("mg", tol=1e-10)
+    l2, nrm = s.element_errors(x, c["d"], ngauss=4)
+    r2, rn = O.bz_element_errors(c["n"], c["n"], c["L"], c["L"], 4, x, c["d"])
+    assert np.abs(l2 - r2).max() <= 1e-12 * np.abs(r2).max()
+    assert l2.max() > 0
+    s.close()

@@ -142,3 +142,31 @@ def test_mg_pcg_matches_direct():
     assert np.abs(x - xd).max() / np.abs(xd).max() < 1e-8
     x2, it2, rr2 = B.pcg(precond="jacobi", tol=1e-10, maxit=20000)
     assert it2 > 3 * it  # multigrid is a much stronger preconditioner
+
+
+def _bezier_samples(nx, ny, Lx, Ly, x, ng):
+    """The surface of control points x sampled at the ng x ng Gauss points of every element."""
+    gx, _ = np.polynomial.legendre.leggauss(ng)
+    t = 0.5 * (gx + 1.0)
+    B = np.stack([(1 - t) ** 3, 3 * t * (1 - t) ** 2, 3 * t * t * (1 - t), t ** 3], 1)  # [q][a]
+    X = x.reshape(3 * ny + 1, 3 * nx + 1)
+    out = np.empty((ny, nx, ng, ng))
+    for ey in range(ny):
+        for ex in range(nx):
+            C = X[3 * ey:3 * ey + 4, 3 * ex:3 * ex + 4]  # [j][i]
+            out[ey, ex] = B @ C @ B.T  # [qj][qi]
+    return out.ravel()
+
+
+@pytest.mark.parametrize("ng", [2, 4, 5])
+def test_element_error_estimate_pins(ng):
+    """compute_element_l2_error: zero for data on the surface; a constant offset d gives
+    |d| sqrt(area) (normalized |d|), since the Gauss weights on [0,1]^2 sum to 1."""
+    nx, ny, Lx, Ly = 6, 5, 3.0, 2.5
+    x = np.random.default_rng(ng).standard_normal((3 * nx + 1) * (3 * ny + 1))
+    z = _bezier_samples(nx, ny, Lx, Ly, x, ng)
+    l2, nrm = O.bz_element_errors(nx, ny, Lx, Ly, ng, x, z)
+    assert np.abs(l2).max() < 1e-12
+    l2, nrm = O.bz_element_errors(nx, ny, Lx, Ly, ng, x, z + 0.25)
+    area = (Lx / nx) * (Ly / ny)
+    assert np.allclose(l2, 0.25 * np.sqrt(area), rtol=1e-12) and np.allclose(nrm, 0.25, rtol=1e-12)
