@@ -7,6 +7,7 @@
 //
 // Channels (padded for the MMA shapes): 16 (9 used) -> 32 -> 32 -> 32 -> 16 (9 used); ReLU
 // after layers 1-3. Layouts: activations NHWC [b][h][w][c]; weights [co][tap][ci] (tap = dy*3+dx).
+#include <algorithm>
 #include <cuda_bf16.h>
 
 #include <cmath>
@@ -34,83 +35,137 @@ __device__ __forceinline__ void mma_bf16(float c[4], uint32_t a0, uint32_t a1, u
         : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
 }
 
+// 16-byte asynchronous global -> shared copy; src_bytes = 0 writes zeros
+__device__ __forceinline__ void cp_async16(void *dst, const void *src, int src_bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
+                 "l"(src), "r"(src_bytes)
+                 : "memory");
+}
+
+// four 8x8 bf16 matrices from shared memory, one row address per lane
+__device__ __forceinline__ void ldsm_x4(const bf16 *p, uint32_t &r0, uint32_t &r1, uint32_t &r2, uint32_t &r3) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];"
+                 : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
+                 : "r"((uint32_t)__cvta_generic_to_shared(p)));
+}
+
 // Y = conv3x3(X, W) (+ bias) (+ ReLU); X, W bf16; Y bf16 (OUTF32 = false) or f32.
+// Persistent over tiles of TH x TW pixels: a CTA stages the layer's weights once, then walks
+// tiles (b, ty, tx) = blockIdx.x, blockIdx.x + gridDim.x, ... staging each tile's input halo.
 // Shared memory: input halo (TH+2) x (TW+2) pixels with pixel stride CIN+8, and the weights
 // with output-channel stride 9*CIN+8 (both paddings remove shared-memory bank conflicts of
 // the fragment loads).
+// conv tiles: TH rows x CTW pixels, one warp per row computing two 16-pixel MMA tiles (the B
+// fragments of the weights are shared by both)
+constexpr int CTW = 32;
+template <int CIN, int COUT>
+constexpr size_t conv_smem_bytes() {
+    return (size_t)2 * (TH + 2) * (CTW + 2) * (CIN + 8) * 2 + (size_t)COUT * (9 * CIN + 8) * 2;
+}
+
 template <int CIN, int COUT, bool RELU, bool OUTF32>
-__global__ void __launch_bounds__(256) conv3x3_kernel(int H, int W, const bf16 *__restrict__ X,
+__global__ void __launch_bounds__(256) conv3x3_kernel(int B, int H, int W, const bf16 *__restrict__ X,
                                                       const bf16 *__restrict__ Wt,
                                                       const float *__restrict__ bias, void *Yv) {
-    constexpr int PS = CIN + 8, WS = 9 * CIN + 8, HP = TH + 2, WP = TW + 2;
-    __shared__ __align__(16) bf16 Xs[HP * WP * PS];
-    __shared__ __align__(16) bf16 Ws[COUT * WS];
-    const int b = blockIdx.z;
-    const int h0 = blockIdx.y * TH, w0 = blockIdx.x * TW;
-    const bf16 *Xb = X + (size_t)b * H * W * CIN;
-    // stage weights (32-bit copies)
-    for (int i = threadIdx.x; i < COUT * 9 * CIN / 2; i += blockDim.x) {
-        const int e = 2 * i, co = e / (9 * CIN), r = e % (9 * CIN);
-        *reinterpret_cast<uint32_t *>(&Ws[co * WS + r]) = reinterpret_cast<const uint32_t *>(Wt)[i];
+    constexpr int PS = CIN + 8, WS = 9 * CIN + 8, HP = TH + 2, WP = CTW + 2, C8 = CIN / 8;
+    extern __shared__ __align__(16) unsigned char conv_smem[];
+    bf16 *Xs0 = reinterpret_cast<bf16 *>(conv_smem);  // double-buffered input halo
+    bf16 *Ws = Xs0 + 2 * HP * WP * PS;
+    const int ntx = (W + CTW - 1) / CTW, nty = (H + TH - 1) / TH;
+    const int64_t ntiles = (int64_t)ntx * nty * B;
+    // asynchronous 16-byte copies of the tile's halo into buffer `buf` (zeros outside the image)
+    auto stage_halo = [&](int64_t tile, int buf) {
+        const int b = (int)(tile / ((int64_t)ntx * nty)), r2 = (int)(tile % ((int64_t)ntx * nty));
+        const int h0 = (r2 / ntx) * TH, w0 = (r2 % ntx) * CTW;
+        const bf16 *Xb = X + (size_t)b * H * W * CIN;
+        bf16 *Xs = Xs0 + buf * HP * WP * PS;
+        for (int i = threadIdx.x; i < HP * WP * C8; i += blockDim.x) {
+            const int pix = i / C8, c8 = i % C8;
+            const int hh = h0 - 1 + pix / WP, ww = w0 - 1 + pix % WP;
+            const bool in = hh >= 0 && hh < H && ww >= 0 && ww < W;
+            cp_async16(&Xs[pix * PS + 8 * c8], in ? Xb + ((size_t)hh * W + ww) * CIN + 8 * c8 : Xb, in ? 16 : 0);
+        }
+    };
+    // the layer's weights, once per CTA, together with the first tile's halo
+    for (int i = threadIdx.x; i < COUT * 9 * C8; i += blockDim.x) {
+        const int co = i / (9 * C8), c8 = i % (9 * C8);
+        cp_async16(&Ws[co * WS + 8 * c8], Wt + (size_t)co * 9 * CIN + 8 * c8, 16);
     }
-    // stage the input halo, zero outside the image
-    for (int i = threadIdx.x; i < HP * WP * (CIN / 2); i += blockDim.x) {
-        const int pix = i / (CIN / 2), cp = i % (CIN / 2);
-        const int hh = h0 - 1 + pix / WP, ww = w0 - 1 + pix % WP;
-        uint32_t v = 0u;
-        if (hh >= 0 && hh < H && ww >= 0 && ww < W)
-            v = reinterpret_cast<const uint32_t *>(Xb + ((size_t)hh * W + ww) * CIN)[cp];
-        *reinterpret_cast<uint32_t *>(&Xs[pix * PS + 2 * cp]) = v;
-    }
-    __syncthreads();
+    if (blockIdx.x < ntiles) stage_halo(blockIdx.x, 0);
+    asm volatile("cp.async.commit_group;" ::: "memory");
     const int warp = threadIdx.x / 32, lane = threadIdx.x % 32, g = lane >> 2, t = lane & 3;
-    const int h = h0 + warp;
-    float acc[COUT / 8][4];
+    // fragments by ldmatrix.x4: lane l addresses row (l % 8) + 8 ((l / 8) % 2) of the A tile
+    // (pixels of the strip) at channel offset 8 (l / 16), and output channel
+    // 8 (j + l / 16) + l % 8 of the B tile at k offset 8 ((l / 8) % 2)
+    const int arow = (lane & 7) + 8 * ((lane >> 3) & 1), acol = 8 * (lane >> 4);
+    const int brow = (lane & 7) + 8 * (lane >> 4), bcol = 8 * ((lane >> 3) & 1);
+    int buf = 0;
+    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, buf ^= 1) {
+        const int b = (int)(tile / ((int64_t)ntx * nty)), r2 = (int)(tile % ((int64_t)ntx * nty));
+        const int h0 = (r2 / ntx) * TH, w0 = (r2 % ntx) * CTW;
+        // prefetch the next tile's halo into the other buffer (last read in the previous
+        // iteration, behind its closing barrier)
+        if (tile + gridDim.x < ntiles) stage_halo(tile + gridDim.x, buf ^ 1);
+        asm volatile("cp.async.commit_group;" ::: "memory");
+        asm volatile("cp.async.wait_group 1;" ::: "memory");  // all but the newest group
+        __syncthreads();
+        const bf16 *Xs = Xs0 + buf * HP * WP * PS;
+        const int h = h0 + warp;
+        float acc[2][COUT / 8][4];
 #pragma unroll
-    for (int j = 0; j < COUT / 8; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.f;
+        for (int mt = 0; mt < 2; ++mt)
 #pragma unroll
-    for (int tap = 0; tap < 9; ++tap) {
-        const int dy = tap / 3, dx = tap % 3;
-        // pixel m of the strip reads halo pixel (warp + dy, m + dx)
-        const bf16 *xr0 = &Xs[((warp + dy) * WP + (g + dx)) * PS];
-        const bf16 *xr1 = &Xs[((warp + dy) * WP + (g + 8 + dx)) * PS];
+            for (int j = 0; j < COUT / 8; ++j) acc[mt][j][0] = acc[mt][j][1] = acc[mt][j][2] = acc[mt][j][3] = 0.f;
 #pragma unroll
-        for (int kc = 0; kc < CIN; kc += 16) {
-            const uint32_t a0 = *reinterpret_cast<const uint32_t *>(xr0 + kc + 2 * t);
-            const uint32_t a1 = *reinterpret_cast<const uint32_t *>(xr1 + kc + 2 * t);
-            const uint32_t a2 = *reinterpret_cast<const uint32_t *>(xr0 + kc + 2 * t + 8);
-            const uint32_t a3 = *reinterpret_cast<const uint32_t *>(xr1 + kc + 2 * t + 8);
+        for (int tap = 0; tap < 9; ++tap) {
+            const int dy = tap / 3, dx = tap % 3;
+            // pixel m of the strip reads halo pixel (warp + dy, m + dx)
+            const bf16 *xa = &Xs[((warp + dy) * WP + (arow + dx)) * PS + acol];
+#pragma unroll
+            for (int kc = 0; kc < CIN; kc += 16) {
+                uint32_t a[2][4];
+                ldsm_x4(xa + kc, a[0][0], a[0][1], a[0][2], a[0][3]);
+                ldsm_x4(xa + 16 * PS + kc, a[1][0], a[1][1], a[1][2], a[1][3]);
+#pragma unroll
+                for (int j = 0; j < COUT / 8; j += 2) {
+                    uint32_t b0, b1, b2, b3;
+                    ldsm_x4(&Ws[(8 * j + brow) * WS + tap * CIN + kc + bcol], b0, b1, b2, b3);
+#pragma unroll
+                    for (int mt = 0; mt < 2; ++mt) {
+                        mma_bf16(acc[mt][j], a[mt][0], a[mt][1], a[mt][2], a[mt][3], b0, b1);
+                        mma_bf16(acc[mt][j + 1], a[mt][0], a[mt][1], a[mt][2], a[mt][3], b2, b3);
+                    }
+                }
+            }
+        }
+        if (h < H) {
 #pragma unroll
             for (int j = 0; j < COUT / 8; ++j) {
-                const bf16 *wr = &Ws[(8 * j + g) * WS + tap * CIN + kc];
-                const uint32_t b0 = *reinterpret_cast<const uint32_t *>(wr + 2 * t);
-                const uint32_t b1 = *reinterpret_cast<const uint32_t *>(wr + 2 * t + 8);
-                mma_bf16(acc[j], a0, a1, a2, a3, b0, b1);
+                const int co = 8 * j + 2 * t;
+                const float b0 = bias ? bias[co] : 0.f, b1 = bias ? bias[co + 1] : 0.f;
+#pragma unroll
+                for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+                    for (int half = 0; half < 2; ++half) {
+                        const int w = w0 + 16 * mt + g + 8 * half;
+                        if (w >= W) continue;
+                        float v0 = acc[mt][j][2 * half] + b0, v1 = acc[mt][j][2 * half + 1] + b1;
+                        if (RELU) { v0 = fmaxf(v0, 0.f); v1 = fmaxf(v1, 0.f); }
+                        const size_t o = (((size_t)b * H + h) * W + w) * COUT + co;
+                        if (OUTF32) {
+                            float *Y = static_cast<float *>(Yv);
+                            Y[o] = v0;
+                            Y[o + 1] = v1;
+                        } else {
+                            bf16 *Y = static_cast<bf16 *>(Yv);
+                            *reinterpret_cast<__nv_bfloat162 *>(&Y[o]) = __floats2bfloat162_rn(v0, v1);
+                        }
+                    }
             }
         }
+        __syncthreads();  // every warp is done with this buffer before it is refilled
     }
-    if (h >= H) return;
-#pragma unroll
-    for (int j = 0; j < COUT / 8; ++j) {
-        const int co = 8 * j + 2 * t;
-        const float b0 = bias ? bias[co] : 0.f, b1 = bias ? bias[co + 1] : 0.f;
-#pragma unroll
-        for (int half = 0; half < 2; ++half) {
-            const int w = w0 + g + 8 * half;
-            if (w >= W) continue;
-            float v0 = acc[j][2 * half] + b0, v1 = acc[j][2 * half + 1] + b1;
-            if (RELU) { v0 = fmaxf(v0, 0.f); v1 = fmaxf(v1, 0.f); }
-            const size_t o = (((size_t)b * H + h) * W + w) * COUT + co;
-            if (OUTF32) {
-                float *Y = static_cast<float *>(Yv);
-                Y[o] = v0;
-                Y[o + 1] = v1;
-            } else {
-                bf16 *Y = static_cast<bf16 *>(Yv);
-                *reinterpret_cast<__nv_bfloat162 *>(&Y[o]) = __floats2bfloat162_rn(v0, v1);
-            }
-        }
-    }
+    asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
 // dW partials of one layer for one CTA tile: dW[co][tap][ci] += dZ[p][co] * A[p + shift][ci],
@@ -239,37 +294,58 @@ __global__ void crop_kernel(int B, int ch, int cw, int H, int W, const int *sel,
 
 // superpixel packing of a control-point field (nd x nd, nd = 3n + 1) scaled by 1/rms
 __global__ void pack_kernel(int n, const double *r, const double *rr_ptr, double inv_len, bf16 *X) {
+    // one thread per superpixel (I, J): its 9 control points 3I..3I+2 x 3J..3J+2 (three runs of
+    // three consecutive values) become channels 0..8, channels 9..15 are zero; one 32-byte store
     const int S = n + 1, nd = 3 * n + 1;
-    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i >= (int64_t)S * S * 16) return;
-    const int c = (int)(i % 16);
-    const int64_t p = i / 16;
-    const int I = (int)(p % S), J = (int)(p / S);
-    float v = 0.f;
-    if (c < 9) {
-        const int gi = 3 * I + c % 3, gj = 3 * J + c / 3;
-        if (gi < nd && gj < nd) {
-            const double rr = *rr_ptr;
-            const double sc = rr > 0 ? 1.0 / sqrt(rr * inv_len) : 0.0;
-            v = (float)(r[gi + (int64_t)nd * gj] * sc);
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= S * S) return;
+    const int I = p % S, J = p / S;
+    const double rr = *rr_ptr;
+    const double sc = rr > 0 ? 1.0 / sqrt(rr * inv_len) : 0.0;
+    __align__(16) bf16 v[16];
+#pragma unroll
+    for (int c = 0; c < 16; ++c) v[c] = __float2bfloat16_rn(0.f);
+#pragma unroll
+    for (int b = 0; b < 3; ++b) {
+        const int gj = 3 * J + b;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const int gi = 3 * I + a;
+            if (gi < nd && gj < nd) v[a + 3 * b] = __float2bfloat16_rn((float)(r[gi + (int64_t)nd * gj] * sc));
         }
     }
-    X[i] = __float2bfloat16_rn(v);
+    uint4 *dst = reinterpret_cast<uint4 *>(X + (size_t)p * 16);
+    dst[0] = reinterpret_cast<const uint4 *>(v)[0];
+    dst[1] = reinterpret_cast<const uint4 *>(v)[1];
 }
 
-// z (+)= rms(r) out_scale Y on the control points (add = 1 adds to a base already in z)
+// z (+)= rms(r) out_scale Y on the control points (add = 1 adds to a base already in z); one
+// thread per superpixel writes its (up to) 9 control points
 __global__ void unpack_kernel(int n, const float *Y, const double *rr_ptr, double inv_len,
                               double out_scale, double *z, int add, const int *stop) {
     if (stop && *stop) return;
     const int S = n + 1, nd = 3 * n + 1;
-    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (t >= (int64_t)nd * nd) return;
-    const int gi = (int)(t % nd), gj = (int)(t / nd);
-    const int I = gi / 3, J = gj / 3, c = (gi % 3) + 3 * (gj % 3);
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= S * S) return;
+    const int I = p % S, J = p / S;
     const double rr = *rr_ptr;
     const double sc = sqrt(rr * inv_len);
-    const double v = (double)Y[((int64_t)J * S + I) * 16 + c] * sc * out_scale;
-    z[t] = add ? z[t] + v : v;
+    const float4 *src = reinterpret_cast<const float4 *>(Y + (size_t)p * 16);
+    const float4 y0 = src[0], y1 = src[1], y2 = src[2];
+    const float y[9] = {y0.x, y0.y, y0.z, y0.w, y1.x, y1.y, y1.z, y1.w, y2.x};
+#pragma unroll
+    for (int b = 0; b < 3; ++b) {
+        const int gj = 3 * J + b;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const int gi = 3 * I + a;
+            if (gi < nd && gj < nd) {
+                const size_t t = gi + (size_t)nd * gj;
+                const double v = (double)y[a + 3 * b] * sc * out_scale;
+                z[t] = add ? z[t] + v : v;
+            }
+        }
+    }
 }
 
 inline unsigned nb(int64_t n, int bs = 256) { return (unsigned)((n + bs - 1) / bs); }
@@ -277,8 +353,21 @@ inline unsigned nb(int64_t n, int bs = 256) { return (unsigned)((n + bs - 1) / b
 template <int CIN, int COUT, bool RELU, bool OUTF32>
 void conv(cudaStream_t s, int B, int H, int W, const bf16 *X, const bf16 *Wt, const float *bias,
           void *Y) {
-    dim3 grid((W + TW - 1) / TW, (H + TH - 1) / TH, B);
-    conv3x3_kernel<CIN, COUT, RELU, OUTF32><<<grid, 256, 0, s>>>(H, W, X, Wt, bias, Y);
+    // persistent grid: as many CTAs as are resident at once (the weights are staged once each)
+    constexpr size_t smem = conv_smem_bytes<CIN, COUT>();
+    static int resident = 0;
+    if (!resident) {
+        int dev = 0, nsm = 0, per = 0;
+        DRF_CUDA(cudaGetDevice(&dev));
+        DRF_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+        DRF_CUDA(cudaFuncSetAttribute(conv3x3_kernel<CIN, COUT, RELU, OUTF32>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        DRF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, conv3x3_kernel<CIN, COUT, RELU, OUTF32>, 256, smem));
+        resident = nsm * (per > 0 ? per : 1);
+    }
+    const int64_t ntiles = (int64_t)((W + CTW - 1) / CTW) * ((H + TH - 1) / TH) * B;
+    const unsigned grid = (unsigned)std::min<int64_t>(ntiles, resident);
+    conv3x3_kernel<CIN, COUT, RELU, OUTF32><<<grid, 256, smem, s>>>(B, H, W, X, Wt, bias, Y);
     DRF_LAUNCHED();
 }
 
@@ -421,10 +510,10 @@ void cnn_precondition(CnnNet *net, cudaStream_t s, int n, const double *r, const
     cudaStream_t keep = net->stream;
     net->stream = s;
     net->ensure(pix);
-    pack_kernel<<<nb(pix * 16), 256, 0, s>>>(n, r, rr_dev, 1.0 / (double)(nd * nd), net->act[0].p);
+    pack_kernel<<<nb(pix), 256, 0, s>>>(n, r, rr_dev, 1.0 / (double)(nd * nd), net->act[0].p);
     DRF_LAUNCHED();
     net->forward(1, S, S);
-    unpack_kernel<<<nb(nd * nd), 256, 0, s>>>(n, net->out.p, rr_dev, 1.0 / (double)(nd * nd), out_scale,
+    unpack_kernel<<<nb(pix), 256, 0, s>>>(n, net->out.p, rr_dev, 1.0 / (double)(nd * nd), out_scale,
                                               z, add, stop);
     DRF_LAUNCHED();
     net->stream = keep;
