@@ -857,6 +857,31 @@ __global__ void __launch_bounds__(BS) jacobi_kernel(LevelDev L, const double *r,
     z[t] = r[t] / d;
 }
 
+// the finest level's diagonal of Q (as jacobi_kernel forms it), stored once per handle
+__global__ void __launch_bounds__(BS) diag_kernel(LevelDev L, double *d) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= (int64_t)L.nd * L.nd) return;
+    const int gi = (int)(t % L.nd), gj = (int)(t / L.nd);
+    double v = ridge(L, gi, gj);
+    const int ex1 = min(gi / 3, L.n - 1), ey1 = min(gj / 3, L.n - 1);
+    const int ex0 = (gi % 3 == 0 && gi > 0) ? gi / 3 - 1 : ex1;
+    const int ey0 = (gj % 3 == 0 && gj > 0) ? gj / 3 - 1 : ey1;
+    for (int ey = ey0; ey <= ey1; ++ey)
+        for (int ex = ex0; ex <= ex1; ++ex) {
+            const int a = (gi - 3 * ex) + 4 * (gj - 3 * ey);
+            v += L.K[a * 16 + a];
+        }
+    d[t] = v;
+}
+
+// z = r / d with the stored diagonal (the same division as jacobi_kernel)
+__global__ void __launch_bounds__(BS) jacobi_diag_kernel(int64_t n, const double *d, const double *r, double *z,
+                                                         const int *stop) {
+    if (stop && *stop) return;
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t < n) z[t] = r[t] / d[t];
+}
+
 __global__ void copy_kernel(int64_t n, const double *a, double *b, const int *stop) {
     if (stop && *stop) return;
     const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -1051,6 +1076,7 @@ struct drf_bz {
     cudaStream_t stream = nullptr, own = nullptr;
     int64_t ndof = 0;
     DevBuf<double> dat, Bq, b, bs, x, r, z, p, q, scal, part, mgbuf, coarse;  // b: assembled rhs, bs: rhs of the current solve
+    DevBuf<double> diag;  // finest diagonal of Q for the Jacobi steps (formed at first use)
     DevBuf<int> ctl;
     struct Lv {
         DevBuf<double> K, rho, binv, x, b, r;
@@ -1079,6 +1105,12 @@ struct drf_bz {
         return L;
     }
     int finest() const { return (int)lv.size() - 1; }
+    // the finest diagonal of Q, formed once per operator (outside any graph capture)
+    void form_diag() {
+        if (diag.n < (size_t)ndof) diag.alloc(ndof);
+        diag_kernel<<<nblk(ndof), BS, 0, stream>>>(levdev(finest()), diag.p);
+        DRF_LAUNCHED();
+    }
     // transfer tables between level l - 1 and level l
     TransferDev tdev(int l) const {
         TransferDev T;
@@ -1112,15 +1144,13 @@ struct drf_bz {
             copy_kernel<<<nblk(n), BS, 0, stream>>>(n, rin, zout, stop);
             DRF_LAUNCHED();
         } else if (kind == 1) {
-            jacobi_kernel<<<nblk(n), BS, 0, stream>>>(levdev(L), rin, zout, stop);
+            jacobi_diag_kernel<<<nblk(n), BS, 0, stream>>>(n, diag.p, rin, zout, stop);
             DRF_LAUNCHED();
         } else if (kind == 3) {
             // Jacobi base (positive definite: a descent direction for any residual) plus the
-            // learned correction of the error it leaves
-            jacobi_kernel<<<nblk(n), BS, 0, stream>>>(levdev(L), rin, zout, stop);
-            DRF_LAUNCHED();
+            // learned correction of the error it leaves, formed in the network's output pass
             cnn_precondition(cnn_net(cnn), stream, lv[L].n, rin, scal.p + S_RR, cnn_scale, zout, 1,
-                             stop);
+                             stop, diag.p);
         } else {
             vcycle(rin, zout);
         }
@@ -1474,6 +1504,7 @@ int drf_bz_create(const drf_bz_grid_desc *g, const double *dgauss, drf_bz **out)
         // per-block partials: the fused apply-dot writes one value per apply block
         h->part.alloc(std::max<size_t>(4096, (size_t)nblk(h->ndof) + 16));
         h->ctl.alloc(3);
+        h->form_diag();
         bz_rhs_kernel<<<nblk(h->ndof), BS, 0, h->stream>>>(F.n, F.nd, h->dat.p, h->Bq.p, g->lambda, h->b.p);
         DRF_LAUNCHED();
         DRF_CUDA(cudaStreamSynchronize(h->stream));
@@ -1609,6 +1640,7 @@ int drf_mg_setup(drf_bz *h, int coarsest_n, int pre, int post) {
         const char *em = std::getenv("DRF_BZ_ELEM_SMOOTHER_MIN");
         h->elem_min = em ? std::max<int64_t>(0, std::atoll(em)) : ELEM_THREAD_MIN_ELEMS;
         h->mg_ready = true;
+        h->form_diag();
         if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; h->graph_kind = -1; }
     });
 }

@@ -319,10 +319,12 @@ __global__ void pack_kernel(int n, const double *r, const double *rr_ptr, double
     dst[1] = reinterpret_cast<const uint4 *>(v)[1];
 }
 
-// z (+)= rms(r) out_scale Y on the control points (add = 1 adds to a base already in z); one
-// thread per superpixel writes its (up to) 9 control points
+// z (+)= rms(r) out_scale Y on the control points (add = 1 adds to a base already in z; with
+// jr, jd non-null the base is the Jacobi step jr / jd instead); one thread per superpixel
+// writes its (up to) 9 control points
 __global__ void unpack_kernel(int n, const float *Y, const double *rr_ptr, double inv_len,
-                              double out_scale, double *z, int add, const int *stop) {
+                              double out_scale, double *z, int add, const int *stop, const double *jr,
+                              const double *jd) {
     if (stop && *stop) return;
     const int S = n + 1, nd = 3 * n + 1;
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -342,7 +344,7 @@ __global__ void unpack_kernel(int n, const float *Y, const double *rr_ptr, doubl
             if (gi < nd && gj < nd) {
                 const size_t t = gi + (size_t)nd * gj;
                 const double v = (double)y[a + 3 * b] * sc * out_scale;
-                z[t] = add ? z[t] + v : v;
+                z[t] = jr ? jr[t] / jd[t] + v : (add ? z[t] + v : v);
             }
         }
     }
@@ -504,7 +506,7 @@ struct CnnNet {
 
 // packs r (control points) and runs the network; z (+)= rms(r) * out_scale * net(r / rms(r))
 void cnn_precondition(CnnNet *net, cudaStream_t s, int n, const double *r, const double *rr_dev,
-                      double out_scale, double *z, int add, const int *stop) {
+                      double out_scale, double *z, int add, const int *stop, const double *jac_diag) {
     const int S = n + 1;
     const int64_t pix = (int64_t)S * S, nd = 3 * n + 1;
     cudaStream_t keep = net->stream;
@@ -514,7 +516,7 @@ void cnn_precondition(CnnNet *net, cudaStream_t s, int n, const double *r, const
     DRF_LAUNCHED();
     net->forward(1, S, S);
     unpack_kernel<<<nb(pix), 256, 0, s>>>(n, net->out.p, rr_dev, 1.0 / (double)(nd * nd), out_scale,
-                                              z, add, stop);
+                                              z, add, stop, jac_diag ? r : nullptr, jac_diag);
     DRF_LAUNCHED();
     net->stream = keep;
 }

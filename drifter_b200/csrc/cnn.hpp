@@ -11,6 +11,8 @@ void cnn_prepare(CnnNet *net, int n);
 // z (+)= rms(r) * out_scale * net(r / rms(r)) on the control-point grid of n x n elements
 // (add = 1 adds to the base already in z); rr_dev points to r.r on the device; kernels return
 // early when *stop is set.
+// z (+)= the network's correction of r; with jac_diag non-null z = r / jac_diag + correction
+// (the Jacobi base and the correction in one pass)
 void cnn_precondition(CnnNet *net, cudaStream_t s, int n, const double *r, const double *rr_dev,
-                      double out_scale, double *z, int add, const int *stop);
+                      double out_scale, double *z, int add, const int *stop, const double *jac_diag = nullptr);
 }  // namespace drf
