@@ -208,6 +208,9 @@ def run_cg(stream, reps=3):
     out = {"workload": c["name"] + " cubic Bezier, lambda=1, eps=1e-4, FP64 PCG to 1e-10",
            "dofs": s.ndof, "train_s": round(train_s, 2), "train_loss": info["loss"]}
     sols = {}
+    import torch
+    torch.cuda.synchronize()
+    torch.cuda.profiler.start()  # the solves only (ncu --profile-from-start off), not the training
     for pc in ("mg", "cnn", "jacobi", "none"):
         s.solve(pc, tol=1e-10, maxit=5000)  # warm-up (graph capture)
         best = None
@@ -217,6 +220,8 @@ def run_cg(stream, reps=3):
                 best = inf
         sols[pc] = x
         out[pc] = {"iters": best["iters"], "ms": round(best["ms"], 3), "relres": best["relres"]}
+    torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
     out["cnn_vs_mg_speedup"] = round(out["mg"]["ms"] / out["cnn"]["ms"], 3)
     out["cnn_vs_mg_solution_rel_diff"] = float(np.abs(sols["cnn"] - sols["mg"]).max() /
                                                np.abs(sols["mg"]).max())
