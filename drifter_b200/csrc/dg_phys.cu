@@ -733,14 +733,24 @@ constexpr int baro_min_blocks(int threads, int np) {
 }
 #define BARO_BOUNDS __launch_bounds__(CPB * NP * NP, baro_min_blocks(CPB * NP * NP, NP))
 
-// One tile of BARO_CPB columns: the barotropic right-hand side Phi(U) at this thread's 2D node.
-// FK is the face flux (the model's flux2d). Every global load, the neighbours' face values
-// included, is issued before the tile barrier.
+// One tile of CPB columns: the barotropic right-hand side Phi(U) at this thread's 2D node.
+// FK is the face flux (the model's flux2d).
+//  * Volume terms: each node stores its state, h, 1/H and its momentum-flux products
+//    (hu u, hu v, hv v) in shared memory once; the derivative sums read them.
+//  * Face terms: the 4(N+1) face nodes of an element side by side are work items spread over
+//    the element's threads (one flux per thread for N >= 3), not evaluated by the face nodes
+//    themselves, so no warp runs the flux twice (x then y) under divergence. Each item writes
+//    F*(U-, U+) - F(U-) to shared memory; a node subtracts its x face's, then its y face's.
+//  * Every global load (own state, the face items' neighbour values) is issued before the
+//    first tile barrier; the tidal elevation is evaluated only by items on a tidal side.
 template <int NP, int FK, int CPB>
-__device__ __forceinline__ bool baro_tile_phi(const BaroArgs &a, int64_t tile, double &re, double &ru,
+__device__ __forceinline__ bool baro_tile_phi(const BaroArgs &a, int64_t tile, double toff, double &re, double &ru,
                                               double &rv, int64_t &t) {
-    constexpr int NP2 = NP * NP, N = NP - 1;
-    __shared__ double sE[CPB * NP2], sU[CPB * NP2], sV[CPB * NP2], sI[CPB * NP2], sD[NP2];
+    constexpr int NP2 = NP * NP, N = NP - 1, NF = 4 * NP;
+    constexpr int NI = (NF + NP2 - 1) / NP2;  // face items per thread
+    __shared__ double sE[CPB * NP2], sU[CPB * NP2], sV[CPB * NP2], sB[CPB * NP2], sI[CPB * NP2];
+    __shared__ double sUU[CPB * NP2], sUV[CPB * NP2], sVV[CPB * NP2], sD[NP2];
+    __shared__ double sF[CPB * NF * 3];  // per element and face item: d = F* - F(U-)
     const Geo &G = a.G;
     const int lc = threadIdx.x / NP2, an = threadIdx.x % NP2, i = an % NP, j = an / NP;
     const int64_t c = tile * CPB + lc;
@@ -748,87 +758,102 @@ __device__ __forceinline__ bool baro_tile_phi(const BaroArgs &a, int64_t tile, d
     if (threadIdx.x < NP2) sD[threadIdx.x] = cBs[NP].D[threadIdx.x];
     t = c * NP2 + an;
     const int ex = (int)(c % G.nx), ey = (int)(c / G.nx);
-    // the neighbour node across this node's x face (i = 0 or N) and y face (j = 0 or N)
-    int64_t qx = -1, qy = -1;
-    if (valid && i == 0 && ex > 0) qx = (c - 1) * NP2 + N + NP * j;
-    if (valid && i == N && ex < G.nx - 1) qx = (c + 1) * NP2 + NP * j;
-    if (valid && j == 0 && ey > 0) qy = (c - G.nx) * NP2 + i + NP * N;
-    if (valid && j == N && ey < G.ny - 1) qy = (c + G.nx) * NP2 + i;
     double e = 0.0, hb = 0.0, hu0 = 0.0, hv0 = 0.0, fc = 0.0, fx = 0.0, fy = 0.0;
-    double xR[4] = {0.0, 0.0, 0.0, 0.0}, yR[4] = {0.0, 0.0, 0.0, 0.0};
     if (valid) {
         e = a.e[t]; hb = a.h[t]; hu0 = a.hu[t]; hv0 = a.hv[t]; fc = a.f[t];
         if (a.Fx) { fx = a.Fx[t]; fy = a.Fy[t]; }
     }
-    if (qx >= 0) { xR[0] = a.e[qx]; xR[1] = a.h[qx]; xR[2] = a.hu[qx]; xR[3] = a.hv[qx]; }
-    if (qy >= 0) { yR[0] = a.e[qy]; yR[1] = a.h[qy]; yR[2] = a.hu[qy]; yR[3] = a.hv[qy]; }
+    // this thread's face items: side s = it / NP (0 -x, 1 +x, 2 -y, 3 +y), position k = it % NP;
+    // the neighbour's e, h, hu, hv across the face (q < 0 on a basin side)
+    int64_t qn[NI];
+    double nb[NI][4];
+#pragma unroll
+    for (int r = 0; r < NI; ++r) {
+        const int it = an + r * NP2;
+        qn[r] = -1;
+        nb[r][0] = nb[r][1] = nb[r][2] = nb[r][3] = 0.0;
+        if (!valid || it >= NF) continue;
+        const int s = it / NP, k = it % NP;
+        if (s == 0 && ex > 0) qn[r] = (c - 1) * NP2 + N + NP * k;
+        if (s == 1 && ex < G.nx - 1) qn[r] = (c + 1) * NP2 + NP * k;
+        if (s == 2 && ey > 0) qn[r] = (c - G.nx) * NP2 + k + NP * N;
+        if (s == 3 && ey < G.ny - 1) qn[r] = (c + G.nx) * NP2 + k;
+        if (qn[r] >= 0) {
+            nb[r][0] = a.e[qn[r]]; nb[r][1] = a.h[qn[r]]; nb[r][2] = a.hu[qn[r]]; nb[r][3] = a.hv[qn[r]];
+        }
+    }
     const double H = valid ? e + hb : 1.0;
+    const double iH = 1.0 / H;
     if (valid) {
-        sE[threadIdx.x] = e;
-        sU[threadIdx.x] = hu0;
-        sV[threadIdx.x] = hv0;
-        sI[threadIdx.x] = 1.0 / H;
+        const int n = threadIdx.x;
+        const double u = hu0 * iH, v = hv0 * iH;
+        sE[n] = e; sU[n] = hu0; sV[n] = hv0; sB[n] = hb; sI[n] = iH;
+        sUU[n] = hu0 * u; sUV[n] = hv0 * u; sVV[n] = hv0 * v;
     }
     __syncthreads();
-    if (!valid) return false;
-    const int b0 = lc * NP2;
-    double dhu = 0, dhv = 0, auu = 0, auv = 0, avu = 0, avv = 0, gex = 0, gey = 0;
+    // face items: the flux difference at face node (fi, fj) of this element
 #pragma unroll
-    for (int m = 0; m < NP; ++m) {
-        const int px = b0 + m + NP * j, py = b0 + i + NP * m;
-        const double dxm = sD[i * NP + m], dym = sD[j * NP + m];
-        const double ux = sU[px], vx = sV[px], ix = sI[px];
-        const double uy = sU[py], vy = sV[py], iy = sI[py];
-        dhu += dxm * ux;
-        dhv += dym * vy;
-        auu += dxm * ux * ux * ix;
-        avu += dxm * vx * ux * ix;
-        auv += dym * uy * vy * iy;
-        avv += dym * vy * vy * iy;
-        gex += dxm * sE[px];
-        gey += dym * sE[py];
-    }
-    re = -(G.cx * dhu + G.cy * dhv);
-    ru = -(G.cx * auu + G.cy * auv) - G.g * H * G.cx * gex + fc * hv0 + fx;
-    rv = -(G.cx * avu + G.cy * avv) - G.g * H * G.cy * gey - fc * hu0 + fy;
-    const bool bxf = i == 0 || i == N, byf = j == 0 || j == N;
-    if (!(bxf || byf)) return true;
-    const double etide = tide_at(G, a.tdev[0] + a.toff);
-    const double UL[3] = {H, hu0, hv0};
-    const double ihL = sI[threadIdx.x], cL = FK == DRF_FLUX_LF ? sqrt(G.g * (H < 1e-10 ? 1e-10 : H)) : 0.0;
-    // x face first, then y face (a corner node has both)
-#pragma unroll
-    for (int f = 0; f < 2; ++f) {
-        if (f == 0 ? !bxf : !byf) continue;
-        const int s = f == 0 ? (i == 0 ? 0 : 1) : (j == 0 ? 2 : 3);
+    for (int r = 0; r < NI; ++r) {
+        const int it = an + r * NP2;
+        if (!valid || it >= NF) continue;
+        const int s = it / NP, k = it % NP;
+        const int fi = s == 0 ? 0 : (s == 1 ? N : k), fj = s <= 1 ? k : (s == 2 ? 0 : N);
+        const int ln = lc * NP2 + fi + NP * fj;
+        const double HL = sE[ln] + sB[ln];  // the node's own H, recomputed exactly
+        const double UL[3] = {HL, sU[ln], sV[ln]};
         const double nx = s == 0 ? -1.0 : (s == 1 ? 1.0 : 0.0);
         const double ny = s == 2 ? -1.0 : (s == 3 ? 1.0 : 0.0);
-        const double L = s <= 1 ? G.Lx : G.Ly;
-        const int64_t q = f == 0 ? qx : qy;
-        const double *nb = f == 0 ? xR : yR;
         double UR[3];
-        if (q >= 0) {
-            UR[0] = nb[0] + nb[1]; UR[1] = nb[2]; UR[2] = nb[3];
+        if (qn[r] >= 0) {
+            UR[0] = nb[r][0] + nb[r][1]; UR[1] = nb[r][2]; UR[2] = nb[r][3];
         } else if ((s == 0 ? G.bc[0] : (s == 1 ? G.bc[1] : (s == 2 ? G.bc[2] : G.bc[3]))) == DRF_BC_TIDE) {
-            UR[0] = etide + hb;
-            const double r = UR[0] / H;
-            UR[1] = UL[1] * r; UR[2] = UL[2] * r;
+            UR[0] = tide_at(G, a.tdev[0] + toff) + sB[ln];
+            const double rr = UR[0] / HL;
+            UR[1] = UL[1] * rr; UR[2] = UL[2] * rr;
         } else {
-            UR[0] = H; UR[1] = UL[1]; UR[2] = UL[2];
+            UR[0] = HL; UR[1] = UL[1]; UR[2] = UL[2];
             if (s <= 1) UR[1] = -UL[1]; else UR[2] = -UL[2];
         }
         double d[3];
         if (FK == DRF_FLUX_LF) {
-            lf_minus_phys(UL, ihL, cL, UR, nx, ny, G.g, d);
+            lf_minus_phys(UL, sI[ln], sqrt(G.g * (HL < 1e-10 ? 1e-10 : HL)), UR, nx, ny, G.g, d);
         } else {
             double Fs[3], Fm[3];
             sw_flux(FK, UL, UR, nx, ny, G.g, Fs);
             sw_phys_flux(UL, nx, ny, G.g, Fm);
             d[0] = Fs[0] - Fm[0]; d[1] = Fs[1] - Fm[1]; d[2] = Fs[2] - Fm[2];
         }
-        re -= L * d[0];
-        ru -= L * d[1];
-        rv -= L * d[2];
+        double *o = sF + (lc * NF + it) * 3;
+        o[0] = d[0]; o[1] = d[1]; o[2] = d[2];
+    }
+    const int b0 = lc * NP2;
+    double dhu = 0, dhv = 0, auu = 0, auv = 0, avu = 0, avv = 0, gex = 0, gey = 0;
+#pragma unroll
+    for (int m = 0; m < NP; ++m) {
+        const int px = b0 + m + NP * j, py = b0 + i + NP * m;
+        const double dxm = sD[i * NP + m], dym = sD[j * NP + m];
+        dhu += dxm * sU[px];
+        dhv += dym * sV[py];
+        auu += dxm * sUU[px];
+        avu += dxm * sUV[px];
+        auv += dym * sUV[py];
+        avv += dym * sVV[py];
+        gex += dxm * sE[px];
+        gey += dym * sE[py];
+    }
+    __syncthreads();  // the face items are in sF
+    if (!valid) return false;
+    re = -(G.cx * dhu + G.cy * dhv);
+    ru = -(G.cx * auu + G.cy * auv) - G.g * H * G.cx * gex + fc * hv0 + fx;
+    rv = -(G.cx * avu + G.cy * avv) - G.g * H * G.cy * gey - fc * hu0 + fy;
+    // x face first, then y face (a corner node has both)
+    if (i == 0 || i == N) {
+        const double *d = sF + (lc * NF + (i == 0 ? 0 : NP) + j) * 3;
+        re -= G.Lx * d[0]; ru -= G.Lx * d[1]; rv -= G.Lx * d[2];
+    }
+    if (j == 0 || j == N) {
+        const double *d = sF + (lc * NF + (j == 0 ? 2 * NP : 3 * NP) + i) * 3;
+        re -= G.Ly * d[0]; ru -= G.Ly * d[1]; rv -= G.Ly * d[2];
     }
     return true;
 }
@@ -837,18 +862,18 @@ template <int NP, int FK, int CPB>
 __global__ void baro_rhs_kernel(BaroArgs a, double *ke, double *ku, double *kv) {
     double re, ru, rv;
     int64_t t;
-    if (!baro_tile_phi<NP, FK, CPB>(a, blockIdx.x, re, ru, rv, t)) return;
+    if (!baro_tile_phi<NP, FK, CPB>(a, blockIdx.x, a.toff, re, ru, rv, t)) return;
     ke[t] = re; ku[t] = ru; kv[t] = rv;
 }
 
 // F = (3D-integrated increment)/dt - Phi(U^n); keeps HU^n, HV^n for the transport correction.
 template <int NP, int FK, int CPB>
-__device__ __forceinline__ void baro_force_body(const BaroArgs &a, int64_t tile, double dt, const double *dHU3,
+__device__ __forceinline__ void baro_force_body(const BaroArgs &a, int64_t tile, double toff, double dt, const double *dHU3,
                                                 const double *dHV3, double *Fx, double *Fy, double *HUo,
                                                 double *HVo) {
     double re, ru, rv;
     int64_t t;
-    if (!baro_tile_phi<NP, FK, CPB>(a, tile, re, ru, rv, t)) return;
+    if (!baro_tile_phi<NP, FK, CPB>(a, tile, toff, re, ru, rv, t)) return;
     Fx[t] = dHU3[t] / dt - ru;
     Fy[t] = dHV3[t] / dt - rv;
     HUo[t] = a.hu[t];
@@ -857,16 +882,16 @@ __device__ __forceinline__ void baro_force_body(const BaroArgs &a, int64_t tile,
 template <int NP, int FK, int CPB>
 __global__ void baro_force_kernel(BaroArgs a, double dt, const double *dHU3, const double *dHV3,
                                   double *Fx, double *Fy, double *HUo, double *HVo) {
-    baro_force_body<NP, FK, CPB>(a, blockIdx.x, dt, dHU3, dHV3, Fx, Fy, HUo, HVo);
+    baro_force_body<NP, FK, CPB>(a, blockIdx.x, a.toff, dt, dHU3, dHV3, Fx, Fy, HUo, HVo);
 }
 
 // Heun predictor: k1 = Phi(U^m), U* = U^m + dtb k1
 template <int NP, int FK, int CPB>
-__device__ __forceinline__ void baro_pred_body(const BaroArgs &a, int64_t tile, double dtb, double *k1e,
+__device__ __forceinline__ void baro_pred_body(const BaroArgs &a, int64_t tile, double toff, double dtb, double *k1e,
                                                double *k1u, double *k1v, double *es, double *us, double *vs) {
     double re, ru, rv;
     int64_t t;
-    if (!baro_tile_phi<NP, FK, CPB>(a, tile, re, ru, rv, t)) return;
+    if (!baro_tile_phi<NP, FK, CPB>(a, tile, toff, re, ru, rv, t)) return;
     k1e[t] = re; k1u[t] = ru; k1v[t] = rv;
     es[t] = a.e[t] + dtb * re;
     us[t] = a.hu[t] + dtb * ru;
@@ -875,17 +900,17 @@ __device__ __forceinline__ void baro_pred_body(const BaroArgs &a, int64_t tile, 
 template <int NP, int FK, int CPB>
 __global__ void BARO_BOUNDS baro_pred_kernel(BaroArgs a, double dtb, double *k1e, double *k1u, double *k1v,
                                  double *es, double *us, double *vs) {
-    baro_pred_body<NP, FK, CPB>(a, blockIdx.x, dtb, k1e, k1u, k1v, es, us, vs);
+    baro_pred_body<NP, FK, CPB>(a, blockIdx.x, a.toff, dtb, k1e, k1u, k1v, es, us, vs);
 }
 
 // Heun corrector: U^{m+1} = U^m + dtb/2 (k1 + Phi(U*)); accumulates eta for its time mean
 template <int NP, int FK, int CPB>
-__device__ __forceinline__ void baro_corr_body(const BaroArgs &a, int64_t tile, double dtb, const double *k1e,
+__device__ __forceinline__ void baro_corr_body(const BaroArgs &a, int64_t tile, double toff, double dtb, const double *k1e,
                                                const double *k1u, const double *k1v, double *e, double *hu,
                                                double *hv, double *esum, int first) {
     double re, ru, rv;
     int64_t t;
-    if (!baro_tile_phi<NP, FK, CPB>(a, tile, re, ru, rv, t)) return;
+    if (!baro_tile_phi<NP, FK, CPB>(a, tile, toff, re, ru, rv, t)) return;
     const double hd = 0.5 * dtb;
     const double en = e[t] + hd * (k1e[t] + re);
     e[t] = en;
@@ -897,7 +922,7 @@ template <int NP, int FK, int CPB>
 __global__ void BARO_BOUNDS baro_corr_kernel(BaroArgs a, double dtb, const double *k1e, const double *k1u,
                                  const double *k1v, double *e, double *hu, double *hv,
                                  double *esum, int first) {
-    baro_corr_body<NP, FK, CPB>(a, blockIdx.x, dtb, k1e, k1u, k1v, e, hu, hv, esum, first);
+    baro_corr_body<NP, FK, CPB>(a, blockIdx.x, a.toff, dtb, k1e, k1u, k1v, e, hu, hv, esum, first);
 }
 
 __global__ void baro_finish_kernel(int64_t n2, int nsub, double dt, const double *esum,
@@ -1037,7 +1062,7 @@ __global__ void baro_force_ens_kernel(BaroArgs a, BaroEns E, const double *dHU3,
     shift_baro(a, m, w.x);
     a.toff = 0.0;
     const int64_t o = m.off2;
-    baro_force_body<NP, FK, BARO_CPB>(a, w.y, m.dt, dHU3 + o, dHV3 + o, Fx + o, Fy + o, HUo + o, HVo + o);
+    baro_force_body<NP, FK, BARO_CPB>(a, w.y, a.toff, m.dt, dHU3 + o, dHV3 + o, Fx + o, Fy + o, HUo + o, HVo + o);
 }
 template <int NP, int FK, int CPB = BARO_CPB>
 __global__ void BARO_BOUNDS baro_pred_ens_kernel(BaroArgs a, BaroEns E, double *k1e, double *k1u,
@@ -1048,7 +1073,7 @@ __global__ void BARO_BOUNDS baro_pred_ens_kernel(BaroArgs a, BaroEns E, double *
     const double dtb = m.dt / E.nsub;
     a.toff = __dmul_rn((double)E.sub, dtb);
     const int64_t o = m.off2;
-    baro_pred_body<NP, FK, BARO_CPB>(a, w.y, dtb, k1e + o, k1u + o, k1v + o, es + o, us + o, vs + o);
+    baro_pred_body<NP, FK, BARO_CPB>(a, w.y, a.toff, dtb, k1e + o, k1u + o, k1v + o, es + o, us + o, vs + o);
 }
 template <int NP, int FK, int CPB = BARO_CPB>
 __global__ void BARO_BOUNDS baro_corr_ens_kernel(BaroArgs a, BaroEns E, const double *k1e, const double *k1u,
@@ -1060,7 +1085,7 @@ __global__ void BARO_BOUNDS baro_corr_ens_kernel(BaroArgs a, BaroEns E, const do
     const double dtb = m.dt / E.nsub;
     a.toff = __dadd_rn(__dmul_rn((double)E.sub, dtb), dtb);  // unfused, as the host computes it
     const int64_t o = m.off2;
-    baro_corr_body<NP, FK, BARO_CPB>(a, w.y, dtb, k1e + o, k1u + o, k1v + o, e + o, hu + o, hv + o, esum + o,
+    baro_corr_body<NP, FK, BARO_CPB>(a, w.y, a.toff, dtb, k1e + o, k1u + o, k1v + o, e + o, hu + o, hv + o, esum + o,
                            E.sub == 0);
 }
 
@@ -1076,6 +1101,167 @@ __global__ void baro_finish_ens_kernel(int64_t n2, int nsub, const EnsMember *me
     eta_avg[t] = esum[t] / nsub;
     corrU[t] = HU[t] - (HUo[t] + dHU3[t]);
     corrV[t] = HV[t] - (HVo[t] + dHV3[t]);
+}
+
+// ------------------------------------------------------- persistent barotropic step (FP64)
+// All barotropic work of one baroclinic step in ONE cooperative launch: the slow-forcing pass,
+// nsub Heun subcycles (predictor and corrector passes over every tile) and the finish pass.
+// Tiles go to CTAs as b, b + gridDim.x, ... in every pass, so each thread meets the same
+// nodes in every pass and only the face neighbours cross CTAs; a grid barrier separates the
+// passes that read neighbours written by the pass before. Every node sees the arithmetic of
+// the per-pass kernels above, in the same order, so both forms give identical results.
+struct SubcycleArgs {
+    double dt, dtb;            // one model: baroclinic step and substep
+    int nsub, ntiles;
+    const EnsMember *mem;      // ensemble: member table and the (member, tile) list
+    const int2 *tiles;
+    int nmem;
+    const double *dHU3, *dHV3;
+    double *Fx, *Fy, *HUo, *HVo, *k1e, *k1u, *k1v, *es, *us, *vs;
+    double *eta, *HU, *HV, *esum, *eta_avg, *corrU, *corrV;
+    double *tdev;              // the model's clock (an ensemble: member 0's, the others follow)
+    unsigned *sync;            // [0] barrier arrivals, [1] CTAs finished, [2] abort; zero at launch
+    int *err;
+};
+
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned *p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Grid-wide barrier of a cooperative launch (all CTAs resident): the n-th barrier completes
+// when n * gridDim.x arrivals are counted. The wait is bounded; a CTA that gives up, or that
+// sees another CTA's abort word, sets the abort word and the status word and returns false.
+__device__ __forceinline__ bool grid_barrier(unsigned *sync, unsigned target, int *err) {
+    __shared__ int s_go;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd(&sync[0], 1u);
+        int go = 1;
+        for (long it = 0; ld_acquire_gpu(&sync[0]) < target; ++it) {
+            if (it > (1L << 22) || ld_acquire_gpu(&sync[2]) != 0u) {
+                go = 0;
+                break;
+            }
+            __nanosleep(32);
+        }
+        if (!go) {
+            atomicExch(&sync[2], 1u);
+            atomicExch(err, DRF_E_TIMEOUT);
+        }
+        __threadfence();
+        s_go = go;
+    }
+    __syncthreads();
+    return s_go != 0;
+}
+
+// Pass item w: fn(args, tile, 2D offset, step, substep) with the pass's arguments as they are
+// (one model) or shifted to the item's member (an ensemble).
+template <bool ENS, class F>
+__device__ __forceinline__ void sub_item(const SubcycleArgs &s, const BaroArgs &base, int w, F &&fn) {
+    if constexpr (ENS) {
+        const int2 t = s.tiles[w];
+        const EnsMember &m = s.mem[t.x];
+        BaroArgs a = base;
+        shift_baro(a, m, t.x);
+        fn(a, (int64_t)t.y, m.off2, m.dt, m.dt / s.nsub);
+    } else {
+        fn(base, (int64_t)w, (int64_t)0, s.dt, s.dtb);
+    }
+}
+
+// af, ap, ac: the forcing, predictor and corrector passes' arguments (state pointers).
+template <int NP, int FK, int CPB, bool ENS>
+__global__ void BARO_BOUNDS baro_subcycles_kernel(const __grid_constant__ BaroArgs af,
+                                                  const __grid_constant__ BaroArgs ap,
+                                                  const __grid_constant__ BaroArgs ac,
+                                                  const __grid_constant__ SubcycleArgs s) {
+    constexpr int NP2 = NP * NP;
+    unsigned nbar = 0;
+    // slow forcing F = dHU3/dt - Phi(U^n); the first predictor reads only this thread's F
+    for (int w = blockIdx.x; w < s.ntiles; w += gridDim.x) {
+        __syncthreads();  // the tile's shared memory is reused
+        sub_item<ENS>(s, af, w, [&](const BaroArgs &a, int64_t tile, int64_t o, double dt, double) {
+            baro_force_body<NP, FK, CPB>(a, tile, 0.0, dt, s.dHU3 + o, s.dHV3 + o, s.Fx + o, s.Fy + o, s.HUo + o,
+                                         s.HVo + o);
+        });
+    }
+    for (int m = 0; m < s.nsub; ++m) {
+        for (int w = blockIdx.x; w < s.ntiles; w += gridDim.x) {
+            __syncthreads();
+            sub_item<ENS>(s, ap, w, [&](const BaroArgs &a, int64_t tile, int64_t o, double, double dtb) {
+                baro_pred_body<NP, FK, CPB>(a, tile, __dmul_rn((double)m, dtb), dtb, s.k1e + o, s.k1u + o,
+                                            s.k1v + o, s.es + o, s.us + o, s.vs + o);
+            });
+        }
+        if (!grid_barrier(s.sync, ++nbar * gridDim.x, s.err)) return;
+        for (int w = blockIdx.x; w < s.ntiles; w += gridDim.x) {
+            __syncthreads();
+            sub_item<ENS>(s, ac, w, [&](const BaroArgs &a, int64_t tile, int64_t o, double, double dtb) {
+                // the substep's end time, unfused as the host computes it
+                baro_corr_body<NP, FK, CPB>(a, tile, __dadd_rn(__dmul_rn((double)m, dtb), dtb), dtb, s.k1e + o,
+                                            s.k1u + o, s.k1v + o, s.eta + o, s.HU + o, s.HV + o, s.esum + o,
+                                            m == 0);
+            });
+        }
+        if (m + 1 < s.nsub && !grid_barrier(s.sync, ++nbar * gridDim.x, s.err)) return;
+    }
+    // finish: eta's time mean and the transport correction at this thread's own nodes
+    for (int w = blockIdx.x; w < s.ntiles; w += gridDim.x) {
+        sub_item<ENS>(s, af, w, [&](const BaroArgs &a, int64_t tile, int64_t o, double, double) {
+            const int64_t c = tile * CPB + threadIdx.x / NP2;
+            if (c >= a.ncol) return;
+            const int64_t t = o + c * NP2 + threadIdx.x % NP2;
+            s.eta_avg[t] = s.esum[t] / s.nsub;
+            s.corrU[t] = s.HU[t] - (s.HUo[t] + s.dHU3[t]);
+            s.corrV[t] = s.HV[t] - (s.HVo[t] + s.dHV3[t]);
+        });
+    }
+    // the clock(s) advance once every CTA is past its last read of them
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(&s.sync[1], 1u) == gridDim.x - 1) {
+            __threadfence();
+            if constexpr (ENS) {
+                for (int i = 0; i < s.nmem; ++i) s.tdev[i] = s.tdev[i] + s.mem[i].dt;
+            } else {
+                s.tdev[0] = s.tdev[0] + s.dt;
+            }
+        }
+    }
+}
+
+// Launches baro_subcycles_kernel cooperatively, with as many CTAs as can be resident (at most
+// one per tile), after zeroing its barrier words on the same stream.
+template <int NP, int FK, int CPB, bool ENS>
+void launch_subcycles(const BaroArgs &af, const BaroArgs &ap, const BaroArgs &ac, const SubcycleArgs &s,
+                      cudaStream_t st) {
+    auto fn = baro_subcycles_kernel<NP, FK, CPB, ENS>;
+    const int threads = CPB * NP * NP;
+    int dev = 0, nsm = 0, per_sm = 0;
+    DRF_CUDA(cudaGetDevice(&dev));
+    DRF_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    DRF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, 0));
+    DRF_CHECK(per_sm >= 1, DRF_E_UNSUPPORTED, "the barotropic kernel cannot be resident");
+    const int64_t cap = (int64_t)per_sm * nsm;
+    const unsigned grid = (unsigned)(s.ntiles < cap ? s.ntiles : cap);
+    DRF_CUDA(cudaMemsetAsync(s.sync, 0, 3 * sizeof(unsigned), st));
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3((unsigned)threads);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    DRF_CUDA(cudaLaunchKernelEx(&cfg, fn, af, ap, ac, s));
+    DRF_LAUNCHED();
 }
 
 template <typename T, int NP>
@@ -1309,6 +1495,10 @@ struct drf_dg {
     DevBuf<double> d2;         // 2D FP64 arrays
     DevBuf<int> errbuf;        // device status word written by bounded waits
     int *err = nullptr;        // the status word in use (errbuf, or the ensemble's)
+    DevBuf<unsigned> syncbuf;  // grid-barrier words of the persistent barotropic launch
+    // barotropic step as one persistent launch (false: one launch per pass); fixed when the
+    // step graphs are built, from DRIFTER_B200_BARO_PERSISTENT (1 selects the persistent form)
+    bool baro_persist = false;
     // 3D arrays: q3p + (array * n3s + node) * tsz; n3s = n3 for a model that owns its memory,
     // the pool length for an ensemble member (a view into the ensemble's pools)
     unsigned char *q3p = nullptr;
@@ -1435,6 +1625,24 @@ struct drf_dg {
         return b;
     }
 
+    // arguments of the persistent barotropic launch over this model's arrays
+    SubcycleArgs subcycle_args(double dt, int nsub, int ntiles) {
+        SubcycleArgs s{};
+        s.dt = dt; s.dtb = dt / nsub; s.nsub = nsub; s.ntiles = ntiles;
+        s.dHU3 = dHU3; s.dHV3 = dHV3;
+        s.Fx = Fx; s.Fy = Fy; s.HUo = HUo; s.HVo = HVo;
+        s.k1e = k1[0]; s.k1u = k1[1]; s.k1v = k1[2];
+        s.es = us[0]; s.us = us[1]; s.vs = us[2];
+        s.eta = eta; s.HU = HU; s.HV = HV; s.esum = esum; s.eta_avg = eta_avg;
+        s.corrU = corrU; s.corrV = corrV;
+        s.tdev = tdev;
+        s.sync = syncbuf.p;
+        s.err = err;
+        return s;
+    }
+    // kernel launches of one baroclinic step: 5 stages, then the barotropic step
+    uint64_t launches_per_step(int nsub) const { return baro_persist ? 6 : 5 + 2 + 2 * (uint64_t)nsub; }
+
     template <typename T, int NP>
     void enqueue_step(int in, double dt, int nsub) {
         const int out = 1 - in;
@@ -1446,6 +1654,19 @@ struct drf_dg {
             src = dst;
         }
         // after 5 stages the state is in `out`; the barotropic tile is the tuned one
+        if (baro_persist) {
+            dispatch_cpb(baro_cpb, [&](auto cpbc) {
+                constexpr int CPB = decltype(cpbc)::value;
+                dispatch_flux(G.flux2d, [&](auto fk) {
+                    constexpr int FK = decltype(fk)::value;
+                    launch_subcycles<NP, FK, CPB, false>(
+                        baro<NP>(eta, HU, HV, false, 0.0), baro<NP>(eta, HU, HV, true, 0.0),
+                        baro<NP>(us[0], us[1], us[2], true, 0.0),
+                        subcycle_args(dt, nsub, (int)((ncol + CPB - 1) / CPB)), stream);
+                });
+            });
+            return;
+        }
         dispatch_cpb(baro_cpb, [&](auto cpbc) {
             constexpr int CPB = decltype(cpbc)::value;
             const unsigned nbt = (unsigned)((ncol + CPB - 1) / CPB);
@@ -1692,6 +1913,8 @@ int drf_dg_create(const drf_mesh_desc *mesh, const drf_dg_params *params, const 
         m->stream = m->own;
         m->errbuf.alloc(1);
         DRF_CUDA(cudaMemset(m->errbuf.p, 0, sizeof(int)));
+        m->syncbuf.alloc(4);
+        DRF_CUDA(cudaMemset(m->syncbuf.p, 0, 4 * sizeof(unsigned)));
         m->q3.alloc((size_t)16 * m->n3 * m->tsz);
         DRF_CUDA(cudaMemset(m->q3.p, 0, m->q3.n));
         m->d2.alloc((size_t)drf_dg::N2ARRAYS * m->n2 + 8);
@@ -1848,6 +2071,8 @@ int drf_dg_step_modesplit(drf_dg *m, double dt, int nsub, int nsteps) {
         m->tune_baro();  // first step only: outside any capture
         if (m->graph_nsub != nsub || m->graph_dt != dt) {
             m->drop_graphs();
+            const char *pe = std::getenv("DRIFTER_B200_BARO_PERSISTENT");
+            m->baro_persist = pe && pe[0] == '1';
             for (int in = 0; in < 2; ++in) {
                 cudaGraph_t g = nullptr;
                 DRF_CUDA(cudaStreamBeginCapture(m->stream, cudaStreamCaptureModeThreadLocal));
@@ -1872,7 +2097,7 @@ int drf_dg_step_modesplit(drf_dg *m, double dt, int nsub, int nsteps) {
         }
         for (int s = 0; s < nsteps; ++s) {
             DRF_CUDA(cudaGraphLaunch(m->graph[m->cur], m->stream));
-            launch_counter().fetch_add(5 + 2 + 2 * (uint64_t)nsub);
+            launch_counter().fetch_add(m->launches_per_step(nsub));
             m->cur = 1 - m->cur;
             m->pending = true;
         }
@@ -2179,6 +2404,8 @@ struct drf_ens {
     DevBuf<unsigned char> q3;                  // 16 pooled 3D arrays
     DevBuf<double> d2;                         // 26 pooled 2D arrays + one clock per member
     DevBuf<int> errbuf;
+    DevBuf<unsigned> syncbuf;  // grid-barrier words of the persistent barotropic launch
+    bool baro_persist = false;  // as drf_dg::baro_persist
     DevBuf<EnsMember> table;
     DevBuf<int2> items, tiles;
     std::vector<EnsMember> htab;
@@ -2213,6 +2440,22 @@ struct drf_ens {
             dg3d_stage_ens_kernel<T, NP><<<grid, threads, smem, stream>>>(a, table.p, items.p, nitems);
             DRF_LAUNCHED();
             src = dst;
+        }
+        if (baro_persist) {
+            SubcycleArgs sa = m0->subcycle_args(0.0, nsub, ntiles);
+            sa.mem = table.p;
+            sa.tiles = tiles.p;
+            sa.nmem = (int)mem.size();
+            sa.sync = syncbuf.p;
+            sa.err = errbuf.p;
+            dispatch_flux(m0->G.flux2d, [&](auto fk) {
+                constexpr int FK = decltype(fk)::value;
+                launch_subcycles<NP, FK, BARO_CPB, true>(
+                    m0->template baro<NP>(m0->eta, m0->HU, m0->HV, false, 0.0),
+                    m0->template baro<NP>(m0->eta, m0->HU, m0->HV, true, 0.0),
+                    m0->template baro<NP>(m0->us[0], m0->us[1], m0->us[2], true, 0.0), sa, stream);
+            });
+            return;
         }
         const int bt = BARO_CPB * NP * NP;
         dispatch_flux(m0->G.flux2d, [&](auto fk) {
@@ -2281,6 +2524,8 @@ int drf_ens_create(int nmembers, const drf_mesh_desc *meshes, const drf_dg_param
         e->stream = e->own;
         e->errbuf.alloc(1);
         DRF_CUDA(cudaMemset(e->errbuf.p, 0, sizeof(int)));
+        e->syncbuf.alloc(4);
+        DRF_CUDA(cudaMemset(e->syncbuf.p, 0, 4 * sizeof(unsigned)));
         e->q3.alloc((size_t)16 * e->n3tot * m0.tsz);
         DRF_CUDA(cudaMemset(e->q3.p, 0, e->q3.n));
         e->d2.alloc((size_t)(drf_dg::N2ARRAYS - 1) * e->n2tot + nmembers);
@@ -2396,6 +2641,8 @@ int drf_ens_step(drf_ens *e, const double *dt, int nsub, int nsteps) {
                                      cudaMemcpyHostToDevice, e->stream));
         if (e->graph_nsub != nsub) {
             e->drop_graphs();
+            const char *pe = std::getenv("DRIFTER_B200_BARO_PERSISTENT");
+            e->baro_persist = pe && pe[0] == '1';
             for (int in = 0; in < 2; ++in) {
                 cudaGraph_t g = nullptr;
                 DRF_CUDA(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
@@ -2419,7 +2666,7 @@ int drf_ens_step(drf_ens *e, const double *dt, int nsub, int nsteps) {
         }
         for (int s = 0; s < nsteps; ++s) {
             DRF_CUDA(cudaGraphLaunch(e->graph[e->cur], e->stream));
-            launch_counter().fetch_add(5 + 2 + 2 * (uint64_t)nsub);
+            launch_counter().fetch_add(e->baro_persist ? 6 : 5 + 2 + 2 * (uint64_t)nsub);
             e->cur = 1 - e->cur;
         }
         for (auto &m : e->mem) {

@@ -229,6 +229,42 @@ def test_autotuned_barotropic_tile_matches_default_tile(monkeypatch):
         assert relerr(a[k], b[k]) <= 1e-15, k
 
 
+@pytest.mark.parametrize("precision,flux2d,nsub", [("fp64", "lf", 20), ("fp64", "hllc", 1), ("fp64", "roe", 3),
+                                                    ("mixed", "lf", 20)])
+def test_persistent_barotropic_step_agrees_with_per_pass_launches(monkeypatch, precision, flux2d, nsub):
+    """DRIFTER_B200_BARO_PERSISTENT=1 runs the barotropic step as ONE cooperative launch with
+    grid barriers between its passes, in place of one launch per pass. Every node evaluates the
+    same formulas in both forms; the two kernels are compiled separately, so the compiler may
+    fuse a multiply-add in one and not the other. A face-flux difference F* - F(U-) cancels ~1e6
+    of its terms' magnitude (0.5 g h^2 against the jump), which lifts such a rounding difference
+    to ~1e-12 of eta after two HLLC steps: the states agree to 1e-11 relative (the oracle
+    comparisons hold 1e-10). 128 x 128 columns give more tiles than CTAs at every tile size, so
+    CTAs walk several tiles per pass. The substep is the case's (dt scaled with nsub), so the
+    run stays stable."""
+    case = configs.c2(nx=128, ny=128, nz=1, order=3, precision=precision, Lx=400e3, flux2d=flux2d)
+    case = configs.perturb(case)
+    case["dt"] = case["dt"] * nsub / case["nsub"]
+    per = OceanModel(case["cfg"], case["h"], case["f"], case["taux"], case["tauy"])
+    per.upload_state(case["q"], case["eta"])
+    per.step(case["dt"], nsub, 0)  # builds the step graphs
+    before = launch_count()
+    per.step(case["dt"], nsub, 2)
+    per.sync()
+    assert launch_count() - before == 2 * (5 + 2 + 2 * nsub)
+    monkeypatch.setenv("DRIFTER_B200_BARO_PERSISTENT", "1")
+    pers = OceanModel(case["cfg"], case["h"], case["f"], case["taux"], case["tauy"])
+    pers.upload_state(case["q"], case["eta"])
+    pers.step(case["dt"], nsub, 0)
+    before = launch_count()
+    pers.step(case["dt"], nsub, 2)
+    pers.sync()
+    assert launch_count() - before == 2 * 6  # 5 stages + one barotropic launch per step
+    a, b = pers.download_state(), per.download_state()
+    assert a["t"] == b["t"] and np.abs(a["eta"]).max() < 10.0
+    for k in ("eta", "HU", "HV", "eta_avg", "Hu", "Hv", "HT", "HS"):
+        assert relerr(a[k], b[k]) <= 1e-11, (k, relerr(a[k], b[k]))
+
+
 def test_time_copy_leaves_the_state_unchanged():
     case = _tidal_small("mixed", order=4, nx=6, ny=4, nz=4)
     gpu = OceanModel(case["cfg"], case["h"], case["f"], case["taux"], case["tauy"])

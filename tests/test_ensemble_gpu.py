@@ -1,8 +1,10 @@
 """Uneven ensembles (C5 layout) on the GPU, through the C ABI.
 
-An ensemble steps all members with one persistent stage launch per LSRK stage; each member
-must end exactly where the same model stepped alone ends (the kernels do the same arithmetic
-per column), and an FP64 member must match the FP64 oracle to 1e-10 relative, the tolerance of
+An ensemble steps all members with one persistent stage launch per LSRK stage and one launch
+per barotropic pass over every member's tiles; each member must end where the same model stepped
+alone ends (both evaluate the same formulas per node; the ensemble's barotropic kernels are
+separately compiled instances, whose multiply-add fusion may differ, so they agree to 1e-11
+relative), and an FP64 member must match the FP64 oracle to 1e-10 relative, the tolerance of
 the single-model split-step test.
 """
 import dataclasses
@@ -56,9 +58,38 @@ def test_ensemble_members_equal_single_runs(precision):
         s = solo.download_state()
         assert g["t"] == s["t"]
         for k in ("eta", "HU", "HV", "eta_avg", "Hu", "Hv", "HT", "HS"):
-            assert relerr(g[k], s[k]) <= 1e-15, (c["name"], k)
+            assert relerr(g[k], s[k]) <= 1e-11, (c["name"], k, relerr(g[k], s[k]))
         solo.close()
     ens.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_ensemble_persistent_barotropic_agrees_with_per_pass_launches(monkeypatch, precision):
+    """The ensemble's barotropic step as one cooperative launch over every member's tiles
+    (DRIFTER_B200_BARO_PERSISTENT=1) agrees with the per-pass launches to rounding: the same
+    formulas per node, in kernels the compiler may contract differently."""
+    cases = _members(precision, SIZES)
+    per = Ensemble(cases)
+    for m, c in zip(per.members, cases):
+        m.upload_state(c["q"], c["eta"])
+    dts = [c["dt"] for c in cases]
+    per.step(dts, 20, 3)
+    monkeypatch.setenv("DRIFTER_B200_BARO_PERSISTENT", "1")
+    pers = Ensemble(cases)
+    for m, c in zip(pers.members, cases):
+        m.upload_state(c["q"], c["eta"])
+    pers.step(dts, 20, 0)
+    before = launch_count()
+    pers.step(dts, 20, 3)
+    pers.sync()
+    assert launch_count() - before == 3 * 6
+    for ma, mb in zip(pers.members, per.members):
+        a, b = ma.download_state(), mb.download_state()
+        assert a["t"] == b["t"]
+        for k in ("eta", "HU", "HV", "eta_avg", "Hu", "Hv", "HT", "HS"):
+            assert relerr(a[k], b[k]) <= 1e-11, (k, relerr(a[k], b[k]))
+    pers.close()
+    per.close()
 
 
 def test_ensemble_fp64_member_matches_oracle():
