@@ -1807,6 +1807,7 @@ int drf_pcg_solve(drf_bz *h, const double *bh, double *xh, double tol, int maxit
         if (iters) *iters = it;
         if (relres) *relres = sc[S_BB] > 0 ? std::sqrt(sc[S_RR] / sc[S_BB]) : 0.0;
         if (ms) *ms = t;
+        if (kind == 3) cnn_check(cnn_net(h->cnn), h->stream);
         DRF_CHECK(std::isfinite(sc[S_RR]), DRF_E_NONFINITE, "PCG diverged (non-finite residual)");
     });
 }

@@ -8,9 +8,11 @@
 // Channels (padded for the MMA shapes): 16 (9 used) -> 32 -> 32 -> 32 -> 16 (9 used); ReLU
 // after layers 1-3. Layouts: activations NHWC [b][h][w][c]; weights [co][tap][ci] (tap = dy*3+dx).
 #include <algorithm>
+#include <cuda.h>
 #include <cuda_bf16.h>
 
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <random>
@@ -166,6 +168,280 @@ __global__ void __launch_bounds__(256) conv3x3_kernel(int B, int H, int W, const
         __syncthreads();  // every warp is done with this buffer before it is refilled
     }
     asm volatile("cp.async.wait_all;" ::: "memory");
+}
+
+// ------------------------------------------------------------ tcgen05 (5th-generation) conv
+// The same conv3x3 as conv3x3_kernel as an implicit GEMM on Blackwell's tcgen05 tensor cores:
+// M = 128 output pixels (a 16 x 8 tile), N = COUT, K = 9 taps x CIN in steps of 16. Operands
+// are read by the tensor core from shared memory through matrix descriptors; the FP32
+// accumulator lives in tensor memory (TMEM) and is read back with tcgen05.ld for the epilogue.
+//
+// Shared-memory operand layouts (K-major, no swizzle: "core matrices" of 8 rows x 16 bytes,
+// the 8 rows 16 bytes apart):
+//  * input halo, 18 x 10 pixels, planar by 8-channel chunk: [c8][pixel][8 channels]. For tap
+//    (dy, dx) the A rows of output row r are halo pixels (r + dy) * 10 + dx + 0..7, consecutive,
+//    so the 16 eight-row groups are 10 pixels (160 B) apart (the stride byte offset) and the
+//    two channel chunks of one K step a plane apart (the leading byte offset);
+//  * weights [tap][c8][co][8 channels]: eight-row groups of output channels 128 B apart, the
+//    two chunks of a K step COUT x 16 B apart.
+// Persistent CTAs of 4 warps walk tiles; per tile one thread issues the 9 x CIN/16 MMAs into
+// one of two TMEM accumulators and commits them to an mbarrier, while all threads write the
+// previous tile from the other accumulator. Halos rotate through three buffers: the next tile's
+// halo is requested (cp.async) at the start of an iteration, a whole iteration before its MMAs.
+constexpr int TCH = 16, TCW = 8;  // tile rows x pixels per row (M = 128)
+
+__device__ __forceinline__ uint32_t sh_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// shared-memory matrix descriptor: start address, leading and stride byte offsets (all >> 4),
+// descriptor version 1 (bits 46-47), base offset 0, no swizzle (layout type 0, bits 61-63)
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+// instruction descriptor of kind::f16: D F32 (bits 4-5 = 1), A and B BF16 (bits 7-9, 10-12 = 1),
+// both K-major (bits 15, 16 = 0), N >> 3 in bits 17-22, M >> 4 in bits 24-28
+template <int M, int N>
+constexpr uint32_t umma_idesc_bf16() {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+__device__ __forceinline__ void umma_bf16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                          uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+__device__ __forceinline__ void umma_commit(uint64_t *bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(sh_u32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+// 16 consecutive 32-bit TMEM columns of this thread's lane (warp w reads lanes 32w..32w+31)
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+        : "r"(taddr)
+        : "memory");
+}
+__device__ __forceinline__ void tmem_ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+template <int CIN, int COUT>
+struct TcConv {
+    static constexpr int C8 = CIN / 8, HP = TCH + 2, WP = TCW + 2, PLANE = HP * WP;
+    // one 8-channel plane of the halo as the tensor copy writes it ([HP][WP][8] bf16), its
+    // stride rounded up to 128 B (the alignment of a tensor copy's destination)
+    static constexpr uint32_t PLANE_TX = (uint32_t)PLANE * 16, PLANE_B = (PLANE_TX + 127) / 128 * 128;
+    static constexpr uint32_t HALO_B = (uint32_t)C8 * PLANE_B;  // one halo stage
+    static constexpr uint32_t W_B = 9u * C8 * COUT * 16;
+    static constexpr int NS = 3;  // halo stages
+    static constexpr int NA = 4;  // TMEM accumulators
+    static constexpr uint32_t NCOL = NA * COUT <= 32 ? 32 : (NA * COUT <= 64 ? 64 : 128);
+    // mbarriers: full[NS], empty[NS], acc_full[NA], acc_empty[NA]; then the TMEM address, an
+    // abort flag and the bias
+    static constexpr uint32_t BAR_B = 8u * (2 * NS + 2 * NA) + 16 + 4 * COUT;
+    // at least 46 KB per CTA, so that at most 4 CTAs share an SM and their TMEM (4 x 128 of
+    // 512 columns) is always free: a CTA never waits in tcgen05.alloc
+    static constexpr size_t NEED = NS * (size_t)HALO_B + W_B + BAR_B;
+    static constexpr size_t SMEM = NEED < 47104 ? 47104 : NEED;
+    static constexpr int THREADS = 192;  // warp 0 producer, warp 1 MMA issuer, warps 2-5 epilogue
+};
+
+// bounded wait on an mbarrier phase that also gives up when another role set the abort flag
+// (abort may be null: then only the bound ends it)
+__device__ __forceinline__ bool tc_wait(uint64_t *bar, uint32_t parity, volatile int *abort) {
+    const uint32_t a = sh_u32(bar);
+    for (long it = 0; it < (1L << 22); ++it) {
+        uint32_t done;
+        asm volatile(
+            "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if ((it & 255) == 255 && abort && *abort) return false;
+    }
+    return false;
+}
+__device__ __forceinline__ void tc_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(sh_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void tc_bar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(sh_u32(bar)), "r"(count) : "memory");
+}
+
+// Warp-specialised persistent CTA; every CTA walks tiles blockIdx.x, blockIdx.x + gridDim.x, ...
+// (local index k):
+//  * warp 0, one lane, stages halo k into stage k % NS (after the MMAs of tile k - NS released
+//    it) with one tensor copy (TMA) per 8-channel plane; the copies complete full[stage] by
+//    their byte count, and pixels outside the image arrive as zeros;
+//  * warp 1, one lane, waits on full[stage] and on acc_empty[k % NA], issues the tile's MMAs
+//    into accumulator k % NA and commits them to empty[stage] and acc_full[k % NA];
+//  * warps 2-5 wait on acc_full, read the accumulator (warp w reads TMEM lanes 32 (w % 4) ..),
+//    release it on acc_empty (one arrival per warp) and write the tile.
+template <int CIN, int COUT, bool RELU, bool OUTF32>
+__global__ void __launch_bounds__(192) conv3x3_tc_kernel(int B, int H, int W, const __grid_constant__ CUtensorMap xmap,
+                                                         const bf16 *__restrict__ Wt,
+                                                         const float *__restrict__ bias, void *Yv, int *err) {
+    using P = TcConv<CIN, COUT>;
+    constexpr int C8 = P::C8, WP = P::WP, NS = P::NS, NA = P::NA;
+    constexpr uint32_t IDESC = umma_idesc_bf16<128, COUT>();
+    static_assert(CIN % 16 == 0 && COUT % 16 == 0 && COUT <= 32, "tcgen05 conv shape");
+    extern __shared__ __align__(128) unsigned char tc_smem[];
+    unsigned char *halo = tc_smem;                   // [NS][C8][PLANE_B]
+    unsigned char *wsm = tc_smem + NS * P::HALO_B;  // [9][C8][COUT][16 B]
+    uint64_t *full = reinterpret_cast<uint64_t *>(wsm + P::W_B);
+    uint64_t *empty = full + NS, *acc_full = empty + NS, *acc_empty = acc_full + NA;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(acc_empty + NA);
+    volatile int *abort = reinterpret_cast<volatile int *>(tmem_slot + 1);
+    float *sbias = reinterpret_cast<float *>(tmem_slot + 4);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ntx = (W + TCW - 1) / TCW, nty = (H + TCH - 1) / TCH;
+    const int64_t per_img = (int64_t)ntx * nty, ntiles = per_img * B;
+    const int nloc = blockIdx.x < ntiles ? (int)((ntiles - 1 - blockIdx.x) / gridDim.x) + 1 : 0;
+
+    // the layer's weights (and bias) once per CTA, by every thread, visible to the async proxy
+    for (int i = threadIdx.x; i < COUT * 9 * C8; i += blockDim.x) {
+        const int co = i / (9 * C8), r = i % (9 * C8), tap = r / C8, c8 = r % C8;
+        cp_async16(wsm + ((size_t)(tap * C8 + c8) * COUT + co) * 16, Wt + (size_t)co * 9 * CIN + tap * CIN + 8 * c8,
+                   16);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    for (int i = threadIdx.x; i < COUT; i += blockDim.x) sbias[i] = bias ? bias[i] : 0.f;
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < NS; ++i) { tc_bar_init(&full[i], 1); tc_bar_init(&empty[i], 1); }
+        for (int i = 0; i < NA; ++i) { tc_bar_init(&acc_full[i], 1); tc_bar_init(&acc_empty[i], 4); }
+        *abort = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(sh_u32(tmem_slot)),
+                     "r"(P::NCOL)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+    bool ok = true;
+
+    if (warp == 0) {
+        // ---- producer: halo k into stage k % NS by C8 tensor copies, one per channel plane
+        if (lane == 0) {
+            const uint64_t map = reinterpret_cast<uint64_t>(&xmap);
+            for (int k = 0; k < nloc && ok; ++k) {
+                const int s = k % NS;
+                if (k >= NS) ok = tc_wait(&empty[s], (uint32_t)(((k / NS) - 1) & 1), abort);
+                if (!ok) break;
+                const int64_t tile = blockIdx.x + (int64_t)k * gridDim.x;
+                const int b = (int)(tile / per_img), r2 = (int)(tile % per_img);
+                const int h0 = (r2 / ntx) * TCH, w0 = (r2 % ntx) * TCW;
+                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(sh_u32(&full[s])),
+                             "r"((uint32_t)(C8 * P::PLANE_TX))
+                             : "memory");
+#pragma unroll
+                for (int c8 = 0; c8 < C8; ++c8)
+                    asm volatile(
+                        "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+                        " [%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(sh_u32(halo + s * P::HALO_B + c8 * P::PLANE_B)),
+                        "l"(map), "r"(0), "r"(c8), "r"(w0 - 1), "r"(h0 - 1), "r"(b), "r"(sh_u32(&full[s]))
+                        : "memory");
+            }
+        }
+        __syncwarp();
+    } else if (warp == 1) {
+        // ---- MMA issuer
+        if (lane == 0) {
+            const uint32_t wb = sh_u32(wsm);
+            for (int k = 0; k < nloc && ok; ++k) {
+                const int s = k % NS, a = k % NA;
+                ok = tc_wait(&full[s], (uint32_t)((k / NS) & 1), abort);
+                if (ok && k >= NA) ok = tc_wait(&acc_empty[a], (uint32_t)(((k / NA) - 1) & 1), abort);
+                if (!ok) break;
+                tc_fence_after();
+                const uint32_t hb = sh_u32(halo + s * P::HALO_B), d = tmem + (uint32_t)(a * COUT);
+#pragma unroll
+                for (int tap = 0; tap < 9; ++tap) {
+                    const int dy = tap / 3, dx = tap % 3;
+#pragma unroll
+                    for (int ks = 0; ks < C8 / 2; ++ks) {
+                        const uint64_t ad = umma_desc(hb + (uint32_t)(2 * ks * P::PLANE_B + (dy * WP + dx) * 16),
+                                                      P::PLANE_B, WP * 16);
+                        const uint64_t bd = umma_desc(wb + (uint32_t)((tap * C8 + 2 * ks) * COUT * 16), COUT * 16, 128);
+                        umma_bf16(d, ad, bd, IDESC, (tap | ks) != 0);
+                    }
+                }
+                umma_commit(&empty[s]);
+                umma_commit(&acc_full[a]);
+            }
+            // nothing may be in flight when TMEM is freed: the last commit's phase, waited for
+            // even after an abort (bounded)
+            if (nloc > 0) tc_wait(&acc_full[(nloc - 1) % NA], (uint32_t)(((nloc - 1) / NA) & 1), nullptr);
+        }
+        __syncwarp();
+    } else {
+        // ---- epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31 = tile pixels m
+        const int q = warp & 3, m = 32 * q + lane;
+        for (int k = 0; k < nloc && ok; ++k) {
+            const int a = k % NA;
+            ok = tc_wait(&acc_full[a], (uint32_t)((k / NA) & 1), abort);
+            if (__any_sync(0xffffffffu, !ok)) { ok = false; break; }
+            tc_fence_after();
+            float f[COUT];
+#pragma unroll
+            for (int c0 = 0; c0 < COUT; c0 += 16) {
+                uint32_t v[16];
+                tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(a * COUT + c0), v);
+                tmem_ld_wait();
+#pragma unroll
+                for (int j = 0; j < 16; ++j) f[c0 + j] = __uint_as_float(v[j]);
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) tc_arrive(&acc_empty[a]);  // the accumulator may be overwritten
+            const int64_t tile = blockIdx.x + (int64_t)k * gridDim.x;
+            const int b = (int)(tile / per_img), r2 = (int)(tile % per_img);
+            const int h = (r2 / ntx) * TCH + m / TCW, w = (r2 % ntx) * TCW + m % TCW;
+            if (h >= H || w >= W) continue;
+            const size_t o = (((size_t)b * H + h) * W + w) * COUT;
+#pragma unroll
+            for (int j = 0; j < COUT; ++j) {
+                f[j] += sbias[j];
+                if (RELU) f[j] = fmaxf(f[j], 0.f);
+            }
+            if (OUTF32) {
+                float4 *Y = reinterpret_cast<float4 *>(static_cast<float *>(Yv) + o);
+#pragma unroll
+                for (int j = 0; j < COUT / 4; ++j) Y[j] = make_float4(f[4 * j], f[4 * j + 1], f[4 * j + 2], f[4 * j + 3]);
+            } else {
+                uint32_t p[COUT / 2];
+#pragma unroll
+                for (int j = 0; j < COUT / 2; ++j) {
+                    __nv_bfloat162 t2 = __floats2bfloat162_rn(f[2 * j], f[2 * j + 1]);
+                    p[j] = *reinterpret_cast<uint32_t *>(&t2);
+                }
+                uint4 *Y = reinterpret_cast<uint4 *>(static_cast<bf16 *>(Yv) + o);
+#pragma unroll
+                for (int j = 0; j < COUT / 8; ++j) Y[j] = make_uint4(p[4 * j], p[4 * j + 1], p[4 * j + 2], p[4 * j + 3]);
+            }
+        }
+    }
+    if (!ok) {
+        *abort = 1;
+        atomicExch(err, DRF_E_TIMEOUT);
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(P::NCOL) : "memory");
+    }
 }
 
 // dW partials of one layer for one CTA tile: dW[co][tap][ci] += dZ[p][co] * A[p + shift][ci],
@@ -352,9 +628,80 @@ __global__ void unpack_kernel(int n, const float *Y, const double *rr_ptr, doubl
 
 inline unsigned nb(int64_t n, int bs = 256) { return (unsigned)((n + bs - 1) / bs); }
 
+// the tcgen05 conv: persistent, as many CTAs as are resident (at most one per tile)
+// Tensor map of an NHWC bf16 activation tensor for the conv's halo copies: dimensions
+// (8 channels, CIN/8 channel chunks, W, H, B), box (8, 1, TCW + 2, TCH + 2, 1): one copy brings
+// one 8-channel plane of a tile's halo; coordinates outside the image read zeros.
+template <int CIN>
+CUtensorMap conv_halo_map(const bf16 *X, int B, int H, int W) {
+    CUtensorMap m;
+    const cuuint64_t dims[5] = {8, (cuuint64_t)(CIN / 8), (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)B};
+    const cuuint64_t strides[4] = {16, (cuuint64_t)CIN * 2, (cuuint64_t)W * CIN * 2, (cuuint64_t)H * W * CIN * 2};
+    const cuuint32_t box[5] = {8, 1, TCW + 2, TCH + 2, 1};
+    const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+    // the driver's encoder, looked up through the runtime (the library does not link the driver)
+    using Encode = decltype(&cuTensorMapEncodeTiled);
+    static Encode encode = [] {
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        DRF_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+        DRF_CHECK(fn && q == cudaDriverEntryPointSuccess, DRF_E_CUDA, "cuTensorMapEncodeTiled not available");
+        return reinterpret_cast<Encode>(fn);
+    }();
+    const CUresult r = encode(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<bf16 *>(X), dims, strides, box, estr,
+                              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    DRF_CHECK(r == CUDA_SUCCESS, DRF_E_CUDA, "cuTensorMapEncodeTiled failed for the conv input");
+    return m;
+}
+
+template <int CIN, int COUT, bool RELU, bool OUTF32>
+void conv_tc(cudaStream_t s, int B, int H, int W, const bf16 *X, const bf16 *Wt, const float *bias, void *Y,
+             int *err) {
+    constexpr size_t smem = TcConv<CIN, COUT>::SMEM;
+    static int resident = 0;
+    if (!resident) {
+        int dev = 0, nsm = 0, smpm = 0, rsv = 0;
+        DRF_CUDA(cudaGetDevice(&dev));
+        DRF_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+        DRF_CUDA(cudaDeviceGetAttribute(&smpm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+        DRF_CUDA(cudaDeviceGetAttribute(&rsv, cudaDevAttrReservedSharedMemoryPerBlock, dev));
+        DRF_CUDA(cudaFuncSetAttribute(conv3x3_tc_kernel<CIN, COUT, RELU, OUTF32>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        // CTAs per SM by shared memory (the limiting resource), at most 512 TMEM columns' worth;
+        // DRIFTER_B200_CONV_CTAS_PER_SM lowers it
+        int per = smpm / (int)(smem + rsv);
+        per = std::max(1, std::min(per, 512 / (int)TcConv<CIN, COUT>::NCOL));
+        if (const char *e = std::getenv("DRIFTER_B200_CONV_CTAS_PER_SM"))
+            per = std::max(1, std::min(per, std::atoi(e)));
+        resident = nsm * per;
+    }
+    const int64_t ntiles = (int64_t)((W + TCW - 1) / TCW) * ((H + TCH - 1) / TCH) * B;
+    const unsigned grid = (unsigned)std::min<int64_t>(ntiles, resident);
+    DRF_CHECK(reinterpret_cast<uintptr_t>(X) % 16 == 0, DRF_E_INVALID, "conv input not 16-byte aligned");
+    const CUtensorMap xmap = conv_halo_map<CIN>(X, B, H, W);
+    conv3x3_tc_kernel<CIN, COUT, RELU, OUTF32><<<grid, TcConv<CIN, COUT>::THREADS, smem, s>>>(B, H, W, xmap, Wt, bias,
+                                                                                          Y, err);
+    DRF_LAUNCHED();
+}
+
+// DRIFTER_B200_CNN_MMA=tcgen05 selects the tcgen05 conv; the default is the warp-level mma.sync
+// kernel, which is the faster of the two on the C4 network (32 channels: N = 32 per MMA)
+inline bool use_tcgen05() {
+    static const int v = [] {
+        const char *e = std::getenv("DRIFTER_B200_CNN_MMA");
+        return (e && std::strcmp(e, "tcgen05") == 0) ? 1 : 0;
+    }();
+    return v != 0;
+}
+
 template <int CIN, int COUT, bool RELU, bool OUTF32>
 void conv(cudaStream_t s, int B, int H, int W, const bf16 *X, const bf16 *Wt, const float *bias,
-          void *Y) {
+          void *Y, int *err) {
+    if (use_tcgen05()) {
+        conv_tc<CIN, COUT, RELU, OUTF32>(s, B, H, W, X, Wt, bias, Y, err);
+        return;
+    }
     // persistent grid: as many CTAs as are resident at once (the weights are staged once each)
     constexpr size_t smem = conv_smem_bytes<CIN, COUT>();
     static int resident = 0;
@@ -374,20 +721,21 @@ void conv(cudaStream_t s, int B, int H, int W, const bf16 *X, const bf16 *Wt, co
 }
 
 void conv_layer(cudaStream_t s, int l, int B, int H, int W, const bf16 *X, const bf16 *Wt,
-                const float *bias, void *Y) {
+                const float *bias, void *Y, int *err) {
     switch (l) {
-    case 0: conv<16, 32, true, false>(s, B, H, W, X, Wt, bias, Y); break;
-    case 1: conv<32, 32, true, false>(s, B, H, W, X, Wt, bias, Y); break;
-    case 2: conv<32, 32, true, false>(s, B, H, W, X, Wt, bias, Y); break;
-    default: conv<32, 16, false, true>(s, B, H, W, X, Wt, bias, Y); break;
+    case 0: conv<16, 32, true, false>(s, B, H, W, X, Wt, bias, Y, err); break;
+    case 1: conv<32, 32, true, false>(s, B, H, W, X, Wt, bias, Y, err); break;
+    case 2: conv<32, 32, true, false>(s, B, H, W, X, Wt, bias, Y, err); break;
+    default: conv<32, 16, false, true>(s, B, H, W, X, Wt, bias, Y, err); break;
     }
 }
 
 // input-gradient conv of layer l (l = 1..3): dX (CIN_l channels, f32) = conv(dZ_l, Wflip_l)
-void conv_back(cudaStream_t s, int l, int B, int H, int W, const bf16 *dZb, const bf16 *Wf, float *dX) {
+void conv_back(cudaStream_t s, int l, int B, int H, int W, const bf16 *dZb, const bf16 *Wf, float *dX,
+               int *err) {
     switch (l) {
-    case 3: conv<16, 32, false, true>(s, B, H, W, dZb, Wf, nullptr, dX); break;
-    default: conv<32, 32, false, true>(s, B, H, W, dZb, Wf, nullptr, dX); break;
+    case 3: conv<16, 32, false, true>(s, B, H, W, dZb, Wf, nullptr, dX, err); break;
+    default: conv<32, 32, false, true>(s, B, H, W, dZb, Wf, nullptr, dX, err); break;
     }
 }
 
@@ -410,6 +758,7 @@ struct CnnNet {
     cudaStream_t stream = nullptr, own = nullptr;
     // FP32 masters (packed like the oracle: per layer W then b), Adam moments, gradients
     DevBuf<float> wm, am, av, grad;
+    DevBuf<int> status;  // device status word (DRF_E_TIMEOUT when a bounded wait gave up)
     DevBuf<bf16> wb, wflip;
     size_t off_w[4], off_b[4], off_wb[4], nparam = 0, nwb = 0;
     int64_t adam_t = 0;
@@ -438,6 +787,8 @@ struct CnnNet {
         for (auto *b : {&wm, &am, &av, &grad}) b->alloc(nparam);
         wb.alloc(nwb);
         wflip.alloc(nwb);
+        status.alloc(1);
+        DRF_CUDA(cudaMemset(status.p, 0, sizeof(int)));
         DRF_CUDA(cudaMemset(am.p, 0, nparam * 4));
         DRF_CUDA(cudaMemset(av.p, 0, nparam * 4));
         DRF_CUDA(cudaStreamCreateWithFlags(&own, cudaStreamNonBlocking));
@@ -467,8 +818,8 @@ struct CnnNet {
     // forward from act[0]; output f32 in `out`
     void forward(int B, int H, int W) {
         for (int l = 0; l < 3; ++l)
-            conv_layer(stream, l, B, H, W, act[l].p, wb.p + off_wb[l], wm.p + off_b[l], act[l + 1].p);
-        conv_layer(stream, 3, B, H, W, act[3].p, wb.p + off_wb[3], wm.p + off_b[3], out.p);
+            conv_layer(stream, l, B, H, W, act[l].p, wb.p + off_wb[l], wm.p + off_b[l], act[l + 1].p, status.p);
+        conv_layer(stream, 3, B, H, W, act[3].p, wb.p + off_wb[3], wm.p + off_b[3], out.p, status.p);
     }
     // backward of the mean-square loss against tgt; fills grad; returns device loss partials
     void backward(int B, int H, int W, const float *tgt) {
@@ -487,7 +838,7 @@ struct CnnNet {
             // dZ_l in bf16 for the input-gradient conv
             f32_to_bf16_kernel<<<nb(pix * CH[l + 1]), 256, 0, stream>>>(pix * CH[l + 1], dZ, dzb.p);
             DRF_LAUNCHED();
-            conv_back(stream, l, B, H, W, dzb.p, wflip.p + off_wb[l], dx.p);
+            conv_back(stream, l, B, H, W, dzb.p, wflip.p + off_wb[l], dx.p, status.p);
             // dZ_{l-1} = dX * relu'(Z_{l-1}) into dz (the previous dZ is no longer read)
             relu_back_kernel<<<nb(pix * CH[l]), 256, 0, stream>>>(pix * CH[l], dx.p, act[l].p, dz.p, dzb.p);
             DRF_LAUNCHED();
@@ -522,6 +873,16 @@ void cnn_precondition(CnnNet *net, cudaStream_t s, int n, const double *r, const
 }
 
 void cnn_prepare(CnnNet *net, int n) { net->ensure((int64_t)(n + 1) * (n + 1)); }
+
+void cnn_check(CnnNet *net, cudaStream_t s) {
+    int st = 0;
+    DRF_CUDA(cudaMemcpyAsync(&st, net->status.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    DRF_CUDA(cudaStreamSynchronize(s));
+    if (st != 0) {
+        DRF_CUDA(cudaMemsetAsync(net->status.p, 0, sizeof(int), s));
+        throw Error(st, "a device-side wait of the network gave up (status " + std::to_string(st) + ")");
+    }
+}
 
 }  // namespace drf
 
@@ -625,7 +986,7 @@ int drf_cnn_forward_backward(drf_cnn *h, int B, int H, int W, const double *X, c
                 for (size_t i = 0; i < g.size(); ++i) grad[i] = g[i];
             }
         }
-        DRF_CUDA(cudaStreamSynchronize(n.stream));
+        cnn_check(&n, n.stream);
     });
 }
 
@@ -688,7 +1049,7 @@ int drf_cnn_train(drf_cnn *h, int steps, int batch, int crop, double lr, uint64_
                 ++nacc;
             }
         }
-        DRF_CUDA(cudaStreamSynchronize(n.stream));
+        cnn_check(&n, n.stream);
         if (loss) *loss = nacc ? acc / nacc : 0.0;
     });
 }

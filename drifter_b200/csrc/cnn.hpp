@@ -15,4 +15,6 @@ void cnn_prepare(CnnNet *net, int n);
 // (the Jacobi base and the correction in one pass)
 void cnn_precondition(CnnNet *net, cudaStream_t s, int n, const double *r, const double *rr_dev,
                       double out_scale, double *z, int add, const int *stop, const double *jac_diag = nullptr);
+// surfaces (and clears) the network's device status word: throws when a bounded wait gave up
+void cnn_check(CnnNet *net, cudaStream_t s);
 }  // namespace drf

@@ -46,6 +46,40 @@ def test_gradient_matches_reference():
     assert rl2(g, go) < 2e-2
 
 
+_TC_CHILD = """
+import sys, numpy as np
+from drifter_b200.cnn import CNN
+rng = np.random.default_rng(5)
+X = np.zeros((2, 19, 37, 16)); X[..., :9] = rng.standard_normal((2, 19, 37, 9))
+T = np.zeros((2, 19, 37, 16)); T[..., :9] = rng.standard_normal((2, 19, 37, 9))
+Y, g, loss = CNN(seed=6).forward_backward(X, T)
+np.savez(sys.argv[1], Y=Y, g=g, loss=loss)
+"""
+
+
+def test_tcgen05_conv_equals_mma_sync_conv(tmp_path):
+    """DRIFTER_B200_CNN_MMA=tcgen05 runs every conv of the network (forward and input-gradient)
+    on the tcgen05 kernel: TMA halo copies, MMAs from shared-memory descriptors into TMEM,
+    tcgen05.ld epilogue. Both kernels add the same FP32 products of each 16-channel step in the
+    same tap order, so the forward output, the loss and the gradient are bit-identical to the
+    mma.sync kernel's (ragged 19 x 37 images, batch 2). The choice is read once per process:
+    each form runs in its own child process."""
+    import os
+    import subprocess
+    import sys
+
+    out = {}
+    for form in ("sync", "tcgen05"):
+        env = dict(os.environ, DRIFTER_B200_CNN_MMA=form)
+        path = tmp_path / f"{form}.npz"
+        subprocess.run([sys.executable, "-c", _TC_CHILD, str(path)], env=env, check=True, timeout=600)
+        out[form] = np.load(path)
+    a, b = out["sync"], out["tcgen05"]
+    assert np.isfinite(a["Y"]).all() and np.abs(a["Y"]).max() > 0
+    for k in ("Y", "g", "loss"):
+        assert np.array_equal(a[k], b[k]), k
+
+
 def test_superpixel_layout():
     # control point (gi, gj) -> superpixel (I, J) = (gi // 3, gj // 3), channel gi % 3 + 3 (gj % 3)
     # (the layout of the library's pack/unpack kernels)
