@@ -668,12 +668,13 @@ void conv_tc(cudaStream_t s, int B, int H, int W, const bf16 *X, const bf16 *Wt,
         DRF_CUDA(cudaDeviceGetAttribute(&rsv, cudaDevAttrReservedSharedMemoryPerBlock, dev));
         DRF_CUDA(cudaFuncSetAttribute(conv3x3_tc_kernel<CIN, COUT, RELU, OUTF32>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        // CTAs per SM by shared memory (the limiting resource), at most 512 TMEM columns' worth;
-        // DRIFTER_B200_CONV_CTAS_PER_SM lowers it
-        int per = smpm / (int)(smem + rsv);
-        per = std::max(1, std::min(per, 512 / (int)TcConv<CIN, COUT>::NCOL));
+        // CTAs per SM: 2 (the fastest of 1-4 measured at C4), fewer if shared memory or the 512
+        // TMEM columns allow fewer; DRIFTER_B200_CONV_CTAS_PER_SM sets it within those limits
+        int per = std::min(smpm / (int)(smem + rsv), 512 / (int)TcConv<CIN, COUT>::NCOL);
+        const int cap = per;
+        per = std::max(1, std::min(per, 2));
         if (const char *e = std::getenv("DRIFTER_B200_CONV_CTAS_PER_SM"))
-            per = std::max(1, std::min(per, std::atoi(e)));
+            per = std::max(1, std::min(cap, std::atoi(e)));
         resident = nsm * per;
     }
     const int64_t ntiles = (int64_t)((W + TCW - 1) / TCW) * ((H + TCH - 1) / TCH) * B;
