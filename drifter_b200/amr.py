@@ -24,11 +24,45 @@ def _sigs():
         "drf_amr_upload": [vp, dp], "drf_amr_download": [vp, dp],
         "drf_amr_step": [vp, C.c_int, C.c_int, dp, C.c_double, C.c_int],
         "drf_amr_time_rhs": [vp, C.c_int, C.c_int, dp, C.c_int, dp, dp],
+        "drf_amr_build_mesh": [C.c_int, C.c_int, vp, vp, vp, C.c_double, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp,
+                               vp, vp, vp],
     }
     for k, a in sigs.items():
         getattr(L, k).argtypes = a
         getattr(L, k).restype = C.c_int
     return L
+
+
+def build_mesh(lx, ly, lz, L: float = 1.0) -> dict:
+    """Elements and face connections of a column-wise directionally refined mesh from the
+    native builder (drf_amr_build_mesh, the producer of OctreeAdapter::build_face_connections'
+    tables, src/mesh/octree_adapter.cpp:369). lx, ly, lz: (ny, nx) per-column levels. Returns
+    the dict of configs.amr_mesh (n_elem, level, box, conf, bnd, ifaces, col_levels) plus the
+    interfaces as the arrays drf_amr_create takes ("if_arrays")."""
+    Lb = _sigs()
+    lx, ly, lz = (np.ascontiguousarray(a, np.int32) for a in (lx, ly, lz))
+    ny, nx = lx.shape
+    ptr = lambda a: a.ctypes.data_as(C.c_void_p) if a is not None else None
+    cnt = [C.c_int64() for _ in range(4)]
+    args = [nx, ny, ptr(lx), ptr(ly), ptr(lz), float(L)] + [C.c_void_p(C.addressof(c)) for c in cnt]
+    check(Lb.drf_amr_build_mesh(*args, *([None] * 9)))
+    ne, nc, nb, ni = (c.value for c in cnt)
+    level = np.zeros((ne, 3), np.int32)
+    box = np.zeros((ne, 6))
+    conf = np.zeros((nc, 4), np.int64)
+    bnd = np.zeros((nb, 2), np.int64)
+    t = np.zeros(ni, np.int32)
+    ce = np.zeros(ni, np.int64)
+    cf = np.zeros(ni, np.int32)
+    fe = np.zeros((ni, 4), np.int64)
+    ff = np.zeros((ni, 4), np.int32)
+    check(Lb.drf_amr_build_mesh(*args, ptr(level), ptr(box), ptr(conf), ptr(bnd), ptr(t), ptr(ce), ptr(cf),
+                                ptr(fe), ptr(ff)))
+    ifaces = [(int(t[i]), int(ce[i]), int(cf[i]), [int(v) for v in fe[i] if v >= 0],
+               [int(v) for v in ff[i] if v >= 0]) for i in range(ni)]
+    col_levels = np.stack([lx.ravel(), ly.ravel(), lz.ravel()], 1).astype(np.int64)
+    return dict(n_elem=ne, level=level.astype(np.int64), box=box, conf=conf, bnd=bnd, ifaces=ifaces,
+                col_levels=col_levels, if_arrays=(t, ce, cf, fe, ff))
 
 
 class DG3DIntegration:
@@ -41,17 +75,21 @@ class DG3DIntegration:
         self.nd = (order + 1) ** 3
         conf = np.ascontiguousarray(mesh["conf"], np.int64).reshape(-1, 4)
         bnd = np.ascontiguousarray(mesh["bnd"], np.int64).reshape(-1, 2)
-        ifs = mesh["ifaces"]
-        n = len(ifs)
-        t = np.zeros(n, np.int32)
-        ce = np.zeros(n, np.int64)
-        cf = np.zeros(n, np.int32)
-        fe = -np.ones((n, 4), np.int64)
-        ff = -np.ones((n, 4), np.int32)
-        for i, (ty, e, f, fes, ffs) in enumerate(ifs):
-            t[i], ce[i], cf[i] = ty, e, f
-            fe[i, :len(fes)] = fes
-            ff[i, :len(ffs)] = ffs
+        if "if_arrays" in mesh:  # the native builder's arrays
+            t, ce, cf, fe, ff = (np.ascontiguousarray(a) for a in mesh["if_arrays"])
+            n = len(t)
+        else:
+            ifs = mesh["ifaces"]
+            n = len(ifs)
+            t = np.zeros(n, np.int32)
+            ce = np.zeros(n, np.int64)
+            cf = np.zeros(n, np.int32)
+            fe = -np.ones((n, 4), np.int64)
+            ff = -np.ones((n, 4), np.int32)
+            for i, (ty, e, f, fes, ffs) in enumerate(ifs):
+                t[i], ce[i], cf[i] = ty, e, f
+                fe[i, :len(fes)] = fes
+                ff[i, :len(ffs)] = ffs
         self._keep = (conf, bnd, t, ce, cf, fe, ff)
         ptr = lambda a: a.ctypes.data_as(C.c_void_p)
         h = C.c_void_p()

@@ -354,8 +354,10 @@ def c3(nb: int = 256, order: int = 3, seed: int = SEED, hurst: float = 0.7):
     """C3: directional AMR (4 levels per horizontal direction, 2 vertically) refined towards a
     seeded fBm (Hurst 0.7) coastline on an nb x nb base grid, N=3; a scalar field advected
     with a constant velocity (the scalar conservation law of DG3DIntegration::compute_rhs)."""
+    from .amr import build_mesh  # the native builder; amr_mesh above is its Python statement
+
     lx, ly, lz = c3_levels(nb, hurst, seed)
-    mesh = amr_mesh(lx, ly, lz)
+    mesh = build_mesh(lx, ly, lz)
     npn = order + 1
     rng = np.random.default_rng(seed + 3)
     box = mesh["box"]

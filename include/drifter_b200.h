@@ -337,6 +337,25 @@ int drf_mortar_apply(drf_mortar *h, int flux_kind, const double *a, const double
 int drf_mortar_apply_device(drf_mortar *h, int flux_kind, const double *a, const double *d_U,
                             double *d_rhs);
 
+/* ------------------------------------------------------------------ AMR mesh and faces
+ * The face tables of a column-wise directionally refined mesh, as
+ * OctreeAdapter::build_face_connections (src/mesh/octree_adapter.cpp:369) types them with
+ * get_connection_type (include/dg/face_connection.hpp:110): nx x ny base columns over an
+ * L x L basin (depth 1), column c = ix + nx iy split into 2^lx[c] x 2^ly[c] x 2^lz[c] cells
+ * (levels 0..10, neighbouring columns 2:1 balanced). Outputs, in the order drf_amr_create takes
+ * them:
+ *  - elements grouped by level tuple; elem_level n_elem x 3, elem_box n_elem x (lo xyz, hi xyz);
+ *  - conf n_conf x (e1, f1, e2, f2) conforming pairs and bnd n_bnd x (e, f) boundary faces;
+ *  - n_if non-conforming interfaces grouped by type (1 Fine2x1, 2 Fine1x2, 5 Fine2x2): the
+ *    coarse element and face, and up to 4 fine elements and faces (-1 padded) in the sub-face
+ *    order of MortarSpace::compute_subface_bounds (src/dg/mortar.cpp:27).
+ * Face f has its normal along axis f / 2, positive when f is odd. Call with null array outputs
+ * to get the counts, then again with arrays of those sizes. Host-only (no device memory). */
+int drf_amr_build_mesh(int nx, int ny, const int *lx, const int *ly, const int *lz, double L, int64_t *n_elem,
+                       int64_t *n_conf, int64_t *n_bnd, int64_t *n_if, int *elem_level, double *elem_box,
+                       int64_t *conf, int64_t *bnd, int *if_type, int64_t *if_coarse_elem, int *if_coarse_face,
+                       int64_t *if_fine_elem, int *if_fine_face);
+
 /* ------------------------------------------------------------------ AMR scalar DG
  * DG3DIntegration::compute_rhs (src/dg/operators_3d.cpp:228) for u_t + div(a u) = 0 with a
  * constant velocity a on a directionally refined hexahedral mesh of one order N (1..5), in the
