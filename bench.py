@@ -49,6 +49,9 @@ def parse():
 
 
 def dist_init(n):
+    """One process per GPU (RANK / WORLD_SIZE / LOCAL_RANK from the launcher). The process group
+    is NCCL; DRIFTER_B200_DIST_BACKEND=gloo selects gloo (the CPU tests of this logic). Its
+    timeout is short, so ranks that wait for a rank that died end with an error."""
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local = int(os.environ.get("LOCAL_RANK", 0))
@@ -56,8 +59,8 @@ def dist_init(n):
         import datetime
 
         import torch.distributed as dist
-        backend = "nccl"
-        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+        backend = os.environ.get("DRIFTER_B200_DIST_BACKEND", "nccl")
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
     return rank, world, local
 
 
@@ -72,9 +75,17 @@ def max_over_ranks(x, world):
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def job_rate(units_per_rank, ms_local, world):
+    """Whole-job throughput: the units all ranks processed over the slowest rank's device time
+    (max over ranks). Returns (max ms, units per second)."""
+    ms_max = max_over_ranks(ms_local, world)
+    return ms_max, world * units_per_rank / (ms_max / 1e3)
 
 
 class ClockSampler:
@@ -383,9 +394,8 @@ def run_ours(args, rank, world, local):
     launches = launch_count() - l0
     ms = e0.elapsed_time(e1)
     ck = clocks.stop()
-    ms_max = max_over_ranks(ms, world)
+    ms_max, value = job_rate(ndof * 5 * args.steps, ms, world)
     ms_step = ms_max / args.steps
-    value = world * ndof * 5 * args.steps / (ms_max / 1e3)
 
     tuning = model.tuning()  # autotuned barotropic tile (chosen at the first step)
 
