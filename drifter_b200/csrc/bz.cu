@@ -772,12 +772,14 @@ __global__ void alpha_kernel(PcgCtl c, int nparts) {
 }
 
 // x += alpha p ; r -= alpha q ; partial r.r
-__global__ void __launch_bounds__(BS) xr_update_kernel(int64_t n, PcgCtl c, const double *p,
-                                                       const double *q, double *x, double *r) {
+__global__ void __launch_bounds__(BS) xr_update_kernel(int64_t n, PcgCtl c, const double *__restrict__ p,
+                                                       const double *__restrict__ q, double *__restrict__ x,
+                                                       double *__restrict__ r) {
     __shared__ double red[BS];
     if (*c.stop) return;
     const double a = c.sc[S_ALPHA];
     double s = 0.0;
+#pragma unroll 4
     for (int64_t t = blockIdx.x * (int64_t)BS + threadIdx.x; t < n; t += (int64_t)gridDim.x * BS) {
         x[t] += a * p[t];
         const double rn = r[t] - a * q[t];
@@ -794,6 +796,75 @@ __global__ void __launch_bounds__(BS) xr_update_kernel(int64_t n, PcgCtl c, cons
 }
 
 // rr = sum(part); convergence test; iteration count
+// x += alpha p, r -= alpha q and the Jacobi step z = r / d in one pass, with per-block partials
+// of r.r (part) and r.z (part + gridDim.x). Same grid-stride loop and block reduction as
+// xr_update_kernel followed by jacobi_diag_kernel and dot_kernel: the iterates are unchanged.
+__global__ void __launch_bounds__(BS) xr_jacobi_kernel(int64_t n, PcgCtl c, const double *__restrict__ p,
+                                                       const double *__restrict__ q, const double *__restrict__ d,
+                                                       double *__restrict__ x, double *__restrict__ r,
+                                                       double *__restrict__ z) {
+    __shared__ double red[2][BS];
+    if (*c.stop) return;
+    const double a = c.sc[S_ALPHA];
+    double s = 0.0, s2 = 0.0;
+    // distinct arrays (restrict): the loads of later elements need not wait for earlier stores
+#pragma unroll 4
+    for (int64_t t = blockIdx.x * (int64_t)BS + threadIdx.x; t < n; t += (int64_t)gridDim.x * BS) {
+        x[t] += a * p[t];
+        const double rn = r[t] - a * q[t];
+        r[t] = rn;
+        s += rn * rn;
+        const double zn = rn / d[t];
+        z[t] = zn;
+        s2 += rn * zn;
+    }
+    red[0][threadIdx.x] = s;
+    red[1][threadIdx.x] = s2;
+    __syncthreads();
+    for (int k = BS / 2; k > 0; k >>= 1) {
+        if (threadIdx.x < k) {
+            red[0][threadIdx.x] += red[0][threadIdx.x + k];
+            red[1][threadIdx.x] += red[1][threadIdx.x + k];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        c.part[blockIdx.x] = red[0][0];
+        c.part[gridDim.x + blockIdx.x] = red[1][0];
+    }
+}
+// conv_kernel and beta_kernel in one CTA: r.r from part[0, nparts) (convergence, iteration
+// count), r.z from part[zoff, zoff + nparts) (beta; zoff = 0 when z = r); beta is left as it was
+// once the iteration converged, as beta_kernel returns early then
+__global__ void conv_beta_kernel(PcgCtl c, int nparts, int zoff) {
+    __shared__ double red[2][BS];
+    if (*c.stop) return;
+    double s = 0.0, s2 = 0.0;
+    for (int i = threadIdx.x; i < nparts; i += BS) {
+        s += c.part[i];
+        s2 += c.part[zoff + i];
+    }
+    red[0][threadIdx.x] = s;
+    red[1][threadIdx.x] = s2;
+    __syncthreads();
+    for (int k = BS / 2; k > 0; k >>= 1) {
+        if (threadIdx.x < k) {
+            red[0][threadIdx.x] += red[0][threadIdx.x + k];
+            red[1][threadIdx.x] += red[1][threadIdx.x + k];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        c.sc[S_RR] = red[0][0];
+        *c.iters += 1;
+        if (!(red[0][0] > c.sc[S_TOL2] * c.sc[S_BB]) || *c.iters >= *c.maxit) {
+            *c.stop = 1;
+        } else {
+            c.sc[S_BETA] = red[1][0] / c.sc[S_RZ];
+            c.sc[S_RZ] = red[1][0];
+        }
+    }
+}
 __global__ void conv_kernel(PcgCtl c, int nparts) {
     __shared__ double red[BS];
     if (*c.stop) return;
@@ -830,10 +901,11 @@ __global__ void beta_kernel(PcgCtl c, int nparts) {
 }
 
 // p = z + beta p (beta = 0 and p = z when init)
-__global__ void __launch_bounds__(BS) p_update_kernel(int64_t n, PcgCtl c, const double *z, double *p,
-                                                      int init) {
+__global__ void __launch_bounds__(BS) p_update_kernel(int64_t n, PcgCtl c, const double *__restrict__ z,
+                                                      double *__restrict__ p, int init) {
     if (*c.stop) return;
     const double be = init ? 0.0 : c.sc[S_BETA];
+#pragma unroll 4
     for (int64_t t = blockIdx.x * (int64_t)BS + threadIdx.x; t < n; t += (int64_t)gridDim.x * BS)
         p[t] = z[t] + be * p[t];
 }
@@ -1252,6 +1324,18 @@ struct drf_bz {
         const int na = apply(Lf, p.p, nullptr, q.p, 0, part.p, c.stop);
         alpha_kernel<<<1, BS, 0, stream>>>(c, na);
         DRF_LAUNCHED();
+        if (kind == 0 || kind == 1) {
+            // z = r (none) or r / d (Jacobi) formed in the x, r update pass; the convergence
+            // check and beta in one CTA
+            if (kind == 1) xr_jacobi_kernel<<<nparts(), BS, 0, stream>>>(ndof, c, p.p, q.p, diag.p, x.p, r.p, z.p);
+            else xr_update_kernel<<<nparts(), BS, 0, stream>>>(ndof, c, p.p, q.p, x.p, r.p);
+            DRF_LAUNCHED();
+            conv_beta_kernel<<<1, BS, 0, stream>>>(c, (int)nparts(), kind == 1 ? (int)nparts() : 0);
+            DRF_LAUNCHED();
+            p_update_kernel<<<nparts(), BS, 0, stream>>>(ndof, c, kind == 1 ? z.p : r.p, p.p, 0);
+            DRF_LAUNCHED();
+            return;
+        }
         xr_update_kernel<<<nparts(), BS, 0, stream>>>(ndof, c, p.p, q.p, x.p, r.p);
         DRF_LAUNCHED();
         conv_kernel<<<1, BS, 0, stream>>>(c, (int)nparts());
