@@ -1340,13 +1340,15 @@ struct drf_bz {
         DRF_LAUNCHED();
         conv_kernel<<<1, BS, 0, stream>>>(c, (int)nparts());
         DRF_LAUNCHED();
-        precondition(kind, r.p, z.p, c.stop);
         if (kind == 3) {
-            dot2_kernel<<<nparts(), BS, 0, stream>>>(ndof, z.p, r.p, q.p, part.p, c.stop);
-            DRF_LAUNCHED();
-            beta_fcg_kernel<<<1, BS, 0, stream>>>(c, (int)nparts());
+            // z = r / d + the network's correction, with the partials of z.r and z.q (flexible
+            // CG) from the same pass
+            const int nb = cnn_precondition(cnn_net(cnn), stream, lv[Lf].n, r.p, scal.p + S_RR, cnn_scale, z.p, 1,
+                                            c.stop, diag.p, q.p, part.p);
+            beta_fcg_kernel<<<1, BS, 0, stream>>>(c, nb);
             DRF_LAUNCHED();
         } else {
+            precondition(kind, r.p, z.p, c.stop);
             dot_kernel<<<nparts(), BS, 0, stream>>>(ndof, r.p, z.p, part.p, c.stop);
             DRF_LAUNCHED();
             beta_kernel<<<1, BS, 0, stream>>>(c, (int)nparts());

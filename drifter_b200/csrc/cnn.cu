@@ -598,31 +598,62 @@ __global__ void pack_kernel(int n, const double *r, const double *rr_ptr, double
 // z (+)= rms(r) out_scale Y on the control points (add = 1 adds to a base already in z; with
 // jr, jd non-null the base is the Jacobi step jr / jd instead); one thread per superpixel
 // writes its (up to) 9 control points
-__global__ void unpack_kernel(int n, const float *Y, const double *rr_ptr, double inv_len,
-                              double out_scale, double *z, int add, const int *stop, const double *jr,
-                              const double *jd) {
+__global__ void __launch_bounds__(256) unpack_kernel(int n, const float *Y, const double *rr_ptr, double inv_len,
+                                                     double out_scale, double *z, int add, const int *stop,
+                                                     const double *jr, const double *jd, const double *dq,
+                                                     double *part) {
+    // with part non-null, also the block partials of z.jr (part[block]) and z.dq
+    // (part[gridDim.x + block]): the dot products of flexible CG, in the pass that forms z
+    __shared__ double red[2][8];
     if (stop && *stop) return;
     const int S = n + 1, nd = 3 * n + 1;
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= S * S) return;
-    const int I = p % S, J = p / S;
-    const double rr = *rr_ptr;
-    const double sc = sqrt(rr * inv_len);
-    const float4 *src = reinterpret_cast<const float4 *>(Y + (size_t)p * 16);
-    const float4 y0 = src[0], y1 = src[1], y2 = src[2];
-    const float y[9] = {y0.x, y0.y, y0.z, y0.w, y1.x, y1.y, y1.z, y1.w, y2.x};
+    double s1 = 0.0, s2 = 0.0;
+    if (p < S * S) {
+        const int I = p % S, J = p / S;
+        const double rr = *rr_ptr;
+        const double sc = sqrt(rr * inv_len);
+        const float4 *src = reinterpret_cast<const float4 *>(Y + (size_t)p * 16);
+        const float4 y0 = src[0], y1 = src[1], y2 = src[2];
+        const float y[9] = {y0.x, y0.y, y0.z, y0.w, y1.x, y1.y, y1.z, y1.w, y2.x};
 #pragma unroll
-    for (int b = 0; b < 3; ++b) {
-        const int gj = 3 * J + b;
+        for (int b = 0; b < 3; ++b) {
+            const int gj = 3 * J + b;
 #pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            const int gi = 3 * I + a;
-            if (gi < nd && gj < nd) {
-                const size_t t = gi + (size_t)nd * gj;
-                const double v = (double)y[a + 3 * b] * sc * out_scale;
-                z[t] = jr ? jr[t] / jd[t] + v : (add ? z[t] + v : v);
+            for (int a = 0; a < 3; ++a) {
+                const int gi = 3 * I + a;
+                if (gi < nd && gj < nd) {
+                    const size_t t = gi + (size_t)nd * gj;
+                    const double v = (double)y[a + 3 * b] * sc * out_scale;
+                    const double zn = jr ? jr[t] / jd[t] + v : (add ? z[t] + v : v);
+                    z[t] = zn;
+                    if (part) {
+                        s1 += zn * jr[t];
+                        s2 += zn * dq[t];
+                    }
+                }
             }
         }
+    }
+    if (!part) return;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+        s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        red[0][threadIdx.x >> 5] = s1;
+        red[1][threadIdx.x >> 5] = s2;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0.0, b = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+            a += red[0][w];
+            b += red[1][w];
+        }
+        part[blockIdx.x] = a;
+        part[gridDim.x + blockIdx.x] = b;
     }
 }
 
@@ -857,8 +888,9 @@ struct CnnNet {
 };
 
 // packs r (control points) and runs the network; z (+)= rms(r) * out_scale * net(r / rms(r))
-void cnn_precondition(CnnNet *net, cudaStream_t s, int n, const double *r, const double *rr_dev,
-                      double out_scale, double *z, int add, const int *stop, const double *jac_diag) {
+int cnn_precondition(CnnNet *net, cudaStream_t s, int n, const double *r, const double *rr_dev,
+                     double out_scale, double *z, int add, const int *stop, const double *jac_diag,
+                     const double *dq, double *part) {
     const int S = n + 1;
     const int64_t pix = (int64_t)S * S, nd = 3 * n + 1;
     cudaStream_t keep = net->stream;
@@ -867,10 +899,12 @@ void cnn_precondition(CnnNet *net, cudaStream_t s, int n, const double *r, const
     pack_kernel<<<nb(pix), 256, 0, s>>>(n, r, rr_dev, 1.0 / (double)(nd * nd), net->act[0].p);
     DRF_LAUNCHED();
     net->forward(1, S, S);
+    DRF_CHECK(!part || jac_diag, DRF_E_INVALID, "the fused dot products need the Jacobi base (r)");
     unpack_kernel<<<nb(pix), 256, 0, s>>>(n, net->out.p, rr_dev, 1.0 / (double)(nd * nd), out_scale,
-                                              z, add, stop, jac_diag ? r : nullptr, jac_diag);
+                                              z, add, stop, jac_diag ? r : nullptr, jac_diag, dq, part);
     DRF_LAUNCHED();
     net->stream = keep;
+    return (int)nb(pix);
 }
 
 void cnn_prepare(CnnNet *net, int n) { net->ensure((int64_t)(n + 1) * (n + 1)); }

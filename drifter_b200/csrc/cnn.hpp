@@ -13,8 +13,11 @@ void cnn_prepare(CnnNet *net, int n);
 // early when *stop is set.
 // z (+)= the network's correction of r; with jac_diag non-null z = r / jac_diag + correction
 // (the Jacobi base and the correction in one pass)
-void cnn_precondition(CnnNet *net, cudaStream_t s, int n, const double *r, const double *rr_dev,
-                      double out_scale, double *z, int add, const int *stop, const double *jac_diag = nullptr);
+// With dq and part non-null (and jac_diag set), the unpack pass also writes per-block partials
+// of z.r (part[block]) and z.dq (part[nblocks + block]); returns the number of blocks.
+int cnn_precondition(CnnNet *net, cudaStream_t s, int n, const double *r, const double *rr_dev,
+                     double out_scale, double *z, int add, const int *stop, const double *jac_diag = nullptr,
+                     const double *dq = nullptr, double *part = nullptr);
 // surfaces (and clears) the network's device status word: throws when a bounded wait gave up
 void cnn_check(CnnNet *net, cudaStream_t s);
 }  // namespace drf
