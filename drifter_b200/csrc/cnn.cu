@@ -1,9 +1,12 @@
 // Learned preconditioner for the Bezier smoother's CG: a 4-layer conv3x3 network on 3x3
 // "superpixels" of the control-point grid (space-to-depth exposes the element structure:
 // superpixel (I, J) holds the 9 control points 3I..3I+2 x 3J..3J+2 as channels), BF16
-// activations and weights with FP32 accumulation on the tensor cores (mma.sync m16n8k16,
-// implicit GEMM: M = 16 pixels of a row, N = output channels, K = 9 taps x input channels),
-// trained on the GPU by the backward kernels below with Adam.
+// activations and weights with FP32 accumulation on the tensor cores, trained on the GPU by the
+// backward kernels below with Adam. Two forms of the conv, bit-identical in their results:
+//  * conv3x3_kernel (default): warp-level mma.sync m16n8k16 implicit GEMM (M = 16 pixels of a
+//    row, N = output channels, K = 9 taps x input channels);
+//  * conv3x3_tc_kernel (DRIFTER_B200_CNN_MMA=tcgen05): tcgen05 MMAs (M = 128 pixels) from
+//    shared-memory descriptors into TMEM, TMA halo copies, warp-specialised.
 //
 // Channels (padded for the MMA shapes): 16 (9 used) -> 32 -> 32 -> 32 -> 16 (9 used); ReLU
 // after layers 1-3. Layouts: activations NHWC [b][h][w][c]; weights [co][tap][ci] (tap = dy*3+dx).
