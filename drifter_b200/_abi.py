@@ -51,6 +51,7 @@ _SIGS = {
     "drf_last_error": (C.c_int, [C.c_char_p, C.c_size_t]),
     "drf_version": (C.c_char_p, []),
     "drf_kernel_launch_count": (C.c_uint64, []),
+    "drf_device_alloc_count": (C.c_uint64, []),
     "drf_sw_flux_batch": (C.c_int, [C.c_int, C.c_int64, _dp, _dp, _dp, C.c_double, _dp]),
     "drf_compat_compute_rhs": (C.c_int, [C.c_int, C.c_int, C.POINTER(_dp), _dp, _dp, _dp,
                                          C.POINTER(_dp)]),
@@ -137,3 +138,8 @@ def dptr_array(arrs):
 
 def launch_count() -> int:
     return int(lib().drf_kernel_launch_count())
+
+
+def alloc_count() -> int:
+    """Device allocations (cudaMalloc) the library has made since it was loaded."""
+    return int(lib().drf_device_alloc_count())

@@ -220,6 +220,7 @@ struct drf_amr {
     DevBuf<double> U, R, res, out;  // device state, weak rhs, LSRK register, caller-visible rhs
     drf_mortar *mortar = nullptr;
     cudaGraphExec_t graph = nullptr;
+    uint64_t graph_kernels = 0;  // kernel nodes of the step graph
     int g_mode = -1, g_flux = -1;
     double g_a[3] = {0, 0, 0}, g_dt = 0.0;
 
@@ -480,28 +481,16 @@ int drf_amr_step(drf_amr *h, int mode, int flux_kind, const double *a, double dt
         if (!h->graph || h->g_mode != mode || h->g_flux != flux_kind || h->g_dt != dt ||
             std::memcmp(h->g_a, a, sizeof(h->g_a)) != 0) {
             h->drop_graph();
-            cudaGraph_t g = nullptr;
-            DRF_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-            try {
-                h->enqueue_step(mode, flux_kind, a, dt);
-            } catch (...) {
-                cudaStreamEndCapture(h->stream, &g);
-                if (g) cudaGraphDestroy(g);
-                throw;
-            }
-            DRF_CUDA(cudaStreamEndCapture(h->stream, &g));
-            cudaError_t e = cudaGraphInstantiate(&h->graph, g, 0);
-            cudaGraphDestroy(g);
-            DRF_CUDA(e);
+            h->graph = capture_graph(h->stream, [&] { h->enqueue_step(mode, flux_kind, a, dt); },
+                                     &h->graph_kernels);
             h->g_mode = mode;
             h->g_flux = flux_kind;
             h->g_dt = dt;
             std::memcpy(h->g_a, a, sizeof(h->g_a));
         }
-        const uint64_t per_step = 5 * (2 + (h->mortar ? 2 : 0));
         for (int s = 0; s < nsteps; ++s) {
             DRF_CUDA(cudaGraphLaunch(h->graph, h->stream));
-            launch_counter().fetch_add(per_step);
+            launch_counter().fetch_add(h->graph_kernels);
         }
     });
 }

@@ -1165,6 +1165,7 @@ struct drf_bz {
     double cnn_scale = 1.0;
     cudaGraphExec_t graph = nullptr;
     int graph_kind = -1, graph_chunk = 0;
+    uint64_t graph_kernels = 0;  // kernel nodes of the chunk graph
 
     ~drf_bz() {
         if (graph) cudaGraphExecDestroy(graph);
@@ -1467,26 +1468,16 @@ int pcg_run(drf_bz *h, int kind, double tol, int maxit) {
     if (!done && maxit > 0) {
         if (!h->graph || h->graph_kind != kind || h->graph_chunk != chunk) {
             if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }
-            cudaGraph_t g = nullptr;
-            DRF_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-            try {
+            h->graph = capture_graph(h->stream, [&] {
                 for (int k = 0; k < chunk; ++k) h->pcg_iteration(kind);
-            } catch (...) {
-                cudaStreamEndCapture(h->stream, &g);
-                if (g) cudaGraphDestroy(g);
-                throw;
-            }
-            DRF_CUDA(cudaStreamEndCapture(h->stream, &g));
-            cudaError_t e = cudaGraphInstantiate(&h->graph, g, 0);
-            cudaGraphDestroy(g);
-            DRF_CUDA(e);
+            }, &h->graph_kernels);
             h->graph_kind = kind;
             h->graph_chunk = chunk;
         }
         int ctl[2] = {0, 0};
         while (true) {
             DRF_CUDA(cudaGraphLaunch(h->graph, h->stream));
-            launch_counter().fetch_add(1);
+            launch_counter().fetch_add(h->graph_kernels);
             DRF_CUDA(cudaMemcpyAsync(ctl, h->ctl.p, sizeof(ctl), cudaMemcpyDeviceToHost, h->stream));
             DRF_CUDA(cudaStreamSynchronize(h->stream));
             if (ctl[0] || ctl[1] >= maxit) break;
@@ -1917,17 +1908,11 @@ int drf_bz_jacobi_pcg_noalloc(const drf_bz_grid_desc *g, const double *d_b, doub
         DRF_CHECK(nd <= NOALLOC_MAX_ND && n <= NOALLOC_MAX_DOF, DRF_E_UNSUPPORTED,
                   "grid too large for the allocation-free solve: at most " +
                       std::to_string(NOALLOC_MAX_DOF) + " control points (nx <= 170)");
-        // device address of the scratch array, looked up once per device with it current
-        static double *base[64] = {nullptr};
-        int dev = 0;
-        DRF_CUDA(cudaGetDevice(&dev));
-        DRF_CHECK(dev >= 0 && dev < 64, DRF_E_UNSUPPORTED, "device ordinal out of range");
-        if (!base[dev]) {
-            void *ptr = nullptr;
-            DRF_CUDA(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
-            base[dev] = static_cast<double *>(ptr);
-        }
-        double *K = base[dev], *rho = K + 256, *r = rho + NOALLOC_MAX_ND;
+        // device address of the scratch array in the current device's context, looked up on
+        // every call (cheap, allocates nothing, and stays right if the context was re-created)
+        void *sym = nullptr;
+        DRF_CUDA(cudaGetSymbolAddress(&sym, g_noalloc_scratch));
+        double *K = static_cast<double *>(sym), *rho = K + 256, *r = rho + NOALLOC_MAX_ND;
         double *z = r + NOALLOC_MAX_DOF, *p = z + NOALLOC_MAX_DOF, *q = p + NOALLOC_MAX_DOF;
         double *part = q + NOALLOC_MAX_DOF, *scal = part + NOALLOC_PARTS;
         int *ctl = reinterpret_cast<int *>(scal + 16);
@@ -1973,23 +1958,29 @@ int drf_bz_jacobi_pcg_noalloc(const drf_bz_grid_desc *g, const double *d_b, doub
         DRF_CUDA(cudaStreamSynchronize(st));
         int cl[3] = {0, 0, maxit};
         if (sc[S_RR] > tol2 * sc[S_BB] && maxit > 0) {
+            // iterations are queued 8 at a time between reads of the control word: after
+            // convergence (or at maxit) every kernel returns early on it, so the extra ones
+            // change nothing
+            constexpr int chunk = 8;
             while (true) {
-                bz_apply_kernel<<<nb, BS, 0, st>>>(L, p, nullptr, q, 0, part, ctl);
-                DRF_LAUNCHED();
-                alpha_kernel<<<1, BS, 0, st>>>(c, (int)nb);
-                DRF_LAUNCHED();
-                xr_update_kernel<<<np, BS, 0, st>>>(n, c, p, q, d_x, r);
-                DRF_LAUNCHED();
-                conv_kernel<<<1, BS, 0, st>>>(c, (int)np);
-                DRF_LAUNCHED();
-                jacobi_kernel<<<nb, BS, 0, st>>>(L, r, z, ctl);
-                DRF_LAUNCHED();
-                dot_kernel<<<np, BS, 0, st>>>(n, r, z, part, ctl);
-                DRF_LAUNCHED();
-                beta_kernel<<<1, BS, 0, st>>>(c, (int)np);
-                DRF_LAUNCHED();
-                p_update_kernel<<<np, BS, 0, st>>>(n, c, z, p, 0);
-                DRF_LAUNCHED();
+                for (int k = 0; k < chunk; ++k) {
+                    bz_apply_kernel<<<nb, BS, 0, st>>>(L, p, nullptr, q, 0, part, ctl);
+                    DRF_LAUNCHED();
+                    alpha_kernel<<<1, BS, 0, st>>>(c, (int)nb);
+                    DRF_LAUNCHED();
+                    xr_update_kernel<<<np, BS, 0, st>>>(n, c, p, q, d_x, r);
+                    DRF_LAUNCHED();
+                    conv_kernel<<<1, BS, 0, st>>>(c, (int)np);
+                    DRF_LAUNCHED();
+                    jacobi_kernel<<<nb, BS, 0, st>>>(L, r, z, ctl);
+                    DRF_LAUNCHED();
+                    dot_kernel<<<np, BS, 0, st>>>(n, r, z, part, ctl);
+                    DRF_LAUNCHED();
+                    beta_kernel<<<1, BS, 0, st>>>(c, (int)np);
+                    DRF_LAUNCHED();
+                    p_update_kernel<<<np, BS, 0, st>>>(n, c, z, p, 0);
+                    DRF_LAUNCHED();
+                }
                 DRF_CUDA(cudaMemcpyAsync(cl, ctl, sizeof(cl), cudaMemcpyDeviceToHost, st));
                 DRF_CUDA(cudaStreamSynchronize(st));
                 if (cl[0] || cl[1] >= maxit) break;

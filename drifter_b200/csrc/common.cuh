@@ -20,6 +20,11 @@ struct Error : std::runtime_error {
 };
 void set_last_error(const std::string &msg);
 std::atomic<uint64_t> &launch_counter();
+// Device allocations made by this library (every cudaMalloc goes through DevBuf::alloc).
+std::atomic<uint64_t> &alloc_counter();
+// Nonzero while the calling thread is capturing a stream into a graph: kernels queued then are
+// counted when the graph is launched, not when they are queued.
+int &capture_depth();
 
 #define DRF_CUDA(call)                                                                       \
     do {                                                                                     \
@@ -33,11 +38,12 @@ std::atomic<uint64_t> &launch_counter();
         if (!(cond)) throw ::drf::Error(code, msg); \
     } while (0)
 
-// After every kernel launch: count it and surface launch-configuration errors.
-#define DRF_LAUNCHED()                                  \
-    do {                                                \
-        ::drf::launch_counter().fetch_add(1);           \
-        DRF_CUDA(cudaGetLastError());                   \
+// After every kernel launch: count it (unless it was only queued into a graph being
+// captured) and surface launch-configuration errors.
+#define DRF_LAUNCHED()                                                      \
+    do {                                                                    \
+        if (::drf::capture_depth() == 0) ::drf::launch_counter().fetch_add(1); \
+        DRF_CUDA(cudaGetLastError());                                       \
     } while (0)
 
 // C-ABI wrapper: converts exceptions into status codes.
@@ -87,6 +93,7 @@ struct DevBuf {
         release();
         n = count;
         if (count) {
+            alloc_counter().fetch_add(1);
             cudaError_t e = cudaMalloc(&p, count * sizeof(T));
             if (e != cudaSuccess) {
                 p = nullptr;
@@ -114,5 +121,43 @@ struct DevBuf {
 };
 
 bool all_finite(const double *x, size_t n);
+
+// Captures what `enqueue` queues on `stream` (thread-local capture mode) into an executable
+// graph. `kernels` receives the number of kernel nodes in it, which a caller adds to the launch
+// counter per replay. The capture is ended, and the partial graph destroyed, if `enqueue` throws.
+template <class F>
+cudaGraphExec_t capture_graph(cudaStream_t stream, F &&enqueue, uint64_t *kernels) {
+    cudaGraph_t g = nullptr;
+    DRF_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+    ++capture_depth();
+    try {
+        enqueue();
+    } catch (...) {
+        --capture_depth();
+        cudaStreamEndCapture(stream, &g);
+        if (g) cudaGraphDestroy(g);
+        throw;
+    }
+    --capture_depth();
+    DRF_CUDA(cudaStreamEndCapture(stream, &g));
+    size_t nn = 0;
+    cudaError_t e = cudaGraphGetNodes(g, nullptr, &nn);
+    uint64_t nk = 0;
+    if (e == cudaSuccess && nn) {
+        std::vector<cudaGraphNode_t> nodes(nn);
+        e = cudaGraphGetNodes(g, nodes.data(), &nn);
+        for (size_t i = 0; e == cudaSuccess && i < nn; ++i) {
+            cudaGraphNodeType t;
+            e = cudaGraphNodeGetType(nodes[i], &t);
+            if (e == cudaSuccess && t == cudaGraphNodeTypeKernel) ++nk;
+        }
+    }
+    cudaGraphExec_t x = nullptr;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&x, g, 0);
+    cudaGraphDestroy(g);
+    DRF_CUDA(e);
+    if (kernels) *kernels = nk;
+    return x;
+}
 
 }  // namespace drf

@@ -1513,6 +1513,7 @@ struct drf_dg {
     int cur = 0;
     bool pending = false;  // a transport correction in corrU/corrV is not yet in q(cur)
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    uint64_t graph_kernels[2] = {0, 0};  // kernel nodes of each step graph
     double graph_dt = 0.0;
     // barotropic tile chosen by the autotuner (0 = not tuned yet) and the candidates' times
     int baro_cpb = 0;
@@ -1640,8 +1641,6 @@ struct drf_dg {
         s.err = err;
         return s;
     }
-    // kernel launches of one baroclinic step: 5 stages, then the barotropic step
-    uint64_t launches_per_step(int nsub) const { return baro_persist ? 6 : 5 + 2 + 2 * (uint64_t)nsub; }
 
     template <typename T, int NP>
     void enqueue_step(int in, double dt, int nsub) {
@@ -2073,31 +2072,20 @@ int drf_dg_step_modesplit(drf_dg *m, double dt, int nsub, int nsteps) {
             m->drop_graphs();
             const char *pe = std::getenv("DRIFTER_B200_BARO_PERSISTENT");
             m->baro_persist = pe && pe[0] == '1';
-            for (int in = 0; in < 2; ++in) {
-                cudaGraph_t g = nullptr;
-                DRF_CUDA(cudaStreamBeginCapture(m->stream, cudaStreamCaptureModeThreadLocal));
-                try {
+            for (int in = 0; in < 2; ++in)
+                m->graph[in] = capture_graph(m->stream, [&] {
                     m->with_types([&](auto tv, auto npc) {
                         using T = decltype(tv);
                         constexpr int NP = decltype(npc)::value;
                         m->template enqueue_step<T, NP>(in, dt, nsub);
                     });
-                } catch (...) {
-                    cudaStreamEndCapture(m->stream, &g);
-                    if (g) cudaGraphDestroy(g);
-                    throw;
-                }
-                DRF_CUDA(cudaStreamEndCapture(m->stream, &g));
-                cudaError_t e = cudaGraphInstantiate(&m->graph[in], g, 0);
-                cudaGraphDestroy(g);
-                DRF_CUDA(e);
-            }
+                }, &m->graph_kernels[in]);
             m->graph_nsub = nsub;
             m->graph_dt = dt;
         }
         for (int s = 0; s < nsteps; ++s) {
             DRF_CUDA(cudaGraphLaunch(m->graph[m->cur], m->stream));
-            launch_counter().fetch_add(m->launches_per_step(nsub));
+            launch_counter().fetch_add(m->graph_kernels[m->cur]);
             m->cur = 1 - m->cur;
             m->pending = true;
         }
@@ -2414,6 +2402,7 @@ struct drf_ens {
     int64_t n3tot = 0, n2tot = 0;
     cudaStream_t stream = nullptr, own = nullptr;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    uint64_t graph_kernels[2] = {0, 0};  // kernel nodes of each step graph
     int graph_nsub = 0;
     int cur = 0;
 
@@ -2643,30 +2632,19 @@ int drf_ens_step(drf_ens *e, const double *dt, int nsub, int nsteps) {
             e->drop_graphs();
             const char *pe = std::getenv("DRIFTER_B200_BARO_PERSISTENT");
             e->baro_persist = pe && pe[0] == '1';
-            for (int in = 0; in < 2; ++in) {
-                cudaGraph_t g = nullptr;
-                DRF_CUDA(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
-                try {
+            for (int in = 0; in < 2; ++in)
+                e->graph[in] = capture_graph(e->stream, [&] {
                     e->mem[0]->with_types([&](auto tv, auto npc) {
                         using T = decltype(tv);
                         constexpr int NP = decltype(npc)::value;
                         e->template enqueue<T, NP>(in, nsub);
                     });
-                } catch (...) {
-                    cudaStreamEndCapture(e->stream, &g);
-                    if (g) cudaGraphDestroy(g);
-                    throw;
-                }
-                DRF_CUDA(cudaStreamEndCapture(e->stream, &g));
-                cudaError_t st = cudaGraphInstantiate(&e->graph[in], g, 0);
-                cudaGraphDestroy(g);
-                DRF_CUDA(st);
-            }
+                }, &e->graph_kernels[in]);
             e->graph_nsub = nsub;
         }
         for (int s = 0; s < nsteps; ++s) {
             DRF_CUDA(cudaGraphLaunch(e->graph[e->cur], e->stream));
-            launch_counter().fetch_add(e->baro_persist ? 6 : 5 + 2 + 2 * (uint64_t)nsub);
+            launch_counter().fetch_add(e->graph_kernels[e->cur]);
             e->cur = 1 - e->cur;
         }
         for (auto &m : e->mem) {

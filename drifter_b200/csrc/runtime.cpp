@@ -14,6 +14,16 @@ std::atomic<uint64_t> &launch_counter() {
     return c;
 }
 
+std::atomic<uint64_t> &alloc_counter() {
+    static std::atomic<uint64_t> c{0};
+    return c;
+}
+
+int &capture_depth() {
+    static thread_local int d = 0;
+    return d;
+}
+
 bool all_finite(const double *x, size_t n) {
     for (size_t i = 0; i < n; ++i)
         if (!std::isfinite(x[i])) return false;
@@ -146,5 +156,7 @@ int drf_last_error(char *buf, size_t n) {
 const char *drf_version(void) { return "drifter_b200 0.1 (sm_100a)"; }
 
 uint64_t drf_kernel_launch_count(void) { return drf::launch_counter().load(); }
+
+uint64_t drf_device_alloc_count(void) { return drf::alloc_counter().load(); }
 
 }  // extern "C"

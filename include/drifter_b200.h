@@ -40,9 +40,14 @@ enum { DRF_RK_EULER = 0, DRF_RK_MIDPOINT = 1, DRF_RK_SSP3 = 2, DRF_RK_RK4 = 3, D
 
 /* Copies the last error message of the calling thread into buf (NUL-terminated). */
 int drf_last_error(char *buf, size_t n);
-/* Library version string and the number of kernels this library has launched. */
+/* Library version string and the number of kernels this library has launched (kernels replayed
+ * from a CUDA graph count once per replay; queuing them into a graph being captured does not
+ * count). No reference counterpart: launch accounting of this library. */
 const char *drf_version(void);
 uint64_t drf_kernel_launch_count(void);
+/* Number of device allocations (cudaMalloc) this library has made since it was loaded. No
+ * reference counterpart: lets a caller verify that a call allocated nothing. */
+uint64_t drf_device_alloc_count(void);
 
 /* ------------------------------------------------------------------ fluxes
  * Batched shallow-water numerical flux F*(U_L, U_R, n) on the GPU, U = (h, hu, hv).
@@ -283,10 +288,10 @@ int drf_bz_set_cnn(drf_bz *h, drf_cnn *net, double out_scale);
  * solution out); stream is a cudaStream_t (NULL = legacy default stream).
  * Scratch: one file-scope device array of 8.5 MB in libdrifter_b200.so, held on every device
  * that loads the library until process exit; grids up to 262,144 control points (nx <= 170),
- * larger sizes return DRF_E_UNSUPPORTED. It calls no cudaMalloc/cudaFree. The first call on a
- * device looks up the array's device address (cudaGetSymbolAddress) and must come before any
- * stream capture on that device. Every call shares the array: calls that overlap on the GPU
- * (other host threads, other streams) race and must be serialised by the caller. */
+ * larger sizes return DRF_E_UNSUPPORTED. It calls no cudaMalloc/cudaFree. Every call looks up
+ * the array's address in the current device's context (cudaGetSymbolAddress) and waits for its
+ * stream between batches of 8 iterations. Every call shares the array: calls that overlap on the
+ * GPU (other host threads, other streams) race and must be serialised by the caller. */
 int drf_bz_jacobi_pcg_noalloc(const drf_bz_grid_desc *grid, const double *d_b, double *d_x,
                               double tol, int maxit, void *stream, int *iters, double *relres);
 

@@ -286,15 +286,26 @@ static void matvec(const Vec &M, int n, const double *x, double *y) {
     }
 }
 
+// The element operator's tables, built once as DG3DElementOperator holds them
+// (src/dg/operators_3d.cpp:14-45): LGL basis, dense 3D derivative matrices (quirk Q2) and the
+// sigma weights (src/physics/mode_splitting.cpp:80-85).
+struct CompatOps {
+    Basis1D b;
+    Vec Dx, Dy, Dz, sw;
+    explicit CompatOps(int order) : b(make_lgl(order)) {
+        build_dense_3d(b, Dx, Dy, Dz);
+        sw.resize(b.np());
+        for (int k = 0; k < b.np(); ++k) sw[k] = 0.5 * b.weights[k];
+    }
+};
+
 // src/physics/primitive_equations.cpp:136-393 (element) and :428 (solver loop).
-void compat_compute_rhs(int order, int nel, const double *const in[6], const double *hh,
-                        const double *ff, const CompatParams &p, double *const out[5]) {
-    Basis1D b = make_lgl(order);
+static void compat_rhs_elements(const CompatOps &ops, int nel, const double *const in[6],
+                                const double *hh, const double *ff, const CompatParams &p,
+                                double *const out[5]) {
+    const Basis1D &b = ops.b;
+    const Vec &Dx = ops.Dx, &Dy = ops.Dy, &Dz = ops.Dz, &sw = ops.sw;
     const int np = b.np(), nd = np * np * np, nh = np * np, nv = np;
-    Vec Dx, Dy, Dz;
-    build_dense_3d(b, Dx, Dy, Dz);
-    Vec sw(nv);
-    for (int k = 0; k < nv; ++k) sw[k] = 0.5 * b.weights[k];
     Vec H(nd), Hinv(nd), u(nd), v(nd), T(nd), S(nd), t1(nd), t2(nd), t3(nd), a(nd), c(nd);
     for (int e = 0; e < nel; ++e) {
         const size_t o = (size_t)e * nd;
@@ -335,8 +346,8 @@ void compat_compute_rhs(int order, int nel, const double *const in[6], const dou
             for (int i = 0; i < nd; ++i) {
                 dHu[i] = 0.0 - advu[i];
                 dHv[i] = 0.0 - advv[i];
-                dHu[i] += ff[o + i] * Hv[i];
-                dHv[i] += -ff[o + i] * Hu[i];
+                dHu[i] += f[i] * Hv[i];
+                dHv[i] += -f[i] * Hu[i];
                 dHu[i] += -p.g * H[i] * dex[i];
                 dHv[i] += -p.g * H[i] * dey[i];
             }
@@ -390,6 +401,12 @@ void compat_compute_rhs(int order, int nel, const double *const in[6], const dou
             for (int k = 0; k < nv; ++k) deta[(i + j * np) * nv + k] = d2;
         }
     }
+}
+
+void compat_compute_rhs(int order, int nel, const double *const in[6], const double *hh,
+                        const double *ff, const CompatParams &p, double *const out[5]) {
+    const CompatOps ops(order);
+    compat_rhs_elements(ops, nel, in, hh, ff, p, out);
 }
 
 // src/physics/mode_splitting.cpp:136-600 per element (quirks Q1, Q4, Q10 replicated).
@@ -536,6 +553,7 @@ void compat_ssprk3_step(int order, int nel, double dt, double *const st6[6], con
     };
     pack(U);
     Vec om(st6[5], st6[5] + (size_t)nel * nd);
+    const CompatOps ops(order);  // the element operator, built once (not per element or stage)
     auto rhs = [&](const Vec &X, Vec &dX) {
         // unpack_state into per-element arrays, then the element loop in chunks
         const int nt = std::max(1, nthreads);
@@ -547,7 +565,7 @@ void compat_ssprk3_step(int order, int nel, double dt, double *const st6[6], con
                 for (int v = 0; v < 5; ++v) out[v].assign(nd, 0.0);
                 const double *ip[6] = {in[0].data(), in[1].data(), in[2].data(), in[3].data(), in[4].data(), in[5].data()};
                 double *op[5] = {out[0].data(), out[1].data(), out[2].data(), out[3].data(), out[4].data()};
-                compat_compute_rhs(order, 1, ip, hh + (size_t)e * nd, ff + (size_t)e * nd, p, op);
+                compat_rhs_elements(ops, 1, ip, hh + (size_t)e * nd, ff + (size_t)e * nd, p, op);
                 for (int v = 0; v < 5; ++v) std::copy(out[v].begin(), out[v].end(), dX.begin() + e * per + v * nd);
             }
         };

@@ -201,6 +201,22 @@ def test_lake_at_rest_stays_at_rest_on_gpu():
     assert np.abs(s["eta"]).max() < 1e-12 and np.abs(s["Hu"]).max() < 1e-8
 
 
+def test_launch_count_counts_graph_replays_not_capture(monkeypatch):
+    """Kernels queued while the step graphs are captured are not launches; each replay of a
+    step graph counts its kernel nodes (5 stages, force, predictor and corrector per subcycle,
+    finish)."""
+    monkeypatch.setenv("DRIFTER_B200_TUNE", "0")
+    case = configs.c1(nx=6, ny=5, nz=3)
+    gpu = OceanModel(case["cfg"], case["h"], case["f"], case["taux"], case["tauy"])
+    gpu.upload_state(case["q"], case["eta"])
+    gpu.sync()
+    before = launch_count()
+    gpu.step(case["dt"], case["nsub"], 1)  # captures both step graphs, replays one
+    gpu.sync()
+    assert launch_count() - before == 5 + 2 + 2 * case["nsub"]
+    gpu.close()
+
+
 def test_time_stage_reports_positive_rate():
     case = configs.c1(nx=8, ny=8, nz=4, precision="mixed")
     gpu = OceanModel(case["cfg"], case["h"], case["f"], case["taux"], case["tauy"])

@@ -11,7 +11,7 @@ import numpy as np
 import pytest
 
 import pyoracle as O
-from drifter_b200._abi import check, lib
+from drifter_b200._abi import alloc_count, check, lib
 from drifter_b200.bezier import BezierSmoother, BzGridDesc
 
 pytestmark = pytest.mark.gpu
@@ -37,13 +37,15 @@ def _noalloc_solve(desc, b, torch):
     stream = torch.cuda.current_stream()
     torch.cuda.synchronize()
     free0 = torch.cuda.mem_get_info()[0]
+    n0 = alloc_count()
     it, rr = C.c_int(), C.c_double()
     check(L.drf_bz_jacobi_pcg_noalloc(C.byref(desc), C.c_void_p(db.data_ptr()),
                                       C.c_void_p(dx.data_ptr()), 1e-10, 5000,
                                       C.c_void_p(stream.cuda_stream), C.byref(it), C.byref(rr)))
+    n1 = alloc_count()
     torch.cuda.synchronize()
     free1 = torch.cuda.mem_get_info()[0]
-    return dx.cpu().numpy(), it.value, rr.value, free0 - free1
+    return dx.cpu().numpy(), it.value, rr.value, n1 - n0, free0 - free1
 
 
 def test_noalloc_matches_existing_entry_point_on_two_calls():
@@ -54,14 +56,17 @@ def test_noalloc_matches_existing_entry_point_on_two_calls():
         s = BezierSmoother(n, n, L, L, _data(n, L, seed), lam=1.0, ridge_epsilon=1e-4)
         b = s.rhs()
         x_ref, info = s.solve("jacobi", tol=1e-10, maxit=5000)
-        x, it, rr, dmem = _noalloc_solve(s.desc, b, torch)
+        x, it, rr, nalloc, dmem = _noalloc_solve(s.desc, b, torch)
+        # no cudaMalloc inside the library on either call (its own allocation counter)
+        assert nalloc == 0
         deltas.append(dmem)
         assert rr <= 1e-10
         assert abs(it - info["iters"]) <= 1
         assert np.abs(x - x_ref).max() / np.abs(x_ref).max() < REL_TOL
         s.close()
-    # the second call runs already-loaded kernels: device memory in use must not change
-    assert deltas[1] == 0
+    # loose extra check (free memory is device-wide, so other users of the GPU move it): the
+    # second call runs already-loaded kernels and should leave it unchanged
+    assert abs(deltas[1]) <= 2 << 20
 
 
 def test_noalloc_rejects_oversized_grid():
