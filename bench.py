@@ -43,7 +43,9 @@ def parse():
     ap.add_argument("--no-cg", action="store_true", help="skip the C4 Bezier CG comparison")
     ap.add_argument("--no-ens", action="store_true", help="skip the C5 ensemble measurement")
     ap.add_argument("--no-amr", action="store_true", help="skip the C3 AMR measurement")
-    ap.add_argument("--only", choices=["amr", "ens", "cg"], default=None,
+    ap.add_argument("--no-baroclinic", action="store_true",
+                    help="skip the C2 measurement with the baroclinic pressure gradient on")
+    ap.add_argument("--only", choices=["amr", "ens", "cg", "baro"], default=None,
                     help="run one workload section alone and print its JSON (profiling aid)")
     return ap.parse_args()
 
@@ -241,6 +243,53 @@ def run_cg(stream, reps=3):
     return out
 
 
+def run_baroclinic(stream, steps=10, warmup=3):
+    """C2 with the equation of state on (the baroclinic pressure gradient against the linear
+    reference stratification): the cost of the pressure integral and gradient in the stage
+    kernel, and the mixed-precision surface error against the FP64 GPU form over a short
+    window (the coupled baroclinic step grows on C2's steep seamount flanks within about a
+    hundred steps, so it is not run for the config's 500)."""
+    import torch
+    from drifter_b200 import configs
+    from drifter_b200.dg import DGConfig, OceanModel
+    case = configs.c2(baroclinic=True)
+    cfg = case["cfg"]
+    dt, nsub = case["dt"], case["nsub"]
+    m = OceanModel(cfg, case["h"], case["f"], case["taux"], case["tauy"])
+    m.set_stream(stream.cuda_stream)
+    m.upload_state(case["q"], case["eta"])
+    m.step(dt, nsub, warmup)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    m.step(dt, nsub, steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    sm = m.download_state()
+    st = m.time_stage(nrep=5 * steps)
+    m.close()
+    cfg64 = DGConfig(**{**cfg.__dict__, "precision": "fp64"})
+    m64 = OceanModel(cfg64, case["h"], case["f"], case["taux"], case["tauy"])
+    m64.set_stream(stream.cuda_stream)
+    m64.upload_state(case["q"], case["eta"])
+    m64.step(dt, nsub, warmup + steps)
+    s64 = m64.download_state()
+    vmax = m64.diagnostics()["max_speed"]
+    m64.close()
+    peak, _ = measured_peaks()
+    ndof = 4 * cfg.n3
+    gbs = st["alg_bytes"] / (st["ms"] / 1e3) / 1e9
+    return {"workload": case["name"] + " with the baroclinic pressure gradient (linear EOS, "
+                                       "reference stratification 20 C - 0.008 C/m)",
+            "value": ndof * 5 / (ms / 1e3), "unit": UNIT, "ms_per_step": ms,
+            "stage_kernel_ms": st["ms"], "stage_alg_bytes": st["alg_bytes"],
+            "roofline_frac": gbs / peak, "achieved_gbs": gbs,
+            "eta_rel_err_mixed_vs_fp64": float(np.linalg.norm(sm["eta"] - s64["eta"]) /
+                                               np.linalg.norm(s64["eta"])),
+            "steps_compared": warmup + steps, "max_speed_m_s": vmax}
+
+
 def run_ensemble(stream, steps=5, warmup=3):
     """C5: 64 independent N=3 runs of uneven size stepped together (one persistent stage launch
     per LSRK stage for all members, one graph per baroclinic step), against the same members
@@ -356,7 +405,7 @@ def run_only(args, local):
     import torch
     torch.cuda.set_device(local)
     stream = torch.cuda.Stream()
-    fn = {"amr": run_amr, "ens": run_ensemble, "cg": run_cg}[args.only]
+    fn = {"amr": run_amr, "ens": run_ensemble, "cg": run_cg, "baro": run_baroclinic}[args.only]
     out = fn(stream, steps=args.steps, warmup=args.warmup) if args.only != "cg" else fn(stream)
     print(json.dumps({"only": args.only, **out}), flush=True)
 
@@ -436,13 +485,13 @@ def run_ours(args, rank, world, local):
            "ms_per_step": 1e3 * e2e_s / args.steps,
            "host_ms_per_call": {k: round(1e3 * v / args.steps, 3) for k, v in calls.items()}}
 
-    # FP64 GPU form of the same step and the mixed-precision surface error against it
+    # FP64 GPU form of the same step, and the mixed-precision surface error against it over the
+    # config's full length (both forms stepped from the initial state)
     fp64 = None
     if not args.no_fp64:
-        sm = model.download_state()
-        nsteps_done = args.warmup + 2 * args.steps
         del model
         torch.cuda.synchronize()
+        nref = max(case["steps"], args.warmup + 2 * args.steps)
         from drifter_b200.dg import DGConfig
         cfg64 = DGConfig(**{**cfg.__dict__, "precision": "fp64"})
         m64 = OceanModel(cfg64, case["h"], case["f"], case["taux"], case["tauy"])
@@ -453,18 +502,31 @@ def run_ours(args, rank, world, local):
         e0.record(stream)
         m64.step(dt, nsub, 2 * args.steps)
         e1.record(stream)
+        m64.step(dt, nsub, nref - args.warmup - 2 * args.steps)
         torch.cuda.synchronize()
         ms64 = max_over_ranks(e0.elapsed_time(e1), world) / (2 * args.steps)
         s64 = m64.download_state()
+        m64.close()
+        mm = OceanModel(cfg, case["h"], case["f"], case["taux"], case["tauy"])
+        mm.set_stream(stream.cuda_stream)
+        mm.upload_state(case["q"], case["eta"])
+        mm.step(dt, nsub, nref)
+        sm = mm.download_state()
+        mm.close()
         err = float(np.linalg.norm(sm["eta"] - s64["eta"]) / np.linalg.norm(s64["eta"]))
         fp64 = {"value": world * ndof * 5 / (ms64 / 1e3), "ms_per_step": ms64,
-                "eta_rel_err_mixed_vs_fp64": err, "steps_compared": nsteps_done}
+                "eta_rel_err_mixed_vs_fp64": err, "steps_compared": nref,
+                "max_abs_eta_m": float(np.abs(s64["eta"]).max())}
 
     # Bezier smoother CG on C4 (512x512, 2.36 M control points): time to the FP64 1e-10 residual
     # with the multigrid and the learned preconditioner (plus Jacobi and none for reference)
     cg = None
     if not args.no_cg:
         cg = run_cg(stream)
+
+    baro = None
+    if not args.no_baroclinic:
+        baro = run_baroclinic(stream)
 
     ens = None
     if not args.no_ens:
@@ -497,6 +559,7 @@ def run_ours(args, rank, world, local):
             "cpu_baseline": cpu,
             "e2e": e2e,
             "fp64_gpu": fp64,
+            "baroclinic": baro,
             "cg": cg,
             "ensemble": ens,
             "amr": amr,

@@ -41,7 +41,9 @@ class DGParams(C.Structure):
     _fields_ = [("g", C.c_double), ("rho0", C.c_double), ("nu_h", C.c_double),
                 ("nu_v", C.c_double), ("kappa_v_T", C.c_double), ("kappa_v_S", C.c_double),
                 ("cd", C.c_double), ("flux2d", C.c_int32), ("precision", C.c_int32),
-                ("bc", C.c_int32 * 4), ("tide_amp", C.c_double), ("tide_period", C.c_double)]
+                ("bc", C.c_int32 * 4), ("tide_amp", C.c_double), ("tide_period", C.c_double),
+                ("alpha", C.c_double), ("beta", C.c_double), ("T0", C.c_double), ("S0", C.c_double),
+                ("Tref_s", C.c_double), ("Tref_dz", C.c_double)]
 
 
 _lib = None

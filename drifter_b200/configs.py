@@ -4,7 +4,9 @@ C1  plain FP64 DG, CPU-runnable: 100x100 km closed basin, 16x16x4 hexes, N=3, Ga
     seamount 50-500 m, uniform 0.1 N/m^2 wind stress, T/S constant, 20 barotropic subcycles.
 C2  uniform large DG: 200x200 km, 128x128x16 hexes, N=4, depth 20 m + 32 random Gaussians
     clipped to [20, 2000] m, M2 tide (1 m, 44714 s) on the west boundary, linear T
-    stratification (20 C surface to 4 C bottom), S = 35.
+    stratification with level isotherms (20 C at the surface to 4 C at 2000 m), S = 35, passive
+    unless the equation of state is switched on (c2(baroclinic=True)), whose pressure gradient
+    is then taken against the same profile as reference stratification.
 C5  uneven ensemble: 64 independent runs, N=3, meshes 16..64 x 16..64 x 4..8 hexes, per-member
     seeded bathymetry (Gaussian bumps over a sloping shelf) and wind stress 0-0.2 N/m^2, mixed
     precision.
@@ -18,6 +20,9 @@ import numpy as np
 from .dg import DGConfig
 
 SEED = 20261203
+# C2's linear stratification: 20 C at the surface, 4 C at 2000 m depth
+C2_T_SURFACE = 20.0
+C2_T_DZ = 16.0 / 2000.0
 
 
 def lgl_nodes(order: int) -> np.ndarray:
@@ -78,15 +83,24 @@ def c1(nx=16, ny=16, nz=4, order=3, precision="fp64", seed=SEED, flux2d="lf"):
                 steps=100, name=f"C1 {nx}x{ny}x{nz} N={order}")
 
 
-def c2(nx=128, ny=128, nz=16, order=4, precision="mixed", seed=SEED, flux2d="lf", Lx=200e3):
+def c2(nx=128, ny=128, nz=16, order=4, precision="mixed", seed=SEED, flux2d="lf", Lx=200e3,
+       wscale=None, baroclinic=False):
+    """wscale scales the seamount widths (default Lx / 200 km: a shrunk copy of the basin;
+    1.0 keeps C2's 5-40 km widths, and so its slopes, in a smaller basin).
+
+    baroclinic=True switches the equation of state on (the stratification's pressure gradient,
+    against the same profile as reference stratification); by default the stratification is a
+    passive tracer. On C2's seamount flanks (slopes to 0.19) the coupled baroclinic step grows
+    within about a hundred steps, so the 500-step workload runs with the tracer passive."""
     rng = np.random.default_rng(seed)
+    eos = {} if baroclinic else {"alpha": 0.0, "beta": 0.0}
     cfg = DGConfig(nx=nx, ny=ny, nz=nz, order=order, Lx=Lx, Ly=Lx, precision=precision,
                    flux2d=flux2d, bc=("tide", "wall", "wall", "wall"), tide_amp=1.0,
-                   tide_period=44714.0)
+                   tide_period=44714.0, Tref_s=C2_T_SURFACE, Tref_dz=C2_T_DZ, **eos)
     X, Y, Sg = node_coords(cfg)
     h = np.full(cfg.n2, 20.0)
     amp = rng.uniform(0.0, 1980.0, 32)
-    wid = rng.uniform(5e3, 40e3, 32) * (Lx / 200e3)
+    wid = rng.uniform(5e3, 40e3, 32) * (Lx / 200e3 if wscale is None else wscale)
     cx = rng.uniform(0.0, Lx, 32)
     cy = rng.uniform(0.0, Lx, 32)
     for a, w, x0, y0 in zip(amp, wid, cx, cy):
@@ -97,7 +111,7 @@ def c2(nx=128, ny=128, nz=16, order=4, precision="mixed", seed=SEED, flux2d="lf"
     tauy = np.zeros(cfg.n2)
     eta = np.zeros(cfg.n2)
     H3 = expand_2d_to_3d(cfg, h + eta)
-    T = 4.0 + 16.0 * (1.0 + Sg)
+    T = C2_T_SURFACE + C2_T_DZ * (expand_2d_to_3d(cfg, eta) + Sg * H3)  # T(z), z = eta + sigma H
     q = [np.zeros(cfg.n3), np.zeros(cfg.n3), T * H3, 35.0 * H3]
     nsub = 20
     dt = _cfl_dt(cfg, h.max(), nsub)
@@ -173,7 +187,8 @@ def c4(n: int = 512, L: float = 51200.0, seed: int = SEED, lam: float = 1.0, eps
 def c5_member(i: int, nx: int, ny: int, nz: int, order: int = 3, precision: str = "mixed",
               seed: int = SEED) -> dict:
     """Member i of the C5 ensemble: a closed 2 km-per-element basin with its own seeded
-    bathymetry (20-1000 m: a sloping shelf plus 8 Gaussian bumps) and uniform wind stress."""
+    bathymetry (20-1000 m: a sloping shelf plus 8 Gaussian bumps) and uniform wind stress;
+    temperature and salinity uniform (10 C, 35)."""
     rng = np.random.default_rng(seed + 1000 + i)
     L = 2e3
     cfg = DGConfig(nx=nx, ny=ny, nz=nz, order=order, Lx=nx * L, Ly=ny * L, precision=precision)
@@ -191,8 +206,8 @@ def c5_member(i: int, nx: int, ny: int, nz: int, order: int = 3, precision: str 
     tauy = np.full(cfg.n2, tau * np.sin(ang))
     eta = np.zeros(cfg.n2)
     H3 = expand_2d_to_3d(cfg, h + eta)
-    T = 8.0 + 8.0 * (1.0 + Sg)
-    q = [np.zeros(cfg.n3), np.zeros(cfg.n3), T * H3, 35.0 * H3]
+    # T and S at the equation of state's reference values: a wind-driven, unstratified member
+    q = [np.zeros(cfg.n3), np.zeros(cfg.n3), cfg.T0 * H3, cfg.S0 * H3]
     nsub = 20
     dt = _cfl_dt(cfg, h.max(), nsub)
     return dict(cfg=cfg, h=h, f=f, taux=taux, tauy=tauy, q=q, eta=eta, dt=dt, nsub=nsub,

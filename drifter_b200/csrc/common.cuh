@@ -76,10 +76,15 @@ HostBasis make_lgl_basis(int order);
 
 constexpr int MAXNP = 6;
 
-// Basis tables for device code (both precisions), uploaded once per process.
+// Basis tables for device code (both precisions), uploaded once per process. Ai is the
+// inverse of the strong-form derivative with the value at x = -1 lifted in,
+// (D + e_0 e_0^T / w_0)^-1, and a0 = Ai e_0 / w_0: the sigma velocity that is consistent with
+// the discrete tracer divergence is solved with them.
 struct DevBasis {
     double D[MAXNP * MAXNP], D2[MAXNP * MAXNP], S[MAXNP * MAXNP], w[MAXNP], x[MAXNP];
+    double Ai[MAXNP * MAXNP], a0[MAXNP];
     float Df[MAXNP * MAXNP], D2f[MAXNP * MAXNP], Sf[MAXNP * MAXNP], wf[MAXNP], xf[MAXNP];
+    float Aif[MAXNP * MAXNP], a0f[MAXNP];
 };
 
 // Device-memory RAII buffer.

@@ -42,6 +42,8 @@ struct BT<double, NP> {
     __device__ static double S(int i) { return cBs[NP].S[i]; }
     __device__ static double w(int i) { return cBs[NP].w[i]; }
     __device__ static double x(int i) { return cBs[NP].x[i]; }
+    __device__ static double Ai(int i) { return cBs[NP].Ai[i]; }
+    __device__ static double a0(int i) { return cBs[NP].a0[i]; }
 };
 template <int NP>
 struct BT<float, NP> {
@@ -50,6 +52,8 @@ struct BT<float, NP> {
     __device__ static float S(int i) { return cBs[NP].Sf[i]; }
     __device__ static float w(int i) { return cBs[NP].wf[i]; }
     __device__ static float x(int i) { return cBs[NP].xf[i]; }
+    __device__ static float Ai(int i) { return cBs[NP].Aif[i]; }
+    __device__ static float a0(int i) { return cBs[NP].a0f[i]; }
 };
 
 struct Geo {
@@ -58,6 +62,10 @@ struct Geo {
     double cx, cy, cs, Lx, Ly, Ls, dsig;
     double g, rho0, nu_h, nu_v, kT, kS, cd;
     double tide_amp, tide_w;
+    // linear equation of state of the baroclinic pressure gradient; eos = 0 switches it off
+    double alpha, beta, T0, S0;
+    double Tref_s, Tref_dz;  // reference stratification T_ref(z) = Tref_s + Tref_dz z
+    int eos;
 };
 
 __device__ __forceinline__ double tide_at(const Geo &G, double t) {
@@ -71,6 +79,12 @@ struct StageArgs {
     T *res[4];
     const double *eta, *h, *f, *taux, *tauy, *tdev;
     const double *corrU, *corrV;  // pending transport correction added to Hu, Hv on load (or null)
+    // pending volume correction of the tracers (with corrU): HT, HS scaled by 1 + corrR
+    const double *corrR;
+    // stage elevation of the baroclinic pressure (the step's eta at its first stage), and in an
+    // LSRK stage its update: etab_out = etab + B (A rese + dt deta), rese the 2D register
+    const double *etab;
+    double *etab_out, *rese;
     double toff;
     double *dHU3, *dHV3;
     T *omega_out;
@@ -181,15 +195,38 @@ __device__ __forceinline__ P2<double> p2add(P2<double> a, P2<double> b) { return
 __device__ __forceinline__ P2<double> p2sub(P2<double> a, P2<double> b) { return {a.x - b.x, a.y - b.y}; }
 
 // Shared-memory plan of the stage kernel for one water column (ncn = nz*(N+1)^3 nodes):
-//   two mbarriers (16 B), the FP64 column increments of the earlier stages [2][(N+1)^2],
-//   sQ[4][ncn] state, sRes[4][ncn] LSRK 2N register, sR[4][ncn]
-//   right-hand side, sD[ncn] horizontal divergence -> layer integrals (in place), per layer x
-//   2D-node increments, the column's 2D fields (1/H, H, eta), its pressure-gradient rows and
-//   1 + sigma per z node.
+//   three mbarriers (32 B), the FP64 column increments of the earlier stages [2][(N+1)^2],
+//   sQ[4][ncn] state, sRes[4][ncn] LSRK 2N register, sR[4][ncn] right-hand side, sD[ncn]
+//   horizontal divergence, per layer x 2D-node increments, the
+//   column's 2D fields (1/H, H, eta), its pressure-gradient rows, 1 + sigma per z node and the
+//   baroclinic pressure's 2D rows (its stage elevation, depth, 1 / depth and the slopes of
+//   both), and per layer x 2D-node quadrature totals of the divergence.
+// The baroclinic pressure P = H B at the column's nodes and across its four sides is formed
+// before the horizontal passes in the register slots of HT and HS (whose register is staged
+// after those passes), and its layer totals in sD; for N + 1 <= 3 the side values (and for
+// N = 1 the layer totals) do not fit there and take a tail of their own.
+template <int NP>
+struct StageTail {
+    static constexpr bool pn_in_res = 4 * NP * NP <= NP * NP * NP;  // sides' P in sRes[3]
+    static constexpr bool tb_in_d = NP + 4 <= NP * NP;             // layer totals in sD
+    static size_t elems(int nz) {
+        return (pn_in_res ? 0 : (size_t)4 * nz * NP * NP) + (tb_in_d ? 0 : (size_t)nz * NP * (NP + 4));
+    }
+};
+inline size_t stage_tail_elems(int nz, int np) {
+    switch (np) {
+    case 2: return StageTail<2>::elems(nz);
+    case 3: return StageTail<3>::elems(nz);
+    case 4: return StageTail<4>::elems(nz);
+    case 5: return StageTail<5>::elems(nz);
+    default: return StageTail<6>::elems(nz);
+    }
+}
 inline size_t stage_smem_bytes(int nz, int np, size_t tsz) {
     const int np2 = np * np, ncn = nz * np2 * np;
-    return 16 + (size_t)2 * np2 * 8 +
-           ((size_t)13 * ncn + (size_t)2 * nz * np2 + 5 * np2 + (size_t)nz * np) * tsz;
+    return 32 + (size_t)2 * np2 * 8 +
+           ((size_t)13 * ncn + (size_t)3 * nz * np2 + 12 * np2 + (size_t)nz * np + stage_tail_elems(nz, np)) *
+               tsz;
 }
 
 // One CTA per water column; work is organised in pencils (lines of N+1 nodes) so every
@@ -200,18 +237,21 @@ inline size_t stage_smem_bytes(int nz, int np, size_t tsz) {
 // mbarrier waits expect and `init` says whether this CTA still has to initialise the two
 // mbarriers (the first column a CTA processes). Returns false when a bounded wait gave up
 // (the status word is set); the CTA must then stop.
-template <typename T, int NP>
+// NZ > 0 compiles the column for that layer count (its sizes and shared-memory offsets become
+// constants); NZ = 0 takes the layer count from the arguments.
+template <typename T, int NP, int NZ = 0>
 __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, int c, uint32_t ph, bool init) {
     constexpr int NP2 = NP * NP, NP3 = NP2 * NP, N = NP - 1;
     using B = BT<T, NP>;
     const Geo &G = a.G;
-    const int nz = G.nz, ncn = nz * NP3, npen = nz * NP2;
+    const int nz = NZ > 0 ? NZ : G.nz, ncn = nz * NP3, npen = nz * NP2;
     const int ex = c % G.nx, ey = c / G.nx;
     const size_t base = (size_t)c * ncn;
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    // mbarriers: state, register of (Hu, Hv), register of (HT, HS)
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw);
-    double *sOld = reinterpret_cast<double *>(smem_raw + 16);  // [2][NP2] column increments so far
-    T *sQ = reinterpret_cast<T *>(smem_raw + 16 + 2 * NP2 * sizeof(double));  // [4][ncn]
+    double *sOld = reinterpret_cast<double *>(smem_raw + 32);  // [2][NP2] column increments so far
+    T *sQ = reinterpret_cast<T *>(smem_raw + 32 + 2 * NP2 * sizeof(double));  // [4][ncn]
     T *sRes = sQ + 4 * ncn;                        // [4][ncn]
     T *sR = sRes + 4 * ncn;                        // [4][ncn]
     T *sD = sR + 4 * ncn;                          // [ncn] divergence -> layer integrals
@@ -220,6 +260,20 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, int c, uint3
     T *sIH = sL2 + nz * NP2, *sHt = sIH + NP2, *sEt = sHt + NP2;
     T *sPx = sEt + NP2, *sPy = sPx + NP2;          // g H d(eta)/dx, g H d(eta)/dy per 2D node
     T *sS1 = sPy + NP2;                            // [nz][NP] 1 + sigma at the column's z nodes
+    // the baroclinic pressure's 2D rows (stage elevation etab): etab, Hb = etab + h, 1 / Hb,
+    // g d(etab)/dx, g d(etab)/dy, g dHb/dx, g dHb/dy
+    T *sEb = sS1 + nz * NP, *sHb = sEb + NP2, *sIHb = sHb + NP2;
+    T *sGEx = sIHb + NP2, *sGEy = sGEx + NP2, *sGHx = sGEy + NP2, *sGHy = sGHx + NP2;
+    T *sQl = sGHy + NP2;  // [nz][NP2] layer quadrature totals of the horizontal divergence
+    T *tail = sQl + nz * NP2;
+    // baroclinic pressure P = H B (B = int_sigma^0 b, b the density anomaly / rho0): at the
+    // column's nodes, across its sides [side][face node][layer][k], and the layer totals of b
+    // [layer][2D node] and [side][face node][layer]; alive from the pre-pass to the y pass
+    using Tl = StageTail<NP>;
+    T *sP = sRes + 2 * ncn;
+    T *sPn = Tl::pn_in_res ? sRes + 3 * ncn : tail;
+    T *sTb = Tl::tb_in_d ? sD : tail + (Tl::pn_in_res ? 0 : 4 * nz * NP2);
+    T *sTbn = sTb + nz * NP2;
     __shared__ int s_ok;
 
     // tidal elevation: evaluated once per CTA, and only by a column on a tidal side
@@ -234,6 +288,9 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, int c, uint3
     const T Lx = (T)G.Lx, Ly = (T)G.Ly, Ls = (T)G.Ls;
     const T g = (T)G.g;
     const bool need_res = a.mode == 0 && !a.first;
+    // with the baroclinic pressure on, the register of (HT, HS) is staged after the horizontal
+    // passes (its shared memory holds P until then)
+    const bool late = need_res && G.eos;
     // the column increments of the earlier stages, read while the column is being staged
     if (a.mode == 0 && !a.first)
         for (int t = threadIdx.x; t < NP2; t += blockDim.x) {
@@ -247,6 +304,7 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, int c, uint3
             if (init) {
                 mbar_init(&bars[0], 1);
                 mbar_init(&bars[1], 1);
+                mbar_init(&bars[2], 1);
             } else {
                 // shared memory of the previous column was read and written by this CTA's
                 // threads: order those accesses before the bulk copies overwrite it
@@ -256,10 +314,14 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, int c, uint3
             mbar_expect_tx(&bars[0], 4 * bytes);
 #pragma unroll
             for (int v = 0; v < 4; ++v) bulk_g2s(sQ + v * ncn, a.qin[v] + base, bytes, &bars[0]);
+            // the register in two halves, each completing one phase of its own barrier
             if (need_res) {
-                mbar_expect_tx(&bars[1], 4 * bytes);
-#pragma unroll
-                for (int v = 0; v < 4; ++v) bulk_g2s(sRes + v * ncn, a.res[v] + base, bytes, &bars[1]);
+                mbar_expect_tx(&bars[1], 2 * bytes);
+                for (int v = 0; v < 2; ++v) bulk_g2s(sRes + v * ncn, a.res[v] + base, bytes, &bars[1]);
+                if (!late) {
+                    mbar_expect_tx(&bars[2], 2 * bytes);
+                    for (int v = 2; v < 4; ++v) bulk_g2s(sRes + v * ncn, a.res[v] + base, bytes, &bars[2]);
+                }
             }
         }
     } else {
@@ -267,8 +329,7 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, int c, uint3
 #pragma unroll
             for (int v = 0; v < 4; ++v) sQ[v * ncn + n] = a.qin[v][base + n];
             if (need_res)
-#pragma unroll
-                for (int v = 0; v < 4; ++v) sRes[v * ncn + n] = a.res[v][base + n];
+                for (int v = 0; v < (late ? 2 : 4); ++v) sRes[v * ncn + n] = a.res[v][base + n];
         }
     }
     for (int t = threadIdx.x; t < NP2; t += blockDim.x) {
@@ -288,6 +349,28 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, int c, uint3
         }
         sPx[t] = g * (T)H * cx * gex;
         sPy[t] = g * (T)H * cy * gey;
+        if (G.eos) {
+            // the baroclinic pressure's column: depth Hb = etab + h and g dz/dx|_sigma =
+            // g d(etab)/dx + sigma g dHb/dx (element-local derivatives)
+            const double *bc = a.etab + (size_t)c * NP2, *hc = a.h + (size_t)c * NP2;
+            T gex2 = 0, gey2 = 0, ghx = 0, ghy = 0;
+#pragma unroll
+            for (int m = 0; m < NP; ++m) {
+                const T ex_ = (T)bc[m + NP * j], ey_ = (T)bc[i + NP * m];
+                gex2 += B::D(i * NP + m) * ex_;
+                gey2 += B::D(j * NP + m) * ey_;
+                ghx += B::D(i * NP + m) * (ex_ + (T)hc[m + NP * j]);
+                ghy += B::D(j * NP + m) * (ey_ + (T)hc[i + NP * m]);
+            }
+            const double Hb = bc[t] + hc[t];
+            sEb[t] = (T)bc[t];
+            sHb[t] = (T)Hb;
+            sIHb[t] = (T)(1.0 / Hb);
+            sGEx[t] = g * cx * gex2;
+            sGEy[t] = g * cy * gey2;
+            sGHx[t] = g * cx * ghx;
+            sGHy[t] = g * cy * ghy;
+        }
     }
     for (int t = threadIdx.x; t < nz * NP; t += blockDim.x) {
         const int ez = t / NP, k = t % NP;
@@ -312,6 +395,9 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, int c, uint3
         if (a.corrU) {
             o.q[0] += (T)a.corrU[n2];
             o.q[1] += (T)a.corrV[n2];
+            const T dr = (T)a.corrR[n2];
+            o.q[2] = fma(o.q[2], dr, o.q[2]);
+            o.q[3] = fma(o.q[3], dr, o.q[3]);
         }
         const double e = a.eta[n2];
         o.e = (T)e;
@@ -357,6 +443,131 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, int c, uint3
             const int an = n % NP2;
             sQ[n] += (T)a.corrU[(size_t)c * NP2 + an];
             sQ[ncn + n] += (T)a.corrV[(size_t)c * NP2 + an];
+            const T dr = (T)a.corrR[(size_t)c * NP2 + an];
+            sQ[2 * ncn + n] = fma(sQ[2 * ncn + n], dr, sQ[2 * ncn + n]);
+            sQ[3 * ncn + n] = fma(sQ[3 * ncn + n], dr, sQ[3 * ncn + n]);
+        }
+        __syncthreads();
+    }
+
+    // ---- baroclinic pressure (linear equation of state). The density anomaly against the
+    // reference stratification, b = beta (S - S0) - alpha (T - T_ref(z)) (T = HT / H, S = HS / H
+    // formed as deviations to keep their digits, z = eta + sigma H), at every node;
+    // B(sigma) = int_sigma^0 b is the sum of the totals of the layers from this one up minus the
+    // layer integral J_k = (dsig/2) sum_m S[k][m] b_m, and P = H B (p' = rho0 g P). The same is
+    // formed along the neighbouring columns' face lines (their P is the face value P+). The
+    // force on (Hu, Hv) is taken in flux form, -g [d(H P)/dx|_sigma - d(P dz/dx|_sigma)/dsigma]
+    // with dz/dx|_sigma = d(eta)/dx + sigma dH/dx: its sigma part is formed here along the
+    // column's z lines and starts the right-hand side of Hu and Hv; the horizontal passes add
+    // the x and y parts.
+    if (G.eos) {
+        const T al = (T)G.alpha, be = (T)G.beta, S0 = (T)G.S0;
+        const T Trs = (T)G.Tref_s, Trz = (T)G.Tref_dz;
+        const T hd2 = (T)(0.5 * G.dsig);
+        const int nfl = 4 * NP * nz;  // neighbour face lines: (side, face node, layer)
+        // the neighbouring column across side sd and the face node (ni, nj) of face line tt
+        auto face_line = [&](int sd, int tt, int &ni, int &nj) -> int {
+            int nc = -1;
+            ni = tt; nj = tt;
+            if (sd == 0 && ex > 0) { nc = c - 1; ni = N; }
+            if (sd == 1 && ex < G.nx - 1) { nc = c + 1; ni = 0; }
+            if (sd == 2 && ey > 0) { nc = c - G.nx; nj = N; }
+            if (sd == 3 && ey < G.ny - 1) { nc = c + G.nx; nj = 0; }
+            return nc;
+        };
+        // phase 1: layer integrals J_k into sP / sPn, layer totals into sTb / sTbn
+        for (int t = threadIdx.x; t < npen + nfl; t += blockDim.x) {
+            T bv[NP];
+            T *dst, *tot;
+            int dstep;
+            if (t < npen) {
+                const int ez = t / NP2, an = t % NP2, e0 = ez * NP3 + an;
+                const T iH = sIHb[an], H = sHb[an], et = sEb[an];
+#pragma unroll
+                for (int m = 0; m < NP; ++m) {
+                    const int n = e0 + NP2 * m;
+                    const T Tr = fma(Trz, fma(sS1[ez * NP + m] - T(1), H, et), Trs);
+                    bv[m] = fma(be, fma(sQ[3 * ncn + n], iH, -S0), -al * fma(sQ[2 * ncn + n], iH, -Tr));
+                }
+                dst = sP + e0;
+                dstep = NP2;
+                tot = sTb + ez * NP2 + an;
+            } else {
+                const int f = t - npen, sd = f / (NP * nz), tt = (f / nz) % NP, ez = f % nz;
+                int ni, nj;
+                const int nc = face_line(sd, tt, ni, nj);
+                if (nc < 0) continue;
+                const size_t n2 = (size_t)nc * NP2 + ni + NP * nj;
+                const double en = a.etab[n2], Hd = en + a.h[n2];
+                const T Hn = (T)Hd, etn = (T)en;
+                // the neighbour's pending tracer volume correction, folded into 1 / H
+                const T iHn = (T)((a.corrU ? 1.0 + a.corrR[n2] : 1.0) / Hd);
+                const size_t nb = (size_t)nc * ncn + (size_t)ez * NP3 + ni + NP * nj;
+#pragma unroll
+                for (int m = 0; m < NP; ++m) {
+                    const T Tr = fma(Trz, fma(sS1[ez * NP + m] - T(1), Hn, etn), Trs);
+                    bv[m] = fma(be, fma(a.qin[3][nb + NP2 * m], iHn, -S0),
+                                -al * fma(a.qin[2][nb + NP2 * m], iHn, -Tr));
+                }
+                dst = sPn + ((sd * NP + tt) * nz + ez) * NP;
+                dstep = 1;
+                tot = sTbn + (sd * NP + tt) * nz + ez;
+            }
+#pragma unroll
+            for (int k = 0; k < NP; ++k) {
+                T sk = 0;
+#pragma unroll
+                for (int m = 0; m < NP; ++m) sk += B::S(k * NP + m) * bv[m];
+                const T J = k == 0 ? T(0) : hd2 * sk;
+                dst[dstep * k] = J;
+                if (k == N) *tot = J;
+            }
+        }
+        __syncthreads();
+        // phase 2: P = H (sum of the layer totals from this layer up - J_k), in place; the
+        // column's z lines also form the sigma part of the force, g d(P dz/dx)/dsigma
+        for (int t = threadIdx.x; t < npen + nfl; t += blockDim.x) {
+            if (t < npen) {
+                const int ez = t / NP2, an = t % NP2, e0 = ez * NP3 + an;
+                T Tab = 0;
+                for (int e = nz - 1; e >= ez; --e) Tab += sTb[e * NP2 + an];
+                const T H = sHb[an];
+                const T px = sGEx[an], py = sGEy[an], hx = sGHx[an], hy = sGHy[an];
+                T Pk[NP], zx[NP], zy[NP];
+#pragma unroll
+                for (int k = 0; k < NP; ++k) {
+                    Pk[k] = H * (Tab - sP[e0 + NP2 * k]);
+                    sP[e0 + NP2 * k] = Pk[k];
+                    // g dz/dx|_sigma = g d(etab)/dx + sigma g dHb/dx
+                    const T sg = sS1[ez * NP + k] - T(1);
+                    zx[k] = fma(sg, hx, px);
+                    zy[k] = fma(sg, hy, py);
+                }
+#pragma unroll
+                for (int k = 0; k < NP; ++k) {
+                    T sx = 0, sy = 0;
+#pragma unroll
+                    for (int m = 0; m < NP; ++m) {
+                        sx += B::D(k * NP + m) * (Pk[m] * zx[m]);
+                        sy += B::D(k * NP + m) * (Pk[m] * zy[m]);
+                    }
+                    sR[e0 + NP2 * k] = cs * sx;
+                    sR[ncn + e0 + NP2 * k] = cs * sy;
+                }
+            } else {
+                const int f = t - npen, sd = f / (NP * nz), tt = (f / nz) % NP, ez = f % nz;
+                int ni, nj;
+                const int nc = face_line(sd, tt, ni, nj);
+                if (nc < 0) continue;
+                const size_t n2 = (size_t)nc * NP2 + ni + NP * nj;
+                const T Hn = (T)(a.etab[n2] + a.h[n2]);
+                const T *tl = sTbn + (sd * NP + tt) * nz;
+                T Tab = 0;
+                for (int e = nz - 1; e >= ez; --e) Tab += tl[e];
+                T *pl = sPn + ((sd * NP + tt) * nz + ez) * NP;
+#pragma unroll
+                for (int k = 0; k < NP; ++k) pl[k] = Hn * (Tab - pl[k]);
+            }
         }
         __syncthreads();
     }
@@ -370,7 +581,8 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, int c, uint3
     const bool hdiff = G.nu_h > 0.0;
     // one horizontal pencil: axis 0 (x, sides 0/1) or 1 (y, sides 2/3), a compile-time
     // constant of each instance; nodes e0 + st*m
-    auto hpass = [&](auto AX, int e0, int st, int iy, int jx, const Side &o0, const Side &oN) {
+    auto hpass = [&](auto AX, int e0, int st, int iy, int jx, const Side &o0, const Side &oN, T Pp0,
+                     T PpN) {
         constexpr int axis = decltype(AX)::value;
         const T cd = axis == 0 ? cx : cy, Ld = axis == 0 ? Lx : Ly;
         const T ep0 = o0.e, epN = oN.e, Hp0 = o0.H, HpN = oN.H;
@@ -402,6 +614,24 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, int c, uint3
                 if (i == N) d += Ld * (T(0.5) * (qN + qb) - qN);
                 if (axis == 0) sD[e0 + st * i] = d;
                 else sD[e0 + st * i] += d;
+            }
+        }
+        // (3) baroclinic pressure: -g d(H P)/dx|_sigma with the central face value, added to the
+        // momentum component of this direction (the pre-pass left the sigma part there, and the
+        // x pass's momentum pair adds to it)
+        if (G.eos) {
+            T HP[NP];  // H P along the pencil
+#pragma unroll
+            for (int m = 0; m < NP; ++m) HP[m] = sHb[an2(m)] * sP[e0 + st * m];
+#pragma unroll
+            for (int i = 0; i < NP; ++i) {
+                T dP = 0;
+#pragma unroll
+                for (int m = 0; m < NP; ++m) dP += B::D(i * NP + m) * HP[m];
+                T fp = cd * dP;
+                if (i == 0) fp -= Ld * (T(0.5) * (Pp0 - HP[0]));
+                if (i == N) fp += Ld * (T(0.5) * (PpN - HP[N]));
+                sR[(axis == 0 ? 0 : ncn) + e0 + st * i] -= g * fp;
             }
         }
         // normal velocities and LF speeds at both ends
@@ -455,7 +685,7 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, int c, uint3
                     }
                 }
                 const int n = e0 + st * i, v0 = 2 * pr;
-                if (axis == 0) {
+                if (axis == 0 && !(pr == 0 && G.eos)) {
                     sR[v0 * ncn + n] = r.x;
                     sR[(v0 + 1) * ncn + n] = r.y;
                 } else {
@@ -465,13 +695,34 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, int c, uint3
             }
         }
     };
+    // H+ P+ across side sd at the pencil end node nEnd (2D node anEnd): the neighbour's face
+    // line, else the mirror value on a wall, else the exterior depth squared times this
+    // column's B
+    auto pplus = [&](bool has, int sd, int tt, int ez, int k, int nEnd, int anEnd, const Side &o) -> T {
+        if (!G.eos) return T(0);
+        if (has) {
+            int ni, nj;
+            const int nc = sd <= 1 ? (sd == 0 ? c - 1 : c + 1) : (sd == 2 ? c - G.nx : c + G.nx);
+            ni = sd == 0 ? N : (sd == 1 ? 0 : tt);
+            nj = sd == 2 ? N : (sd == 3 ? 0 : tt);
+            const size_t n2 = (size_t)nc * NP2 + ni + NP * nj;
+            return (T)(a.etab[n2] + a.h[n2]) * sPn[((sd * NP + tt) * nz + ez) * NP + k];
+        }
+        const T HPm = sHb[anEnd] * sP[nEnd];
+        const int bcs = sd == 0 ? G.bc[0] : (sd == 1 ? G.bc[1] : (sd == 2 ? G.bc[2] : G.bc[3]));
+        if (bcs != DRF_BC_TIDE) return HPm;
+        const T r = o.H * sIHb[anEnd];
+        return r * r * HPm;
+    };
     // x pencils (j, k, layer); the first one's neighbour faces were prefetched
     auto xpencil = [&](int p, Side &o0, Side &oN, bool h0, bool hN) {
         const int ez = p / NP2, j = p % NP, k = (p / NP) % NP;
         const int e0 = ez * NP3 + NP * (j + NP * k);
         if (!h0) basin_side(0, 0, j, e0, o0);
         if (!hN) basin_side(1, N, j, e0 + N, oN);
-        hpass(std::integral_constant<int, 0>{}, e0, 1, j, 0, o0, oN);
+        const T Pp0 = pplus(h0, 0, j, ez, k, e0, NP * j, o0);
+        const T PpN = pplus(hN, 1, j, ez, k, e0 + N, N + NP * j, oN);
+        hpass(std::integral_constant<int, 0>{}, e0, 1, j, 0, o0, oN, Pp0, PpN);
     };
     if (threadIdx.x < npen) xpencil(threadIdx.x, fx0, fxN, hx0, hxN);
     for (int p = threadIdx.x + blockDim.x; p < npen; p += blockDim.x) {
@@ -495,7 +746,9 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, int c, uint3
         const int e0 = ez * NP3 + i + NP2 * k;
         if (!h0) basin_side(2, i, 0, e0, o0);
         if (!hN) basin_side(3, i, N, e0 + NP * N, oN);
-        hpass(std::integral_constant<int, 1>{}, e0, NP, 0, i, o0, oN);
+        const T Pp0 = pplus(h0, 2, i, ez, k, e0, i, o0);
+        const T PpN = pplus(hN, 3, i, ez, k, e0 + NP * N, i + NP * N, oN);
+        hpass(std::integral_constant<int, 1>{}, e0, NP, 0, i, o0, oN, Pp0, PpN);
     };
     if (threadIdx.x < npen) ypencil(threadIdx.x, fy0, fyN, hy0, hyN);
     for (int p = threadIdx.x + blockDim.x; p < npen; p += blockDim.x) {
@@ -505,21 +758,29 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, int c, uint3
         ypencil(p, o0, oN, h0, hN);
     }
     __syncthreads();
-    // ---- layer integrals J_k = (dsig/2) sum_m S[k][m] delta_m: z pencils
+    // the register of (HT, HS) now that P is no longer read from its shared memory
+    if (late) {
+        if (a.bulk) {
+            if (threadIdx.x == 0) {
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                const uint32_t bytes = (uint32_t)(ncn * sizeof(T));
+                mbar_expect_tx(&bars[2], 2 * bytes);
+                for (int v = 2; v < 4; ++v) bulk_g2s(sRes + v * ncn, a.res[v] + base, bytes, &bars[2]);
+            }
+        } else {
+            for (int n = threadIdx.x; n < ncn; n += blockDim.x)
+                for (int v = 2; v < 4; ++v) sRes[v * ncn + n] = a.res[v][base + n];
+        }
+    }
+    // ---- layer quadrature totals of the horizontal divergence, Q = (dsig/2) sum_k w_k delta_k
     const T hds = (T)(0.5 * G.dsig);
     for (int p = threadIdx.x; p < npen; p += blockDim.x) {
         const int ez = p / NP2, an = p % NP2;
         const int e0 = ez * NP3 + an;
-        T del[NP];
+        T sq = 0;
 #pragma unroll
-        for (int m = 0; m < NP; ++m) del[m] = sD[e0 + NP2 * m];
-#pragma unroll
-        for (int k = 0; k < NP; ++k) {
-            T s = 0;
-#pragma unroll
-            for (int m = 0; m < NP; ++m) s += B::S(k * NP + m) * del[m];
-            sD[e0 + NP2 * k] = (k == 0) ? T(0) : hds * s;
-        }
+        for (int m = 0; m < NP; ++m) sq += B::w(m) * sD[e0 + NP2 * m];
+        sQl[ez * NP2 + an] = hds * sq;
     }
     __syncthreads();
 
@@ -533,25 +794,47 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, int c, uint3
             return false;
         }
     }
+    // the (HT, HS) half of the register: each thread waits for it before its first (HT, HS) pair
+    bool w2 = !(a.bulk && need_res);
+    __shared__ int s_ok2;
+    if (threadIdx.x == 0) s_ok2 = 1;
+    __syncthreads();
     for (int p = threadIdx.x; p < npen; p += blockDim.x) {
         const int ez = p / NP2, an = p % NP2;
         const int e0 = ez * NP3 + an;
         const T iH = sIH[an], fa = (T)a.f[(size_t)c * NP2 + an];
         const bool bed = ez == 0, top = ez == nz - 1;
-        // omega of this pencil: H omega(sigma) = -I(sigma) + (1 + sigma) I(top), with I the
-        // cumulative layer integral (the layer totals summed bottom-up, as a sequential scan)
-        T Ib = 0;
-        for (int e = 0; e < ez; ++e) Ib = Ib + sD[e * NP3 + an + NP2 * N];
-        T It = Ib;
-        for (int e = ez; e < nz; ++e) It = It + sD[e * NP3 + an + NP2 * N];
-        if (a.mode == 1 && a.deta_out && bed) a.deta_out[(size_t)c * NP2 + an] = -(double)It;
+        // the sigma velocity consistent with the discrete divergence: per layer, bottom up,
+        // H omega = y solves cs D y + Ls e_0 (y_0 - M0) = I - delta (the strong-form continuity
+        // with the mass flux M0 through the layer's bottom face lifted in), I the column's
+        // quadrature total of delta; with the LGL weights each layer passes on M1 = M0 + dsig I
+        // - Q(layer), and the flux through the surface is 0 by the choice of I
+        T Iq = 0, M0 = 0;
+        for (int e = 0; e < nz; ++e) Iq += sQl[e * NP2 + an];
+        const T dsg = (T)G.dsig;
+        for (int e = 0; e < ez; ++e) M0 += dsg * Iq - sQl[e * NP2 + an];
+        const T M1 = top ? T(0) : M0 + (dsg * Iq - sQl[ez * NP2 + an]);
+        if (bed) M0 = 0;
+        if (a.mode == 1 && a.deta_out && bed) a.deta_out[(size_t)c * NP2 + an] = -(double)Iq;
+        if (a.mode == 0 && bed) {  // the stage elevation, advanced like the 3D state
+            const size_t i2 = (size_t)c * NP2 + an;
+            const double re = (a.first ? 0.0 : (double)a.A * a.rese[i2]) - (double)a.dt * (double)Iq;
+            a.rese[i2] = re;
+            a.etab_out[i2] = a.etab[i2] + (double)a.B * re;
+        }
         T om[NP];
+        {
+            T gq[NP];
 #pragma unroll
-        for (int k = 0; k < NP; ++k) {
-            const T I = Ib + sD[e0 + NP2 * k];
-            const T s1 = sS1[ez * NP + k];
-            om[k] = (-I + s1 * It) * iH;
-            if (a.mode == 1 && a.omega_out) a.omega_out[base + e0 + NP2 * k] = om[k];
+            for (int m = 0; m < NP; ++m) gq[m] = Iq - sD[e0 + NP2 * m];
+#pragma unroll
+            for (int k = 0; k < NP; ++k) {
+                T sy = 0;
+#pragma unroll
+                for (int m = 0; m < NP; ++m) sy += B::Ai(k * NP + m) * gq[m];
+                om[k] = fma(hds, sy, B::a0(k) * M0) * iH;
+                if (a.mode == 1 && a.omega_out) a.omega_out[base + e0 + NP2 * k] = om[k];
+            }
         }
         // bed stress (only the bottom layer's k = 0 node) and surface stress
         T fbx = 0, fby = 0;
@@ -568,15 +851,19 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, int c, uint3
         }
         const T w0 = om[0] * T(-1), wN = om[N];
         const int nb0 = (ez - 1) * NP3 + an + NP2 * N, nbN = (ez + 1) * NP3 + an;
-        // omega is continuous across layer faces by construction (the neighbour's end value
-        // is computed from the same prefix and sigma), so the neighbour's value is this one's
-        const T wp0 = bed ? T(0) : w0, wpN = top ? T(0) : wN;
-        const T lam0 = fmax(fabs(w0), fabs(wp0)), lamN = fmax(fabs(wN), fabs(wpN));
+        // face fluxes n M q_up / H: the mass flux carries the upwind value (from below when it
+        // is upward)
+        const bool up0 = !bed && M0 > T(0), dn1 = !top && M1 < T(0);
+        const T f0 = -M0 * iH, f1 = M1 * iH;
         P2<T> inc = bc(T(0));
         // vertical diffusion kappa / H d2(q / H)/dsigma2 with the 1/H of q / H taken out of the sum
         const T ihc = iH * cs * cs * iH;
 #pragma unroll 1
         for (int pr = 0; pr < 2; ++pr) {
+            if (pr == 1 && !w2) {
+                if (!mbar_wait(&bars[2], ph)) s_ok2 = 0;
+                w2 = true;
+            }
             const int v0 = 2 * pr, v1 = v0 + 1;
             // the pair's output arrays, selected without indexing the parameter arrays
             T *const res0 = pr == 0 ? a.res[0] : a.res[2], *const res1 = pr == 0 ? a.res[1] : a.res[3];
@@ -606,33 +893,19 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, int c, uint3
                     r.y += -fa * q[k].x;
                 }
                 if (k == 0) {
-                    const T wm = w0;
-                    if (!bed) {
-                        const P2<T> qpp = {sQ[v0 * ncn + nb0], sQ[v1 * ncn + nb0]};
-                        const P2<T> fs = p2sub(p2mul(bc(T(0.5)), p2add(p2mul(q[0], bc(wm)), p2mul(qpp, bc(wp0)))),
-                                               p2mul(bc(T(0.5) * lam0), p2sub(qpp, q[0])));
-                        r = p2fma(bc(-Ls), p2sub(fs, p2mul(q[0], bc(wm))), r);
-                    } else {
-                        r = p2fma(bc(-Ls), p2sub(bc(T(0)), p2mul(q[0], bc(wm))), r);
-                        if (pr == 0) {
-                            r.x += fbx;
-                            r.y += fby;
-                        }
+                    const P2<T> qup = up0 ? P2<T>{sQ[v0 * ncn + nb0], sQ[v1 * ncn + nb0]} : q[0];
+                    r = p2fma(bc(-Ls), p2sub(p2mul(qup, bc(f0)), p2mul(q[0], bc(w0))), r);
+                    if (bed && pr == 0) {
+                        r.x += fbx;
+                        r.y += fby;
                     }
                 }
                 if (k == N) {
-                    const T wm = wN;
-                    if (!top) {
-                        const P2<T> qpp = {sQ[v0 * ncn + nbN], sQ[v1 * ncn + nbN]};
-                        const P2<T> fs = p2sub(p2mul(bc(T(0.5)), p2add(p2mul(q[N], bc(wm)), p2mul(qpp, bc(wpN)))),
-                                               p2mul(bc(T(0.5) * lamN), p2sub(qpp, q[N])));
-                        r = p2fma(bc(-Ls), p2sub(fs, p2mul(q[N], bc(wm))), r);
-                    } else {
-                        r = p2fma(bc(-Ls), p2sub(bc(T(0)), p2mul(q[N], bc(wm))), r);
-                        if (pr == 0) {
-                            r.x += fsx;
-                            r.y += fsy;
-                        }
+                    const P2<T> qup = dn1 ? P2<T>{sQ[v0 * ncn + nbN], sQ[v1 * ncn + nbN]} : q[N];
+                    r = p2fma(bc(-Ls), p2sub(p2mul(qup, bc(f1)), p2mul(q[N], bc(wN))), r);
+                    if (top && pr == 0) {
+                        r.x += fsx;
+                        r.y += fsy;
                     }
                 }
                 const size_t gi = base + n;
@@ -655,6 +928,13 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, int c, uint3
         if (a.mode == 0) {
             sL1[ez * NP2 + an] = inc.x;
             sL2[ez * NP2 + an] = inc.y;
+        }
+    }
+    if (a.bulk && need_res) {
+        __syncthreads();
+        if (!s_ok2) {
+            if (threadIdx.x == 0) atomicExch(a.err, DRF_E_TIMEOUT);
+            return false;
         }
     }
     if (a.mode == 0) {
@@ -682,9 +962,19 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, int c, uint3
 }
 
 // One model: one CTA per water column.
-template <typename T, int NP>
+template <typename T, int NP, int NZ>
 __global__ void __launch_bounds__(STAGE_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) dg3d_stage_kernel(StageArgs<T> a) {
-    stage_column<T, NP>(a, blockIdx.x, 0u, true);
+    stage_column<T, NP, NZ>(a, blockIdx.x, 0u, true);
+}
+// Layer counts the single-model stage kernel is compiled for (others run the NZ = 0 form):
+// 4 (config C1) and 16 (C2) at orders 3 and 4.
+template <typename T, int NP, class F>
+void dispatch_stage_nz(int nz, F &&f) {
+    if constexpr (NP == 4 || NP == 5) {
+        if (nz == 4) return f(dg3d_stage_kernel<T, NP, 4>);
+        if (nz == 16) return f(dg3d_stage_kernel<T, NP, 16>);
+    }
+    f(dg3d_stage_kernel<T, NP, 0>);
 }
 
 // ------------------------------------------------------------------------- barotropic (FP64)
@@ -925,16 +1215,26 @@ __global__ void BARO_BOUNDS baro_corr_kernel(BaroArgs a, double dtb, const doubl
     baro_corr_body<NP, FK, CPB>(a, blockIdx.x, a.toff, dtb, k1e, k1u, k1v, e, hu, hv, esum, first);
 }
 
+// the tracer volume correction: the 3D stages moved HT, HS with the column divergence of the
+// 3D transport (stage elevation etbf at the step's end), the barotropic step ended at eta;
+// scaling the columns' tracers by (eta + h) / (etbf + h) = 1 + corrR keeps T = HT / H
+__device__ __forceinline__ double tracer_volume_correction(double eta, double etbf, double h) {
+    return (eta - etbf) / (etbf + h);
+}
+
 __global__ void baro_finish_kernel(int64_t n2, int nsub, double dt, const double *esum,
                                    double *eta_avg, const double *HU, const double *HV,
                                    const double *HUo, const double *HVo, const double *dHU3,
-                                   const double *dHV3, double *corrU, double *corrV, double *tdev) {
+                                   const double *dHV3, double *corrU, double *corrV, double *tdev,
+                                   const double *eta, const double *etbf, const double *h,
+                                   double *corrR) {
     const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (t == 0) tdev[0] = tdev[0] + dt;
     if (t >= n2) return;
     eta_avg[t] = esum[t] / nsub;
     corrU[t] = HU[t] - (HUo[t] + dHU3[t]);
     corrV[t] = HV[t] - (HVo[t] + dHV3[t]);
+    corrR[t] = tracer_volume_correction(eta[t], etbf[t], h[t]);
 }
 
 // Memory-only counterpart of the stage kernel: the same CTA shape and dynamic shared memory
@@ -1000,8 +1300,10 @@ __device__ __forceinline__ void shift_stage(StageArgs<T> &a, const EnsMember &m,
         a.res[v] += m.off3;
     }
     a.eta += m.off2; a.h += m.off2; a.f += m.off2; a.taux += m.off2; a.tauy += m.off2;
-    if (a.corrU) { a.corrU += m.off2; a.corrV += m.off2; }
+    if (a.corrU) { a.corrU += m.off2; a.corrV += m.off2; a.corrR += m.off2; }
     a.dHU3 += m.off2; a.dHV3 += m.off2;
+    a.etab += m.off2;
+    if (a.etab_out) { a.etab_out += m.off2; a.rese += m.off2; }
     a.tdev += idx;
     a.dt = (T)m.dt;
     a.bulk = m.bulk;
@@ -1016,13 +1318,14 @@ __global__ void __launch_bounds__(STAGE_MAX_THREADS, sizeof(T) == 4 ? 2 : 1)
     dg3d_stage_ens_kernel(StageArgs<T> a, const EnsMember *mem, const int2 *items, int nitems) {
     __shared__ StageArgs<T> sa;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    if (threadIdx.x == 0) {  // the column's two mbarriers, initialised once per CTA
+    if (threadIdx.x == 0) {  // the column's three mbarriers, initialised once per CTA
         uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw);
         mbar_init(&bars[0], 1);
         mbar_init(&bars[1], 1);
+        mbar_init(&bars[2], 1);
     }
-    // each column staged by bulk copies completes one phase of both barriers (the register
-    // barrier only in stages that read the register, which is the same for every item)
+    // each column staged by bulk copies completes one phase of every barrier (the two register
+    // barriers only in stages that read the register, which is the same for every item)
     uint32_t ph = 0;
     for (int w = blockIdx.x; w < nitems; w += gridDim.x) {
         const int2 wi = items[w];
@@ -1094,13 +1397,15 @@ __global__ void baro_finish_ens_kernel(int64_t n2, int nsub, const EnsMember *me
                                        const double *esum, double *eta_avg, const double *HU,
                                        const double *HV, const double *HUo, const double *HVo,
                                        const double *dHU3, const double *dHV3, double *corrU,
-                                       double *corrV, double *tdev) {
+                                       double *corrV, double *tdev, const double *eta,
+                                       const double *etbf, const double *h, double *corrR) {
     const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (t < nmem) tdev[t] = tdev[t] + mem[t].dt;
     if (t >= n2) return;
     eta_avg[t] = esum[t] / nsub;
     corrU[t] = HU[t] - (HUo[t] + dHU3[t]);
     corrV[t] = HV[t] - (HVo[t] + dHV3[t]);
+    corrR[t] = tracer_volume_correction(eta[t], etbf[t], h[t]);
 }
 
 // ------------------------------------------------------- persistent barotropic step (FP64)
@@ -1119,9 +1424,14 @@ struct SubcycleArgs {
     const double *dHU3, *dHV3;
     double *Fx, *Fy, *HUo, *HVo, *k1e, *k1u, *k1v, *es, *us, *vs;
     double *eta, *HU, *HV, *esum, *eta_avg, *corrU, *corrV;
+    const double *etbf;        // stage elevation at the end of the 3D stages
+    double *corrR;             // tracer volume correction
     double *tdev;              // the model's clock (an ensemble: member 0's, the others follow)
     unsigned *sync;            // [0] barrier arrivals, [1] CTAs finished, [2] abort; zero at launch
     int *err;
+    // failure-detection check: the CTA of this index withholds its arrival at the first grid
+    // barrier, so every CTA's bounded wait there gives up (-1: none, the normal case)
+    int hold;
 };
 
 __device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned *p) {
@@ -1133,15 +1443,16 @@ __device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned *p) {
 // Grid-wide barrier of a cooperative launch (all CTAs resident): the n-th barrier completes
 // when n * gridDim.x arrivals are counted. The wait is bounded; a CTA that gives up, or that
 // sees another CTA's abort word, sets the abort word and the status word and returns false.
-__device__ __forceinline__ bool grid_barrier(unsigned *sync, unsigned target, int *err) {
+// `arrive` false withholds this CTA's arrival (the failure-detection check only).
+__device__ __forceinline__ bool grid_barrier(unsigned *sync, unsigned target, int *err, bool arrive = true) {
     __shared__ int s_go;
     __syncthreads();
     if (threadIdx.x == 0) {
         __threadfence();
-        atomicAdd(&sync[0], 1u);
+        if (arrive) atomicAdd(&sync[0], 1u);
         int go = 1;
         for (long it = 0; ld_acquire_gpu(&sync[0]) < target; ++it) {
-            if (it > (1L << 22) || ld_acquire_gpu(&sync[2]) != 0u) {
+            if (it > (1L << 21) || ld_acquire_gpu(&sync[2]) != 0u) {
                 go = 0;
                 break;
             }
@@ -1197,7 +1508,8 @@ __global__ void BARO_BOUNDS baro_subcycles_kernel(const __grid_constant__ BaroAr
                                             s.k1v + o, s.es + o, s.us + o, s.vs + o);
             });
         }
-        if (!grid_barrier(s.sync, ++nbar * gridDim.x, s.err)) return;
+        const bool arrive = !(nbar == 0 && (int)blockIdx.x == s.hold);
+        if (!grid_barrier(s.sync, ++nbar * gridDim.x, s.err, arrive)) return;
         for (int w = blockIdx.x; w < s.ntiles; w += gridDim.x) {
             __syncthreads();
             sub_item<ENS>(s, ac, w, [&](const BaroArgs &a, int64_t tile, int64_t o, double, double dtb) {
@@ -1218,6 +1530,7 @@ __global__ void BARO_BOUNDS baro_subcycles_kernel(const __grid_constant__ BaroAr
             s.eta_avg[t] = s.esum[t] / s.nsub;
             s.corrU[t] = s.HU[t] - (s.HUo[t] + s.dHU3[t]);
             s.corrV[t] = s.HV[t] - (s.HVo[t] + s.dHV3[t]);
+            s.corrR[t] = tracer_volume_correction(s.eta[t], s.etbf[t], a.h[t - o]);
         });
     }
     // the clock(s) advance once every CTA is past its last read of them
@@ -1265,8 +1578,8 @@ void launch_subcycles(const BaroArgs &af, const BaroArgs &ap, const BaroArgs &ac
 }
 
 template <typename T, int NP>
-__global__ void correct3d_kernel(int64_t n3, int nz, T *Hu, T *Hv, const double *cu,
-                                 const double *cv) {
+__global__ void correct3d_kernel(int64_t n3, int nz, T *Hu, T *Hv, T *HT, T *HS, const double *cu,
+                                 const double *cv, const double *cr) {
     constexpr int NP2 = NP * NP, NP3 = NP2 * NP;
     const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (t >= n3) return;
@@ -1275,6 +1588,9 @@ __global__ void correct3d_kernel(int64_t n3, int nz, T *Hu, T *Hv, const double 
     const int64_t i2 = c * NP2 + an;
     Hu[t] = Hu[t] + (T)cu[i2];
     Hv[t] = Hv[t] + (T)cv[i2];
+    const T dr = (T)cr[i2];
+    HT[t] = fma(HT[t], dr, HT[t]);
+    HS[t] = fma(HS[t], dr, HS[t]);
 }
 
 // depth integral per 2D node of a 3D field (FP64 accumulation)
@@ -1339,8 +1655,8 @@ __device__ __forceinline__ void block_reduce(double (&v)[Q], const int (&op)[Q],
 template <typename T, int NP>
 __global__ void __launch_bounds__(256) diag3d_kernel(int ncol, int nz, const T *Hu, const T *Hv, const T *HT,
                                                      const T *HS, const double *eta, const double *h,
-                                                     const double *corrU, const double *corrV, double wvol,
-                                                     double *part) {
+                                                     const double *corrU, const double *corrV,
+                                                     const double *corrR, double wvol, double *part) {
     constexpr int NP2 = NP * NP, NP3 = NP2 * NP;
     __shared__ double red[6][8];
     const int ncn = nz * NP3;
@@ -1352,15 +1668,18 @@ __global__ void __launch_bounds__(256) diag3d_kernel(int ncol, int nz, const T *
             const size_t i2 = (size_t)c * NP2 + an, t = base + ln;
             const double H = eta[i2] + h[i2];
             const double wv = wvol * cBs[NP].w[i] * cBs[NP].w[j] * cBs[NP].w[k];
-            T huT = Hu[t], hvT = Hv[t];
+            T huT = Hu[t], hvT = Hv[t], htT = HT[t], hsT = HS[t];
             if (corrU) {
                 huT = huT + (T)corrU[i2];
                 hvT = hvT + (T)corrV[i2];
+                const T dr = (T)corrR[i2];
+                htT = fma(htT, dr, htT);
+                hsT = fma(hsT, dr, hsT);
             }
-            const double hu = huT, hv = hvT, ht = HT[t];
+            const double hu = huT, hv = hvT, ht = htT;
             v[0] += wv * 0.5 * (hu * hu + hv * hv) / H;
             v[1] += wv * ht;
-            v[2] += wv * (double)HS[t];
+            v[2] += wv * (double)hsT;
             v[3] = fmax(v[3], sqrt(hu * hu + hv * hv) / H);
             v[4] = fmax(v[4], ht / H);
             v[5] = fmin(v[5], ht / H);
@@ -1499,6 +1818,10 @@ struct drf_dg {
     // barotropic step as one persistent launch (false: one launch per pass); fixed when the
     // step graphs are built, from DRIFTER_B200_BARO_PERSISTENT (1 selects the persistent form)
     bool baro_persist = false;
+    // failure-detection check of the persistent barotropic launch: the CTA that withholds its
+    // first grid-barrier arrival (-1 none); fixed when the step graphs are built, from
+    // DRIFTER_B200_DEBUG_HOLD_ARRIVAL
+    int debug_hold = -1;
     // 3D arrays: q3p + (array * n3s + node) * tsz; n3s = n3 for a model that owns its memory,
     // the pool length for an ensemble member (a view into the ensemble's pools)
     unsigned char *q3p = nullptr;
@@ -1509,7 +1832,7 @@ struct drf_dg {
            *HU = nullptr, *HV = nullptr, *eta_avg = nullptr, *esum = nullptr, *Fx = nullptr,
            *Fy = nullptr, *HUo = nullptr, *HVo = nullptr, *k1[3] = {}, *us[3] = {}, *dHU3 = nullptr,
            *dHV3 = nullptr, *tdev = nullptr, *scratch2 = nullptr, *corrU = nullptr,
-           *corrV = nullptr;
+           *corrV = nullptr, *etb[2] = {}, *rese = nullptr, *corrR = nullptr;
     int cur = 0;
     bool pending = false;  // a transport correction in corrU/corrV is not yet in q(cur)
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
@@ -1525,10 +1848,10 @@ struct drf_dg {
     void *res(int v) { return q3p + ((size_t)8 + v) * n3s * tsz; }
     void *tmp(int v) { return q3p + ((size_t)12 + v) * n3s * tsz; }
 
-    // 2D arrays per model (26 named arrays, then the model time)
-    static constexpr int N2ARRAYS = 27;
+    // 2D arrays per model (28 named arrays, then the model time)
+    static constexpr int N2ARRAYS = 29;
     // Points the model at its device memory: 16 3D arrays of stride3 values from q3base and
-    // 26 2D arrays of stride2 values from d2base; tdev_ is its clock and err_ its status word.
+    // 28 2D arrays of stride2 values from d2base; tdev_ is its clock and err_ its status word.
     void bind(unsigned char *q3base, int64_t stride3, double *d2base, int64_t stride2, double *tdev_,
               int *err_) {
         q3p = q3base;
@@ -1542,6 +1865,7 @@ struct drf_dg {
         for (int i = 0; i < 3; ++i) us[i] = take();
         dHU3 = take(); dHV3 = take(); scratch2 = take();
         corrU = take(); corrV = take();
+        etb[0] = take(); etb[1] = take(); rese = take(); corrR = take();
         tdev = tdev_;
         err = err_;
     }
@@ -1571,7 +1895,7 @@ struct drf_dg {
                       bool with_corr = false) {
         const StageArgs<T> a = stage_args<T>(in, out, s, dt, mode, rout, omega_out, deta_out, eta_use, toff,
                                              with_corr);
-        dg3d_stage_kernel<T, NP><<<ncol, stage_threads(), smem, stream>>>(a);
+        dispatch_stage_nz<T, NP>(G.nz, [&](auto kern) { kern<<<ncol, stage_threads(), smem, stream>>>(a); });
         DRF_LAUNCHED();
     }
     template <typename T>
@@ -1585,6 +1909,11 @@ struct drf_dg {
             a.res[v] = mode == 1 ? (T *)rout[v] : (T *)res(v);
         }
         a.eta = eta_use; a.h = h; a.f = f; a.taux = taux; a.tauy = tauy; a.tdev = tdev;
+        // the baroclinic pressure's stage elevation: the step's eta at its first stage, then
+        // ping-pong buffers advanced by the stages (an RHS-only launch reads eta_use)
+        a.etab = (mode == 1 || s == 0) ? eta_use : etb[(s - 1) % 2];
+        a.etab_out = mode == 1 ? nullptr : etb[s % 2];
+        a.rese = mode == 1 ? nullptr : rese;
         a.toff = toff;
         a.dHU3 = dHU3; a.dHV3 = dHV3;
         a.omega_out = omega_out; a.deta_out = deta_out;
@@ -1592,6 +1921,7 @@ struct drf_dg {
         a.mode = mode; a.first = (s == 0);
         a.corrU = with_corr ? corrU : nullptr;
         a.corrV = with_corr ? corrV : nullptr;
+        a.corrR = with_corr ? corrR : nullptr;
         a.bulk = ((size_t)G.nz * np3 * sizeof(T)) % 16 == 0;
         a.err = err;
         a.G = G;
@@ -1602,11 +1932,12 @@ struct drf_dg {
     template <typename T, int NP>
     void materialize_t() {
         if (!pending) return;
-        correct3d_kernel<T, NP><<<blocks_for(n3), 256, 0, stream>>>(n3, G.nz, (T *)q(cur, 0),
-                                                                  (T *)q(cur, 1), corrU, corrV);
+        correct3d_kernel<T, NP><<<blocks_for(n3), 256, 0, stream>>>(
+            n3, G.nz, (T *)q(cur, 0), (T *)q(cur, 1), (T *)q(cur, 2), (T *)q(cur, 3), corrU, corrV, corrR);
         DRF_LAUNCHED();
         DRF_CUDA(cudaMemsetAsync(corrU, 0, n2 * 8, stream));
         DRF_CUDA(cudaMemsetAsync(corrV, 0, n2 * 8, stream));
+        DRF_CUDA(cudaMemsetAsync(corrR, 0, n2 * 8, stream));
         pending = false;
     }
     void materialize() {
@@ -1636,9 +1967,11 @@ struct drf_dg {
         s.es = us[0]; s.us = us[1]; s.vs = us[2];
         s.eta = eta; s.HU = HU; s.HV = HV; s.esum = esum; s.eta_avg = eta_avg;
         s.corrU = corrU; s.corrV = corrV;
+        s.etbf = etb[0]; s.corrR = corrR;
         s.tdev = tdev;
         s.sync = syncbuf.p;
         s.err = err;
+        s.hold = debug_hold;
         return s;
     }
 
@@ -1689,7 +2022,7 @@ struct drf_dg {
         });
         baro_finish_kernel<<<blocks_for(n2), 256, 0, stream>>>(n2, nsub, dt, esum, eta_avg, HU, HV,
                                                                HUo, HVo, dHU3, dHV3, corrU, corrV,
-                                                               tdev);
+                                                               tdev, eta, etb[0], h, corrR);
         DRF_LAUNCHED();
     }
 
@@ -1733,6 +2066,43 @@ void upload_phys_basis(const HostBasis &b) {
     for (int i = 0; i < b.np; ++i) {
         db.w[i] = b.w[i]; db.x[i] = b.x[i];
         db.wf[i] = (float)b.w[i]; db.xf[i] = (float)b.x[i];
+    }
+    // (D + e_0 e_0^T / w_0)^-1 by Gauss-Jordan elimination with partial pivoting
+    {
+        const int n = b.np;
+        std::vector<double> A(b.D), I((size_t)n * n, 0.0);
+        A[0] += 1.0 / b.w[0];
+        for (int i = 0; i < n; ++i) I[(size_t)i * n + i] = 1.0;
+        for (int c = 0; c < n; ++c) {
+            int pr = c;
+            for (int r = c + 1; r < n; ++r)
+                if (std::fabs(A[(size_t)r * n + c]) > std::fabs(A[(size_t)pr * n + c])) pr = r;
+            for (int k = 0; k < n; ++k) {
+                std::swap(A[(size_t)c * n + k], A[(size_t)pr * n + k]);
+                std::swap(I[(size_t)c * n + k], I[(size_t)pr * n + k]);
+            }
+            const double d = A[(size_t)c * n + c];
+            for (int k = 0; k < n; ++k) {
+                A[(size_t)c * n + k] /= d;
+                I[(size_t)c * n + k] /= d;
+            }
+            for (int r = 0; r < n; ++r) {
+                if (r == c) continue;
+                const double f = A[(size_t)r * n + c];
+                for (int k = 0; k < n; ++k) {
+                    A[(size_t)r * n + k] -= f * A[(size_t)c * n + k];
+                    I[(size_t)r * n + k] -= f * I[(size_t)c * n + k];
+                }
+            }
+        }
+        for (int i = 0; i < n * n; ++i) {
+            db.Ai[i] = I[i];
+            db.Aif[i] = (float)I[i];
+        }
+        for (int k = 0; k < n; ++k) {
+            db.a0[k] = I[(size_t)k * n] / b.w[0];
+            db.a0f[k] = (float)db.a0[k];
+        }
     }
     DRF_CUDA(cudaMemcpyToSymbol(cBs, &db, sizeof(db), (size_t)b.np * sizeof(DevBasis)));
     if (dev < 64) done[dev][b.np] = true;
@@ -1815,6 +2185,9 @@ void drf_dg::setup(const drf_mesh_desc *mesh, const drf_dg_params *params, const
     G.kT = params->kappa_v_T; G.kS = params->kappa_v_S; G.cd = params->cd;
     G.tide_amp = params->tide_amp;
     G.tide_w = params->tide_period != 0.0 ? 2.0 * M_PI / params->tide_period : 0.0;
+    G.alpha = params->alpha; G.beta = params->beta; G.T0 = params->T0; G.S0 = params->S0;
+    G.Tref_s = params->Tref_s; G.Tref_dz = params->Tref_dz;
+    G.eos = (params->alpha != 0.0 || params->beta != 0.0) ? 1 : 0;
     upload_phys_basis(basis);
     // shared memory of the stage kernel: 9 column arrays + per-layer bases + 2D scalars
     smem = stage_smem_bytes(mesh->nz, np, tsz);
@@ -1828,7 +2201,9 @@ void drf_dg::setup(const drf_mesh_desc *mesh, const drf_dg_params *params, const
     with_types([&](auto tv, auto npc) {
         using T = decltype(tv);
         constexpr int NP = decltype(npc)::value;
-        allow_max_dynamic_smem(reinterpret_cast<const void *>(dg3d_stage_kernel<T, NP>), maxsm);
+        dispatch_stage_nz<T, NP>(mesh->nz, [&](auto kern) {
+            allow_max_dynamic_smem(reinterpret_cast<const void *>(kern), maxsm);
+        });
     });
 }
 
@@ -1990,6 +2365,7 @@ int drf_dg_upload_state(drf_dg *m, const double *const *q4, const double *eta, d
         DRF_CUDA(cudaMemcpyAsync(m->tdev, &t, 8, cudaMemcpyHostToDevice, m->stream));
         DRF_CUDA(cudaMemsetAsync(m->corrU, 0, m->n2 * 8, m->stream));
         DRF_CUDA(cudaMemsetAsync(m->corrV, 0, m->n2 * 8, m->stream));
+        DRF_CUDA(cudaMemsetAsync(m->corrR, 0, m->n2 * 8, m->stream));
         m->pending = false;
         DRF_CUDA(cudaStreamSynchronize(m->stream));
         m->drop_graphs();
@@ -2072,6 +2448,8 @@ int drf_dg_step_modesplit(drf_dg *m, double dt, int nsub, int nsteps) {
             m->drop_graphs();
             const char *pe = std::getenv("DRIFTER_B200_BARO_PERSISTENT");
             m->baro_persist = pe && pe[0] == '1';
+            const char *ph = std::getenv("DRIFTER_B200_DEBUG_HOLD_ARRIVAL");
+            m->debug_hold = ph && ph[0] ? std::atoi(ph) : -1;
             for (int in = 0; in < 2; ++in)
                 m->graph[in] = capture_graph(m->stream, [&] {
                     m->with_types([&](auto tv, auto npc) {
@@ -2247,7 +2625,8 @@ int drf_dg_diagnostics(drf_dg *m, double *out10) {
             diag3d_kernel<T, NP><<<nb3, 256, 0, m->stream>>>(
                 m->ncol, m->G.nz, (const T *)m->q(c, 0), (const T *)m->q(c, 1), (const T *)m->q(c, 2),
                 (const T *)m->q(c, 3), m->eta, m->h, m->pending ? m->corrU : nullptr,
-                m->pending ? m->corrV : nullptr, 0.125 * dx * dy * m->G.dsig, p3);
+                m->pending ? m->corrV : nullptr, m->pending ? m->corrR : nullptr,
+                0.125 * dx * dy * m->G.dsig, p3);
             DRF_LAUNCHED();
             diag2d_kernel<NP><<<nb2, 256, 0, m->stream>>>(m->n2, m->G.nz, m->eta, m->h,
                                                          0.25 * dx * dy, m->G.g, p2);
@@ -2339,10 +2718,12 @@ int drf_dg_time_stage(drf_dg *m, int nrep, double *ms, double *alg_bytes, double
         // algorithmic bytes of one stage: per 3D DOF (node x variable) state read + write and
         // 2N-register read + write, plus the horizontal face traces of the 4 neighbouring
         // columns (4/(N+1) of a state read); per 2D node eta, h, f (+ surface stress on the top
-        // layer) reads and the FP64 column-increment read + write.
+        // layer) reads and the FP64 column-increment read + write; with the baroclinic pressure
+        // the stage elevation's read and write and its register's read and write per 2D node.
         const double s = (double)m->tsz;
         const double per_dof = s * (4.0 + 4.0 / m->np);
-        if (alg_bytes) *alg_bytes = (double)m->n3 * 4.0 * per_dof + (double)m->n2 * 8.0 * (3 + 2 + 4);
+        const int n2words = 3 + 2 + 4 + (m->G.eos ? 4 : 0);
+        if (alg_bytes) *alg_bytes = (double)m->n3 * 4.0 * per_dof + (double)m->n2 * 8.0 * n2words;
         if (ndof) *ndof = (double)m->n3 * 4.0;
     });
 }
@@ -2393,7 +2774,11 @@ struct drf_ens {
     DevBuf<double> d2;                         // 26 pooled 2D arrays + one clock per member
     DevBuf<int> errbuf;
     DevBuf<unsigned> syncbuf;  // grid-barrier words of the persistent barotropic launch
-    bool baro_persist = false;  // as drf_dg::baro_persist
+    bool baro_persist = false;
+    // failure-detection check of the persistent barotropic launch: the CTA that withholds its
+    // first grid-barrier arrival (-1 none); fixed when the step graphs are built, from
+    // DRIFTER_B200_DEBUG_HOLD_ARRIVAL
+    int debug_hold = -1;  // as drf_dg::baro_persist
     DevBuf<EnsMember> table;
     DevBuf<int2> items, tiles;
     std::vector<EnsMember> htab;
@@ -2468,7 +2853,7 @@ struct drf_ens {
         const int64_t nfin = n2tot > (int64_t)mem.size() ? n2tot : (int64_t)mem.size();
         baro_finish_ens_kernel<<<blocks_for(nfin), 256, 0, stream>>>(
             n2tot, nsub, table.p, (int)mem.size(), m0->esum, m0->eta_avg, m0->HU, m0->HV, m0->HUo, m0->HVo,
-            m0->dHU3, m0->dHV3, m0->corrU, m0->corrV, m0->tdev);
+            m0->dHU3, m0->dHV3, m0->corrU, m0->corrV, m0->tdev, m0->eta, m0->etb[0], m0->h, m0->corrR);
         DRF_LAUNCHED();
     }
 };

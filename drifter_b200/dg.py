@@ -110,6 +110,16 @@ class DGConfig:
     bc: tuple = ("wall", "wall", "wall", "wall")
     tide_amp: float = 0.0
     tide_period: float = 44714.0
+    # linear equation of state (EquationOfState include/physics/equation_of_state.hpp:35-40);
+    # alpha = beta = 0 switches the baroclinic pressure gradient off
+    alpha: float = 2e-4
+    beta: float = 7.6e-4
+    T0: float = 10.0
+    S0: float = 35.0
+    # reference stratification T_ref(z) = Tref_s + Tref_dz z subtracted before the pressure
+    # integral (its own pressure has no horizontal gradient); (T0, 0) subtracts nothing
+    Tref_s: float = 10.0
+    Tref_dz: float = 0.0
 
     @property
     def np_(self) -> int:
@@ -129,6 +139,8 @@ def _mesh_params(cfg: DGConfig):
     prm = _abi.DGParams()
     prm.g, prm.rho0, prm.nu_h, prm.nu_v = cfg.g, cfg.rho0, cfg.nu_h, cfg.nu_v
     prm.kappa_v_T, prm.kappa_v_S, prm.cd = cfg.kappa_v_T, cfg.kappa_v_S, cfg.cd
+    prm.alpha, prm.beta, prm.T0, prm.S0 = cfg.alpha, cfg.beta, cfg.T0, cfg.S0
+    prm.Tref_s, prm.Tref_dz = cfg.Tref_s, cfg.Tref_dz
     prm.flux2d = _abi.FLUX[cfg.flux2d]
     prm.precision = _abi.PREC[cfg.precision]
     for s in range(4):

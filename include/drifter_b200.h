@@ -93,6 +93,15 @@ typedef struct {
     int32_t precision;                     /* DRF_PREC_FP64 or DRF_PREC_MIXED */
     int32_t bc[4];                         /* west, east, south, north: DRF_BC_* */
     double tide_amp, tide_period;          /* tidal elevation on DRF_BC_TIDE sides */
+    /* linear equation of state rho = rho0 (1 - alpha (T - T0) + beta (S - S0)) of the
+     * baroclinic pressure gradient (EquationOfState include/physics/equation_of_state.hpp:35-40,
+     * defaults 2e-4, 7.6e-4, 10, 35); alpha = beta = 0 switches that gradient off */
+    double alpha, beta, T0, S0;
+    /* horizontally uniform reference stratification T_ref(z) = Tref_s + Tref_dz z (z <= 0 up
+     * from the surface, S_ref = S0): the pressure is integrated from the density anomaly
+     * against it (its own pressure has no horizontal gradient). Tref_s = T0, Tref_dz = 0
+     * subtracts nothing. */
+    double Tref_s, Tref_dz;
 } drf_dg_params;
 
 /* Creates the model: h (bathymetry > 0), f (Coriolis), taux/tauy (surface stress, N/m^2)

@@ -28,6 +28,8 @@ static PhysParams phys_from(const int *iv, const double *dv) {
     p.Lx = dv[0]; p.Ly = dv[1]; p.g = dv[2]; p.rho0 = dv[3]; p.nu_h = dv[4]; p.nu_v = dv[5];
     p.kappa_v_T = dv[6]; p.kappa_v_S = dv[7]; p.cd = dv[8]; p.tide_amp = dv[9];
     p.tide_period = dv[10];
+    p.alpha = dv[11]; p.beta = dv[12]; p.T0 = dv[13]; p.S0 = dv[14];
+    p.Tref_s = dv[15]; p.Tref_dz = dv[16];
     return p;
 }
 
@@ -118,11 +120,13 @@ int orc_phys_get_state(void *hd, double *const *q4, double *eta, double *HU, dou
     })
 }
 
-int orc_phys_rhs(void *hd, double *const *r4, double *omega, double *deta) {
+// etab: the baroclinic pressure's surface elevation (null: the model's eta)
+int orc_phys_rhs(void *hd, double *const *r4, double *omega, double *deta, const double *etab) {
     ORC_TRY({
         auto *m = static_cast<PhysModel *>(hd);
-        Vec R[4], om, de;
-        m->rhs3d(m->Q, m->eta, m->t, R, &om, &de);
+        Vec R[4], om, de, eb;
+        if (etab) eb.assign(etab, etab + m->n2);
+        m->rhs3d(m->Q, m->eta, m->t, R, &om, &de, etab ? &eb : nullptr);
         for (int v = 0; v < 4; ++v) std::memcpy(r4[v], R[v].data(), sizeof(double) * m->n3);
         std::memcpy(omega, om.data(), sizeof(double) * m->n3);
         std::memcpy(deta, de.data(), sizeof(double) * m->n2);

@@ -7,6 +7,7 @@
 #include <cmath>
 #include <stdexcept>
 #include <thread>
+#include <functional>
 
 namespace orc {
 
@@ -143,6 +144,33 @@ static void fill_S(Basis1D &b) {
     }
 }
 
+// Ainv = (D + e_0 e_0^T / w_0)^-1 by Gauss-Jordan elimination with partial pivoting.
+static void fill_Ainv(Basis1D &b) {
+    const int n = b.np();
+    Vec A(b.D), I(n * n, 0.0);
+    A[0] += 1.0 / b.weights[0];
+    for (int i = 0; i < n; ++i) I[i * n + i] = 1.0;
+    for (int c = 0; c < n; ++c) {
+        int pr = c;
+        for (int r = c + 1; r < n; ++r)
+            if (std::abs(A[r * n + c]) > std::abs(A[pr * n + c])) pr = r;
+        for (int k = 0; k < n; ++k) {
+            std::swap(A[c * n + k], A[pr * n + k]);
+            std::swap(I[c * n + k], I[pr * n + k]);
+        }
+        const double d = A[c * n + c];
+        for (int k = 0; k < n; ++k) { A[c * n + k] /= d; I[c * n + k] /= d; }
+        for (int r = 0; r < n; ++r) {
+            if (r == c) continue;
+            const double f = A[r * n + c];
+            for (int k = 0; k < n; ++k) { A[r * n + k] -= f * A[c * n + k]; I[r * n + k] -= f * I[c * n + k]; }
+        }
+    }
+    b.Ainv = I;
+    b.a0.assign(n, 0.0);
+    for (int k = 0; k < n; ++k) b.a0[k] = I[k * n + 0] / b.weights[0];
+}
+
 Basis1D make_lgl(int order) {
     Basis1D b;
     b.order = order;
@@ -150,6 +178,7 @@ Basis1D make_lgl(int order) {
     b.bary = barycentric_weights(b.nodes);
     b.D = derivative_matrix(b.nodes);
     fill_S(b);
+    fill_Ainv(b);
     return b;
 }
 Basis1D make_gl(int order) {
@@ -709,21 +738,96 @@ void PhysModel::column_integral(const Vec &g3, Vec &out2) const {
         }
 }
 
+// Runs fn(c0, c1) on contiguous ranges of the ncol water columns on the host's threads
+// (ORACLE_THREADS in the environment caps them; 1 runs inline).
+static void for_columns(int ncol, const std::function<void(int, int)> &fn) {
+    int nt = (int)std::thread::hardware_concurrency();
+    if (const char *e = std::getenv("ORACLE_THREADS")) nt = std::atoi(e);
+    nt = std::max(1, std::min(nt, ncol / 4));
+    if (nt <= 1) {
+        fn(0, ncol);
+        return;
+    }
+    std::vector<std::thread> th;
+    for (int t = 0; t < nt; ++t)
+        th.emplace_back(fn, (int)((long)ncol * t / nt), (int)((long)ncol * (t + 1) / nt));
+    for (auto &x : th) x.join();
+}
+
+// Hydrostatic pressure of the density anomaly, PressureGradientElement::hydrostatic_pressure
+// (include/physics/pressure_gradient.hpp:232-249: p(k) = sum_{j>=k} w_j g rho H, a surface-down
+// column sum) taken over the whole water column and integrated exactly per layer with the
+// integration matrix S: p'/rho0 = g H B(sigma), B(sigma) = int_sigma^0 b dsigma'. The density
+// is the reference's linear equation of state (src/physics/mode_splitting.cpp:589-598).
+void PhysModel::baroclinic_B(const Vec *Qin, const Vec &etaf, Vec &b3, Vec &B3) const {
+    const int N = p.order, nz = p.nz;
+    b3.assign(n3, 0.0);
+    B3.assign(n3, 0.0);
+    for_columns(ncol, [&](int cb, int ce) {
+    for (int c = cb; c < ce; ++c) {
+        const size_t base = (size_t)c * nz * np3;
+        for (int a = 0; a < np2; ++a) {
+            // b - b_ref(z) = beta (S - S0) - alpha (T - T_ref(z)), T = HT / H, S = HS / H,
+            // z = eta + sigma H
+            const double e = etaf[(size_t)c * np2 + a], H = e + h[(size_t)c * np2 + a];
+            const double iH = 1.0 / H;
+            for (int ez = 0; ez < nz; ++ez)
+                for (int k = 0; k < np; ++k) {
+                    const size_t n = base + (size_t)ez * np3 + a + np2 * k;
+                    const double sg = -1.0 + dsig * (ez + 0.5 * (b.nodes[k] + 1.0));
+                    const double Tr = p.Tref_s + p.Tref_dz * (e + sg * H);
+                    b3[n] = p.beta * (Qin[3][n] * iH - p.S0) - p.alpha * (Qin[2][n] * iH - Tr);
+                }
+            // I(sigma) = int_{-1}^{sigma} b, layer by layer (as the omega scan); B = I(0) - I
+            double Ib = 0.0;
+            std::vector<double> I((size_t)nz * np);
+            for (int ez = 0; ez < nz; ++ez) {
+                double J[16];
+                for (int k = 0; k < np; ++k) {
+                    double s = 0.0;
+                    for (int m = 0; m < np; ++m)
+                        s += b.S[k * np + m] * b3[base + (size_t)ez * np3 + a + np2 * m];
+                    J[k] = 0.5 * dsig * s;
+                }
+                J[0] = 0.0;
+                for (int k = 0; k < np; ++k) I[ez * np + k] = Ib + J[k];
+                Ib += J[N];
+            }
+            for (int ez = 0; ez < nz; ++ez)
+                for (int k = 0; k < np; ++k) {
+                    double Bv = Ib - I[ez * np + k];
+                    if (ez == nz - 1 && k == N) Bv = 0.0;
+                    B3[base + (size_t)ez * np3 + a + np2 * k] = Bv;
+                }
+        }
+    }
+    });
+}
+
 void PhysModel::rhs3d(const Vec *Qin, const Vec &etaf, double tb, Vec *R, Vec *omega3,
-                      Vec *deta2) const {
+                      Vec *deta2, const Vec *etab_in) const {
+    const Vec &etab = etab_in ? *etab_in : etaf;
     const int N = p.order, nz = p.nz;
     const double *D = b.D.data();
     const double wend = b.weights[0];
     const double Lx = (2.0 / dx) / wend, Ly = (2.0 / dy) / wend, Ls = (2.0 / dsig) / wend;
     const double cx = 2.0 / dx, cy = 2.0 / dy, cs = 2.0 / dsig;
     const int ncn = nz * np3;
-    Vec om(ncn), del(ncn), Icol(ncn);
-    Vec Hc(np2), iHc(np2);
     if (omega3) omega3->assign(n3, 0.0);
     if (deta2) deta2->assign(n2, 0.0);
     for (int v = 0; v < 4; ++v) R[v].assign(n3, 0.0);
     const double etide = tide(tb);
-    for (int c = 0; c < ncol; ++c) {
+    // baroclinic pressure: b and B at every node (neighbour columns' B is read at faces)
+    const bool baroclinic = p.alpha != 0.0 || p.beta != 0.0;
+    Vec b3, B3;
+    if (baroclinic) baroclinic_B(Qin, etab, b3, B3);
+    // water columns are independent given the inputs: split them over host threads (each
+    // column is computed by one thread in the same order, so the result does not depend on
+    // the thread count)
+    for_columns(ncol, [&](int c0, int c1) {
+    Vec om(ncn), del(ncn), Mf((size_t)(nz + 1) * np2);  // Mf: mass flux H omega through layer faces
+    Vec Hc(np2), iHc(np2);
+    for (int c = c0; c < c1; ++c) {
         const int ex = c % p.nx, ey = c / p.nx;
         const size_t base = (size_t)c * ncn;
         auto q = [&](int v, int ez, int i, int j, int k) -> double {
@@ -789,30 +893,37 @@ void PhysModel::rhs3d(const Vec *Qin, const Vec &etaf, double tb, Vec *R, Vec *o
                         }
                         del[ez * np3 + i + np * (j + np * k)] = d;
                     }
-        // ---- column scan: I(sigma) = int_{-1}^{sigma} delta
+        // ---- sigma velocity consistent with the discrete tracer divergence: per layer, bottom
+        // up, H omega = y solves the strong-form continuity cs D y + Ls e_0 (y_0 - y*) = I - delta
+        // with y* the mass flux through the layer's bottom face (0 at the bed) and I the
+        // LGL-quadrature column integral of delta (so that the flux through the surface is 0).
+        // Integrated with the LGL weights each layer gives y*(top) = y*(bottom) + dsig I -
+        // (dsig/2) sum_k w_k delta_k, the prefix that defines the face mass fluxes.
         for (int a = 0; a < np2; ++a) {
-            double Ib = 0.0;
+            const double hds = 0.5 * dsig;
+            double Iq = 0.0;
+            std::vector<double> Ql(nz);
             for (int ez = 0; ez < nz; ++ez) {
-                double J[16];
+                double qv = 0.0;
+                for (int k = 0; k < np; ++k) qv += b.weights[k] * del[ez * np3 + a + np2 * k];
+                Ql[ez] = hds * qv;
+                Iq += Ql[ez];
+            }
+            double ystar = 0.0;
+            for (int ez = 0; ez < nz; ++ez) {
+                Mf[ez * np2 + a] = ystar;
+                double g[16];
+                for (int k = 0; k < np; ++k) g[k] = Iq - del[ez * np3 + a + np2 * k];
                 for (int k = 0; k < np; ++k) {
                     double s = 0.0;
-                    for (int m = 0; m < np; ++m) s += b.S[k * np + m] * del[ez * np3 + a + np2 * m];
-                    J[k] = 0.5 * dsig * s;
+                    for (int m = 0; m < np; ++m) s += b.Ainv[k * np + m] * g[m];
+                    const double y = hds * s + b.a0[k] * ystar;
+                    om[ez * np3 + a + np2 * k] = y * iHc[a];
                 }
-                J[0] = 0.0;
-                for (int k = 0; k < np; ++k) Icol[ez * np3 + a + np2 * k] = Ib + J[k];
-                Ib = Ib + J[N];
+                ystar += dsig * Iq - Ql[ez];
             }
-            const double Itot = Ib;
-            for (int ez = 0; ez < nz; ++ez)
-                for (int k = 0; k < np; ++k) {
-                    double s1 = dsig * (ez + 0.5 * (b.nodes[k] + 1.0));
-                    if (ez == nz - 1 && k == N) s1 = 1.0;
-                    const int idx = ez * np3 + a + np2 * k;
-                    const double Hw = -Icol[idx] + s1 * Itot;
-                    om[idx] = Hw * iHc[a];
-                }
-            if (deta2) (*deta2)[(size_t)c * np2 + a] = -Itot;
+            Mf[nz * np2 + a] = 0.0;  // no flux through the surface
+            if (deta2) (*deta2)[(size_t)c * np2 + a] = -Iq;
         }
         if (omega3)
             for (int n = 0; n < ncn; ++n) (*omega3)[base + n] = om[n];
@@ -846,6 +957,38 @@ void PhysModel::rhs3d(const Vec *Qin, const Vec &etaf, double tb, Vec *R, Vec *o
                         }
                         r[0] += fa * q(1, ez, i, j, k) - p.g * Hh * cx * gex;
                         r[1] += -fa * q(0, ez, i, j, k) - p.g * Hh * cy * gey;
+                        // baroclinic pressure gradient -(H/rho0) grad_z p' with p'/rho0 = g H B:
+                        // -g H [d(H B)/dx|_sigma + b (d(eta)/dx + sigma dH/dx)], as z = eta + sigma H
+                        // gives d(sigma)/dx|_z = -(d(eta)/dx + sigma dH/dx) / H and dp'/dsigma =
+                        // -rho0 g H b (PressureGradientElement::baroclinic_gradient_standard,
+                        // include/physics/pressure_gradient.hpp:251-292). The derivative of P = H B
+                        // is the strong DG derivative with a central face value (below).
+                        if (baroclinic) {
+                            // flux form: H dp'/dx|_z = d(H p')/dx|_sigma - d(p' dz/dx|_sigma)/dsigma,
+                            // p' = rho0 g P, P = Hb B, with the column depth Hb = etab + h of the
+                            // pressure's own elevation; dz/dx|_sigma = d(etab)/dx + sigma dHb/dx
+                            double dPx = 0.0, dPy = 0.0, dEx = 0.0, dEy = 0.0, dHx = 0.0, dHy = 0.0;
+                            for (int m = 0; m < np; ++m) {
+                                const size_t ax = (size_t)c * np2 + m + np * j, ay = (size_t)c * np2 + i + np * m;
+                                const double Hx2 = etab[ax] + h[ax], Hy2 = etab[ay] + h[ay];
+                                dPx += D[i * np + m] * Hx2 * Hx2 * B3[base + (size_t)ez * np3 + m + np * (j + np * k)];
+                                dPy += D[j * np + m] * Hy2 * Hy2 * B3[base + (size_t)ez * np3 + i + np * (m + np * k)];
+                                dEx += D[i * np + m] * etab[ax];
+                                dEy += D[j * np + m] * etab[ay];
+                                dHx += D[i * np + m] * Hx2;
+                                dHy += D[j * np + m] * Hy2;
+                            }
+                            const double Hb = etab[(size_t)c * np2 + a] + h[(size_t)c * np2 + a];
+                            double dSx = 0.0, dSy = 0.0;
+                            for (int m = 0; m < np; ++m) {
+                                const double sgm = -1.0 + dsig * (ez + 0.5 * (b.nodes[m] + 1.0));
+                                const double Pm_ = Hb * B3[base + (size_t)ez * np3 + i + np * (j + np * m)];
+                                dSx += D[k * np + m] * Pm_ * (cx * dEx + sgm * cx * dHx);
+                                dSy += D[k * np + m] * Pm_ * (cy * dEy + sgm * cy * dHy);
+                            }
+                            r[0] -= p.g * (cx * dPx - cs * dSx);
+                            r[1] -= p.g * (cy * dPy - cs * dSy);
+                        }
                         if (p.nu_h > 0.0) {
                             for (int comp = 0; comp < 2; ++comp) {
                                 double sxx = 0.0, syy = 0.0;
@@ -893,23 +1036,47 @@ void PhysModel::rhs3d(const Vec *Qin, const Vec &etaf, double tb, Vec *R, Vec *o
                             const double pj = p.g * Hh * 0.5 * (ep - em);
                             r[0] -= L * pj * nx;
                             r[1] -= L * pj * ny;
+                            if (baroclinic) {
+                                // (H P)+ across the face: the neighbour's Hb^2 B; on a wall the
+                                // mirror state (no jump); on the tidal side the exterior depth with
+                                // this column's B (T, S copied across)
+                                const double Hb = etab[(size_t)c * np2 + a] + h[(size_t)c * np2 + a];
+                                const double Pm = Hb * Hb * B3[base + ln];
+                                double Pp = Pm;
+                                int nc = -1, ni = i, nj = j;
+                                if (s == 0 && ex > 0) { nc = c - 1; ni = N; }
+                                if (s == 1 && ex < p.nx - 1) { nc = c + 1; ni = 0; }
+                                if (s == 2 && ey > 0) { nc = c - p.nx; nj = N; }
+                                if (s == 3 && ey < p.ny - 1) { nc = c + p.nx; nj = 0; }
+                                if (nc >= 0) {
+                                    const size_t n2n = (size_t)nc * np2 + ni + np * nj;
+                                    const double Hbn = etab[n2n] + h[n2n];
+                                    Pp = Hbn * Hbn * B3[(size_t)nc * ncn + (size_t)ez * np3 + ni + np * (nj + np * k)];
+                                } else if (p.bc[s] == 1) {
+                                    Pp = Hp * Hp * B3[base + ln];
+                                }
+                                const double pb = p.g * 0.5 * (Pp - Pm);
+                                r[0] -= L * pb * nx;
+                                r[1] -= L * pb * ny;
+                            }
                         }
-                        // vertical faces
+                        // vertical faces: the layer face's mass flux M (upward) carries the
+                        // upwind value; at the bed and the surface M = 0
                         if (k == 0 || k == N) {
                             const double nrm = k == 0 ? -1.0 : 1.0;
                             const double wm = om[ln] * nrm;
+                            const double M = Mf[(k == 0 ? ez : ez + 1) * np2 + a];
                             const bool interior = (k == 0 && ez > 0) || (k == N && ez < nz - 1);
-                            if (interior) {
-                                const int ez2 = k == 0 ? ez - 1 : ez + 1, k2 = k == 0 ? N : 0;
-                                const double wp = om[ez2 * np3 + i + np * (j + np * k2)] * nrm;
-                                const double lam = std::max(std::abs(wm), std::abs(wp));
-                                for (int v = 0; v < 4; ++v) {
-                                    const double qm = q(v, ez, i, j, k), qpp = q(v, ez2, i, j, k2);
-                                    const double fs = 0.5 * (qm * wm + qpp * wp) - 0.5 * lam * (qpp - qm);
-                                    r[v] -= Ls * (fs - qm * wm);
-                                }
-                            } else {
-                                for (int v = 0; v < 4; ++v) r[v] -= Ls * (0.0 - q(v, ez, i, j, k) * wm);
+                            const int ez2 = k == 0 ? ez - 1 : ez + 1, k2 = k == 0 ? N : 0;
+                            for (int v = 0; v < 4; ++v) {
+                                const double qm = q(v, ez, i, j, k);
+                                // upward flux M q_up / H, q_up from below when M > 0
+                                double qup = qm;
+                                if (interior && ((k == 0) == (M > 0.0))) qup = q(v, ez2, i, j, k2);
+                                const double fs = nrm * M * qup * iH;
+                                r[v] -= Ls * (fs - qm * wm);
+                            }
+                            if (!interior) {
                                 if (k == 0) {
                                     const double uu = q(0, ez, i, j, k) * iH, vv = q(1, ez, i, j, k) * iH;
                                     const double sp = std::sqrt(uu * uu + vv * vv);
@@ -924,6 +1091,7 @@ void PhysModel::rhs3d(const Vec *Qin, const Vec &etaf, double tb, Vec *R, Vec *o
                         for (int v = 0; v < 4; ++v) R[v][base + ln] = r[v];
                     }
     }
+    });
 }
 
 void PhysModel::rhs2d(const Vec &e, const Vec &hu, const Vec &hv, const Vec *Fx, const Vec *Fy,
@@ -997,13 +1165,20 @@ void PhysModel::split_step(double dt, int nsub) {
     Vec R[4], res[4];
     for (int v = 0; v < 4; ++v) res[v].assign(n3, 0.0);
     Vec dHU(n2, 0.0), dHV(n2, 0.0), tmp;
+    // the stage elevation of the baroclinic pressure: advanced with the 3D stages by the
+    // column divergence, so that T = HT / H and S = HS / H see the depth the 3D transport implies
+    Vec etas = eta, rese(n2, 0.0), de;
     for (int s = 0; s < 5; ++s) {
-        rhs3d(Q, eta, t, R, nullptr, nullptr);
+        rhs3d(Q, eta, t, R, nullptr, &de, &etas);
         for (int v = 0; v < 4; ++v)
             for (long n = 0; n < n3; ++n) {
                 res[v][n] = LSRK_A[s] * res[v][n] + dt * R[v][n];
                 Q[v][n] += LSRK_B[s] * res[v][n];
             }
+        for (long a2 = 0; a2 < n2; ++a2) {
+            rese[a2] = LSRK_A[s] * rese[a2] + dt * de[a2];
+            etas[a2] += LSRK_B[s] * rese[a2];
+        }
         Vec inc(n3);
         for (long n = 0; n < n3; ++n) inc[n] = LSRK_B[s] * res[0][n];
         column_integral(inc, tmp);
@@ -1043,6 +1218,21 @@ void PhysModel::split_step(double dt, int nsub) {
                 }
         }
     for (long a = 0; a < n2; ++a) eta_avg[a] = esum[a] / nsub;
+    // volume consistency of the tracers: the 3D stages moved HT and HS with the column
+    // divergence of the 3D transport (depth etas + h); the barotropic step ended at eta + h.
+    // Rescaling the columns' tracer contents by that depth ratio keeps T = HT / H (a uniform
+    // tracer stays uniform); the tracer content changes by the 3D/2D transport mismatch.
+    for (int c = 0; c < ncol; ++c)
+        for (int a2 = 0; a2 < np2; ++a2) {
+            const size_t i2 = (size_t)c * np2 + a2;
+            const double rr = (e[i2] + h[i2]) / (etas[i2] + h[i2]);
+            for (int ez = 0; ez < p.nz; ++ez)
+                for (int k = 0; k < np; ++k) {
+                    const size_t n = ((size_t)c * p.nz + ez) * np3 + a2 + np2 * k;
+                    Q[2][n] *= rr;
+                    Q[3][n] *= rr;
+                }
+        }
     eta = e; HU = u; HV = v;
     t += dt;
 }

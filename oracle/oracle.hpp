@@ -26,6 +26,9 @@ struct Basis1D {
     int order = 0;
     Vec nodes, weights, bary, D;  // D row-major (np x np): D[i*np+j] = l'_j(x_i)
     Vec S;                        // S[k*np+m] = int_{-1}^{x_k} l_m(x) dx (exact)
+    // inverse of the strong-form derivative with the value at x = -1 lifted in:
+    // A = D + e_0 e_0^T / w_0, Ainv row-major; a0 = Ainv e_0 / w_0
+    Vec Ainv, a0;
     int np() const { return order + 1; }
 };
 void legendre(int n, double x, double &L, double &dL);
@@ -82,6 +85,14 @@ struct PhysParams {
     int flux2d = FLUX_LF;
     int bc[4] = {0, 0, 0, 0};  // W, E, S, N: 0 wall, 1 tidal elevation
     double tide_amp = 0.0, tide_period = 44714.0;
+    // linear equation of state rho = rho0 (1 - alpha (T - T0) + beta (S - S0))
+    // (include/physics/equation_of_state.hpp:35-40,161); alpha = beta = 0 switches the
+    // baroclinic pressure gradient off
+    double alpha = 2e-4, beta = 7.6e-4, T0 = 10.0, S0 = 35.0;
+    // horizontally uniform reference stratification T_ref(z) = Tref_s + Tref_dz z (S_ref = S0)
+    // whose hydrostatic pressure has no horizontal gradient at constant z: the force is formed
+    // from the anomaly b - b_ref(z). The default (T0, 0) subtracts nothing.
+    double Tref_s = 10.0, Tref_dz = 0.0;
 };
 
 struct PhysModel {
@@ -102,12 +113,17 @@ struct PhysModel {
     void set_state(const double *const q[4], const double *eta2);
     double tide(double time) const;
     // 3D right-hand side with eta frozen, tidal ghost at time tb. omega3 optional out.
+    // etab (optional, default etaf): the surface elevation the baroclinic pressure gradient
+    // uses (in a mode-split step the stage elevation, advanced with the 3D stages)
     void rhs3d(const Vec *Qin, const Vec &etaf, double tb, Vec *R, Vec *omega3,
-               Vec *deta2) const;
+               Vec *deta2, const Vec *etab = nullptr) const;
     // 2D barotropic operator Phi + forcing (F may be null).
     void rhs2d(const Vec &e, const Vec &hu, const Vec &hv, const Vec *Fx, const Vec *Fy,
                double time, Vec &ke, Vec &khu, Vec &khv) const;
     void column_integral(const Vec &g3, Vec &out2) const;  // int_{-1}^{0} g dsigma per 2D node
+    // buoyancy anomaly b = (rho - rho0) / rho0 at every 3D node and its integral from the node
+    // up to the surface, B(sigma) = int_sigma^0 b dsigma' (hydrostatic pressure p' = rho0 g H B)
+    void baroclinic_B(const Vec *Qin, const Vec &etaf, Vec &b3, Vec &B3) const;
     void split_step(double dt, int nsub);                  // one baroclinic step
     void rk_step(int scheme, double dt);                   // non-split RK of (Q, eta)
     void diagnostics(double out[10]) const;

@@ -125,7 +125,8 @@ class PhysOracle:
         iv = np.array([cfg.nx, cfg.ny, cfg.nz, cfg.order, FLUX[cfg.flux2d]] +
                       [BCS[b] for b in cfg.bc], dtype=np.int32)
         dv = np.array([cfg.Lx, cfg.Ly, cfg.g, cfg.rho0, cfg.nu_h, cfg.nu_v, cfg.kappa_v_T,
-                       cfg.kappa_v_S, cfg.cd, cfg.tide_amp, cfg.tide_period])
+                       cfg.kappa_v_S, cfg.cd, cfg.tide_amp, cfg.tide_period, cfg.alpha,
+                       cfg.beta, cfg.T0, cfg.S0, cfg.Tref_s, cfg.Tref_dz])
         self._keep = [_c(h), _c(f), _c(taux), _c(tauy)]
         L = lib()
         L.orc_phys_create.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp, _dp]
@@ -152,11 +153,15 @@ class PhysOracle:
         return dict(Hu=q[0], Hv=q[1], HT=q[2], HS=q[3], eta=eta, HU=HU, HV=HV, eta_avg=eavg,
                     t=t.value)
 
-    def rhs(self):
+    def rhs(self, etab=None):
+        """3D right-hand side at the current state; etab (optional) is the surface elevation
+        of the baroclinic pressure gradient (default: the model's eta)."""
         n3, n2 = self.cfg.n3, self.cfg.n2
         r = [np.empty(n3) for _ in range(4)]
         om, de = np.empty(n3), np.empty(n2)
-        _chk(lib().orc_phys_rhs(C.c_void_p(self.h), _pa(r), _p(om), _p(de)))
+        eb = None if etab is None else _c(etab)
+        _chk(lib().orc_phys_rhs(C.c_void_p(self.h), _pa(r), _p(om), _p(de),
+                                None if eb is None else _p(eb)))
         return dict(dHu=r[0], dHv=r[1], dHT=r[2], dHS=r[3], omega=om, deta=de)
 
     def rhs2d(self, Fx, Fy, time):

@@ -96,13 +96,14 @@ def _pair(case):
 
 
 def _tidal_small(precision, order=3, nx=5, ny=4, nz=3, flux2d="lf"):
-    case = configs.c2(nx=nx, ny=ny, nz=nz, order=order, precision=precision, Lx=40e3, flux2d=flux2d)
+    case = configs.c2(nx=nx, ny=ny, nz=nz, order=order, precision=precision, Lx=40e3, flux2d=flux2d,
+                      baroclinic=True)
     case = configs.perturb(case)
     case["taux"][:] = 0.05
     return case
 
 
-@pytest.mark.parametrize("order", [2, 3, 4])
+@pytest.mark.parametrize("order", [1, 2, 3, 4, 5])
 def test_phys_rhs_fp64_matches_oracle(order):
     case = _tidal_small("fp64", order=order)
     gpu, ref = _pair(case)
@@ -111,6 +112,29 @@ def test_phys_rhs_fp64_matches_oracle(order):
     assert relerr(g["deta"], r["deta"]) < 1e-10
     for k in ("dHu", "dHv", "dHT", "dHS"):
         assert relerr(g[k], r[k]) < 1e-10, k
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-11), ("mixed", 1e-4)])
+@pytest.mark.parametrize("order", [1, 4])
+def test_baroclinic_pgf_of_a_front_is_exact_on_gpu(precision, tol, order):
+    """Flat bed (H = 100 m), at rest, temperature T0 + gamma x through the whole column: the
+    only tendency is the baroclinic force on Hu, -g H^2 alpha gamma sigma, exactly (the same
+    case pins the oracle in test_oracle_dg.py)."""
+    gamma = 1e-4
+    cfg = configs.DGConfig(nx=6, ny=3, nz=3, order=order, Lx=20e3, Ly=10e3, precision=precision)
+    X, Y, Sg = configs.node_coords(cfg)
+    h = np.full(cfg.n2, 100.0)
+    H3 = configs.expand_2d_to_3d(cfg, h)
+    X3 = configs.expand_2d_to_3d(cfg, X)
+    q = [np.zeros(cfg.n3), np.zeros(cfg.n3), (10.0 + gamma * X3) * H3, cfg.S0 * H3]
+    z2 = np.zeros(cfg.n2)
+    gpu = OceanModel(cfg, h, z2, z2, z2)
+    gpu.upload_state(q, z2)
+    r = gpu.compute_rhs()
+    expect = -cfg.g * H3 ** 2 * cfg.alpha * gamma * Sg
+    assert np.abs(r["dHu"] - expect).max() <= tol * np.abs(expect).max()
+    assert np.abs(r["dHv"]).max() <= tol * np.abs(expect).max()
+    gpu.close()
 
 
 def test_phys_rhs_mixed_matches_oracle():
@@ -279,6 +303,43 @@ def test_persistent_barotropic_step_agrees_with_per_pass_launches(monkeypatch, p
     assert a["t"] == b["t"] and np.abs(a["eta"]).max() < 10.0
     for k in ("eta", "HU", "HV", "eta_avg", "Hu", "Hv", "HT", "HS"):
         assert relerr(a[k], b[k]) <= 1e-11, (k, relerr(a[k], b[k]))
+
+
+def test_bounded_grid_barrier_wait_gives_up_and_the_model_stays_usable(monkeypatch):
+    """Failure detection without a GPU fault. With DRIFTER_B200_DEBUG_HOLD_ARRIVAL=0 the
+    persistent barotropic launch's CTA 0 withholds its arrival at the first grid barrier, so no
+    CTA's bounded wait there can complete: each gives up after its iteration limit (about a
+    second), sets the abort word and the model's status word, and returns. The host reads
+    DRF_E_TIMEOUT at the next synchronisation, which clears the status word. The context stays
+    usable: a model built afterwards in the same process steps normally and agrees with the
+    per-pass launches."""
+    from drifter_b200 import DrfError
+    case = _tidal_small("fp64", nx=9, ny=7)
+    monkeypatch.setenv("DRIFTER_B200_BARO_PERSISTENT", "1")
+    monkeypatch.setenv("DRIFTER_B200_DEBUG_HOLD_ARRIVAL", "0")
+    held = OceanModel(case["cfg"], case["h"], case["f"], case["taux"], case["tauy"])
+    held.upload_state(case["q"], case["eta"])
+    held.step(case["dt"], case["nsub"], 1)
+    with pytest.raises(DrfError) as ei:
+        held.sync()
+    assert ei.value.code == 6  # DRF_E_TIMEOUT
+    held.sync()  # the status word was cleared
+    held.close()
+    monkeypatch.delenv("DRIFTER_B200_DEBUG_HOLD_ARRIVAL")
+    pers = OceanModel(case["cfg"], case["h"], case["f"], case["taux"], case["tauy"])
+    pers.upload_state(case["q"], case["eta"])
+    pers.step(case["dt"], case["nsub"], 2)
+    pers.sync()
+    monkeypatch.delenv("DRIFTER_B200_BARO_PERSISTENT")
+    per = OceanModel(case["cfg"], case["h"], case["f"], case["taux"], case["tauy"])
+    per.upload_state(case["q"], case["eta"])
+    per.step(case["dt"], case["nsub"], 2)
+    a, b = pers.download_state(), per.download_state()
+    assert a["t"] == b["t"]
+    for k in ("eta", "HU", "Hu", "HT"):
+        assert relerr(a[k], b[k]) <= 1e-11, (k, relerr(a[k], b[k]))
+    pers.close()
+    per.close()
 
 
 def test_time_copy_leaves_the_state_unchanged():
