@@ -66,8 +66,9 @@ def _cfl_dt(cfg: DGConfig, hmax: float, nsub: int, cfl: float = 0.3) -> float:
 
 
 def c1(nx=16, ny=16, nz=4, order=3, precision="fp64", seed=SEED, flux2d="lf"):
+    # T and S constant: no baroclinic pressure (the equation of state is off)
     cfg = DGConfig(nx=nx, ny=ny, nz=nz, order=order, Lx=100e3, Ly=100e3, precision=precision,
-                   flux2d=flux2d)
+                   flux2d=flux2d, alpha=0.0, beta=0.0)
     X, Y, Sg = node_coords(cfg)
     r2 = (X - 50e3) ** 2 + (Y - 50e3) ** 2
     h = 500.0 - 450.0 * np.exp(-r2 / (2 * 15e3 ** 2))
@@ -188,10 +189,11 @@ def c5_member(i: int, nx: int, ny: int, nz: int, order: int = 3, precision: str 
               seed: int = SEED) -> dict:
     """Member i of the C5 ensemble: a closed 2 km-per-element basin with its own seeded
     bathymetry (20-1000 m: a sloping shelf plus 8 Gaussian bumps) and uniform wind stress;
-    temperature and salinity uniform (10 C, 35)."""
+    temperature and salinity uniform (10 C, 35), so the equation of state is off."""
     rng = np.random.default_rng(seed + 1000 + i)
     L = 2e3
-    cfg = DGConfig(nx=nx, ny=ny, nz=nz, order=order, Lx=nx * L, Ly=ny * L, precision=precision)
+    cfg = DGConfig(nx=nx, ny=ny, nz=nz, order=order, Lx=nx * L, Ly=ny * L, precision=precision,
+                   alpha=0.0, beta=0.0)
     X, Y, Sg = node_coords(cfg)
     h = 20.0 + 480.0 * X / cfg.Lx
     for _ in range(8):

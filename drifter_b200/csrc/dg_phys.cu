@@ -499,15 +499,16 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, int c, uint3
                 if (nc < 0) continue;
                 const size_t n2 = (size_t)nc * NP2 + ni + NP * nj;
                 const double en = a.etab[n2], Hd = en + a.h[n2];
-                const T Hn = (T)Hd, etn = (T)en;
-                // the neighbour's pending tracer volume correction, folded into 1 / H
-                const T iHn = (T)((a.corrU ? 1.0 + a.corrR[n2] : 1.0) / Hd);
+                const T Hn = (T)Hd, etn = (T)en, iHn = (T)(1.0 / Hd);
+                // the neighbour's pending tracer volume correction, with the arithmetic of the
+                // neighbour's own load (or of the correction applied to the state)
+                const T dr = a.corrU ? (T)a.corrR[n2] : T(0);
                 const size_t nb = (size_t)nc * ncn + (size_t)ez * NP3 + ni + NP * nj;
 #pragma unroll
                 for (int m = 0; m < NP; ++m) {
                     const T Tr = fma(Trz, fma(sS1[ez * NP + m] - T(1), Hn, etn), Trs);
-                    bv[m] = fma(be, fma(a.qin[3][nb + NP2 * m], iHn, -S0),
-                                -al * fma(a.qin[2][nb + NP2 * m], iHn, -Tr));
+                    const T hs = a.qin[3][nb + NP2 * m], ht = a.qin[2][nb + NP2 * m];
+                    bv[m] = fma(be, fma(fma(hs, dr, hs), iHn, -S0), -al * fma(fma(ht, dr, ht), iHn, -Tr));
                 }
                 dst = sPn + ((sd * NP + tt) * nz + ez) * NP;
                 dstep = 1;

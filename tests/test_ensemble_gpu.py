@@ -57,8 +57,12 @@ def test_ensemble_members_equal_single_runs(precision):
         solo.step(c["dt"], 20, 3)
         s = solo.download_state()
         assert g["t"] == s["t"]
+        # the ensemble and the single-model kernels inline the same column function, which the
+        # compiler may contract differently: FP64 members agree to 1e-11, FP32-bulk members to
+        # the FP32 rounding their three steps amplify (1e-6)
+        tol = 1e-11 if precision == "fp64" else 1e-6
         for k in ("eta", "HU", "HV", "eta_avg", "Hu", "Hv", "HT", "HS"):
-            assert relerr(g[k], s[k]) <= 1e-11, (c["name"], k, relerr(g[k], s[k]))
+            assert relerr(g[k], s[k]) <= tol, (c["name"], k, relerr(g[k], s[k]))
         solo.close()
     ens.close()
 

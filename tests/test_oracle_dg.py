@@ -227,7 +227,7 @@ def test_phys_uniform_tracer_stays_uniform_in_the_split_step():
     depth: after 40 steps T stays within 1e-5 of 10 while the heat content is conserved to
     1e-12 (the baroclinic pressure is on, and stays negligible)."""
     case = configs.c1()
-    cfg = case["cfg"]
+    cfg = configs.DGConfig(**{**case["cfg"].__dict__, "alpha": 2e-4, "beta": 7.6e-4})
     o = O.PhysOracle(cfg, case["h"], case["f"], case["taux"], case["tauy"])
     o.set_state(case["q"], case["eta"])
     heat0 = o.diagnostics()["heat"]
