@@ -235,6 +235,20 @@ def run_cg(stream, reps=3):
         out[pc] = {"iters": best["iters"], "ms": round(best["ms"], 3), "relres": best["relres"]}
     torch.cuda.synchronize()
     torch.cuda.profiler.stop()
+    # the reference's multigrid apply (V-cycles to 1e-6 per apply) under flexible CG: host-driven
+    # iterations, so one timed solve
+    x, inf = s.solve("mg_reference", tol=1e-10, maxit=200)
+    out["mg_reference"] = {"iters": inf["iters"], "ms": round(inf["ms"], 3), "relres": inf["relres"]}
+    # roofline of the Jacobi and unpreconditioned solves: algorithmic bytes per control point and
+    # iteration of their fused kernels (Q apply: x in, y out, 16 B; x/r update: p, q, x, r in and
+    # x, r out, 48 B, plus d in and z out for Jacobi, 16 B; p update: z (or r) and p in, p out,
+    # 24 B). The vectors (19 MB each) are largely L2-resident, so the fraction of HBM can pass 1.
+    peak, _ = measured_peaks()
+    out["roofline"] = {}
+    for pc, bpd in (("jacobi", 104), ("none", 88)):
+        gbs = bpd * s.ndof * out[pc]["iters"] / (out[pc]["ms"] / 1e3) / 1e9
+        out["roofline"][pc] = {"bytes_per_dof_iter": bpd, "achieved_gbs": round(gbs, 1),
+                               "frac_of_hbm_peak": round(gbs / peak, 3)}
     out["cnn_vs_mg_speedup"] = round(out["mg"]["ms"] / out["cnn"]["ms"], 3)
     out["cnn_vs_mg_solution_rel_diff"] = float(np.abs(sols["cnn"] - sols["mg"]).max() /
                                                np.abs(sols["mg"]).max())
@@ -315,6 +329,13 @@ def run_ensemble(stream, steps=5, warmup=3):
     ms = e0.elapsed_time(e1) / steps
     info = ens.info()
     diag = ens.members[0].diagnostics()
+    # algorithmic bytes of the five stage launches of one step, all members (each member's stage
+    # as the single model's: per 3D DOF s (4 + 4 / (N + 1)) bytes, per 2D node 9 FP64 words)
+    stage_bytes = 0.0
+    for c in cases:
+        cf = c["cfg"]
+        s_b = 8.0 if cf.precision == "fp64" else 4.0
+        stage_bytes += 5 * (4 * cf.n3 * s_b * (4 + 4.0 / cf.np_) + cf.n2 * 8.0 * 9)
     ens.close()
     del ens
     # the same members one after another (each model's own step graph)
@@ -341,7 +362,12 @@ def run_ensemble(stream, steps=5, warmup=3):
             "dofs": ndof, "columns": info["items"], "stage_grid": info["grid"],
             "value": ndof * 5 / (ms / 1e3), "unit": UNIT, "ms_per_step": ms,
             "sequential_ms_per_step": ms_seq, "speedup_vs_sequential": ms_seq / ms,
-            "member0_max_eta": diag["max_eta"]}
+            "member0_max_eta": diag["max_eta"],
+            # the stages' algorithmic bytes over the whole step's time (barotropic included):
+            # a lower bound of the persistent stage launch's rate
+            "roofline": {"stage_bytes_per_step": stage_bytes,
+                         "step_gbs": stage_bytes / (ms / 1e3) / 1e9,
+                         "frac_of_hbm_peak": stage_bytes / (ms / 1e3) / 1e9 / measured_peaks()[0]}}
 
 
 def run_amr(stream, steps=5, warmup=3):

@@ -12,7 +12,7 @@ import numpy as np
 
 from ._abi import check, dptr, lib
 
-PRECOND = {"none": 0, "jacobi": 1, "mg": 2, "cnn": 3}
+PRECOND = {"none": 0, "jacobi": 1, "mg": 2, "cnn": 3, "mg_reference": 4}
 
 
 class BzGridDesc(C.Structure):
@@ -30,6 +30,7 @@ def _setup_sigs():
         "drf_bz_info": [vp, C.POINTER(C.c_int64), dp, C.POINTER(C.c_int)],
         "drf_bz_get_rhs": [vp, dp], "drf_bz_apply_Q": [vp, dp, dp],
         "drf_mg_setup": [vp, C.c_int, C.c_int, C.c_int], "drf_mg_apply": [vp, dp, dp],
+        "drf_mg_apply_reference": [vp, dp, dp, C.c_double, C.c_int, C.POINTER(C.c_int), dp],
         "drf_bz_precondition": [vp, C.c_int, dp, dp],
         "drf_pcg_solve": [vp, dp, dp, C.c_double, C.c_int, C.c_int, C.POINTER(C.c_int), dp, dp],
         "drf_bz_constraints_apply": [vp, C.c_int, dp, dp],
@@ -90,6 +91,17 @@ class BezierSmoother:
         z = np.empty(self.ndof)
         check(lib().drf_mg_apply(self.h, dptr(r), dptr(z)))
         return z
+
+    def mg_apply_reference(self, r, tol=1e-6, max_vcycles=100):
+        """BezierMultigridPreconditioner::apply as the reference computes it: V-cycles with the
+        row-normalised restriction and one colour order, repeated to tol. Returns (z, cycles,
+        relres)."""
+        r = np.ascontiguousarray(r, dtype=np.float64)
+        z = np.empty(self.ndof)
+        cyc, rel = C.c_int(), C.c_double()
+        check(lib().drf_mg_apply_reference(self.h, dptr(r), dptr(z), tol, max_vcycles,
+                                           C.byref(cyc), C.byref(rel)))
+        return z, cyc.value, rel.value
 
     def precondition(self, r, kind="jacobi"):
         r = np.ascontiguousarray(r, dtype=np.float64)

@@ -284,6 +284,10 @@ __device__ __forceinline__ void schwarz_upd_item(const LevelDev &L, int color, c
 struct TransferDev {
     const int *fc0, *cf0;
     const double *fw, *cw;
+    // row sums of the 1D restriction (non-null: R's rows scaled to sum to one where
+    // |sum - 1| > 1e-10, as BezierMultigridPreconditioner::setup builds R,
+    // src/bathymetry/bezier_multigrid_preconditioner.cpp:209-225)
+    const double *rs;
 };
 
 // r_c = P^T r_f at coarse dof t (fine rows ascending, columns ascending within a row)
@@ -306,6 +310,10 @@ __device__ __forceinline__ void restrict_item(const TransferDev &T, int ndc, int
         for (int p = 0; p < 8; ++p)
             if (w[p] != 0.0) sx += w[p] * row[p];
         s += wq * sx;
+    }
+    if (T.rs) {
+        const double scale = T.rs[ci] * T.rs[cj];
+        if (fabs(scale) > 1e-14 && fabs(scale - 1.0) > 1e-10) s /= scale;
     }
     rc[t] = s;
     xc_zero[t] = 0.0;
@@ -557,11 +565,13 @@ constexpr size_t COARSE_SMEM_MAX = 200 * 1024;
 
 struct CoarseStack {
     int top, pre, post, nc2;
+    int post_forward;  // post-smoothing in the pre-smoothing's colour order (reference V-cycle)
     LevelDev L[COARSE_MAX_LEVELS];
     TransferDev T[COARSE_MAX_LEVELS];  // T[l]: between levels l - 1 and l
     int off[COARSE_MAX_LEVELS];        // shared offset (doubles) of x_l; b_l, r_l follow
     const double *bin;                 // b of level top
     double *xout;                      // x of level top
+    const double *xinit;               // initial x of level top (null: zero)
     const double *Cinv;
 };
 
@@ -596,7 +606,7 @@ __global__ void __launch_bounds__(COARSE_THREADS) bz_coarse_vcycle_kernel(Coarse
         double *xt = X(S.top), *bt = B(S.top);
         for (int i = threadIdx.x; i < n2; i += blockDim.x) {
             bt[i] = S.bin[i];
-            xt[i] = 0.0;
+            xt[i] = S.xinit ? S.xinit[i] : 0.0;
         }
         __syncthreads();
     }
@@ -632,7 +642,7 @@ __global__ void __launch_bounds__(COARSE_THREADS) bz_coarse_vcycle_kernel(Coarse
         const int nd2 = L.nd * L.nd;
         for (int t = threadIdx.x; t < nd2; t += blockDim.x) prolong_item(S.T[l], C.nd, L.nd, X(l - 1), X(l), t);
         __syncthreads();
-        for (int it = 0; it < S.post; ++it) coarse_smooth(L, K, X(l), B(l), R(l), false);
+        for (int it = 0; it < S.post; ++it) coarse_smooth(L, K, X(l), B(l), R(l), S.post_forward != 0);
     }
     {
         const int n2 = S.L[S.top].nd * S.L[S.top].nd;
@@ -664,7 +674,11 @@ __global__ void __launch_bounds__(BS) bz_rhs_kernel(int n, int nd, const double 
 
 // ------------------------------------------------------------------ PCG with device scalars
 // scalar slots
-enum { S_RZ = 0, S_PQ, S_ALPHA, S_RR, S_BETA, S_BB, S_TOL2, S_RZNEW, S_NSLOT };
+enum { S_RZ = 0, S_PQ, S_ALPHA, S_RR, S_BETA, S_BB, S_TOL2, S_RZNEW, S_TMP, S_NSLOT };
+// BezierMultigridPreconditioner's defaults for its apply (vcycle_tolerance, max_vcycles,
+// include/bathymetry/bezier_multigrid_preconditioner.hpp:127-130)
+constexpr double MG_REF_TOL = 1e-6;
+constexpr int MG_REF_MAX_CYCLES = 100;
 struct PcgCtl {
     double *sc;   // scalars
     int *stop;    // 1 once converged (later kernels of the chunk return immediately)
@@ -1153,7 +1167,7 @@ struct drf_bz {
     struct Lv {
         DevBuf<double> K, rho, binv, x, b, r;
         DevBuf<int> fc0, cf0;     // transfer tables from the next coarser level (TransferDev)
-        DevBuf<double> fw, cw;
+        DevBuf<double> fw, cw, rs;
         int n = 0, nd = 0;
     };
     std::vector<Lv> lv;
@@ -1185,9 +1199,11 @@ struct drf_bz {
         DRF_LAUNCHED();
     }
     // transfer tables between level l - 1 and level l
-    TransferDev tdev(int l) const {
+    // ref: the reference's row-normalised restriction
+    TransferDev tdev(int l, bool ref = false) const {
         TransferDev T;
         T.fc0 = lv[l].fc0.p; T.cf0 = lv[l].cf0.p; T.fw = lv[l].fw.p; T.cw = lv[l].cw.p;
+        T.rs = ref ? lv[l].rs.p : nullptr;
         return T;
     }
     unsigned nparts() const { return 1024; }
@@ -1224,9 +1240,41 @@ struct drf_bz {
             // learned correction of the error it leaves, formed in the network's output pass
             cnn_precondition(cnn_net(cnn), stream, lv[L].n, rin, scal.p + S_RR, cnn_scale, zout, 1,
                              stop, diag.p);
+        } else if (kind == 4) {
+            // the reference's apply: V-cycles to its default tolerance (host-driven; never in a graph)
+            mg_apply_reference(rin, zout, MG_REF_TOL, MG_REF_MAX_CYCLES, nullptr);
         } else {
             vcycle(rin, zout);
         }
+    }
+
+    // one flexible-CG iteration with the reference multigrid apply (kind 4), host-driven:
+    // returns false once converged (or at maxit)
+    bool pcg_iteration_reference() {
+        const int Lf = finest();
+        PcgCtl c = pctl();
+        const int na = apply(Lf, p.p, nullptr, q.p, 0, part.p, c.stop);
+        alpha_kernel<<<1, BS, 0, stream>>>(c, na);
+        DRF_LAUNCHED();
+        xr_update_kernel<<<nparts(), BS, 0, stream>>>(ndof, c, p.p, q.p, x.p, r.p);
+        DRF_LAUNCHED();
+        conv_kernel<<<1, BS, 0, stream>>>(c, (int)nparts());
+        DRF_LAUNCHED();
+        int cl[3] = {0, 0, 0};
+        DRF_CUDA(cudaMemcpyAsync(cl, ctl.p, sizeof(cl), cudaMemcpyDeviceToHost, stream));
+        DRF_CUDA(cudaStreamSynchronize(stream));
+        if (cl[0] || cl[1] >= cl[2]) return false;
+        mg_apply_reference(r.p, z.p, MG_REF_TOL, MG_REF_MAX_CYCLES, nullptr);
+        // flexible CG: z.r and z.q partials side by side for beta = -(z.q)/(p.q)
+        dot_kernel<<<nparts(), BS, 0, stream>>>(ndof, z.p, r.p, part.p, nullptr);
+        DRF_LAUNCHED();
+        dot_kernel<<<nparts(), BS, 0, stream>>>(ndof, z.p, q.p, part.p + nparts(), nullptr);
+        DRF_LAUNCHED();
+        beta_fcg_kernel<<<1, BS, 0, stream>>>(c, (int)nparts());
+        DRF_LAUNCHED();
+        p_update_kernel<<<nparts(), BS, 0, stream>>>(ndof, c, z.p, p.p, 0);
+        DRF_LAUNCHED();
+        return true;
     }
 
     // one color step of the Schwarz smoother on a grid-wide level: z of every element of the
@@ -1274,35 +1322,44 @@ struct drf_bz {
         return top;
     }
 
-    // one V-cycle z = M r (z overwritten), finest level uses rin/zout directly
-    void vcycle(const double *rin, double *zout) {
+    // one V-cycle z = M r, finest level uses rin/zout directly. This build's form (ref false):
+    // z overwritten, R = P^T, post-smoothing in reverse colour order, an SPD preconditioner.
+    // ref true: BezierMultigridPreconditioner::v_cycle as written
+    // (src/bathymetry/bezier_multigrid_preconditioner.cpp:740-812), improving the z it is given:
+    // row-normalised R, the same colour order before and after the coarse correction.
+    void vcycle(const double *rin, double *zout, bool ref = false) {
         const int Lf = finest();
         std::vector<double *> X(lv.size()), B(lv.size()), R(lv.size());
         for (int l = 0; l < Lf; ++l) { X[l] = lv[l].x.p; B[l] = lv[l].b.p; R[l] = lv[l].r.p; }
         X[Lf] = zout; B[Lf] = const_cast<double *>(rin); R[Lf] = lv[Lf].r.p;
-        zero_kernel<<<nblk(ndof), BS, 0, stream>>>(ndof, zout, nullptr);
-        DRF_LAUNCHED();
+        if (!ref) {
+            zero_kernel<<<nblk(ndof), BS, 0, stream>>>(ndof, zout, nullptr);
+            DRF_LAUNCHED();
+        }
         const int top = coarse_top();
         for (int l = Lf; l > top; --l) {
             for (int it = 0; it < H.pre; ++it) smooth(l, X[l], B[l], R[l], true);
             const int64_t nd2 = (int64_t)lv[l].nd * lv[l].nd;
             apply(l, X[l], B[l], R[l], 1, nullptr, nullptr);
             const int64_t ndc2 = (int64_t)lv[l - 1].nd * lv[l - 1].nd;
-            bz_restrict_kernel<<<nblk(ndc2), BS, 0, stream>>>(tdev(l), lv[l - 1].nd, lv[l].nd, R[l],
+            bz_restrict_kernel<<<nblk(ndc2), BS, 0, stream>>>(tdev(l, ref), lv[l - 1].nd, lv[l].nd, R[l],
                                                               B[l - 1], X[l - 1]);
             DRF_LAUNCHED();
         }
         CoarseStack S;
         std::memset(&S, 0, sizeof(S));
         S.top = top; S.pre = H.pre; S.post = H.post;
+        S.post_forward = ref ? 1 : 0;
         S.nc2 = lv[0].nd * lv[0].nd;
         S.Cinv = coarse.p;
         S.bin = B[top];
         S.xout = X[top];
+        // the reference cycle improves the finest level's guess; coarser levels start from zero
+        S.xinit = (ref && top == Lf) ? X[top] : nullptr;
         int off = 256;
         for (int l = 0; l <= top; ++l) {
             S.L[l] = levdev(l);
-            if (l > 0) S.T[l] = tdev(l);
+            if (l > 0) S.T[l] = tdev(l, ref);
             S.off[l] = off;
             off += 3 * lv[l].nd * lv[l].nd;
         }
@@ -1313,8 +1370,46 @@ struct drf_bz {
             bz_prolong_kernel<<<nblk(nd2), BS, 0, stream>>>(tdev(l), lv[l - 1].nd, lv[l].nd, X[l - 1],
                                                             X[l]);
             DRF_LAUNCHED();
-            for (int it = 0; it < H.post; ++it) smooth(l, X[l], B[l], R[l], false);
+            for (int it = 0; it < H.post; ++it) smooth(l, X[l], B[l], R[l], ref);
         }
+    }
+
+    // ||v||^2 on the device, read back (synchronises the stream)
+    double norm2(const double *v) {
+        dot_kernel<<<nparts(), BS, 0, stream>>>(ndof, v, v, part.p, nullptr);
+        DRF_LAUNCHED();
+        reduce_kernel<<<1, BS, 0, stream>>>(part.p, (int)nparts(), scal.p + S_TMP);
+        DRF_LAUNCHED();
+        double v2 = 0.0;
+        DRF_CUDA(cudaMemcpyAsync(&v2, scal.p + S_TMP, 8, cudaMemcpyDeviceToHost, stream));
+        DRF_CUDA(cudaStreamSynchronize(stream));
+        return v2;
+    }
+
+    // BezierMultigridPreconditioner::apply (src/bathymetry/bezier_multigrid_preconditioner.cpp:
+    // 690-735): z = 0, then reference V-cycles until ||r - Q z|| < tol ||r|| or max_cycles (the
+    // residual is checked on the host after each cycle). rin must not alias the level buffers.
+    int mg_apply_reference(const double *rin, double *zout, double tol, int max_cycles, double *relres) {
+        const int Lf = finest();
+        zero_kernel<<<nblk(ndof), BS, 0, stream>>>(ndof, zout, nullptr);
+        DRF_LAUNCHED();
+        const double bb = norm2(rin);
+        if (relres) *relres = 0.0;
+        if (std::sqrt(bb) < 1e-30) return 0;
+        const double tol_sq = tol * tol * bb;
+        int cycle = 0;
+        double rr = bb;
+        for (; cycle < max_cycles; ++cycle) {
+            vcycle(rin, zout, true);
+            apply(Lf, zout, rin, lv[Lf].r.p, 1, nullptr, nullptr);
+            rr = norm2(lv[Lf].r.p);
+            if (rr < tol_sq) {
+                ++cycle;
+                break;
+            }
+        }
+        if (relres) *relres = std::sqrt(rr / bb);
+        return cycle;
     }
 
     // one PCG iteration (assumes r, z, p, rz set)
@@ -1463,6 +1558,15 @@ int pcg_run(drf_bz *h, int kind, double tol, int maxit) {
     DRF_CUDA(cudaStreamSynchronize(h->stream));
     int done = 0, it = 0;
     if (!(sc[S_RR] > tol2 * sc[S_BB])) done = 1;
+    if (kind == 4) {  // the reference multigrid apply is a host loop: no graph
+        if (!done && maxit > 0)
+            while (h->pcg_iteration_reference()) {
+            }
+        int cl[2] = {0, 0};
+        DRF_CUDA(cudaMemcpyAsync(cl, h->ctl.p, sizeof(cl), cudaMemcpyDeviceToHost, h->stream));
+        DRF_CUDA(cudaStreamSynchronize(h->stream));
+        return cl[1];
+    }
     // iterations in graph-captured chunks; converged iterations return early on the device
     const int chunk = 8;
     if (!done && maxit > 0) {
@@ -1699,6 +1803,10 @@ int drf_mg_setup(drf_bz *h, int coarsest_n, int pre, int post) {
                 std::vector<double> fw, cw;
                 transfer_tables(h->H.levels[l - 1].n, fc0, fw, cf0, cw);
                 up(lv[l].fc0, fc0); up(lv[l].fw, fw); up(lv[l].cf0, cf0); up(lv[l].cw, cw);
+                std::vector<double> rs(cf0.size(), 0.0);
+                for (size_t c = 0; c < rs.size(); ++c)
+                    for (int k = 0; k < 8; ++k) rs[c] += cw[8 * c + k];
+                up(lv[l].rs, rs);
             }
             if (l < nl - 1) {
                 const size_t n2 = (size_t)Lh.nd * Lh.nd;
@@ -1742,8 +1850,8 @@ int drf_bz_precondition(drf_bz *h, int kind, const double *rh, double *zh) {
     return guard([&] {
         check_bz(h);
         DRF_CHECK(rh && zh, DRF_E_INVALID, "null argument");
-        DRF_CHECK(kind >= 0 && kind <= 3, DRF_E_INVALID, "unknown preconditioner kind");
-        DRF_CHECK(kind != 2 || h->mg_ready, DRF_E_INVALID, "multigrid preconditioner not set up");
+        DRF_CHECK(kind >= 0 && kind <= 4, DRF_E_INVALID, "unknown preconditioner kind");
+        DRF_CHECK((kind != 2 && kind != 4) || h->mg_ready, DRF_E_INVALID, "multigrid preconditioner not set up");
         DRF_CHECK(kind != 3 || h->cnn, DRF_E_INVALID, "no learned preconditioner attached");
         DRF_CUDA(cudaMemcpyAsync(h->r.p, rh, h->ndof * 8, cudaMemcpyHostToDevice, h->stream));
         dot_kernel<<<h->nparts(), BS, 0, h->stream>>>(h->ndof, h->r.p, h->r.p, h->part.p, nullptr);
@@ -1765,6 +1873,23 @@ int drf_mg_apply(drf_bz *h, const double *rh, double *zh) {
         h->vcycle(h->r.p, h->z.p);
         DRF_CUDA(cudaMemcpyAsync(zh, h->z.p, h->ndof * 8, cudaMemcpyDeviceToHost, h->stream));
         DRF_CUDA(cudaStreamSynchronize(h->stream));
+    });
+}
+
+int drf_mg_apply_reference(drf_bz *h, const double *rh, double *zh, double tol, int max_vcycles,
+                           int *cycles, double *relres) {
+    return guard([&] {
+        check_bz(h);
+        DRF_CHECK(h->mg_ready, DRF_E_INVALID, "drf_mg_setup has not been called");
+        DRF_CHECK(rh && zh, DRF_E_INVALID, "null argument");
+        DRF_CHECK(tol > 0 && max_vcycles >= 0, DRF_E_INVALID, "tol must be > 0 and max_vcycles >= 0");
+        DRF_CUDA(cudaMemcpyAsync(h->r.p, rh, h->ndof * 8, cudaMemcpyHostToDevice, h->stream));
+        double rel = 0.0;
+        const int c = h->mg_apply_reference(h->r.p, h->z.p, tol, max_vcycles, &rel);
+        DRF_CUDA(cudaMemcpyAsync(zh, h->z.p, h->ndof * 8, cudaMemcpyDeviceToHost, h->stream));
+        DRF_CUDA(cudaStreamSynchronize(h->stream));
+        if (cycles) *cycles = c;
+        if (relres) *relres = rel;
     });
 }
 
@@ -1860,8 +1985,8 @@ int drf_pcg_solve(drf_bz *h, const double *bh, double *xh, double tol, int maxit
     return guard([&] {
         check_bz(h);
         DRF_CHECK(xh && tol > 0 && maxit >= 0, DRF_E_INVALID, "bad arguments");
-        DRF_CHECK(kind >= 0 && kind <= 3, DRF_E_INVALID, "unknown preconditioner kind");
-        DRF_CHECK(kind != 2 || h->mg_ready, DRF_E_INVALID, "multigrid preconditioner not set up");
+        DRF_CHECK(kind >= 0 && kind <= 4, DRF_E_INVALID, "unknown preconditioner kind");
+        DRF_CHECK((kind != 2 && kind != 4) || h->mg_ready, DRF_E_INVALID, "multigrid preconditioner not set up");
         DRF_CHECK(kind != 3 || h->cnn, DRF_E_INVALID, "no learned preconditioner attached (drf_bz_set_cnn)");
         const int64_t n = h->ndof;
         cudaEvent_t e0, e1;

@@ -235,14 +235,26 @@ int drf_bz_element_errors(drf_bz *h, const double *x, const double *zdata, int n
 /* BezierMultigridPreconditioner::setup (include/bathymetry/bezier_multigrid_preconditioner.hpp:240):
  * levels down to coarsest_n elements per direction, pre/post colored-Schwarz sweeps. */
 int drf_mg_setup(drf_bz *h, int coarsest_n, int pre, int post);
-/* One V-cycle z = M r (BezierMultigridPreconditioner::apply, :246; the reference repeats
- * V-cycles to a tolerance, this entry applies one symmetric cycle). */
+/* One V-cycle z = M r of this build's symmetric form (R = P^T, post-smoothing in reverse colour
+ * order): a fixed SPD preconditioner for plain PCG (BezierMultigridPreconditioner::apply, :246,
+ * repeats V-cycles to a tolerance; drf_mg_apply_reference does that). */
 int drf_mg_apply(drf_bz *h, const double *r, double *z);
-/* z = M r for preconditioner kind (0 none, 1 Jacobi, 2 multigrid, 3 learned). */
+/* BezierMultigridPreconditioner::apply as the reference computes it
+ * (include/bathymetry/bezier_multigrid_preconditioner.hpp:246,
+ * src/bathymetry/bezier_multigrid_preconditioner.cpp:690-812): z = 0, then V-cycles with the
+ * row-normalised restriction (:209-225) and the same colour order before and after the coarse
+ * correction, until ||r - Q z|| < tol ||r|| or max_vcycles (the reference's defaults are 1e-6
+ * and 100). *cycles = V-cycles run, *relres = the final relative residual (either may be NULL). */
+int drf_mg_apply_reference(drf_bz *h, const double *r, double *z, double tol, int max_vcycles,
+                           int *cycles, double *relres);
+/* z = M r for preconditioner kind (0 none, 1 Jacobi, 2 multigrid, 3 learned, 4 the reference's
+ * multigrid apply with its default tolerance). */
 int drf_bz_precondition(drf_bz *h, int kind, const double *r, double *z);
 /* PCG on Q x = b to ||r|| <= tol ||b|| (FP64). b NULL = the assembled right-hand side; x holds
  * the initial guess and returns the solution. kind: 0 none, 1 Jacobi, 2 multigrid V-cycle,
- * 3 learned (Jacobi plus the network's correction, flexible CG). Maps the PCG loop of
+ * 3 learned (Jacobi plus the network's correction, flexible CG), 4 the reference's multigrid
+ * apply (V-cycles to 1e-6, a variable preconditioner: flexible CG, host-driven iterations).
+ * Maps the PCG loop of
  * solve_with_constraints_iterative (src/bathymetry/cg_cubic_bezier_bathymetry_smoother.cpp:479-558)
  * with Q in place of the Schur operator. *ms = device time of the solve. */
 int drf_pcg_solve(drf_bz *h, const double *b, double *x, double tol, int maxit, int kind,

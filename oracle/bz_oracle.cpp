@@ -450,7 +450,12 @@ static void smooth_color(const BzMG &M, int l, int color, double *x, const doubl
         }
 }
 
-static void vcycle(const BzMG &M, int l, double *x, const double *b) {
+// ref = false: this build's SPD V-cycle (R = P^T, post-smoothing in reverse colour order).
+// ref = true: BezierMultigridPreconditioner::v_cycle as written
+// (src/bathymetry/bezier_multigrid_preconditioner.cpp:740-812): R = P^T with its rows scaled to
+// sum to one where they do not already (:209-225, |sum - 1| > 1e-10), and the same smoother
+// (colours 0..3) before and after the coarse correction.
+static void vcycle(const BzMG &M, int l, double *x, const double *b, bool ref = false) {
     const BzLevel &L = M.lv[l];
     const long nd2 = (long)L.nd * L.nd;
     if (l == 0) {
@@ -484,7 +489,22 @@ static void vcycle(const BzMG &M, int l, double *x, const double *b) {
         for (int ci = 0; ci < C.nd; ++ci)
             for (int c = 0; c < 4; ++c) rc[ci + (long)C.nd * (c0 + c)] += w[c] * tmp[ci + (long)C.nd * fj];
     }
-    vcycle(M, l - 1, ec.data(), rc.data());
+    if (ref) {
+        // row sums of R = P^T: separable, (restriction of ones along x) x (along y)
+        std::vector<double> sx(C.nd, 0.0);
+        for (int fi = 0; fi < L.nd; ++fi) {
+            double w[4];
+            const int c0 = p1_row(fi, C.n, Sd, w);
+            for (int c = 0; c < 4; ++c) sx[c0 + c] += w[c];
+        }
+        for (int cj = 0; cj < C.nd; ++cj)
+            for (int ci = 0; ci < C.nd; ++ci) {
+                const double scale = sx[ci] * sx[cj];
+                if (std::abs(scale) > 1e-14 && std::abs(scale - 1.0) > 1e-10)
+                    rc[ci + (long)C.nd * cj] /= scale;
+            }
+    }
+    vcycle(M, l - 1, ec.data(), rc.data(), ref);
     // prolongation x += P e_c
     for (int fj = 0; fj < L.nd; ++fj) {
         double wy[4];
@@ -499,7 +519,33 @@ static void vcycle(const BzMG &M, int l, double *x, const double *b) {
         }
     }
     for (int it = 0; it < M.post; ++it)
-        for (int c = 3; c >= 0; --c) smooth_color(M, l, c, x, b);
+        for (int s2 = 0; s2 < 4; ++s2) smooth_color(M, l, ref ? s2 : 3 - s2, x, b);
+}
+
+// BezierMultigridPreconditioner::apply (src/bathymetry/bezier_multigrid_preconditioner.cpp:
+// 690-735): x = 0, then V-cycles (reference semantics) until ||b - Q x|| < tol ||b|| or
+// max_cycles; returns the cycles run.
+int bz_mg_apply_ref(const BzMG &M, const double *b, double *x, double tol, int max_cycles) {
+    const int l = (int)M.lv.size() - 1;
+    const long nd2 = (long)M.lv[l].nd * M.lv[l].nd;
+    std::fill(x, x + nd2, 0.0);
+    double bb = 0.0;
+    for (long i = 0; i < nd2; ++i) bb += b[i] * b[i];
+    if (std::sqrt(bb) < 1e-30) return 0;
+    const double tol_sq = tol * tol * bb;
+    std::vector<double> qx(nd2);
+    int cycle = 0;
+    for (; cycle < max_cycles; ++cycle) {
+        vcycle(M, l, x, b, true);
+        bz_level_apply(M, l, x, qx.data());
+        double rr = 0.0;
+        for (long i = 0; i < nd2; ++i) rr += (b[i] - qx[i]) * (b[i] - qx[i]);
+        if (rr < tol_sq) {
+            ++cycle;
+            break;
+        }
+    }
+    return cycle;
 }
 
 void bz_mg_vcycle(const BzMG &M, const double *r, double *z) {

@@ -70,6 +70,9 @@ struct BzMG {
 void bz_mg_setup(const BzSystem &S, BzMG &M, int coarsest_n);
 void bz_level_apply(const BzMG &M, int l, const double *x, double *y);
 void bz_mg_vcycle(const BzMG &M, const double *r, double *z);
+// BezierMultigridPreconditioner::apply with the reference's V-cycle (row-normalised R, same
+// colour order before and after the coarse correction), repeated to tol; returns the cycles.
+int bz_mg_apply_ref(const BzMG &M, const double *b, double *x, double tol, int max_cycles);
 // PCG on Q x = b; precond 0 none, 1 Jacobi, 2 MG V-cycle. Returns iterations.
 int bz_pcg(const BzSystem &S, const BzMG *M, int precond, const double *b, double *x, double tol,
            int maxit, double *relres);

@@ -284,6 +284,10 @@ int orc_bz_mg_vcycle(void *hd, const double *r, double *z) {
     ORC_TRY(bz_mg_vcycle(static_cast<BzHandle *>(hd)->M, r, z))
 }
 
+int orc_bz_mg_apply_ref(void *hd, const double *b, double *x, double tol, int max_cycles, int *cycles) {
+    ORC_TRY(*cycles = bz_mg_apply_ref(static_cast<BzHandle *>(hd)->M, b, x, tol, max_cycles))
+}
+
 int orc_bz_pcg(void *hd, int precond, const double *b, double *x, double tol, int maxit,
                int *iters, double *relres) {
     ORC_TRY({

@@ -290,6 +290,14 @@ class BezierOracle:
         _chk(lib().orc_bz_mg_vcycle(C.c_void_p(self.h), _p(_c(r)), _p(z)))
         return z
 
+    def mg_apply_ref(self, b, tol=1e-6, max_cycles=100):
+        """BezierMultigridPreconditioner::apply with the reference's V-cycle, repeated to tol."""
+        x = np.empty(self.ndof)
+        cyc = C.c_int()
+        _chk(lib().orc_bz_mg_apply_ref(C.c_void_p(self.h), _p(_c(b)), _p(x), C.c_double(tol),
+                                       max_cycles, C.byref(cyc)))
+        return x, cyc.value
+
     def pcg(self, b=None, precond="mg", tol=1e-10, maxit=2000, x0=None):
         b = self.vec("b") if b is None else _c(b)
         x = np.zeros(self.ndof) if x0 is None else _c(x0).copy()

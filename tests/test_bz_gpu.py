@@ -49,6 +49,34 @@ def test_vcycle_matches_oracle(n):
     assert rel(g.mg_apply(r), o.vcycle(r)) < 1e-11
 
 
+@pytest.mark.parametrize("n", [4, 16, 32])
+def test_reference_mg_apply_matches_oracle(n):
+    """BezierMultigridPreconditioner::apply as written (row-normalised restriction, one colour
+    order, V-cycles to the tolerance) against the oracle's restatement: the same number of
+    cycles and the same result."""
+    g, o = pair(n)
+    g.mg_setup(2)
+    o.mg_setup(2)
+    b = o.vec("b")
+    for tol in (1e-6, 1e-9):
+        z, cycles, relres = g.mg_apply_reference(b, tol=tol)
+        zo, co = o.mg_apply_ref(b, tol=tol)
+        assert cycles == co and relres < tol
+        assert rel(z, zo) < 1e-10
+
+
+def test_flexible_cg_with_the_reference_mg_apply():
+    """PCG kind 4: the reference's multigrid apply (a variable preconditioner) under flexible
+    CG reaches the FP64 1e-10 residual and the oracle's direct-preconditioned solution."""
+    g, o = pair(32)
+    g.mg_setup(2)
+    o.mg_setup(2)
+    x, info = g.solve("mg_reference", tol=1e-10, maxit=200)
+    xo, ito, rro = o.pcg(precond="mg", tol=1e-12, maxit=5000)
+    assert info["relres"] <= 1e-10 and info["iters"] < 20
+    assert rel(x, xo) < 1e-8
+
+
 @pytest.mark.parametrize("precond", ["none", "jacobi", "mg"])
 def test_pcg_solution_matches_oracle(precond):
     g, o = pair(32)

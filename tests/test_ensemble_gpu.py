@@ -59,8 +59,8 @@ def test_ensemble_members_equal_single_runs(precision):
         assert g["t"] == s["t"]
         # the ensemble and the single-model kernels inline the same column function, which the
         # compiler may contract differently: FP64 members agree to 1e-11, FP32-bulk members to
-        # the FP32 rounding their three steps amplify (1e-6)
-        tol = 1e-11 if precision == "fp64" else 1e-6
+        # the FP32 rounding their three steps amplify (1e-5)
+        tol = 1e-11 if precision == "fp64" else 1e-5
         for k in ("eta", "HU", "HV", "eta_avg", "Hu", "Hv", "HT", "HS"):
             assert relerr(g[k], s[k]) <= tol, (c["name"], k, relerr(g[k], s[k]))
         solo.close()

@@ -170,3 +170,26 @@ def test_element_error_estimate_pins(ng):
     l2, nrm = O.bz_element_errors(nx, ny, Lx, Ly, ng, x, z + 0.25)
     area = (Lx / nx) * (Ly / ny)
     assert np.allclose(l2, 0.25 * np.sqrt(area), rtol=1e-12) and np.allclose(nrm, 0.25, rtol=1e-12)
+
+
+def test_reference_mg_apply_solves_to_its_tolerance():
+    """BezierMultigridPreconditioner::apply as written (src/bathymetry/bezier_multigrid_
+    preconditioner.cpp:690-812): V-cycles with the row-normalised restriction and the same
+    colour order before and after the coarse correction, repeated until ||b - Q x|| < tol ||b||.
+    The normalised R under-weights the coarse correction, so it takes several cycles where this
+    build's Galerkin V-cycle is a single SPD application; at a tight tolerance the result is the
+    direct solution of Q x = b."""
+    B = _fbm_case(16)
+    B.mg_setup(2)
+    b = B.vec("b")
+    Q = B.csr("Q")
+    x, cycles = B.mg_apply_ref(b, tol=1e-6)
+    assert 1 < cycles < 100
+    assert np.linalg.norm(b - Q @ x) < 1e-6 * np.linalg.norm(b)
+    x8, c8 = B.mg_apply_ref(b, tol=1e-9)
+    assert c8 > cycles
+    xd = spl.spsolve(Q.tocsc(), b)
+    assert np.abs(x8 - xd).max() / np.abs(xd).max() < 1e-6
+    # a zero right-hand side returns zero without cycling, as the reference does
+    z, c0 = B.mg_apply_ref(np.zeros_like(b))
+    assert c0 == 0 and not z.any()
