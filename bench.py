@@ -219,7 +219,8 @@ def run_cg(stream, reps=3):
     s.mg_setup(2)
     net.attach(s)
     out = {"workload": c["name"] + " cubic Bezier, lambda=1, eps=1e-4, FP64 PCG to 1e-10",
-           "dofs": s.ndof, "train_s": round(train_s, 2), "train_loss": info["loss"]}
+           "dofs": s.ndof, "train_s": round(train_s, 2), "train_loss": info["loss"],
+           "cnn_conv_autotuned": s.cnn_tuning()}
     sols = {}
     import torch
     torch.cuda.synchronize()

@@ -31,6 +31,7 @@ def _setup_sigs():
         "drf_bz_get_rhs": [vp, dp], "drf_bz_apply_Q": [vp, dp, dp],
         "drf_mg_setup": [vp, C.c_int, C.c_int, C.c_int], "drf_mg_apply": [vp, dp, dp],
         "drf_mg_apply_reference": [vp, dp, dp, C.c_double, C.c_int, C.POINTER(C.c_int), dp],
+        "drf_bz_cnn_tuning": [vp, C.POINTER(C.c_int), dp],
         "drf_bz_precondition": [vp, C.c_int, dp, dp],
         "drf_pcg_solve": [vp, dp, dp, C.c_double, C.c_int, C.c_int, C.POINTER(C.c_int), dp, dp],
         "drf_bz_constraints_apply": [vp, C.c_int, dp, dp],
@@ -102,6 +103,15 @@ class BezierSmoother:
         check(lib().drf_mg_apply_reference(self.h, dptr(r), dptr(z), tol, max_vcycles,
                                            C.byref(cyc), C.byref(rel)))
         return z, cyc.value, rel.value
+
+    def cnn_tuning(self) -> dict:
+        """The attached network's conv form per layer (mma_sync or tcgen05, timed at this size)."""
+        f = (C.c_int * 4)()
+        ms = np.zeros(8)
+        check(lib().drf_bz_cnn_tuning(self.h, f, dptr(ms)))
+        names = ("mma_sync", "tcgen05")
+        return {"forms": [names[v] for v in f],
+                "ms": {names[k]: [round(float(ms[2 * l + k]), 5) for l in range(4)] for k in (0, 1)}}
 
     def precondition(self, r, kind="jacobi"):
         r = np.ascontiguousarray(r, dtype=np.float64)

@@ -1180,6 +1180,8 @@ struct drf_bz {
     cudaGraphExec_t graph = nullptr;
     int graph_kind = -1, graph_chunk = 0;
     uint64_t graph_kernels = 0;  // kernel nodes of the chunk graph
+    double cnn_ms[4][2] = {};     // the attached network's conv autotuning: ms per form per layer
+    int cnn_form[4] = {};         // and the chosen form (0 mma.sync, 1 tcgen05)
 
     ~drf_bz() {
         if (graph) cudaGraphExecDestroy(graph);
@@ -1838,10 +1840,23 @@ int drf_bz_set_cnn(drf_bz *h, drf_cnn *net, double out_scale) {
         h->cnn = net;
         h->cnn_scale = out_scale;
         cnn_prepare(cnn_net(net), h->lv[h->finest()].n);
+        // the conv form of every layer at this grid's size, timed now (before any capture)
+        cnn_tune(cnn_net(net), h->lv[h->finest()].n, h->cnn_ms, h->cnn_form);
         if (h->graph && h->graph_kind == 3) {
             cudaGraphExecDestroy(h->graph);
             h->graph = nullptr;
             h->graph_kind = -1;
+        }
+    });
+}
+
+int drf_bz_cnn_tuning(drf_bz *h, int *form4, double *ms8) {
+    return guard([&] {
+        check_bz(h);
+        DRF_CHECK(h->cnn, DRF_E_INVALID, "no learned preconditioner attached");
+        for (int l = 0; l < 4; ++l) {
+            if (form4) form4[l] = h->cnn_form[l];
+            if (ms8) { ms8[2 * l] = h->cnn_ms[l][0]; ms8[2 * l + 1] = h->cnn_ms[l][1]; }
         }
     });
 }

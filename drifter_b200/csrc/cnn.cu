@@ -16,7 +16,10 @@
 
 #include <cmath>
 #include <cstdlib>
+#include <array>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <memory>
 #include <random>
 #include <vector>
@@ -720,20 +723,39 @@ void conv_tc(cudaStream_t s, int B, int H, int W, const bf16 *X, const bf16 *Wt,
     DRF_LAUNCHED();
 }
 
-// DRIFTER_B200_CNN_MMA=tcgen05 selects the tcgen05 conv; the default is the warp-level mma.sync
-// kernel, which is the faster of the two on the C4 network (32 channels: N = 32 per MMA)
-inline bool use_tcgen05() {
+// Conv form per (layer, batch, height, width): 0 the warp-level mma.sync kernel, 1 the tcgen05
+// kernel. Both compute bit-identical outputs. DRIFTER_B200_CNN_MMA=tcgen05 or =mma_sync forces
+// a form; otherwise the autotuner (cnn_tune) times both at the preconditioner's size and keeps
+// the faster, and untuned shapes (the training batches) take mma.sync.
+inline int forced_conv_form() {
     static const int v = [] {
         const char *e = std::getenv("DRIFTER_B200_CNN_MMA");
-        return (e && std::strcmp(e, "tcgen05") == 0) ? 1 : 0;
+        if (e && std::strcmp(e, "tcgen05") == 0) return 1;
+        if (e && std::strcmp(e, "mma_sync") == 0) return 0;
+        return -1;
     }();
-    return v != 0;
+    return v;
+}
+std::mutex &conv_form_mu() {
+    static std::mutex m;
+    return m;
+}
+std::map<std::array<int, 4>, int> &conv_form_table() {
+    static std::map<std::array<int, 4>, int> t;
+    return t;
+}
+int conv_form(int l, int B, int H, int W) {
+    const int f = forced_conv_form();
+    if (f >= 0) return f;
+    std::lock_guard<std::mutex> lk(conv_form_mu());
+    const auto it = conv_form_table().find({l, B, H, W});
+    return it == conv_form_table().end() ? 0 : it->second;
 }
 
 template <int CIN, int COUT, bool RELU, bool OUTF32>
 void conv(cudaStream_t s, int B, int H, int W, const bf16 *X, const bf16 *Wt, const float *bias,
-          void *Y, int *err) {
-    if (use_tcgen05()) {
+          void *Y, int *err, int form) {
+    if (form == 1) {
         conv_tc<CIN, COUT, RELU, OUTF32>(s, B, H, W, X, Wt, bias, Y, err);
         return;
     }
@@ -755,13 +777,15 @@ void conv(cudaStream_t s, int B, int H, int W, const bf16 *X, const bf16 *Wt, co
     DRF_LAUNCHED();
 }
 
+// form -1: the tuned (or forced, or default) form of this layer and shape
 void conv_layer(cudaStream_t s, int l, int B, int H, int W, const bf16 *X, const bf16 *Wt,
-                const float *bias, void *Y, int *err) {
+                const float *bias, void *Y, int *err, int form = -1) {
+    if (form < 0) form = conv_form(l, B, H, W);
     switch (l) {
-    case 0: conv<16, 32, true, false>(s, B, H, W, X, Wt, bias, Y, err); break;
-    case 1: conv<32, 32, true, false>(s, B, H, W, X, Wt, bias, Y, err); break;
-    case 2: conv<32, 32, true, false>(s, B, H, W, X, Wt, bias, Y, err); break;
-    default: conv<32, 16, false, true>(s, B, H, W, X, Wt, bias, Y, err); break;
+    case 0: conv<16, 32, true, false>(s, B, H, W, X, Wt, bias, Y, err, form); break;
+    case 1: conv<32, 32, true, false>(s, B, H, W, X, Wt, bias, Y, err, form); break;
+    case 2: conv<32, 32, true, false>(s, B, H, W, X, Wt, bias, Y, err, form); break;
+    default: conv<32, 16, false, true>(s, B, H, W, X, Wt, bias, Y, err, form); break;
     }
 }
 
@@ -769,8 +793,8 @@ void conv_layer(cudaStream_t s, int l, int B, int H, int W, const bf16 *X, const
 void conv_back(cudaStream_t s, int l, int B, int H, int W, const bf16 *dZb, const bf16 *Wf, float *dX,
                int *err) {
     switch (l) {
-    case 3: conv<16, 32, false, true>(s, B, H, W, dZb, Wf, nullptr, dX, err); break;
-    default: conv<32, 32, false, true>(s, B, H, W, dZb, Wf, nullptr, dX, err); break;
+    case 3: conv<16, 32, false, true>(s, B, H, W, dZb, Wf, nullptr, dX, err, forced_conv_form() == 1); break;
+    default: conv<32, 32, false, true>(s, B, H, W, dZb, Wf, nullptr, dX, err, forced_conv_form() == 1); break;
     }
 }
 
@@ -911,6 +935,49 @@ int cnn_precondition(CnnNet *net, cudaStream_t s, int n, const double *r, const 
 }
 
 void cnn_prepare(CnnNet *net, int n) { net->ensure((int64_t)(n + 1) * (n + 1)); }
+
+// Autotuner of the conv form at the preconditioner's size ((n + 1)^2 superpixels, batch 1):
+// every layer is timed in both forms on the net's stream (two warm-up launches, then ten
+// between CUDA events) and the faster kept for the life of the process. Must run outside any
+// stream capture. DRIFTER_B200_TUNE=0 (or a forced form) skips it.
+void cnn_tune(CnnNet *net, int n, double ms_out[4][2], int form_out[4]) {
+    const int S = n + 1;
+    for (int l = 0; l < 4; ++l) {
+        form_out[l] = conv_form(l, 1, S, S);
+        ms_out[l][0] = ms_out[l][1] = 0.0;
+    }
+    const char *te = std::getenv("DRIFTER_B200_TUNE");
+    if ((te && te[0] == '0') || forced_conv_form() >= 0) return;
+    net->ensure((int64_t)S * S);
+    cudaStream_t st = net->stream;
+    cudaEvent_t e0, e1;
+    DRF_CUDA(cudaEventCreate(&e0));
+    DRF_CUDA(cudaEventCreate(&e1));
+    for (int l = 0; l < 4; ++l) {
+        const bf16 *X = net->act[l].p;
+        void *Y = l < 3 ? (void *)net->act[l + 1].p : (void *)net->out.p;
+        for (int form = 0; form < 2; ++form) {
+            for (int w = 0; w < 2; ++w)
+                conv_layer(st, l, 1, S, S, X, net->wb.p + net->off_wb[l], net->wm.p + net->off_b[l], Y,
+                           net->status.p, form);
+            DRF_CUDA(cudaEventRecord(e0, st));
+            for (int r = 0; r < 10; ++r)
+                conv_layer(st, l, 1, S, S, X, net->wb.p + net->off_wb[l], net->wm.p + net->off_b[l], Y,
+                           net->status.p, form);
+            DRF_CUDA(cudaEventRecord(e1, st));
+            DRF_CUDA(cudaEventSynchronize(e1));
+            float t = 0.f;
+            DRF_CUDA(cudaEventElapsedTime(&t, e0, e1));
+            ms_out[l][form] = t / 10.0;
+        }
+        form_out[l] = ms_out[l][1] < ms_out[l][0] ? 1 : 0;
+        std::lock_guard<std::mutex> lk(conv_form_mu());
+        conv_form_table()[{l, 1, S, S}] = form_out[l];
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cnn_check(net, st);
+}
 
 void cnn_check(CnnNet *net, cudaStream_t s) {
     int st = 0;

@@ -20,4 +20,7 @@ int cnn_precondition(CnnNet *net, cudaStream_t s, int n, const double *r, const 
                      const double *dq = nullptr, double *part = nullptr);
 // surfaces (and clears) the network's device status word: throws when a bounded wait gave up
 void cnn_check(CnnNet *net, cudaStream_t s);
+// autotunes the conv form (mma.sync or tcgen05) of every layer at the preconditioner's size
+// (n x n elements); ms[l][form] the timed launches, form[l] the choice (outside any capture)
+void cnn_tune(CnnNet *net, int n, double ms[4][2], int form[4]);
 }  // namespace drf

@@ -302,6 +302,11 @@ int drf_cnn_train(drf_cnn *h, int steps, int batch, int crop, double lr, uint64_
 /* attaches a trained network to a smoother as preconditioner kind 3 (output scale s:
  * z = D^-1 r + rms(r) s net(r / rms(r))) */
 int drf_bz_set_cnn(drf_bz *h, drf_cnn *net, double out_scale);
+/* The conv-form autotuning done by drf_bz_set_cnn at the smoother's size: form4[l] = 0 for the
+ * warp-level mma.sync conv, 1 for the tcgen05 conv of layer l (bit-identical outputs);
+ * ms8[2 l + f] = the timed launch of layer l in form f (0 when not tuned: DRIFTER_B200_TUNE=0 or
+ * DRIFTER_B200_CNN_MMA set). No reference counterpart. Either pointer may be NULL. */
+int drf_bz_cnn_tuning(drf_bz *h, int *form4, double *ms8);
 
 /* Allocation-free variant of drf_pcg_solve with the Jacobi preconditioner (kind 1), for callers
  * that cannot allocate device memory. No counterpart in the reference (it has no device code).

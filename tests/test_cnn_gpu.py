@@ -112,3 +112,22 @@ def test_trained_preconditioner_gains_over_plain_cg():
     assert i_cnn["iters"] < i_cg["iters"]
     assert i_cnn["iters"] < i_j["iters"]
     assert np.abs(x_cnn - x_mg).max() / np.abs(x_mg).max() < 1e-8
+
+
+def test_conv_form_autotuner_keeps_the_preconditioner_unchanged(monkeypatch):
+    """Attaching a network to a smoother times both conv forms (mma.sync, tcgen05) of every
+    layer at the smoother's size and keeps the faster; the forms are bit-identical, so the
+    preconditioner's output equals the one with the form forced either way."""
+    n = 48
+    X, Y = O.gauss_points(n, n, 0, 0, 3000.0, 3000.0)
+    s = BezierSmoother(n, n, 3000.0, 3000.0, 100.0 + 0.01 * X, lam=1.0, ridge_epsilon=1e-4)
+    net = CNN(seed=3)
+    net.attach(s)
+    t = s.cnn_tuning()
+    assert all(f in ("mma_sync", "tcgen05") for f in t["forms"])
+    assert all(v > 0 for f in ("mma_sync", "tcgen05") for v in t["ms"][f])
+    r = np.random.default_rng(4).standard_normal(s.ndof)
+    z = s.precondition(r, "cnn")
+    assert np.isfinite(z).all() and np.abs(z).max() > 0
+    s.close()
+    net.close()
