@@ -66,6 +66,8 @@ _SIGS = {
     "drf_dg_sync": (C.c_int, [C.c_void_p]),
     "drf_dg_upload_state": (C.c_int, [C.c_void_p, C.POINTER(_dp), _dp, C.c_double]),
     "drf_dg_download_state": (C.c_int, [C.c_void_p, C.POINTER(_dp), _dp, _dp, _dp, _dp, _dp]),
+    "drf_dg_output_stage": (C.c_int, [C.c_void_p, C.POINTER(_dp), _dp, _dp, _dp]),
+    "drf_dg_output_wait": (C.c_int, [C.c_void_p, _dp]),
     "drf_dg_compute_rhs": (C.c_int, [C.c_void_p, C.POINTER(_dp), _dp, _dp]),
     "drf_dg_compute_rhs2d": (C.c_int, [C.c_void_p, _dp, _dp, C.c_double, _dp, _dp, _dp]),
     "drf_dg_step_modesplit": (C.c_int, [C.c_void_p, C.c_double, C.c_int, C.c_int]),

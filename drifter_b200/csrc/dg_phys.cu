@@ -1594,6 +1594,13 @@ __global__ void correct3d_kernel(int64_t n3, int nz, T *Hu, T *Hv, T *HT, T *HS,
     HS[t] = fma(HS[t], dr, HS[t]);
 }
 
+// FP64 copy of a 3D field (the output snapshot)
+template <typename T>
+__global__ void widen_kernel(int64_t n, const T *__restrict__ src, double *__restrict__ dst) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t < n) dst[t] = (double)src[t];
+}
+
 // depth integral per 2D node of a 3D field (FP64 accumulation)
 template <typename T, int NP>
 __global__ void column_integral_kernel(int64_t n2, int nz, double dsig, const T *q, double *out) {
@@ -1844,6 +1851,12 @@ struct drf_dg {
     double baro_ms[4] = {0.0, 0.0, 0.0, 0.0};
     int graph_nsub = 0;
     size_t smem = 0;
+    // asynchronous output staging: FP64 snapshot buffers (4 3D fields, 4 2D fields and the
+    // time), a copy stream and its events; allocated at the first drf_dg_output_stage
+    DevBuf<double> out3, out2;
+    cudaStream_t ostream = nullptr;
+    cudaEvent_t ev_snap = nullptr, ev_copied = nullptr;
+    bool out_pending = false;
 
     void *q(int buf, int v) { return q3p + ((size_t)buf * 4 + v) * n3s * tsz; }
     void *res(int v) { return q3p + ((size_t)8 + v) * n3s * tsz; }
@@ -1881,6 +1894,12 @@ struct drf_dg {
     }
     ~drf_dg() {
         drop_graphs();
+        if (ostream) {
+            cudaStreamSynchronize(ostream);
+            cudaStreamDestroy(ostream);
+        }
+        if (ev_snap) cudaEventDestroy(ev_snap);
+        if (ev_copied) cudaEventDestroy(ev_copied);
         if (own) cudaStreamDestroy(own);
     }
 
@@ -2387,6 +2406,67 @@ int drf_dg_download_state(drf_dg *m, double *const *q4, double *eta, double *HU,
         if (HV) DRF_CUDA(cudaMemcpy(HV, m->HV, m->n2 * 8, cudaMemcpyDeviceToHost));
         if (eta_avg) DRF_CUDA(cudaMemcpy(eta_avg, m->eta_avg, m->n2 * 8, cudaMemcpyDeviceToHost));
         if (t) DRF_CUDA(cudaMemcpy(t, m->tdev, 8, cudaMemcpyDeviceToHost));
+    });
+}
+
+// Asynchronous output staging (the step either side of the output calls around
+// SimulationDriver's loop, src/io/vtk_writer.cpp): the state is folded (pending transport
+// correction) and snapshot in FP64 on the model's stream, then copied to the caller's host
+// buffers on a copy stream of the model; the model keeps stepping while the copy runs. A new
+// snapshot waits for the previous copy.
+int drf_dg_output_stage(drf_dg *m, double *const *q4, double *eta, double *HU, double *HV) {
+    return guard([&] {
+        check_model(m);
+        DRF_CHECK(!m->view, DRF_E_INVALID, "stage ensemble members' output through their ensemble's stream");
+        if (!m->ostream) {
+            DRF_CUDA(cudaStreamCreateWithFlags(&m->ostream, cudaStreamNonBlocking));
+            DRF_CUDA(cudaEventCreateWithFlags(&m->ev_snap, cudaEventDisableTiming));
+            DRF_CUDA(cudaEventCreateWithFlags(&m->ev_copied, cudaEventDisableTiming));
+        }
+        if (q4 && m->out3.n < (size_t)4 * m->n3) m->out3.alloc((size_t)4 * m->n3);
+        if (m->out2.n < (size_t)3 * m->n2 + 1) m->out2.alloc((size_t)3 * m->n2 + 1);
+        if (m->out_pending) DRF_CUDA(cudaStreamWaitEvent(m->stream, m->ev_copied, 0));
+        m->materialize();
+        if (q4)
+            m->with_types([&](auto tv, auto) {
+                using T = decltype(tv);
+                for (int v = 0; v < 4; ++v)
+                    if (q4[v]) {
+                        widen_kernel<T><<<blocks_for(m->n3), 256, 0, m->stream>>>(
+                            m->n3, (const T *)m->q(m->cur, v), m->out3.p + (size_t)v * m->n3);
+                        DRF_LAUNCHED();
+                    }
+            });
+        const double *src2[3] = {m->eta, m->HU, m->HV};
+        for (int k = 0; k < 3; ++k)
+            DRF_CUDA(cudaMemcpyAsync(m->out2.p + (size_t)k * m->n2, src2[k], m->n2 * 8, cudaMemcpyDeviceToDevice,
+                                     m->stream));
+        DRF_CUDA(cudaMemcpyAsync(m->out2.p + (size_t)3 * m->n2, m->tdev, 8, cudaMemcpyDeviceToDevice, m->stream));
+        DRF_CUDA(cudaEventRecord(m->ev_snap, m->stream));
+        DRF_CUDA(cudaStreamWaitEvent(m->ostream, m->ev_snap, 0));
+        if (q4)
+            for (int v = 0; v < 4; ++v)
+                if (q4[v])
+                    DRF_CUDA(cudaMemcpyAsync(q4[v], m->out3.p + (size_t)v * m->n3, m->n3 * 8,
+                                             cudaMemcpyDeviceToHost, m->ostream));
+        double *dst2[3] = {eta, HU, HV};
+        for (int k = 0; k < 3; ++k)
+            if (dst2[k])
+                DRF_CUDA(cudaMemcpyAsync(dst2[k], m->out2.p + (size_t)k * m->n2, m->n2 * 8, cudaMemcpyDeviceToHost,
+                                         m->ostream));
+        DRF_CUDA(cudaEventRecord(m->ev_copied, m->ostream));
+        m->out_pending = true;
+    });
+}
+
+int drf_dg_output_wait(drf_dg *m, double *t) {
+    return guard([&] {
+        check_model(m);
+        DRF_CHECK(m->out_pending, DRF_E_INVALID, "no output staged (drf_dg_output_stage)");
+        DRF_CUDA(cudaEventSynchronize(m->ev_copied));
+        if (t) DRF_CUDA(cudaMemcpy(t, m->out2.p + (size_t)3 * m->n2, 8, cudaMemcpyDeviceToHost));
+        m->out_pending = false;
+        check_device_status(m);
     });
 }
 

@@ -201,6 +201,23 @@ class OceanModel:
         return dict(Hu=q[0], Hv=q[1], HT=q[2], HS=q[3], eta=eta, HU=HU, HV=HV, eta_avg=eavg,
                     t=t.value)
 
+    def output_stage(self, out: dict) -> None:
+        """Snapshot the state and copy it to the host arrays of `out` (keys Hu, Hv, HT, HS, eta,
+        HU, HV; float64, contiguous, ideally pinned) while later steps run; the arrays hold the
+        snapshot after output_wait()."""
+        q = [out.get(k) for k in ("Hu", "Hv", "HT", "HS")]
+        q4 = dptr_array(q) if any(a is not None for a in q) else None
+        self._staged = out  # kept alive until the copy is done
+        check(lib().drf_dg_output_stage(self.handle, q4, *[dptr(out[k]) if out.get(k) is not None else None
+                                                           for k in ("eta", "HU", "HV")]))
+
+    def output_wait(self) -> float:
+        """Waits for the staged copy; returns the snapshot's model time."""
+        t = C.c_double()
+        check(lib().drf_dg_output_wait(self.handle, C.byref(t)))
+        self._staged = None
+        return t.value
+
     def compute_rhs(self) -> dict:
         n3, n2 = self.cfg.n3, self.cfg.n2
         r = [np.empty(n3) for _ in range(4)]

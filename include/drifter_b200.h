@@ -122,6 +122,17 @@ int drf_dg_upload_state(drf_dg *m, const double *const *q4, const double *eta, d
 int drf_dg_download_state(drf_dg *m, double *const *q4, double *eta, double *HU, double *HV,
                           double *eta_avg, double *t);
 
+/* Asynchronous output staging around the time loop (SimulationDriver's output calls,
+ * src/io/vtk_writer.cpp, write from host copies of the state): the current state (pending
+ * transport correction folded in) is snapshot in FP64 on the model's stream and copied to the
+ * given host buffers on a copy stream of its own, so steps enqueued after this call run while
+ * the copy is in flight. The buffers (q4 = {Hu, Hv, HT, HS} 3D, eta, HU, HV 2D; any may be NULL)
+ * are valid after drf_dg_output_wait, which also returns the snapshot's model time. Pinned
+ * (page-locked) host buffers make the copy asynchronous. A new drf_dg_output_stage waits for the
+ * previous copy on the device, not on the host. */
+int drf_dg_output_stage(drf_dg *m, double *const *q4, double *eta, double *HU, double *HV);
+int drf_dg_output_wait(drf_dg *m, double *t);
+
 /* Coupled right-hand side at the current state (eta frozen): R = {dHu, dHv, dHT, dHS},
  * omega (3D sigma velocity), deta (2D, -int div(Hu) dsigma). Maps
  * PrimitiveEquationsSolver::compute_rhs + apply_interface_fluxes + the column diagnosis

@@ -376,3 +376,38 @@ def test_diagnostics_with_pending_correction_equal_materialized():
     db = b.diagnostics()
     for k in da:
         assert da[k] == db[k], k
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_output_staging_overlaps_steps_and_returns_the_snapshot(precision):
+    """drf_dg_output_stage snapshots the state (its pending transport correction folded in) and
+    copies it to pinned host buffers on the model's copy stream while the next steps run;
+    after output_wait the buffers hold exactly the state download_state returns at that step."""
+    torch = pytest.importorskip("torch")
+    case = _tidal_small(precision, nx=9, ny=7)
+    cfg = case["cfg"]
+    a = OceanModel(cfg, case["h"], case["f"], case["taux"], case["tauy"])
+    b = OceanModel(cfg, case["h"], case["f"], case["taux"], case["tauy"])
+    for m in (a, b):
+        m.upload_state(case["q"], case["eta"])
+        m.step(case["dt"], case["nsub"], 2)
+    pinned = {k: torch.empty(cfg.n3 if k in ("Hu", "Hv", "HT", "HS") else cfg.n2,
+                             dtype=torch.float64).pin_memory().numpy()
+              for k in ("Hu", "Hv", "HT", "HS", "eta", "HU", "HV")}
+    a.output_stage(pinned)
+    a.step(case["dt"], case["nsub"], 3)  # runs while the copy is in flight
+    t = a.output_wait()
+    ref = b.download_state()
+    assert t == ref["t"]
+    for k in pinned:
+        assert np.array_equal(pinned[k], ref[k]), k
+    # a second stage after further steps; the model itself is unaffected by staging
+    a.output_stage(pinned)
+    t2 = a.output_wait()
+    b.step(case["dt"], case["nsub"], 3)
+    ref2 = b.download_state()
+    assert t2 == ref2["t"]
+    for k in pinned:
+        assert np.array_equal(pinned[k], ref2[k]), k
+    a.close()
+    b.close()
