@@ -31,6 +31,13 @@ int main() {
                 s.HT(i) = (10.0 + std::sin(x)) * H;
                 s.HS(i) = 35.0 * H;
                 s.omega(i) = 1e-5 * std::sin(x);
+                // the derived fields (PrimitiveState::update_derived)
+                s.H(i) = H;
+                s.u(i) = s.Hu(i) / H;
+                s.v(i) = s.Hv(i) / H;
+                s.T(i) = s.HT(i) / H;
+                s.S(i) = s.HS(i) / H;
+                s.rho(i) = 1025.0 * (1.0 - 2e-4 * (s.T(i) - 10.0) + 7.6e-4 * (s.S(i) - 35.0));
             }
         }
         PrimitiveEquationsSolver pe(order);

@@ -55,8 +55,8 @@ def test_adapters_equal_the_python_mirror(tmp_path):
     sums = [td[k].sum() for k in ("dHu_dt", "dHv_dt", "deta_dt", "dHT_dt", "dHS_dt")]
     assert _close(res["compat_rhs"], sums, 1e-11)
     full = dict(st)
-    for k in ("H", "u", "v", "T", "S", "rho"):
-        full[k] = np.zeros_like(h)
+    full.update(H=H, u=st["Hu"] / H, v=st["Hv"] / H, T=st["HT"] / H, S=st["HS"] / H)
+    full["rho"] = 1025.0 * (1.0 - 2e-4 * (full["T"] - 10.0) + 7.6e-4 * (full["S"] - 35.0))
     ModeSplittingSolver(3, h, f, subcycles=10).step(5.0, full)
     assert _close(res["compat_step"], [full["eta"].sum(), full["Hu"].sum()], 1e-11)
     # the coupled model
