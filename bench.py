@@ -178,19 +178,27 @@ def make_case(small, mid=False):
     return configs.c2()
 
 
+def compat_sample(nel):
+    """Seeded C2-shaped N=4 element states (500-550 m deep, random transports) for the
+    reference-semantics element RHS."""
+    nd = 125
+    rng = np.random.default_rng(0)
+    h = np.full((nel, nd), 500.0) + rng.uniform(0, 50, (nel, nd))
+    f = np.full((nel, nd), 1e-4)
+    H = h.copy()
+    st = dict(Hu=H * 0.1 * rng.standard_normal((nel, nd)), Hv=H * 0.1 * rng.standard_normal((nel, nd)),
+              eta=np.zeros((nel, nd)), HT=H * 10.0, HS=H * 35.0, omega=np.zeros((nel, nd)))
+    return st, h, f
+
+
 def cpu_baseline(seconds=12.0, threads=1):
     """Reference CPU path (SimulationDriver::step, non-split SSPRK3 over the dense-Kronecker
     element RHS, src/solver/simulation_driver.cpp:108) on C2-shaped N=4 elements."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle as O
     order, nd = 4, 125
-    rng = np.random.default_rng(0)
     nel = 64 * max(1, threads)
-    h = np.full((nel, nd), 500.0) + rng.uniform(0, 50, (nel, nd))
-    f = np.full((nel, nd), 1e-4)
-    H = h.copy()
-    st = dict(Hu=H * 0.1 * rng.standard_normal((nel, nd)), Hv=H * 0.1 * rng.standard_normal((nel, nd)),
-              eta=np.zeros((nel, nd)), HT=H * 10.0, HS=H * 35.0, omega=np.zeros((nel, nd)))
+    st, h, f = compat_sample(nel)
     done, t0 = 0, time.perf_counter()
     while True:
         st = O.compat_ssprk3(order, 1.0, st, h, f, nthreads=threads)
@@ -201,6 +209,25 @@ def cpu_baseline(seconds=12.0, threads=1):
     rate = nel * nd * 4 * 3 * done / el
     return rate, dict(sample=f"{done} SSPRK3 steps x {nel} N=4 elements ({nel*nd*4} DOFs), "
                       f"{el:.1f} s", threads=threads)
+
+
+def same_algorithm(cpu_value, nel=128 * 128 * 16, reps=20):
+    """The reference's element-local RHS (PrimitiveEquationsSolver::compute_rhs with its
+    semantics, FP64) timed on the GPU over C2's element count, from the CPU sample's elements
+    repeated: one algorithm on both sides, so the ratio compares hardware and implementation
+    only. DOF-stages count the 4 transported variables per node and RHS evaluation, as the
+    CPU baseline does."""
+    from drifter_b200.dg import PrimitiveEquationsSolver
+    st, h, f = compat_sample(64)
+    pe = PrimitiveEquationsSolver(4, h, f)
+    ms = pe.time_rhs(st, nel, reps)
+    gpu = nel * 125 * 4 / (ms / 1e3)
+    out = {"workload": f"reference element RHS (FP64), {nel} N=4 elements, device time per launch",
+           "gpu_ms_per_rhs": ms, "gpu_value": gpu, "unit": UNIT}
+    if cpu_value:
+        out["cpu_value_1core"] = cpu_value
+        out["ratio_gpu_over_cpu_1core"] = gpu / cpu_value
+    return out
 
 
 def run_cg(stream, reps=3):
@@ -566,6 +593,9 @@ def run_ours(args, rank, world, local):
     if rank == 0 and not args.no_cpu:
         v, meta = cpu_baseline(seconds=12.0, threads=1)
         cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "port", "sample": meta["sample"]}
+    same = None
+    if rank == 0 and not args.no_cpu:
+        same = same_algorithm(cpu["value"] if cpu else None)
 
     if rank == 0:
         line = {
@@ -584,6 +614,7 @@ def run_ours(args, rank, world, local):
                          "copy_ceiling_gbs": copy["gbs"], "copy_ceiling_frac": copy["gbs"] / peak,
                          "peak_source": f"{peak_kind} MEASURED_PEAKS.json hbm_gbs"},
             "cpu_baseline": cpu,
+            "same_algorithm": same,
             "e2e": e2e,
             "fp64_gpu": fp64,
             "baroclinic": baro,

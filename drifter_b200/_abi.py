@@ -57,6 +57,8 @@ _SIGS = {
     "drf_sw_flux_batch": (C.c_int, [C.c_int, C.c_int64, _dp, _dp, _dp, C.c_double, _dp]),
     "drf_compat_compute_rhs": (C.c_int, [C.c_int, C.c_int, C.POINTER(_dp), _dp, _dp, _dp,
                                          C.POINTER(_dp)]),
+    "drf_compat_time_rhs": (C.c_int, [C.c_int, C.c_int, C.POINTER(_dp), _dp, _dp, _dp, C.c_int,
+                                      C.c_int, _dp]),
     "drf_compat_modesplit_step": (C.c_int, [C.c_int, C.c_int, C.c_double, C.c_int,
                                             C.POINTER(_dp), _dp, _dp, _dp]),
     "drf_dg_create": (C.c_int, [C.POINTER(MeshDesc), C.POINTER(DGParams), _dp, _dp, _dp, _dp,

@@ -6,6 +6,7 @@
 // sum-factorized ((N+1) terms per direction) instead of the reference's dense
 // (N+1)^3 x (N+1)^3 Kronecker matvecs (src/dg/basis_hexahedron.cpp:321); the summation
 // order matches the dense product's non-zero order, so results agree to rounding.
+#include <algorithm>
 #include <cstring>
 #include <mutex>
 
@@ -356,6 +357,55 @@ int drf_compat_compute_rhs(int order, int nel, const double *const *in6, const d
         });
         DRF_LAUNCHED();
         for (int q = 0; q < 5; ++q) DRF_CUDA(cudaMemcpy(out5[q], d[8 + q], 8 * N, cudaMemcpyDeviceToHost));
+    });
+}
+
+int drf_compat_time_rhs(int order, int nsrc, const double *const *in6, const double *h,
+                        const double *f, const double *params8, int nel, int nrep, double *ms) {
+    return guard([&] {
+        DRF_CHECK(nsrc >= 1 && nel >= nsrc && nrep >= 1 && in6 && h && f && params8 && ms,
+                  DRF_E_INVALID, "bad arguments");
+        HostBasis b = make_lgl_basis(order);
+        const size_t nd = (size_t)b.np * b.np * b.np, S = nd * nsrc, N = nd * nel;
+        for (int q = 0; q < 6; ++q)
+            DRF_CHECK(all_finite(in6[q], S), DRF_E_NONFINITE, "non-finite value in state input");
+        upload_basis(b);
+        DevBuf<double> buf(N * 13);
+        double *d[13];
+        for (int q = 0; q < 13; ++q) d[q] = buf.p + q * N;
+        // the nsrc source elements, repeated to nel elements on the device (doubling copies)
+        const double *src[8] = {in6[0], in6[1], in6[2], in6[3], in6[4], in6[5], h, f};
+        for (int q = 0; q < 8; ++q) {
+            DRF_CUDA(cudaMemcpy(d[q], src[q], 8 * S, cudaMemcpyHostToDevice));
+            for (size_t have = S; have < N;) {
+                const size_t c = std::min(have, N - have);
+                DRF_CUDA(cudaMemcpy(d[q] + have, d[q], 8 * c, cudaMemcpyDeviceToDevice));
+                have += c;
+            }
+        }
+        CompatP p = compat_params(params8);
+        cudaEvent_t e0, e1;
+        DRF_CUDA(cudaEventCreate(&e0));
+        DRF_CUDA(cudaEventCreate(&e1));
+        auto launch = [&] {
+            dispatch_np(b.np, [&](auto npc) {
+                constexpr int NP = decltype(npc)::value;
+                compat_rhs_kernel<NP><<<nel, NP * NP * NP>>>(nel, d[0], d[1], d[2], d[3], d[4], d[5],
+                                                             d[6], d[7], p, d[8], d[9], d[10], d[11],
+                                                             d[12]);
+            });
+            DRF_LAUNCHED();
+        };
+        for (int r = 0; r < 3; ++r) launch();  // warm-up
+        DRF_CUDA(cudaEventRecord(e0));
+        for (int r = 0; r < nrep; ++r) launch();
+        DRF_CUDA(cudaEventRecord(e1));
+        DRF_CUDA(cudaEventSynchronize(e1));
+        float t = 0.f;
+        DRF_CUDA(cudaEventElapsedTime(&t, e0, e1));
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        *ms = (double)t / nrep;
     });
 }
 

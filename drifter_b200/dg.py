@@ -65,6 +65,16 @@ class PrimitiveEquationsSolver:
                                            dptr(self.f), dptr(self.params), dptr_array(outs)))
         return dict(zip(("dHu_dt", "dHv_dt", "deta_dt", "dHT_dt", "dHS_dt"), outs))
 
+    def time_rhs(self, states: dict, nel: int, reps: int = 20) -> float:
+        """Device milliseconds of one compute_rhs launch over nel elements: the given elements
+        repeated to nel on the device (the bathymetry and Coriolis arrays with them)."""
+        ins = [_c(states[k]) for k in ("Hu", "Hv", "eta", "HT", "HS", "omega")]
+        ms = np.zeros(1)
+        check(lib().drf_compat_time_rhs(self.order, ins[0].shape[0], dptr_array(ins),
+                                        dptr(self.h), dptr(self.f), dptr(self.params), nel,
+                                        reps, dptr(ms)))
+        return float(ms[0])
+
 
 STATE12 = ("Hu", "Hv", "eta", "HT", "HS", "H", "u", "v", "T", "S", "omega", "rho")
 

@@ -70,6 +70,13 @@ int drf_sw_flux_batch(int kind, int64_t n, const double *UL, const double *UR,
 int drf_compat_compute_rhs(int order, int nel, const double *const *in6, const double *h,
                            const double *f, const double *params8, double *const *out5);
 
+/* Device time of PrimitiveEquationsSolver::compute_rhs (the element-local right-hand side
+ * above) on nel elements: the nsrc given elements are repeated to nel on the device, the kernel
+ * runs 3 untimed and nrep timed launches, and *ms is the mean per launch (CUDA events). Lets a
+ * caller compare the same algorithm on the GPU and on the host. */
+int drf_compat_time_rhs(int order, int nsrc, const double *const *in6, const double *h,
+                        const double *f, const double *params8, int nel, int nrep, double *ms);
+
 /* ModeSplittingSolver::step (include/physics/mode_splitting.hpp:241,
  * src/physics/mode_splitting.cpp:434) on nel elements, in place.
  * st12 = {Hu, Hv, eta, HT, HS, H, u, v, T, S, omega, rho}. */

@@ -54,7 +54,7 @@ int main() {
                     sums[4]);
         ModeSplittingSolver ms(order, OceanConstants{}, 10);
         ms.initialize(h, f);
-        ms.step(5.0, st);
+        ms.step(0.01, st);  // reference coordinates (no metric): a stable step is short
         double se = 0.0, su = 0.0;
         for (const auto &s : st)
             for (int i = 0; i < nd; ++i) { se += s.eta(i); su += s.Hu(i); }
@@ -64,7 +64,7 @@ int main() {
         try {
             ModeSplittingSolver bad(order, OceanConstants{}, 0);
             bad.initialize(h, f);
-            bad.step(5.0, st);
+            bad.step(0.01, st);
         } catch (const std::invalid_argument &) {
             threw = true;
         }
