@@ -93,6 +93,9 @@ struct StageArgs {
     int mode;   // 0: LSRK stage update, 1: write the right-hand side into res[]
     int first;  // 1: A = 0 stage (res not read, column increments overwritten)
     int bulk;   // 1: column blocks are 16-byte aligned -> staged with cp.async.bulk
+    // with bulk staging: the column pf columns ahead (the one a CTA launched about one wave of
+    // resident CTAs later takes) is prefetched into L2 at this column's start; 0 = none
+    int pf;
     int *err;   // device status word (DRF_E_TIMEOUT when a bounded wait gives up)
     Geo G;
 };
@@ -118,6 +121,13 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
             smem_addr(dst)),
         "l"(g), "r"(bytes), "r"(smem_addr(bar))
         : "memory");
+}
+// Bulk prefetch of global memory into L2 (no completion to wait for); 16-byte aligned source,
+// size a multiple of 16.
+__device__ __forceinline__ void bulk_prefetch_l2(const void *src, uint32_t bytes) {
+    uint64_t g;
+    asm volatile("cvta.to.global.u64 %0, %1;" : "=l"(g) : "l"(src));
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(g), "r"(bytes) : "memory");
 }
 // Spins on the barrier's phase with an iteration limit; false when it gave up.
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t phase) {
@@ -274,11 +284,12 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, int c, uint3
     T *sPn = Tl::pn_in_res ? sRes + 3 * ncn : tail;
     T *sTb = Tl::tb_in_d ? sD : tail + (Tl::pn_in_res ? 0 : 4 * nz * NP2);
     T *sTbn = sTb + nz * NP2;
-    __shared__ int s_ok;
+    __shared__ int s_ok, s_ok2;
 
     // tidal elevation: evaluated once per CTA, and only by a column on a tidal side
     __shared__ T s_etide;
     if (threadIdx.x == 0) {
+        s_ok2 = 1;
         const bool tidal = (ex == 0 && G.bc[0] == DRF_BC_TIDE) || (ex == G.nx - 1 && G.bc[1] == DRF_BC_TIDE) ||
                            (ey == 0 && G.bc[2] == DRF_BC_TIDE) || (ey == G.ny - 1 && G.bc[3] == DRF_BC_TIDE);
         s_etide = tidal ? (T)tide_at(G, a.tdev[0] + a.toff) : T(0);
@@ -299,6 +310,14 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, int c, uint3
         }
 
     // ---- stage the column: state (and the 2N register) by TMA bulk copies when aligned
+    if (a.bulk && a.pf > 0 && threadIdx.x >= 32 && threadIdx.x < 40 && c + a.pf < G.nx * G.ny) {
+        // the state and register blocks of the column a later CTA takes, into L2
+        const int v = threadIdx.x - 32;
+        const size_t pb = (size_t)(c + a.pf) * ncn;
+        const uint32_t bytes = (uint32_t)(ncn * sizeof(T));
+        if (v < 4) bulk_prefetch_l2(a.qin[v] + pb, bytes);
+        else if (need_res) bulk_prefetch_l2(a.res[v - 4] + pb, bytes);
+    }
     if (a.bulk) {
         if (threadIdx.x == 0) {
             if (init) {
@@ -786,20 +805,11 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, int c, uint3
     __syncthreads();
 
     // ---- z pencils: advection d/dsigma, Coriolis, vertical diffusion, sigma faces, surface
-    // and bed stresses, then the LSRK update and the FP64 column increments
-    if (a.bulk && need_res) {
-        if (threadIdx.x == 0) s_ok = (int)mbar_wait(&bars[1], ph);
-        __syncthreads();
-        if (!s_ok) {
-            if (threadIdx.x == 0) atomicExch(a.err, DRF_E_TIMEOUT);
-            return false;
-        }
-    }
-    // the (HT, HS) half of the register: each thread waits for it before its first (HT, HS) pair
+    // and bed stresses, then the LSRK update and the FP64 column increments. Each thread
+    // waits for the register halves itself: (Hu, Hv) here, (HT, HS) before its first (HT, HS)
+    // pair; a wait that gives up clears s_ok2, checked at the barrier after the pass.
+    if (a.bulk && need_res && !mbar_wait(&bars[1], ph)) s_ok2 = 0;
     bool w2 = !(a.bulk && need_res);
-    __shared__ int s_ok2;
-    if (threadIdx.x == 0) s_ok2 = 1;
-    __syncthreads();
     for (int p = threadIdx.x; p < npen; p += blockDim.x) {
         const int ez = p / NP2, an = p % NP2;
         const int e0 = ez * NP3 + an;
@@ -810,10 +820,17 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, int c, uint3
         // with the mass flux M0 through the layer's bottom face lifted in), I the column's
         // quadrature total of delta; with the LGL weights each layer passes on M1 = M0 + dsig I
         // - Q(layer), and the flux through the surface is 0 by the choice of I
-        T Iq = 0, M0 = 0;
-        for (int e = 0; e < nz; ++e) Iq += sQl[e * NP2 + an];
+        // Iq the column total, Pq the total of the layers below this one:
+        // M0 = sum over those layers of (dsig Iq - Q(layer)) = ez dsig Iq - Pq
+        T Iq = 0, Pq = 0;
+#pragma unroll 4
+        for (int e = 0; e < nz; ++e) {
+            const T v = sQl[e * NP2 + an];
+            Iq += v;
+            if (e < ez) Pq += v;
+        }
         const T dsg = (T)G.dsig;
-        for (int e = 0; e < ez; ++e) M0 += dsg * Iq - sQl[e * NP2 + an];
+        T M0 = fma((T)ez * dsg, Iq, -Pq);
         const T M1 = top ? T(0) : M0 + (dsg * Iq - sQl[ez * NP2 + an]);
         if (bed) M0 = 0;
         if (a.mode == 1 && a.deta_out && bed) a.deta_out[(size_t)c * NP2 + an] = -(double)Iq;
@@ -1851,6 +1868,9 @@ struct drf_dg {
     double baro_ms[4] = {0.0, 0.0, 0.0, 0.0};
     int graph_nsub = 0;
     size_t smem = 0;
+    // L2 prefetch distance of the stage launch in columns (resident stage CTAs on the device),
+    // 0 for none; DRIFTER_B200_STAGE_PREFETCH=0 in the environment switches it off
+    int stage_pf = 0;
     // asynchronous output staging: FP64 snapshot buffers (4 3D fields, 4 2D fields and the
     // time), a copy stream and its events; allocated at the first drf_dg_output_stage
     DevBuf<double> out3, out2;
@@ -1943,6 +1963,7 @@ struct drf_dg {
         a.corrV = with_corr ? corrV : nullptr;
         a.corrR = with_corr ? corrR : nullptr;
         a.bulk = ((size_t)G.nz * np3 * sizeof(T)) % 16 == 0;
+        a.pf = stage_pf;
         a.err = err;
         a.G = G;
         return a;
@@ -2223,6 +2244,11 @@ void drf_dg::setup(const drf_mesh_desc *mesh, const drf_dg_params *params, const
         constexpr int NP = decltype(npc)::value;
         dispatch_stage_nz<T, NP>(mesh->nz, [&](auto kern) {
             allow_max_dynamic_smem(reinterpret_cast<const void *>(kern), maxsm);
+            int per_sm = 0, nsm = 0;
+            DRF_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+            DRF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, stage_threads(), smem));
+            const char *pe = std::getenv("DRIFTER_B200_STAGE_PREFETCH");
+            stage_pf = (pe && pe[0] == '0') ? 0 : per_sm * nsm;
         });
     });
 }
@@ -2890,8 +2916,9 @@ struct drf_ens {
         int src = in;
         for (int s = 0; s < 5; ++s) {
             const int dst = (s % 2 == 0) ? out : in;
-            const StageArgs<T> a = m0->template stage_args<T>(src, dst, s, 0.0, 0, nullptr, nullptr, nullptr,
-                                                              m0->eta, 0.0, s == 0);
+            StageArgs<T> a = m0->template stage_args<T>(src, dst, s, 0.0, 0, nullptr, nullptr, nullptr,
+                                                        m0->eta, 0.0, s == 0);
+            a.pf = 0;  // the work items are not in column order
             dg3d_stage_ens_kernel<T, NP><<<grid, threads, smem, stream>>>(a, table.p, items.p, nitems);
             DRF_LAUNCHED();
             src = dst;
