@@ -1869,7 +1869,8 @@ struct drf_dg {
     int graph_nsub = 0;
     size_t smem = 0;
     // L2 prefetch distance of the stage launch in columns (resident stage CTAs on the device),
-    // 0 for none; DRIFTER_B200_STAGE_PREFETCH=0 in the environment switches it off
+    // 0 for none; DRIFTER_B200_STAGE_PREFETCH=<waves> in the environment sets it in waves of
+    // resident CTAs (0 switches it off; default 1)
     int stage_pf = 0;
     // asynchronous output staging: FP64 snapshot buffers (4 3D fields, 4 2D fields and the
     // time), a copy stream and its events; allocated at the first drf_dg_output_stage
@@ -2248,7 +2249,8 @@ void drf_dg::setup(const drf_mesh_desc *mesh, const drf_dg_params *params, const
             DRF_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
             DRF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, stage_threads(), smem));
             const char *pe = std::getenv("DRIFTER_B200_STAGE_PREFETCH");
-            stage_pf = (pe && pe[0] == '0') ? 0 : per_sm * nsm;
+            const int waves = pe ? std::atoi(pe) : 1;
+            stage_pf = std::max(waves, 0) * per_sm * nsm;
         });
     });
 }
