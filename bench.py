@@ -421,6 +421,7 @@ def run_amr(stream, steps=5, warmup=3):
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / steps
     ndof = m["n_elem"] * (c["order"] + 1) ** 3
+    adapt = run_amr_adapt(c, gpu)
     gpu.close()
     types = np.bincount([f[0] for f in m["ifaces"]], minlength=6)
     return {"workload": c["name"] + ", complete mode, LF flux, LSRK45",
@@ -428,7 +429,39 @@ def run_amr(stream, steps=5, warmup=3):
             "faces": {"conforming": int(len(m["conf"])), "boundary": int(len(m["bnd"])),
                       "mortar_2x1": int(types[1]), "mortar_1x2": int(types[2]), "mortar_2x2": int(types[5])},
             "value": ndof * 5 / (ms / 1e3), "unit": UNIT, "ms_per_step": ms,
-            "rhs_ms": rhs["ms"], "rhs_gbs": rhs["alg_bytes"] / (rhs["ms"] / 1e3) / 1e9}
+            "rhs_ms": rhs["ms"], "rhs_gbs": rhs["alg_bytes"] / (rhs["ms"] / 1e3) / 1e9,
+            "adapt": adapt}
+
+
+def run_amr_adapt(c, gpu):
+    """One AdaptiveMeshRefinement::adapt of the C3 state after its steps: the estimator and the
+    transfer on the GPU, the column levels, face tables and mortar operators on the host
+    (wall-clock milliseconds of each part, host calls that end with a synchronize)."""
+    from drifter_b200.amr import AdaptiveMeshRefinement, DG3DIntegration, RefinementParams, build_mesh
+    m = c["mesh"]
+    nb = int(round(len(m["col_levels"]) ** 0.5))
+    levels = tuple(np.ascontiguousarray(m["col_levels"][:, d].reshape(nb, nb)) for d in range(3))
+    amr = AdaptiveMeshRefinement(c["order"], RefinementParams(max_level=4))
+    amr.estimate(gpu, m)  # warm-up
+    t = [time.perf_counter()]
+    _, mask, flags = amr.estimate(gpu, m)
+    t.append(time.perf_counter())
+    new_levels, changed = amr.refine_levels(levels, mask, flags)
+    t.append(time.perf_counter())
+    m2 = build_mesh(*new_levels)
+    t.append(time.perf_counter())
+    g2 = DG3DIntegration(c["order"], m2)
+    t.append(time.perf_counter())
+    amr.transfer(gpu, g2, levels, new_levels)
+    t.append(time.perf_counter())
+    nd = (c["order"] + 1) ** 3
+    out = {"columns_changed": int(changed), "hexes_before": int(m["n_elem"]), "hexes_after": int(m2["n_elem"]),
+           "estimate_ms": round(1e3 * (t[1] - t[0]), 3), "refine_levels_ms": round(1e3 * (t[2] - t[1]), 3),
+           "build_mesh_ms": round(1e3 * (t[3] - t[2]), 3), "create_ms": round(1e3 * (t[4] - t[3]), 3),
+           "transfer_ms": round(1e3 * (t[5] - t[4]), 3),
+           "transfer_bytes": int((m["n_elem"] + m2["n_elem"]) * nd * 8)}
+    g2.close()
+    return out
 
 
 def run_reference(args, rank, world):

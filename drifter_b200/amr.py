@@ -5,6 +5,7 @@ whose steps are CUDA graphs. All compute runs in libdrifter_b200.so on the GPU."
 from __future__ import annotations
 
 import ctypes as C
+from dataclasses import dataclass
 
 import numpy as np
 
@@ -26,6 +27,9 @@ def _sigs():
         "drf_amr_time_rhs": [vp, C.c_int, C.c_int, dp, C.c_int, dp, dp],
         "drf_amr_build_mesh": [C.c_int, C.c_int, vp, vp, vp, C.c_double, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp,
                                vp, vp, vp],
+        "drf_amr_estimate": [vp, dp, C.c_double, C.c_double, C.c_double, dp, vp, vp],
+        "drf_amr_refine_levels": [C.c_int, C.c_int, vp, vp, vp, i64, vp, vp, C.c_int, C.c_int, vp, vp, vp, vp],
+        "drf_amr_transfer": [vp, vp, C.c_int, C.c_int, vp, vp, vp, vp, vp, vp],
     }
     for k, a in sigs.items():
         getattr(L, k).argtypes = a
@@ -141,3 +145,84 @@ class DG3DIntegration:
         check(lib().drf_amr_time_rhs(self.h, MODES[mode], FLUX[flux], dptr(av), nrep, C.byref(ms),
                                      C.byref(ab)))
         return dict(ms=ms.value, alg_bytes=ab.value)
+
+
+@dataclass
+class RefinementParams:
+    """RefinementParams (include/amr/refinement.hpp:63)."""
+    refine_threshold: float = 0.1
+    coarsen_threshold: float = 0.01
+    max_level: int = 8
+    min_level: int = 0
+    smoothness_factor: float = 0.5
+
+
+def _iptr(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def element_lengths(mesh: dict) -> np.ndarray:
+    """Characteristic length cbrt(volume) of every element (estimate_element's h,
+    src/amr/refinement.cpp:84-87), from the mesh's element boxes."""
+    b = np.asarray(mesh["box"], dtype=np.float64)
+    return np.cbrt((b[:, 3] - b[:, 0]) * (b[:, 4] - b[:, 1]) * (b[:, 5] - b[:, 2]))
+
+
+class AdaptiveMeshRefinement:
+    """AdaptiveMeshRefinement (include/amr/refinement.hpp, src/amr/refinement.cpp:413) for the
+    column-wise refined meshes of build_mesh: the gradient estimator on the GPU, the column
+    levels (marking, refine / coarsen and 2:1 balance) on the host, the face tables rebuilt by
+    the native builder and the solution carried over on the GPU."""
+
+    def __init__(self, order: int, params: RefinementParams | None = None):
+        self.order = order
+        self.params = params or RefinementParams()
+
+    def estimate(self, model: DG3DIntegration, mesh: dict):
+        """GradientErrorEstimator::estimate of the model's device state: (value, mask, flags)."""
+        Lb = _sigs()
+        p = self.params
+        hchar = np.ascontiguousarray(element_lengths(mesh))
+        ne = model.n_elem
+        val = np.zeros(ne)
+        mask = np.zeros(ne, np.int32)
+        flags = np.zeros(ne, np.int32)
+        check(Lb.drf_amr_estimate(model.h, dptr(hchar), p.refine_threshold, p.coarsen_threshold,
+                                  p.smoothness_factor, dptr(val), _iptr(mask), _iptr(flags)))
+        return val, mask, flags
+
+    def refine_levels(self, levels, mask, flags):
+        """New per-column levels (lx, ly, lz as (ny, nx) arrays) from the element marks, with the
+        number of columns that changed."""
+        Lb = _sigs()
+        lx, ly, lz = (np.ascontiguousarray(a, np.int32) for a in levels)
+        ny, nx = lx.shape
+        out = [np.zeros_like(lx) for _ in range(3)]
+        ch = C.c_int()
+        mask = np.ascontiguousarray(mask, np.int32)
+        flags = np.ascontiguousarray(flags, np.int32)
+        check(Lb.drf_amr_refine_levels(nx, ny, _iptr(lx), _iptr(ly), _iptr(lz), len(mask), _iptr(mask),
+                                       _iptr(flags), self.params.max_level, self.params.min_level,
+                                       *[_iptr(a) for a in out], C.byref(ch)))
+        return tuple(out), ch.value
+
+    def transfer(self, old: DG3DIntegration, new: DG3DIntegration, old_levels, new_levels):
+        """The device state of `old` carried into `new` (transfer_solution with the projections)."""
+        Lb = _sigs()
+        ol = [np.ascontiguousarray(a, np.int32) for a in old_levels]
+        nl = [np.ascontiguousarray(a, np.int32) for a in new_levels]
+        ny, nx = ol[0].shape
+        check(Lb.drf_amr_transfer(old.h, new.h, nx, ny, *[_iptr(a) for a in ol], *[_iptr(a) for a in nl]))
+
+    def adapt(self, model: DG3DIntegration, mesh: dict, levels, L: float = 1.0):
+        """One adaptation (AdaptiveMeshRefinement::adapt, src/amr/refinement.cpp:422): returns
+        (model, mesh, levels, columns changed); the model is a new one on the new mesh holding the
+        carried-over state, or the same one when nothing changed."""
+        _, mask, flags = self.estimate(model, mesh)
+        new_levels, changed = self.refine_levels(levels, mask, flags)
+        if changed == 0:
+            return model, mesh, levels, 0
+        new_mesh = build_mesh(*new_levels, L=L)
+        new_model = DG3DIntegration(self.order, new_mesh)
+        self.transfer(model, new_model, levels, new_levels)
+        return new_model, new_mesh, new_levels, changed

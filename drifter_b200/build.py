@@ -20,14 +20,15 @@ def sources():
 
 def build(verbose: bool = False, jobs: int = 8) -> str:
     os.makedirs(BUILD, exist_ok=True)
-    deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [
+    # a source is rebuilt when it, or any header it may include, is newer than its object
+    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".hpp", ".h"))] + [
         os.path.join(HERE, "..", "include", "drifter_b200.h")]
-    newest_dep = max(os.path.getmtime(d) for d in deps)
+    newest_header = max(os.path.getmtime(d) for d in headers)
     objs, procs = [], []
     for src in sources():
         obj = os.path.join(BUILD, os.path.basename(src) + ".o")
         objs.append(obj)
-        if os.path.exists(obj) and os.path.getmtime(obj) >= newest_dep:
+        if os.path.exists(obj) and os.path.getmtime(obj) >= max(newest_header, os.path.getmtime(src)):
             continue
         cmd = [NVCC, *ARCH, *FLAGS, "-c", src, "-o", obj]
         if src.endswith(".cpp"):

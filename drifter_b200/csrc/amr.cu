@@ -18,12 +18,14 @@
 // global memory), so the result needs no atomics. The mortar kernels (mortar.cu) add the
 // non-conforming lifts in interface order; the mass inverse is fused into the output or the
 // LSRK update.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <memory>
 #include <mutex>
 #include <vector>
 
+#include "amr_layout.hpp"
 #include "common.cuh"
 
 namespace drf {
@@ -204,6 +206,179 @@ void amr_dispatch(int np, F &&f) {
     case 6: f(std::integral_constant<int, 6>{}); break;
     default: throw Error(DRF_E_UNSUPPORTED, "AMR: order must be 1..5");
     }
+}
+
+// ------------------------------------------------------------------ AMR refinement
+// GradientErrorEstimator::estimate_element and compute_directional_mask
+// (src/amr/refinement.cpp:70-160), one warp per element: the element's nodal values are staged
+// in shared memory, the range (max - min) over all of them and along every node line of each
+// axis reduced across the warp. Comparisons only, so the results are exact; value = range x
+// h (the element's characteristic length, supplied), and each block's largest value goes to
+// bmax for the normalisation.
+constexpr int AMR_EST_WARPS = 8;
+template <int NP>
+__global__ void __launch_bounds__(32 * AMR_EST_WARPS)
+    amr_estimate_kernel(int64_t n_elem, const double *__restrict__ U, const double *__restrict__ hchar, double sf,
+                        double *__restrict__ value, int *__restrict__ mask, double *__restrict__ bmax) {
+    constexpr int ND = NP * NP * NP, NL = NP * NP;
+    __shared__ double s[AMR_EST_WARPS][ND];
+    __shared__ double wv[AMR_EST_WARPS];
+    const int w = threadIdx.x / 32, lane = threadIdx.x % 32;
+    const int64_t e = (int64_t)blockIdx.x * AMR_EST_WARPS + w;
+    double v = 0.0;
+    if (e < n_elem) {
+        const double *u = U + e * ND;
+        double mx = -INFINITY, mn = INFINITY;
+        for (int q = lane; q < ND; q += 32) {
+            const double x = u[q];
+            s[w][q] = x;
+            mx = fmax(mx, x);
+            mn = fmin(mn, x);
+        }
+        __syncwarp();
+        double var[3] = {0.0, 0.0, 0.0};
+        for (int l = lane; l < NL; l += 32) {
+            const int a = l % NP, b = l / NP;
+            // node lines along x (j = a, k = b), y (i = a, k = b) and z (i = a, j = b)
+            const int base[3] = {NP * (a + NP * b), a + NL * b, a + NP * b};
+            const int step[3] = {1, NP, NL};
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                double lo = s[w][base[d]], hi = lo;
+#pragma unroll
+                for (int m = 1; m < NP; ++m) {
+                    const double x = s[w][base[d] + step[d] * m];
+                    lo = fmin(lo, x);
+                    hi = fmax(hi, x);
+                }
+                var[d] = fmax(var[d], hi - lo);
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+            mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+#pragma unroll
+            for (int d = 0; d < 3; ++d) var[d] = fmax(var[d], __shfl_xor_sync(0xffffffffu, var[d], o));
+        }
+        v = (mx - mn) * hchar[e];
+        if (lane == 0) {
+            const double mv = fmax(fmax(var[0], var[1]), var[2]);
+            int m = 0;
+            if (mv >= 1e-14) {
+                const double thr = sf * mv;
+                for (int d = 0; d < 3; ++d)
+                    if (var[d] > thr) m |= 1 << d;
+            }
+            value[e] = v;
+            mask[e] = m;
+        }
+    }
+    if (lane == 0) wv[w] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double b = 0.0;
+        for (int k = 0; k < AMR_EST_WARPS; ++k) b = fmax(b, wv[k]);
+        bmax[blockIdx.x] = b;
+    }
+}
+// the largest block maximum (one CTA), then the normalisation and the flags (estimate, :56-67)
+__global__ void amr_max_kernel(const double *__restrict__ part, int64_t n, double *out) {
+    __shared__ double s[1024];
+    double m = 0.0;
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) m = fmax(m, part[i]);
+    s[threadIdx.x] = m;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) s[threadIdx.x] = fmax(s[threadIdx.x], s[threadIdx.x + o]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = s[0];
+}
+__global__ void amr_flags_kernel(int64_t n_elem, const double *__restrict__ vmax, double rt, double ct,
+                                 double *__restrict__ value, int *__restrict__ flags) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n_elem) return;
+    const double m = *vmax;
+    int f = 0;
+    if (m > 1e-14) {
+        const double v = value[e] / m;
+        value[e] = v;
+        f = (v > rt ? 1 : 0) | (v < ct ? 2 : 0);
+    }
+    flags[e] = f;
+}
+
+// The solution carried to new per-column levels: every new node takes, per axis, the old cell
+// on its side and its coordinate there (SolutionProjection::project_to_children on a refined
+// axis, project_from_children on a coarsened one, src/amr/refinement.cpp:217-343; k levels at a
+// time in general), and the old cell's interpolant at that point (interpolate_3d, :345: the
+// Lagrange product formula, then the sum in dof order with separate roundings).
+struct AmrTransferArgs {
+    const double *Uo;
+    double *Un;
+    const int *col_of;          // column of each new element
+    const int *lvo, *lvn;       // old / new levels [3 c + d]
+    const int64_t *offo, *offn; // old / new first element of each column
+    double xn[MAXNP];           // LGL nodes
+    int64_t n_new;
+};
+// old sub-cell and its coordinate of node coordinate x in new sub-cell s, along one axis
+__device__ __forceinline__ void amr_old_cell(int s, int ln, int lo, double x, int &so, double &xo) {
+    if (ln == lo) {
+        so = s;
+        xo = x;
+    } else if (ln > lo) {  // refined k levels: sub-cell r of old cell s >> k
+        const int k = ln - lo, r = s & ((1 << k) - 1);
+        const double cl = -1.0 + 2.0 * r / (1 << k), ch = cl + 2.0 / (1 << k);
+        so = s >> k;
+        xo = cl + 0.5 * (x + 1.0) * (ch - cl);
+    } else {  // coarsened k levels: the old cell on the node's side (0 goes to the upper one)
+        const int k = lo - ln;
+        const int ch = k == 1 ? (x >= 0 ? 1 : 0) : min((1 << k) - 1, (int)floor((x + 1.0) * (1 << (k - 1))));
+        const double cl = -1.0 + 2.0 * ch / (1 << k), chi = cl + 2.0 / (1 << k);
+        so = (s << k) + ch;
+        xo = fmin(1.0, fmax(-1.0, 2.0 * (x - cl) / (chi - cl) - 1.0));
+    }
+}
+template <int NP>
+__global__ void __launch_bounds__(256) amr_transfer_kernel(AmrTransferArgs a) {
+    constexpr int ND = NP * NP * NP, NL = NP * NP;
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= a.n_new * ND) return;
+    const int64_t e = g / ND;
+    const int n = (int)(g % ND);
+    const int m3[3] = {n % NP, (n / NP) % NP, n / NL};
+    const int c = a.col_of[e];
+    const int *ln = a.lvn + 3 * c, *lo = a.lvo + 3 * c;
+    const int64_t loc = e - a.offn[c];
+    const int nxn = 1 << ln[0], nyn = 1 << ln[1];
+    const int s3[3] = {(int)(loc % nxn), (int)((loc / nxn) % nyn), (int)(loc / ((int64_t)nxn * nyn))};
+    int so[3];
+    double L[3][NP];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        double xo;
+        amr_old_cell(s3[d], ln[d], lo[d], a.xn[m3[d]], so[d], xo);
+#pragma unroll
+        for (int i = 0; i < NP; ++i) {
+            double v = 1.0;
+#pragma unroll
+            for (int j = 0; j < NP; ++j)
+                if (j != i) v = __dmul_rn(v, __ddiv_rn(xo - a.xn[j], a.xn[i] - a.xn[j]));
+            L[d][i] = v;
+        }
+    }
+    const int nxo = 1 << lo[0], nyo = 1 << lo[1];
+    const int64_t eo = a.offo[c] + so[0] + (int64_t)nxo * (so[1] + (int64_t)nyo * so[2]);
+    const double *u = a.Uo + eo * ND;
+    double r = 0.0;
+    for (int k = 0; k < NP; ++k)
+        for (int j = 0; j < NP; ++j)
+#pragma unroll
+            for (int i = 0; i < NP; ++i)
+                r = __dadd_rn(r, __dmul_rn(__dmul_rn(__dmul_rn(u[i + NP * (j + NP * k)], L[0][i]), L[1][j]), L[2][k]));
+    a.Un[g] = r;
 }
 
 }  // namespace
@@ -527,6 +702,92 @@ int drf_amr_time_rhs(drf_amr *h, int mode, int flux_kind, const double *a, int n
         const double npf = (double)h->np * h->np;
         const double faces = (mode == 1 ? 2.0 * h->n_conf : 0.0) + 3.0 * h->n_if;
         if (alg_bytes) *alg_bytes = 16.0 * h->n_elem * h->nd + 8.0 * faces * npf + 16.0 * 3.0 * h->n_if * npf;
+    });
+}
+
+// GradientErrorEstimator::estimate (src/amr/refinement.cpp:44-68) of the resident state.
+int drf_amr_estimate(drf_amr *h, const double *hchar, double refine_threshold, double coarsen_threshold,
+                     double smoothness_factor, double *value, int32_t *mask, int32_t *flags) {
+    return guard([&] {
+        amr_check(h);
+        DRF_CHECK(hchar && value && mask && flags, DRF_E_INVALID, "null argument");
+        const int64_t ne = h->n_elem;
+        if (ne == 0) return;
+        DRF_CHECK(all_finite(hchar, (size_t)ne), DRF_E_NONFINITE, "non-finite element length");
+        const int64_t nb = (ne + AMR_EST_WARPS - 1) / AMR_EST_WARPS;
+        DevBuf<double> dh(ne), dv(ne), part(nb + 1);
+        DevBuf<int> dm(ne), df(ne);
+        DRF_CUDA(cudaMemcpyAsync(dh.p, hchar, ne * 8, cudaMemcpyHostToDevice, h->stream));
+        amr_dispatch(h->np, [&](auto npc) {
+            constexpr int NP = decltype(npc)::value;
+            amr_estimate_kernel<NP><<<(unsigned)nb, 32 * AMR_EST_WARPS, 0, h->stream>>>(
+                ne, h->U.p, dh.p, smoothness_factor, dv.p, dm.p, part.p);
+        });
+        DRF_LAUNCHED();
+        amr_max_kernel<<<1, 1024, 0, h->stream>>>(part.p, nb, part.p + nb);
+        DRF_LAUNCHED();
+        amr_flags_kernel<<<(unsigned)((ne + 255) / 256), 256, 0, h->stream>>>(ne, part.p + nb, refine_threshold,
+                                                                               coarsen_threshold, dv.p, df.p);
+        DRF_LAUNCHED();
+        DRF_CUDA(cudaMemcpyAsync(value, dv.p, ne * 8, cudaMemcpyDeviceToHost, h->stream));
+        DRF_CUDA(cudaMemcpyAsync(mask, dm.p, ne * 4, cudaMemcpyDeviceToHost, h->stream));
+        DRF_CUDA(cudaMemcpyAsync(flags, df.p, ne * 4, cudaMemcpyDeviceToHost, h->stream));
+        DRF_CUDA(cudaStreamSynchronize(h->stream));
+    });
+}
+
+// The resident state of `from` (levels old_*) carried into `to` (levels new_*), both of one
+// order over the same nx x ny base columns.
+int drf_amr_transfer(drf_amr *from, drf_amr *to, int nx, int ny, const int *old_lx, const int *old_ly,
+                     const int *old_lz, const int *new_lx, const int *new_ly, const int *new_lz) {
+    return guard([&] {
+        amr_check(from);
+        amr_check(to);
+        DRF_CHECK(from != to, DRF_E_INVALID, "transfer needs two meshes");
+        DRF_CHECK(nx >= 1 && ny >= 1 && old_lx && old_ly && old_lz && new_lx && new_ly && new_lz, DRF_E_INVALID,
+                  "bad arguments");
+        DRF_CHECK(from->order == to->order, DRF_E_INVALID, "meshes of different orders");
+        const int ncol = nx * ny;
+        std::vector<int> lvo(3 * ncol), lvn(3 * ncol);
+        for (int c = 0; c < ncol; ++c) {
+            const int o[3] = {old_lx[c], old_ly[c], old_lz[c]}, n[3] = {new_lx[c], new_ly[c], new_lz[c]};
+            for (int d = 0; d < 3; ++d) {
+                DRF_CHECK(o[d] >= 0 && o[d] <= 10 && n[d] >= 0 && n[d] <= 10, DRF_E_INVALID,
+                          "refinement level out of range (0..10)");
+                lvo[3 * c + d] = o[d];
+                lvn[3 * c + d] = n[d];
+            }
+        }
+        const std::vector<int64_t> offo = amr_column_offsets(ncol, lvo.data()), offn = amr_column_offsets(ncol, lvn.data());
+        DRF_CHECK(offo[ncol] == from->n_elem && offn[ncol] == to->n_elem, DRF_E_INVALID,
+                  "element counts do not match the levels");
+        const int64_t nn = to->n_elem;
+        std::vector<int> col(nn);
+        for (int c = 0; c < ncol; ++c) {
+            const int64_t cells = (int64_t)1 << (lvn[3 * c] + lvn[3 * c + 1] + lvn[3 * c + 2]);
+            for (int64_t e = offn[c]; e < offn[c] + cells; ++e) col[e] = c;
+        }
+        const HostBasis b = make_lgl_basis(from->order);
+        DevBuf<int> dcol(nn), dlvo(3 * ncol), dlvn(3 * ncol);
+        DevBuf<int64_t> doffo(ncol + 1), doffn(ncol + 1);
+        DRF_CUDA(cudaStreamSynchronize(from->stream));
+        cudaStream_t st = to->stream;
+        DRF_CUDA(cudaMemcpyAsync(dcol.p, col.data(), nn * 4, cudaMemcpyHostToDevice, st));
+        DRF_CUDA(cudaMemcpyAsync(dlvo.p, lvo.data(), lvo.size() * 4, cudaMemcpyHostToDevice, st));
+        DRF_CUDA(cudaMemcpyAsync(dlvn.p, lvn.data(), lvn.size() * 4, cudaMemcpyHostToDevice, st));
+        DRF_CUDA(cudaMemcpyAsync(doffo.p, offo.data(), offo.size() * 8, cudaMemcpyHostToDevice, st));
+        DRF_CUDA(cudaMemcpyAsync(doffn.p, offn.data(), offn.size() * 8, cudaMemcpyHostToDevice, st));
+        AmrTransferArgs A{};
+        A.Uo = from->U.p; A.Un = to->U.p; A.col_of = dcol.p; A.lvo = dlvo.p; A.lvn = dlvn.p;
+        A.offo = doffo.p; A.offn = doffn.p; A.n_new = nn;
+        for (int i = 0; i < b.np; ++i) A.xn[i] = b.x[i];
+        const int64_t nthr = nn * from->nd;
+        amr_dispatch(from->np, [&](auto npc) {
+            constexpr int NP = decltype(npc)::value;
+            amr_transfer_kernel<NP><<<(unsigned)((nthr + 255) / 256), 256, 0, st>>>(A);
+        });
+        DRF_LAUNCHED();
+        DRF_CUDA(cudaStreamSynchronize(st));
     });
 }
 

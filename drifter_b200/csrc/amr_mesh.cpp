@@ -15,12 +15,15 @@
 //    sub-face order of MortarSpace::compute_subface_bounds, src/dg/mortar.cpp:27), grouped by
 //    type (stable).
 // Face f has its normal along axis f / 2, positive when f is odd.
+// The refinement of these meshes (new levels per column from the error indicators, with the
+// same 2:1 balance) is drf_amr_refine_levels, below the builder.
 #include <algorithm>
 #include <array>
 #include <cstdint>
 #include <numeric>
 #include <vector>
 
+#include "amr_layout.hpp"
 #include "common.cuh"
 
 namespace {
@@ -63,19 +66,10 @@ struct Mesh {
             for (int d = 0; d < 3; ++d)
                 DRF_CHECK(lv[c][d] >= 0 && lv[c][d] <= 10, DRF_E_INVALID, "refinement level out of range (0..10)");
         }
-        std::vector<int> order(ncol);
-        std::iota(order.begin(), order.end(), 0);
-        std::sort(order.begin(), order.end(), [&](int a, int b) {
-            if (lv[a] != lv[b]) return lv[a] < lv[b];
-            return a < b;
-        });
-        off.assign(ncol, 0);
-        int64_t acc = 0;
-        for (int c : order) {
-            off[c] = acc;
-            acc += (int64_t)1 << (lv[c][0] + lv[c][1] + lv[c][2]);
-        }
-        n_elem = acc;
+        static_assert(sizeof(std::array<int, 3>) == 3 * sizeof(int), "levels must be packed");
+        off = drf::amr_column_offsets(ncol, reinterpret_cast<const int *>(lv.data()));
+        n_elem = off[ncol];
+        off.resize(ncol);
         elevel.assign(n_elem, {0, 0, 0});
         ebox.assign(n_elem, {0, 0, 0, 0, 0, 0});
         const double dxb = L / nx;
@@ -186,6 +180,92 @@ int drf_amr_build_mesh(int nx, int ny, const int *lx, const int *ly, const int *
                 if (if_fine_face) if_fine_face[4 * i + k] = r.ff[k];
             }
         }
+    });
+}
+
+// AdaptiveMeshRefinement::mark_elements / refine / coarsen (src/amr/refinement.cpp:488-530) and
+// OctreeAdapter::balance (src/mesh/octree_adapter.cpp:138) on column-wise levels. An element is
+// marked Refine when its refine flag is set and every level of its column is below max_level
+// (can_refine, :597), with its suggested mask or XYZ when that is NONE; Coarsen when its
+// coarsen flag is set and some level is above min_level (can_coarsen, :602). Elements share
+// their column's levels, so a column is refined along the union of its Refine masks; else,
+// when any of its elements is marked Coarsen, its last refinement is undone along every axis
+// above min_level (the reference merges all siblings of a marked child). Then the balance
+// the builder needs is restored by raising the coarser side, as balance() refines the coarser
+// neighbour: across every face between columns the tangential and vertical levels differ by at
+// most one, and one side is at least as fine as the other along both (a face split in one
+// axis from one side and in the other from the other side has no sub-face order).
+int drf_amr_refine_levels(int nx, int ny, const int *lx, const int *ly, const int *lz, int64_t n_elem,
+                          const int32_t *mask, const int32_t *flags, int max_level, int min_level, int *new_lx,
+                          int *new_ly, int *new_lz, int *changed) {
+    return drf::guard([&] {
+        DRF_CHECK(nx >= 1 && ny >= 1 && lx && ly && lz && mask && flags && new_lx && new_ly && new_lz && changed,
+                  DRF_E_INVALID, "bad arguments");
+        DRF_CHECK(min_level >= 0 && max_level >= min_level && max_level <= 10, DRF_E_INVALID,
+                  "levels must satisfy 0 <= min_level <= max_level <= 10");
+        const int ncol = nx * ny;
+        std::vector<int> lv(3 * ncol);
+        for (int c = 0; c < ncol; ++c) {
+            lv[3 * c] = lx[c];
+            lv[3 * c + 1] = ly[c];
+            lv[3 * c + 2] = lz[c];
+            for (int d = 0; d < 3; ++d)
+                DRF_CHECK(lv[3 * c + d] >= 0 && lv[3 * c + d] <= 10, DRF_E_INVALID,
+                          "refinement level out of range (0..10)");
+        }
+        const std::vector<int64_t> off = drf::amr_column_offsets(ncol, lv.data());
+        DRF_CHECK(off[ncol] == n_elem, DRF_E_INVALID, "element count does not match the levels");
+        std::vector<int> nl(lv);
+        for (int c = 0; c < ncol; ++c) {
+            const int *l = &lv[3 * c];
+            const bool can_refine = l[0] < max_level && l[1] < max_level && l[2] < max_level;
+            const bool can_coarsen = l[0] > min_level || l[1] > min_level || l[2] > min_level;
+            int rmask = 0;
+            bool coarsen = false;
+            for (int64_t e = off[c]; e < off[c] + ((int64_t)1 << (l[0] + l[1] + l[2])); ++e) {
+                if ((flags[e] & 1) && can_refine) rmask |= mask[e] != 0 ? mask[e] : 7;
+                else if ((flags[e] & 2) && can_coarsen) coarsen = true;
+            }
+            for (int d = 0; d < 3; ++d) {
+                if (rmask) nl[3 * c + d] = l[d] + ((rmask >> d) & 1);
+                else if (coarsen && l[d] > min_level) nl[3 * c + d] = l[d] - 1;
+            }
+        }
+        // 2:1 balance across the faces between columns (raise the coarser side until stable)
+        for (bool moved = true; moved;) {
+            moved = false;
+            for (int c = 0; c < ncol; ++c) {
+                const int ix = c % nx, iy = c / nx;
+                const int nb[4] = {ix > 0 ? c - 1 : -1, ix + 1 < nx ? c + 1 : -1, iy > 0 ? c - nx : -1,
+                                   iy + 1 < ny ? c + nx : -1};
+                for (int s = 0; s < 4; ++s) {
+                    if (nb[s] < 0) continue;
+                    const int t1 = s < 2 ? 1 : 0;  // the face's horizontal tangent
+                    const int ax[2] = {t1, 2};
+                    int dif[2];
+                    for (int q = 0; q < 2; ++q) dif[q] = nl[3 * nb[s] + ax[q]] - nl[3 * c + ax[q]];
+                    // one side finer along one face axis and coarser along the other has no
+                    // sub-face split: the column that is coarser along an axis takes the level
+                    const bool crossed = (dif[0] > 0 && dif[1] < 0) || (dif[0] < 0 && dif[1] > 0);
+                    for (int q = 0; q < 2; ++q) {
+                        const int want = dif[q] > 1 ? nl[3 * nb[s] + ax[q]] - 1
+                                                    : (crossed && dif[q] > 0 ? nl[3 * nb[s] + ax[q]] : -1);
+                        if (want > nl[3 * c + ax[q]]) {
+                            nl[3 * c + ax[q]] = want;
+                            moved = true;
+                        }
+                    }
+                }
+            }
+        }
+        int nch = 0;
+        for (int c = 0; c < ncol; ++c) {
+            new_lx[c] = nl[3 * c];
+            new_ly[c] = nl[3 * c + 1];
+            new_lz[c] = nl[3 * c + 2];
+            nch += (nl[3 * c] != lv[3 * c]) || (nl[3 * c + 1] != lv[3 * c + 1]) || (nl[3 * c + 2] != lv[3 * c + 2]);
+        }
+        *changed = nch;
     });
 }
 

@@ -436,6 +436,40 @@ int drf_amr_step(drf_amr *h, int mode, int flux_kind, const double *a, double dt
 int drf_amr_time_rhs(drf_amr *h, int mode, int flux_kind, const double *a, int nrep, double *ms,
                      double *alg_bytes);
 
+/* ------------------------------------------------------------------ AMR refinement
+ * AdaptiveMeshRefinement::adapt (src/amr/refinement.cpp:422) on the column-wise refined meshes
+ * above: estimate on the device, new levels on the host, the face tables rebuilt by
+ * drf_amr_build_mesh, the state carried over on the device.
+ *
+ * GradientErrorEstimator::estimate (:44-68) with estimate_element (:70) and
+ * compute_directional_mask (:95) of the handle's device state: value = (max - min of the
+ * element's nodal values) x hchar (its characteristic length, cbrt of its volume, given per
+ * element), normalised by the largest value when that exceeds 1e-14; flags bit 0 refine
+ * (value > refine_threshold, default 0.1), bit 1 coarsen (value < coarsen_threshold, 0.01),
+ * both 0 when not normalised; mask the RefineMask bits (X 1, Y 2, Z 4,
+ * include/mesh/refine_mask.hpp:13) of the axes whose largest range along a node line exceeds
+ * smoothness_factor (0.5) x the largest of the three, 0 below 1e-14. Host outputs. */
+int drf_amr_estimate(drf_amr *h, const double *hchar, double refine_threshold, double coarsen_threshold,
+                     double smoothness_factor, double *value, int32_t *mask, int32_t *flags);
+/* mark_elements (:488) with can_refine / can_coarsen (:597-605), refine / coarsen, and the 2:1
+ * balance of OctreeAdapter::balance (src/mesh/octree_adapter.cpp:138), per base column: a column
+ * is refined along the union of its elements' Refine masks (XYZ for a Refine element without
+ * one), else one level down along every axis above min_level when any element is marked
+ * Coarsen; then neighbouring columns are raised until, across every face between columns, their
+ * tangential and vertical levels differ by at most one and one side is at least as fine along
+ * both (the meshes drf_amr_build_mesh accepts). Host-only. changed: the number of columns whose
+ * levels changed. */
+int drf_amr_refine_levels(int nx, int ny, const int *lx, const int *ly, const int *lz, int64_t n_elem,
+                          const int32_t *mask, const int32_t *flags, int max_level, int min_level, int *new_lx,
+                          int *new_ly, int *new_lz, int *changed);
+/* transfer_solution (:532) and SolutionProjection (:217-343): the device state of `from`
+ * (levels old_*) carried into `to` (levels new_*, each axis at most one level from the old):
+ * per axis a node takes the old cell on its side, the parent's interpolant on a refined axis
+ * (project_to_children) and the child on the node's side of 0 on a coarsened one
+ * (project_from_children), evaluated by interpolate_3d (:345). Both handles of one order. */
+int drf_amr_transfer(drf_amr *from, drf_amr *to, int nx, int ny, const int *old_lx, const int *old_ly,
+                     const int *old_lz, const int *new_lx, const int *new_ly, const int *new_lz);
+
 #ifdef __cplusplus
 }
 #endif

@@ -417,6 +417,65 @@ def amr_lsrk(order, mesh, mode, flux_kind, a, U, dt, nsteps):
     return u
 
 
+# ----------------------------------------------------------------------------- AMR refinement
+def amr_estimate(order, U, hchar, refine_threshold=0.1, coarsen_threshold=0.01, smoothness_factor=0.5):
+    """GradientErrorEstimator::estimate with compute_directional_mask (src/amr/refinement.cpp:44-160):
+    per element the normalised value, the RefineMask bits and the flags (1 refine, 2 coarsen)."""
+    L = lib()
+    vp = C.c_void_p
+    L.orc_amr_estimate.argtypes = [C.c_int, C.c_long, _dp, _dp, C.c_double, C.c_double, C.c_double, _dp,
+                                   vp, vp]
+    U = _c(U)
+    ne = U.shape[0]
+    val = np.zeros(ne)
+    mask = np.zeros(ne, np.int32)
+    flags = np.zeros(ne, np.int32)
+    ptr = lambda x: x.ctypes.data_as(C.c_void_p)
+    if L.orc_amr_estimate(order, ne, _p(U), _p(_c(hchar)), refine_threshold, coarsen_threshold,
+                          smoothness_factor, _p(val), ptr(mask), ptr(flags)) < 0:
+        raise ValueError("oracle: bad estimate arguments")
+    return val, mask, flags
+
+
+def amr_project_children(order, U_parent, mask):
+    """SolutionProjection::project_to_children (src/amr/refinement.cpp:217)."""
+    L = lib()
+    L.orc_amr_project_children.argtypes = [C.c_int, _dp, C.c_int, _dp]
+    nch = (2 if mask & 1 else 1) * (2 if mask & 2 else 1) * (2 if mask & 4 else 1)
+    nd = (order + 1) ** 3
+    out = np.zeros((nch, nd))
+    if L.orc_amr_project_children(order, _p(_c(U_parent)), mask, _p(out)) < 0:
+        raise ValueError("oracle: bad projection arguments")
+    return out
+
+
+def amr_project_parent(order, U_children, mask):
+    """SolutionProjection::project_from_children (src/amr/refinement.cpp:278)."""
+    L = lib()
+    L.orc_amr_project_parent.argtypes = [C.c_int, _dp, C.c_int, _dp]
+    out = np.zeros((order + 1) ** 3)
+    if L.orc_amr_project_parent(order, _p(_c(U_children)), mask, _p(out)) < 0:
+        raise ValueError("oracle: bad projection arguments")
+    return out
+
+
+def amr_transfer(order, old_levels, new_levels, U_old):
+    """The column-wise remap of a solution between per-column levels ((ncol, 3) arrays over an
+    nx x ny grid given as (ny, nx, 3)), each new node taking the old cell's value at its position."""
+    L = lib()
+    vp = C.c_void_p
+    L.orc_amr_transfer.argtypes = [C.c_int, C.c_int, C.c_int, vp, vp, _dp, _dp]
+    ol = np.ascontiguousarray(old_levels, np.int32)
+    nl = np.ascontiguousarray(new_levels, np.int32)
+    ny, nx = ol.shape[:2]
+    ne = int(sum(1 << int(v) for v in nl.reshape(-1, 3).sum(1)))
+    out = np.zeros((ne, (order + 1) ** 3))
+    ptr = lambda x: x.ctypes.data_as(C.c_void_p)
+    if L.orc_amr_transfer(order, nx, ny, ptr(ol), ptr(nl), _p(_c(U_old)), _p(out)) < 0:
+        raise ValueError("oracle: bad transfer arguments")
+    return out
+
+
 def bz_element_errors(nx, ny, Lx, Ly, ngauss, x, zdata, x0=0.0, y0=0.0):
     """Per-element L2 misfit and normalized error of the adaptive smoother's estimate
     (AdaptiveCGCubicBezierSmoother::compute_element_l2_error)."""
