@@ -81,6 +81,7 @@ _SIGS = {
     "drf_dg_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64),
                               C.POINTER(C.c_int)]),
     "drf_dg_tuning": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), _dp]),
+    "drf_dg_stage_tuning": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), _dp]),
     "drf_dg_time_copy": (C.c_int, [C.c_void_p, C.c_int, _dp, _dp]),
     "drf_ens_create": (C.c_int, [C.c_int, C.POINTER(MeshDesc), C.POINTER(DGParams),
                                  C.POINTER(_dp), C.POINTER(_dp), C.POINTER(_dp), C.POINTER(_dp),

@@ -1868,10 +1868,11 @@ struct drf_dg {
     double baro_ms[4] = {0.0, 0.0, 0.0, 0.0};
     int graph_nsub = 0;
     size_t smem = 0;
-    // L2 prefetch distance of the stage launch in columns (resident stage CTAs on the device),
-    // 0 for none; DRIFTER_B200_STAGE_PREFETCH=<waves> in the environment sets it in waves of
-    // resident CTAs (0 switches it off; default 1)
-    int stage_pf = 0;
+    // L2 prefetch distance of the stage launch in columns, 0 for none: stage_waves waves of
+    // stage_pf_unit resident stage CTAs. Tuned at the first step (0, 1 or 2 waves, each timed:
+    // stage_ms) unless DRIFTER_B200_STAGE_PREFETCH=<waves> fixes it (DRIFTER_B200_TUNE=0: 1)
+    int stage_pf = 0, stage_pf_unit = 0, stage_waves = -1;
+    double stage_ms[3] = {0.0, 0.0, 0.0};
     // asynchronous output staging: FP64 snapshot buffers (4 3D fields, 4 2D fields and the
     // time), a copy stream and its events; allocated at the first drf_dg_output_stage
     DevBuf<double> out3, out2;
@@ -1907,6 +1908,7 @@ struct drf_dg {
     void setup(const drf_mesh_desc *mesh, const drf_dg_params *params, const double *h_,
                const double *f_, const double *taux_, const double *tauy_);
     void tune_baro();
+    void tune_stage();
 
     void drop_graphs() {
         for (auto &g : graph)
@@ -2248,9 +2250,11 @@ void drf_dg::setup(const drf_mesh_desc *mesh, const drf_dg_params *params, const
             int per_sm = 0, nsm = 0;
             DRF_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
             DRF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, stage_threads(), smem));
+            stage_pf_unit = per_sm * nsm;
             const char *pe = std::getenv("DRIFTER_B200_STAGE_PREFETCH");
-            const int waves = pe ? std::atoi(pe) : 1;
-            stage_pf = std::max(waves, 0) * per_sm * nsm;
+            const char *tn = std::getenv("DRIFTER_B200_TUNE");
+            stage_waves = pe ? std::max(std::atoi(pe), 0) : ((tn && tn[0] == '0') ? 1 : -1);
+            stage_pf = (stage_waves < 0 ? 1 : stage_waves) * stage_pf_unit;
         });
     });
 }
@@ -2320,6 +2324,63 @@ void drf_dg::tune_baro() {
     baro_cpb = best;
     std::lock_guard<std::mutex> lk(mu);
     cache[key] = {best, {baro_ms[0], baro_ms[1], baro_ms[2], baro_ms[3]}};
+}
+
+// Stage-launch tuner: the L2 prefetch distance (0, 1 or 2 waves of resident CTAs), each timed
+// on a non-first LSRK stage written into the spare buffers (two warm-up launches, then five
+// between CUDA events; the model state is not modified), the fastest kept. Cached per
+// (device, order, layers, columns, precision, equation of state).
+void drf_dg::tune_stage() {
+    if (stage_waves >= 0) return;
+    static std::mutex mu;
+    static std::map<std::tuple<int, int, int, int, int, int>, std::pair<int, std::array<double, 3>>> cache;
+    int dev = 0;
+    DRF_CUDA(cudaGetDevice(&dev));
+    const auto key = std::make_tuple(dev, np, G.nz, ncol, (int)tsz, G.eos);
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = cache.find(key);
+        if (it != cache.end()) {
+            stage_waves = it->second.first;
+            for (int i = 0; i < 3; ++i) stage_ms[i] = it->second.second[i];
+            stage_pf = stage_waves * stage_pf_unit;
+            return;
+        }
+    }
+    cudaEvent_t e0, e1;
+    DRF_CUDA(cudaEventCreate(&e0));
+    DRF_CUDA(cudaEventCreate(&e1));
+    int best = 1;
+    double best_ms = 1e300;
+    with_types([&](auto tv, auto npc) {
+        using T = decltype(tv);
+        constexpr int NP = decltype(npc)::value;
+        for (int w = 0; w < 3; ++w) {
+            stage_pf = w * stage_pf_unit;
+            auto launch = [&] {
+                launch_stage<T, NP>(cur, 1 - cur, 1, 1e-6, 0, nullptr, nullptr, nullptr, eta, 0.0);
+            };
+            launch();
+            launch();
+            DRF_CUDA(cudaEventRecord(e0, stream));
+            for (int r = 0; r < 5; ++r) launch();
+            DRF_CUDA(cudaEventRecord(e1, stream));
+            DRF_CUDA(cudaEventSynchronize(e1));
+            float t = 0.f;
+            DRF_CUDA(cudaEventElapsedTime(&t, e0, e1));
+            stage_ms[w] = t / 5.0;
+            if (stage_ms[w] < best_ms) {
+                best_ms = stage_ms[w];
+                best = w;
+            }
+        }
+    });
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    stage_waves = best;
+    stage_pf = best * stage_pf_unit;
+    std::lock_guard<std::mutex> lk(mu);
+    cache[key] = {best, {stage_ms[0], stage_ms[1], stage_ms[2]}};
 }
 
 extern "C" {
@@ -2553,6 +2614,7 @@ int drf_dg_step_modesplit(drf_dg *m, double dt, int nsub, int nsteps) {
         DRF_CHECK(dt > 0.0 && std::isfinite(dt), DRF_E_INVALID, "dt must be positive");
         DRF_CHECK(nsteps >= 0, DRF_E_INVALID, "nsteps must be >= 0");
         m->tune_baro();  // first step only: outside any capture
+        m->tune_stage();
         if (m->graph_nsub != nsub || m->graph_dt != dt) {
             m->drop_graphs();
             const char *pe = std::getenv("DRIFTER_B200_BARO_PERSISTENT");
@@ -2862,6 +2924,18 @@ int drf_dg_tuning(drf_dg *m, int *baro_cols_per_cta, double *baro_ms4) {
         if (baro_cols_per_cta) *baro_cols_per_cta = m->baro_cpb;
         if (baro_ms4)
             for (int i = 0; i < 4; ++i) baro_ms4[i] = m->baro_ms[i];
+    });
+}
+
+int drf_dg_stage_tuning(drf_dg *m, int *prefetch_waves, int *prefetch_columns, double *stage_ms3) {
+    return guard([&] {
+        check_model(m);
+        DRF_CHECK(!m->view, DRF_E_INVALID, "ensemble members use the ensemble's stage launch");
+        m->tune_stage();
+        if (prefetch_waves) *prefetch_waves = m->stage_waves;
+        if (prefetch_columns) *prefetch_columns = m->stage_pf;
+        if (stage_ms3)
+            for (int i = 0; i < 3; ++i) stage_ms3[i] = m->stage_ms[i];
     });
 }
 
