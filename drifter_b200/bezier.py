@@ -38,11 +38,45 @@ def _setup_sigs():
         "drf_bz_constrained_solve": [vp, C.c_int, C.c_int, C.c_double, C.c_int, C.c_double, dp,
                                      C.POINTER(C.c_int), dp, dp],
         "drf_bz_element_errors": [vp, dp, dp, C.c_int, dp, dp],
+        "drf_bz_mesh_element_errors": [C.c_int64, dp, dp, dp, C.c_int, dp, dp],
+        "drf_bz_mesh_data_fitting": [C.c_int64, dp, dp, dp, C.c_int, dp, dp, dp],
     }
     for k, a in sigs.items():
         getattr(L, k).argtypes = a
         getattr(L, k).restype = C.c_int
     return L
+
+
+def _c(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def mesh_element_errors(bounds, coeffs, zdata, ngauss: int = 4):
+    """AdaptiveCGCubicBezierSmoother::compute_element_l2_error / estimate_element_error
+    (src/bathymetry/adaptive_cg_cubic_bezier_smoother.cpp:100,142) for every element of a
+    quadtree mesh: bounds (n, 4) as (xmin, ymin, xmax, ymax), coeffs (n, 16) the element's
+    resolved control values, zdata (n, ngauss**2) the data at its Gauss points ([qj][qi]).
+    Returns (l2, normalized)."""
+    L = _setup_sigs()
+    b = _c(bounds).reshape(-1, 4)
+    n = len(b)
+    l2, nrm = np.empty(n), np.empty(n)
+    check(L.drf_bz_mesh_element_errors(n, dptr(b), dptr(_c(coeffs)), dptr(_c(zdata)), ngauss, dptr(l2),
+                                       dptr(nrm)))
+    return l2, nrm
+
+
+def mesh_data_fitting(bounds, zdata, ngauss: int = 4, relax=None):
+    """The element part of CGBezierSmootherBase::assemble_data_fitting_global
+    (src/bathymetry/cg_bezier_smoother_base.cpp:308) on a quadtree mesh: (BtWB (n, 16, 16),
+    BtWd (n, 16), dTWd (n,)); the scatter through the DOF map stays with the caller."""
+    L = _setup_sigs()
+    b = _c(bounds).reshape(-1, 4)
+    n = len(b)
+    K, r, dd = np.empty((n, 16, 16)), np.empty((n, 16)), np.empty(n)
+    rel = dptr(_c(relax)) if relax is not None else None
+    check(L.drf_bz_mesh_data_fitting(n, dptr(b), dptr(_c(zdata)), rel, ngauss, dptr(K), dptr(r), dptr(dd)))
+    return K, r, dd
 
 
 class BezierSmoother:

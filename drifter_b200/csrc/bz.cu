@@ -1653,6 +1653,168 @@ double dev_dot(drf_bz *h, int64_t n, const double *a, const double *b, double *s
 }  // namespace
 }  // namespace drf
 
+namespace drf {
+namespace {
+// Gauss-Legendre nodes and weights on [0, 1] (Newton on the Legendre recurrence): gq[0..n) the
+// nodes in increasing order, gq[n..2n) the weights
+std::vector<double> gauss_legendre_01_newton(int ngauss) {
+    std::vector<double> gq(2 * ngauss);
+    for (int i = 0; i < ngauss; ++i) {
+        double z = std::cos(M_PI * (i + 0.75) / (ngauss + 0.5)), dp = 1.0;
+        for (int it = 0; it < 100; ++it) {
+            double p0 = 1.0, p1 = z;
+            for (int k = 2; k <= ngauss; ++k) {
+                const double p2 = ((2.0 * k - 1.0) * z * p1 - (k - 1.0) * p0) / k;
+                p0 = p1;
+                p1 = p2;
+            }
+            if (ngauss == 1) { p1 = z; p0 = 1.0; }
+            dp = ngauss * (z * p1 - p0) / (z * z - 1.0);
+            const double dz = p1 / dp;
+            z -= dz;
+            if (std::abs(dz) < 1e-16) break;
+        }
+        gq[ngauss - 1 - i] = 0.5 * (z + 1.0);
+        gq[ngauss + ngauss - 1 - i] = 1.0 / ((1.0 - z * z) * dp * dp);
+    }
+    return gq;
+}
+
+// The data-fitting rule of CGBezierSmootherBase::gauss_legendre_01
+// (src/bathymetry/cg_bezier_smoother_base.cpp:28-58): the closed forms of the 1- to 4-point
+// Gauss-Legendre rules on [0, 1] (the reference gives the 4-point rule for every n >= 4).
+void gauss_legendre_01_closed(int n, double pts[4], double wts[4]) {
+    if (n == 1) {
+        pts[0] = 0.5;
+        wts[0] = 1.0;
+    } else if (n == 2) {
+        pts[0] = 0.5 - 0.5 / std::sqrt(3.0);
+        pts[1] = 0.5 + 0.5 / std::sqrt(3.0);
+        wts[0] = wts[1] = 0.5;
+    } else if (n == 3) {
+        pts[0] = 0.5 - 0.5 * std::sqrt(0.6);
+        pts[1] = 0.5;
+        pts[2] = 0.5 + 0.5 * std::sqrt(0.6);
+        wts[0] = wts[2] = 5.0 / 18.0;
+        wts[1] = 8.0 / 18.0;
+    } else {
+        const double a = std::sqrt(3.0 / 7.0 - 2.0 / 7.0 * std::sqrt(6.0 / 5.0));
+        const double b = std::sqrt(3.0 / 7.0 + 2.0 / 7.0 * std::sqrt(6.0 / 5.0));
+        pts[0] = 0.5 * (1.0 - b);
+        pts[1] = 0.5 * (1.0 - a);
+        pts[2] = 0.5 * (1.0 + a);
+        pts[3] = 0.5 * (1.0 + b);
+        const double wa = (18.0 + std::sqrt(30.0)) / 72.0, wb = (18.0 - std::sqrt(30.0)) / 72.0;
+        wts[0] = wts[3] = 0.5 * wb;
+        wts[1] = wts[2] = 0.5 * wa;
+    }
+}
+
+// ------------------------------------------------------------ element lists of quadtree meshes
+// CubicBezierBasis2D::evaluate_bernstein_1d's recurrence (src/bathymetry/cubic_bezier_basis_2d.cpp:42),
+// each product and sum rounded on its own (no fused multiply-add)
+__device__ __forceinline__ void bern3_rn(double t, double B[4]) {
+    const double s = __dadd_rn(1.0, -t);
+    double p[4] = {1.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int deg = 1; deg <= 3; ++deg) {
+        double c[4];
+        c[0] = __dmul_rn(s, p[0]);
+#pragma unroll
+        for (int i = 1; i < deg; ++i) c[i] = __dadd_rn(__dmul_rn(t, p[i - 1]), __dmul_rn(s, p[i]));
+        c[deg] = __dmul_rn(t, p[deg - 1]);
+#pragma unroll
+        for (int i = 0; i <= deg; ++i) p[i] = c[i];
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) B[i] = p[i];
+}
+
+// compute_element_l2_error on an element list: one thread per element, the points in the
+// reference's order (v outer, u inner), each mapped to physical coordinates and back as
+// evaluate(x, y) does, the sums rounded term by term
+__global__ void __launch_bounds__(256) bz_mesh_error_kernel(int64_t n, int ng, const double *__restrict__ bounds,
+                                                            const double *__restrict__ coeffs,
+                                                            const double *__restrict__ zd,
+                                                            const double *__restrict__ gq, double *__restrict__ l2,
+                                                            double *__restrict__ nrm) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    const double x0 = bounds[4 * e], y0 = bounds[4 * e + 1];
+    const double dx = bounds[4 * e + 2] - x0, dy = bounds[4 * e + 3] - y0;
+    double c[16];
+#pragma unroll
+    for (int a = 0; a < 16; ++a) c[a] = coeffs[16 * e + a];
+    double err2 = 0.0;
+    for (int j = 0; j < ng; ++j)
+        for (int i = 0; i < ng; ++i) {
+            const double px = __dadd_rn(x0, __dmul_rn(gq[i], dx)), py = __dadd_rn(y0, __dmul_rn(gq[j], dy));
+            const double u = fmin(1.0, fmax(0.0, __ddiv_rn(px - x0, dx)));
+            const double v = fmin(1.0, fmax(0.0, __ddiv_rn(py - y0, dy)));
+            double bu[4], bv[4];
+            bern3_rn(u, bu);
+            bern3_rn(v, bv);
+            double z = 0.0;
+#pragma unroll
+            for (int b = 0; b < 4; ++b)
+#pragma unroll
+                for (int a = 0; a < 4; ++a) z = __dadd_rn(z, __dmul_rn(__dmul_rn(c[a + 4 * b], bu[a]), bv[b]));
+            const double w = __dmul_rn(gq[ng + i], gq[ng + j]);
+            const double diff = zd[(e * ng + j) * ng + i] - z;
+            err2 = __dadd_rn(err2, __dmul_rn(__dmul_rn(w, diff), diff));
+        }
+    const double err = sqrt(__dmul_rn(__dmul_rn(err2, dx), dy));
+    l2[e] = err;
+    if (nrm) nrm[e] = __ddiv_rn(err, sqrt(__dmul_rn(dx, dy)));
+}
+
+// the element part of assemble_data_fitting_global on an element list: one CTA per element, the
+// 16 basis values of each quadrature point in shared memory, one thread per entry of the
+// 16 x 16 block; points in the reference's order (qi outer, qj inner), each term rounded as
+// weight * B_i * B_j
+__global__ void __launch_bounds__(256) bz_mesh_fit_kernel(int64_t n, int ng, const double *__restrict__ bounds,
+                                                          const double *__restrict__ zd,
+                                                          const double *__restrict__ relax, const double *g01,
+                                                          double *__restrict__ K, double *__restrict__ r,
+                                                          double *__restrict__ dd) {
+    __shared__ double sB[16][16], sw[16], sd[16];
+    const int64_t e = blockIdx.x;
+    const int t = threadIdx.x, nq = ng * ng;
+    const double x0 = bounds[4 * e], y0 = bounds[4 * e + 1];
+    const double jac = __dmul_rn(bounds[4 * e + 2] - x0, bounds[4 * e + 3] - y0);
+    if (t < 16 * nq) {
+        const int q = t / 16, a = t % 16, qi = q / ng, qj = q % ng;
+        double bu[4], bv[4];
+        bern3_rn(g01[qi], bu);
+        bern3_rn(g01[qj], bv);
+        sB[q][a] = __dmul_rn(bu[a % 4], bv[a / 4]);
+        if (a == 0) {
+            const int64_t idx = (e * ng + qj) * ng + qi;
+            const double rel = relax ? relax[idx] : 1.0;
+            sw[q] = __dmul_rn(__dmul_rn(__dmul_rn(g01[4 + qi], g01[4 + qj]), jac), rel);
+            sd[q] = zd[idx];
+        }
+    }
+    __syncthreads();
+    const int a = t / 16, b = t % 16;
+    double acc = 0.0;
+    for (int q = 0; q < nq; ++q) acc = __dadd_rn(acc, __dmul_rn(__dmul_rn(sw[q], sB[q][a]), sB[q][b]));
+    K[256 * e + t] = acc;
+    if (t < 16) {
+        double ra = 0.0;
+        for (int q = 0; q < nq; ++q) ra = __dadd_rn(ra, __dmul_rn(__dmul_rn(sw[q], sB[q][t]), sd[q]));
+        r[16 * e + t] = ra;
+    }
+    if (t == 0) {
+        double s = 0.0;
+        for (int q = 0; q < nq; ++q) s = __dadd_rn(s, __dmul_rn(__dmul_rn(sw[q], sd[q]), sd[q]));
+        dd[e] = s;
+    }
+}
+
+}  // namespace
+}  // namespace drf
+
 extern "C" {
 
 int drf_bz_create(const drf_bz_grid_desc *g, const double *dgauss, drf_bz **out) {
@@ -1750,26 +1912,7 @@ int drf_bz_element_errors(drf_bz *h, const double *xh, const double *zdata, int 
         const drf_bz_grid_desc &g = h->H.g;
         const int64_t ne = (int64_t)g.nx * g.ny, npt = ne * ngauss * ngauss;
         DRF_CHECK(all_finite(zdata, (size_t)npt), DRF_E_NONFINITE, "non-finite data");
-        // Gauss-Legendre nodes and weights on [0, 1] (Newton on the Legendre recurrence)
-        std::vector<double> gq(2 * ngauss);
-        for (int i = 0; i < ngauss; ++i) {
-            double z = std::cos(M_PI * (i + 0.75) / (ngauss + 0.5)), dp = 1.0;
-            for (int it = 0; it < 100; ++it) {
-                double p0 = 1.0, p1 = z;
-                for (int k = 2; k <= ngauss; ++k) {
-                    const double p2 = ((2.0 * k - 1.0) * z * p1 - (k - 1.0) * p0) / k;
-                    p0 = p1;
-                    p1 = p2;
-                }
-                if (ngauss == 1) { p1 = z; p0 = 1.0; }
-                dp = ngauss * (z * p1 - p0) / (z * z - 1.0);
-                const double dz = p1 / dp;
-                z -= dz;
-                if (std::abs(dz) < 1e-16) break;
-            }
-            gq[ngauss - 1 - i] = 0.5 * (z + 1.0);
-            gq[ngauss + ngauss - 1 - i] = 1.0 / ((1.0 - z * z) * dp * dp);
-        }
+        const std::vector<double> gq = gauss_legendre_01_newton(ngauss);
         DevBuf<double> dz((size_t)npt), dgq(gq.size()), dl2(ne), dnrm(normalized ? ne : 1);
         DRF_CUDA(cudaMemcpyAsync(h->z.p, xh, h->ndof * 8, cudaMemcpyHostToDevice, h->stream));
         DRF_CUDA(cudaMemcpyAsync(dz.p, zdata, npt * 8, cudaMemcpyHostToDevice, h->stream));
@@ -1780,6 +1923,63 @@ int drf_bz_element_errors(drf_bz *h, const double *xh, const double *zdata, int 
         DRF_CUDA(cudaMemcpyAsync(l2, dl2.p, ne * 8, cudaMemcpyDeviceToHost, h->stream));
         if (normalized) DRF_CUDA(cudaMemcpyAsync(normalized, dnrm.p, ne * 8, cudaMemcpyDeviceToHost, h->stream));
         DRF_CUDA(cudaStreamSynchronize(h->stream));
+    });
+}
+
+int drf_bz_mesh_element_errors(int64_t n_elem, const double *bounds, const double *coeffs, const double *zdata,
+                               int ngauss, double *l2, double *normalized) {
+    return guard([&] {
+        DRF_CHECK(n_elem >= 0, DRF_E_INVALID, "negative element count");
+        if (n_elem == 0) return;
+        DRF_CHECK(bounds && coeffs && zdata && l2, DRF_E_INVALID, "null argument");
+        DRF_CHECK(ngauss >= 1 && ngauss <= 16, DRF_E_INVALID, "ngauss must be 1..16");
+        const int64_t npt = n_elem * ngauss * ngauss;
+        DRF_CHECK(all_finite(bounds, (size_t)(4 * n_elem)) && all_finite(coeffs, (size_t)(16 * n_elem)) &&
+                      all_finite(zdata, (size_t)npt),
+                  DRF_E_NONFINITE, "non-finite input");
+        for (int64_t e = 0; e < n_elem; ++e)
+            DRF_CHECK(bounds[4 * e + 2] > bounds[4 * e] && bounds[4 * e + 3] > bounds[4 * e + 1], DRF_E_INVALID,
+                      "element bounds must have xmax > xmin and ymax > ymin");
+        const std::vector<double> gq = gauss_legendre_01_newton(ngauss);
+        DevBuf<double> db(4 * n_elem), dc(16 * n_elem), dz(npt), dg(gq.size()), dl(n_elem), dn(normalized ? n_elem : 1);
+        DRF_CUDA(cudaMemcpy(db.p, bounds, 32 * n_elem, cudaMemcpyHostToDevice));
+        DRF_CUDA(cudaMemcpy(dc.p, coeffs, 128 * n_elem, cudaMemcpyHostToDevice));
+        DRF_CUDA(cudaMemcpy(dz.p, zdata, 8 * npt, cudaMemcpyHostToDevice));
+        DRF_CUDA(cudaMemcpy(dg.p, gq.data(), 8 * gq.size(), cudaMemcpyHostToDevice));
+        bz_mesh_error_kernel<<<(unsigned)((n_elem + 255) / 256), 256>>>(n_elem, ngauss, db.p, dc.p, dz.p, dg.p, dl.p,
+                                                                       normalized ? dn.p : nullptr);
+        DRF_LAUNCHED();
+        DRF_CUDA(cudaMemcpy(l2, dl.p, 8 * n_elem, cudaMemcpyDeviceToHost));
+        if (normalized) DRF_CUDA(cudaMemcpy(normalized, dn.p, 8 * n_elem, cudaMemcpyDeviceToHost));
+    });
+}
+
+int drf_bz_mesh_data_fitting(int64_t n_elem, const double *bounds, const double *zdata, const double *relax,
+                             int ngauss, double *BtWB, double *BtWd, double *dTWd) {
+    return guard([&] {
+        DRF_CHECK(n_elem >= 0, DRF_E_INVALID, "negative element count");
+        if (n_elem == 0) return;
+        DRF_CHECK(bounds && zdata && BtWB && BtWd && dTWd, DRF_E_INVALID, "null argument");
+        DRF_CHECK(ngauss >= 1 && ngauss <= 4, DRF_E_INVALID,
+                  "ngauss must be 1..4 (the data-fitting rule has 4 points at most)");
+        const int64_t npt = n_elem * ngauss * ngauss;
+        DRF_CHECK(all_finite(bounds, (size_t)(4 * n_elem)) && all_finite(zdata, (size_t)npt) &&
+                      (!relax || all_finite(relax, (size_t)npt)),
+                  DRF_E_NONFINITE, "non-finite input");
+        double g01[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        gauss_legendre_01_closed(ngauss, g01, g01 + 4);
+        DevBuf<double> db(4 * n_elem), dz(npt), drl(relax ? npt : 1), dg(8), dK(256 * n_elem), dr(16 * n_elem),
+            dd(n_elem);
+        DRF_CUDA(cudaMemcpy(db.p, bounds, 32 * n_elem, cudaMemcpyHostToDevice));
+        DRF_CUDA(cudaMemcpy(dz.p, zdata, 8 * npt, cudaMemcpyHostToDevice));
+        if (relax) DRF_CUDA(cudaMemcpy(drl.p, relax, 8 * npt, cudaMemcpyHostToDevice));
+        DRF_CUDA(cudaMemcpy(dg.p, g01, sizeof(g01), cudaMemcpyHostToDevice));
+        bz_mesh_fit_kernel<<<(unsigned)n_elem, 256>>>(n_elem, ngauss, db.p, dz.p, relax ? drl.p : nullptr, dg.p, dK.p,
+                                                     dr.p, dd.p);
+        DRF_LAUNCHED();
+        DRF_CUDA(cudaMemcpy(BtWB, dK.p, 8 * 256 * n_elem, cudaMemcpyDeviceToHost));
+        DRF_CUDA(cudaMemcpy(BtWd, dr.p, 8 * 16 * n_elem, cudaMemcpyDeviceToHost));
+        DRF_CUDA(cudaMemcpy(dTWd, dd.p, 8 * n_elem, cudaMemcpyDeviceToHost));
     });
 }
 

@@ -256,6 +256,24 @@ int drf_bz_apply_Q(drf_bz *h, const double *x, double *y);
  * normalized[e] = l2[e] / sqrt(dx dy) (may be NULL). */
 int drf_bz_element_errors(drf_bz *h, const double *x, const double *zdata, int ngauss, double *l2,
                           double *normalized);
+
+/* The same estimate on any quadtree mesh of the adaptive smoother (hanging-node meshes
+ * included): n_elem elements, bounds n x (xmin, ymin, xmax, ymax), coeffs n x 16 the element's
+ * Bezier control values (i + 4 j, with hanging-node constraints already resolved), zdata
+ * n x ngauss^2 ([e][qj][qi]). The Bernstein values follow the reference's recurrence
+ * (CubicBezierBasis2D::evaluate_bernstein_1d, src/bathymetry/cubic_bezier_basis_2d.cpp:42) and
+ * every product and sum is rounded in the reference's order. Host buffers. */
+int drf_bz_mesh_element_errors(int64_t n_elem, const double *bounds, const double *coeffs, const double *zdata,
+                               int ngauss, double *l2, double *normalized);
+/* The element part of CGBezierSmootherBase::assemble_data_fitting_global
+ * (src/bathymetry/cg_bezier_smoother_base.cpp:308-364) on any quadtree mesh: per element the
+ * 16 x 16 block BtWB[e][i][j] = sum_q weight B_i B_j, BtWd[e][i] = sum_q weight B_i d and
+ * dTWd[e] = sum_q weight d d, weight = w_qi w_qj dx dy relaxation, with gauss_legendre_01
+ * (:28-58, which has 4 points at most: ngauss 1..4, a caller of the reference's ngauss_data >= 4
+ * passes 4). zdata, relax (NULL: factor 1) n x ngauss^2 ([e][qj][qi]). The scatter into the
+ * global system through the DOF map stays with the caller. Host buffers. */
+int drf_bz_mesh_data_fitting(int64_t n_elem, const double *bounds, const double *zdata, const double *relax,
+                             int ngauss, double *BtWB, double *BtWd, double *dTWd);
 /* BezierMultigridPreconditioner::setup (include/bathymetry/bezier_multigrid_preconditioner.hpp:240):
  * levels down to coarsest_n elements per direction, pre/post colored-Schwarz sweeps. */
 int drf_mg_setup(drf_bz *h, int coarsest_n, int pre, int post);

@@ -476,6 +476,33 @@ def amr_transfer(order, old_levels, new_levels, U_old):
     return out
 
 
+def bz_mesh_element_errors(bounds, coeffs, zdata, ngauss):
+    """compute_element_l2_error / estimate_element_error on a list of quadtree elements
+    (bounds n x 4, coefficients n x 16, data n x ngauss^2): (l2, normalized)."""
+    L = lib()
+    L.orc_bz_mesh_element_errors.argtypes = [C.c_long, _dp, _dp, _dp, C.c_int, _dp, _dp]
+    b = _c(bounds).reshape(-1, 4)
+    n = len(b)
+    l2, nrm = np.empty(n), np.empty(n)
+    if L.orc_bz_mesh_element_errors(n, _p(b), _p(_c(coeffs)), _p(_c(zdata)), ngauss, _p(l2), _p(nrm)) < 0:
+        raise ValueError("oracle: bad element-error arguments")
+    return l2, nrm
+
+
+def bz_mesh_data_fitting(bounds, zdata, ngauss, relax=None):
+    """The element part of assemble_data_fitting_global on a list of quadtree elements:
+    (BtWB n x 16 x 16, BtWd n x 16, dTWd n)."""
+    L = lib()
+    L.orc_bz_mesh_data_fitting.argtypes = [C.c_long, _dp, _dp, _dp, C.c_int, _dp, _dp, _dp]
+    b = _c(bounds).reshape(-1, 4)
+    n = len(b)
+    K, r, dd = np.empty((n, 16, 16)), np.empty((n, 16)), np.empty(n)
+    rel = _p(_c(relax)) if relax is not None else None
+    if L.orc_bz_mesh_data_fitting(n, _p(b), _p(_c(zdata)), rel, ngauss, _p(K), _p(r), _p(dd)) < 0:
+        raise ValueError("oracle: bad data-fitting arguments")
+    return K, r, dd
+
+
 def bz_element_errors(nx, ny, Lx, Ly, ngauss, x, zdata, x0=0.0, y0=0.0):
     """Per-element L2 misfit and normalized error of the adaptive smoother's estimate
     (AdaptiveCGCubicBezierSmoother::compute_element_l2_error)."""
