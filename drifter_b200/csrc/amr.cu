@@ -321,6 +321,9 @@ struct AmrTransferArgs {
     const int *lvo, *lvn;       // old / new levels [3 c + d]
     const int64_t *offo, *offn; // old / new first element of each column
     double xn[MAXNP];           // LGL nodes
+    // Lagrange rows of the one-level cases, [case][node][m]: 0 unchanged, 1 / 2 refined into the
+    // lower / upper half, 3 coarsened (the node's side); other level changes are formed per node
+    const double *rows;
     int64_t n_new;
 };
 // old sub-cell and its coordinate of node coordinate x in new sub-cell s, along one axis
@@ -360,13 +363,20 @@ __global__ void __launch_bounds__(256) amr_transfer_kernel(AmrTransferArgs a) {
     for (int d = 0; d < 3; ++d) {
         double xo;
         amr_old_cell(s3[d], ln[d], lo[d], a.xn[m3[d]], so[d], xo);
+        const int dl = ln[d] - lo[d];
+        if (dl >= -1 && dl <= 1) {
+            const int cs = dl == 0 ? 0 : (dl > 0 ? 1 + (s3[d] & 1) : 3);
 #pragma unroll
-        for (int i = 0; i < NP; ++i) {
-            double v = 1.0;
+            for (int i = 0; i < NP; ++i) L[d][i] = a.rows[(cs * NP + m3[d]) * NP + i];
+        } else {
 #pragma unroll
-            for (int j = 0; j < NP; ++j)
-                if (j != i) v = __dmul_rn(v, __ddiv_rn(xo - a.xn[j], a.xn[i] - a.xn[j]));
-            L[d][i] = v;
+            for (int i = 0; i < NP; ++i) {
+                double v = 1.0;
+#pragma unroll
+                for (int j = 0; j < NP; ++j)
+                    if (j != i) v = __dmul_rn(v, __ddiv_rn(xo - a.xn[j], a.xn[i] - a.xn[j]));
+                L[d][i] = v;
+            }
         }
     }
     const int nxo = 1 << lo[0], nyo = 1 << lo[1];
@@ -768,6 +778,30 @@ int drf_amr_transfer(drf_amr *from, drf_amr *to, int nx, int ny, const int *old_
             for (int64_t e = offn[c]; e < offn[c] + cells; ++e) col[e] = c;
         }
         const HostBasis b = make_lgl_basis(from->order);
+        // the one-level rows, with the kernel's own formulas for the old-cell coordinate and
+        // interpolate_3d's product formula
+        const int np = b.np;
+        std::vector<double> rows((size_t)4 * np * np);
+        for (int cs = 0; cs < 4; ++cs)
+            for (int m = 0; m < np; ++m) {
+                const double x = b.x[m];
+                double xo = x;
+                if (cs == 1 || cs == 2) {
+                    const double cl = -1.0 + 2.0 * (cs - 1) / 2, ch = cl + 2.0 / 2;
+                    xo = cl + 0.5 * (x + 1.0) * (ch - cl);
+                } else if (cs == 3) {
+                    const int c1 = x >= 0 ? 1 : 0;
+                    const double cl = -1.0 + 2.0 * c1 / 2, chi = cl + 2.0 / 2;
+                    xo = std::min(1.0, std::max(-1.0, 2.0 * (x - cl) / (chi - cl) - 1.0));
+                }
+                for (int i = 0; i < np; ++i) {
+                    double v = 1.0;
+                    for (int j = 0; j < np; ++j)
+                        if (j != i) v *= (xo - b.x[j]) / (b.x[i] - b.x[j]);
+                    rows[((size_t)cs * np + m) * np + i] = v;
+                }
+            }
+        DevBuf<double> drows(rows.size());
         DevBuf<int> dcol(nn), dlvo(3 * ncol), dlvn(3 * ncol);
         DevBuf<int64_t> doffo(ncol + 1), doffn(ncol + 1);
         DRF_CUDA(cudaStreamSynchronize(from->stream));
@@ -777,9 +811,10 @@ int drf_amr_transfer(drf_amr *from, drf_amr *to, int nx, int ny, const int *old_
         DRF_CUDA(cudaMemcpyAsync(dlvn.p, lvn.data(), lvn.size() * 4, cudaMemcpyHostToDevice, st));
         DRF_CUDA(cudaMemcpyAsync(doffo.p, offo.data(), offo.size() * 8, cudaMemcpyHostToDevice, st));
         DRF_CUDA(cudaMemcpyAsync(doffn.p, offn.data(), offn.size() * 8, cudaMemcpyHostToDevice, st));
+        DRF_CUDA(cudaMemcpyAsync(drows.p, rows.data(), rows.size() * 8, cudaMemcpyHostToDevice, st));
         AmrTransferArgs A{};
         A.Uo = from->U.p; A.Un = to->U.p; A.col_of = dcol.p; A.lvo = dlvo.p; A.lvn = dlvn.p;
-        A.offo = doffo.p; A.offn = doffn.p; A.n_new = nn;
+        A.offo = doffo.p; A.offn = doffn.p; A.rows = drows.p; A.n_new = nn;
         for (int i = 0; i < b.np; ++i) A.xn[i] = b.x[i];
         const int64_t nthr = nn * from->nd;
         amr_dispatch(from->np, [&](auto npc) {
