@@ -89,6 +89,24 @@ def test_pcg_solution_matches_oracle(precond):
     assert abs(info["iters"] - ito) <= 1
 
 
+def test_c4_full_size_operator_and_jacobi_pcg_match_oracle():
+    """C4 at full size (512 x 512 elements, 2.36 M control points, seeded fBm): the assembled
+    right-hand side and Q x to 1e-12, and the Jacobi-PCG solution at the 1e-10 residual to 1e-8
+    with the same iteration count (+-1), GPU against the FP64 oracle."""
+    c = configs.c4()
+    g = BezierSmoother(c["n"], c["n"], c["L"], c["L"], c["d"], lam=c["lam"], ridge_epsilon=c["eps"])
+    o = O.BezierOracle(c["n"], c["n"], c["L"], c["L"], c["d"], lam=c["lam"], eps=c["eps"])
+    assert rel(g.rhs(), o.vec("b")) < 1e-12
+    x = np.random.default_rng(5).uniform(-1, 1, g.ndof)
+    assert rel(g.apply_Q(x), o.csr("Q") @ x) < 1e-12
+    xs, info = g.solve("jacobi", tol=1e-10, maxit=5000)
+    xo, ito, rro = o.pcg(precond="jacobi", tol=1e-10, maxit=5000)
+    assert info["relres"] <= 1e-10 and rro <= 1e-10
+    assert abs(info["iters"] - ito) <= 1
+    assert rel(xs, xo) < 1e-8
+    g.close()
+
+
 def test_pcg_zero_rhs_and_maxit():
     g, o = pair(8)
     x, info = g.solve("jacobi", b=np.zeros(g.ndof))
