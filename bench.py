@@ -333,8 +333,8 @@ def run_baroclinic(stream, steps=10, warmup=3):
 
 
 def run_ensemble(stream, steps=5, warmup=3):
-    """C5: 64 independent N=3 runs of uneven size stepped together (one persistent stage launch
-    per LSRK stage for all members, one graph per baroclinic step), against the same members
+    """C5: 64 independent N=3 runs of uneven size stepped together (one stage launch per LSRK
+    stage over all members' columns, one graph per baroclinic step), against the same members
     stepped one model after another on the same stream. Device time with CUDA events."""
     import torch
     from drifter_b200 import configs
@@ -392,7 +392,7 @@ def run_ensemble(stream, steps=5, warmup=3):
             "sequential_ms_per_step": ms_seq, "speedup_vs_sequential": ms_seq / ms,
             "member0_max_eta": diag["max_eta"],
             # the stages' algorithmic bytes over the whole step's time (barotropic included):
-            # a lower bound of the persistent stage launch's rate
+            # a lower bound of the stage launch's rate
             "roofline": {"stage_bytes_per_step": stage_bytes,
                          "step_gbs": stage_bytes / (ms / 1e3) / 1e9,
                          "frac_of_hbm_peak": stage_bytes / (ms / 1e3) / 1e9 / measured_peaks()[0]}}

@@ -243,6 +243,15 @@ inline size_t stage_smem_bytes(int nz, int np, size_t tsz) {
 // thread applies the 1D operators to registers, with the operator entries read as
 // warp-uniform constants: x pencils (j,k,layer), y pencils (i,k,layer), z pencils (i,j,layer).
 //
+// Where a column's data live: a single model's arrays (zero offsets, clock 0), or an ensemble
+// member's slices of the pooled arrays (element offsets of its 3D and 2D arrays, its clock, its
+// bulk-copy alignment and its baroclinic step).
+struct ColView {
+    int64_t off3, off2;
+    int tidx, bulk;
+    double dt;
+};
+
 // stage_column is the work of one CTA on column c. `ph` is the phase parity the column's
 // mbarrier waits expect and `init` says whether this CTA still has to initialise the two
 // mbarriers (the first column a CTA processes). Returns false when a bounded wait gave up
@@ -250,13 +259,14 @@ inline size_t stage_smem_bytes(int nz, int np, size_t tsz) {
 // NZ > 0 compiles the column for that layer count (its sizes and shared-memory offsets become
 // constants); NZ = 0 takes the layer count from the arguments.
 template <typename T, int NP, int NZ = 0>
-__device__ __forceinline__ bool stage_column(const StageArgs<T> &a, int c, uint32_t ph, bool init) {
+__device__ __forceinline__ bool stage_column(const StageArgs<T> &a, const Geo &G, const ColView &cv, int c,
+                                             uint32_t ph, bool init) {
     constexpr int NP2 = NP * NP, NP3 = NP2 * NP, N = NP - 1;
     using B = BT<T, NP>;
-    const Geo &G = a.G;
     const int nz = NZ > 0 ? NZ : G.nz, ncn = nz * NP3, npen = nz * NP2;
     const int ex = c % G.nx, ey = c / G.nx;
-    const size_t base = (size_t)c * ncn;
+    const size_t base = (size_t)cv.off3 + (size_t)c * ncn, c2 = (size_t)cv.off2 + (size_t)c * NP2;
+    const T dtc = (T)cv.dt;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     // mbarriers: state, register of (Hu, Hv), register of (HT, HS)
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw);
@@ -292,7 +302,7 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, int c, uint3
         s_ok2 = 1;
         const bool tidal = (ex == 0 && G.bc[0] == DRF_BC_TIDE) || (ex == G.nx - 1 && G.bc[1] == DRF_BC_TIDE) ||
                            (ey == 0 && G.bc[2] == DRF_BC_TIDE) || (ey == G.ny - 1 && G.bc[3] == DRF_BC_TIDE);
-        s_etide = tidal ? (T)tide_at(G, a.tdev[0] + a.toff) : T(0);
+        s_etide = tidal ? (T)tide_at(G, a.tdev[cv.tidx] + a.toff) : T(0);
     }
     T etide = 0;  // read after the first barrier
     const T cx = (T)G.cx, cy = (T)G.cy, cs = (T)G.cs;
@@ -305,12 +315,12 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, int c, uint3
     // the column increments of the earlier stages, read while the column is being staged
     if (a.mode == 0 && !a.first)
         for (int t = threadIdx.x; t < NP2; t += blockDim.x) {
-            sOld[t] = a.dHU3[(size_t)c * NP2 + t];
-            sOld[NP2 + t] = a.dHV3[(size_t)c * NP2 + t];
+            sOld[t] = a.dHU3[c2 + t];
+            sOld[NP2 + t] = a.dHV3[c2 + t];
         }
 
     // ---- stage the column: state (and the 2N register) by TMA bulk copies when aligned
-    if (a.bulk && a.pf > 0 && threadIdx.x >= 32 && threadIdx.x < 40 && c + a.pf < G.nx * G.ny) {
+    if (cv.bulk && a.pf > 0 && threadIdx.x >= 32 && threadIdx.x < 40 && c + a.pf < G.nx * G.ny) {
         // the state and register blocks of the column a later CTA takes, into L2
         const int v = threadIdx.x - 32;
         const size_t pb = (size_t)(c + a.pf) * ncn;
@@ -318,7 +328,7 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, int c, uint3
         if (v < 4) bulk_prefetch_l2(a.qin[v] + pb, bytes);
         else if (need_res) bulk_prefetch_l2(a.res[v - 4] + pb, bytes);
     }
-    if (a.bulk) {
+    if (cv.bulk) {
         if (threadIdx.x == 0) {
             if (init) {
                 mbar_init(&bars[0], 1);
@@ -352,9 +362,9 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, int c, uint3
         }
     }
     for (int t = threadIdx.x; t < NP2; t += blockDim.x) {
-        const double *ec = a.eta + (size_t)c * NP2;
+        const double *ec = a.eta + c2;
         const double e = ec[t];
-        const double H = e + a.h[(size_t)c * NP2 + t];
+        const double H = e + a.h[c2 + t];
         sEt[t] = (T)e;
         sHt[t] = (T)H;
         sIH[t] = (T)(1.0 / H);
@@ -371,7 +381,7 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, int c, uint3
         if (G.eos) {
             // the baroclinic pressure's column: depth Hb = etab + h and g dz/dx|_sigma =
             // g d(etab)/dx + sigma g dHb/dx (element-local derivatives)
-            const double *bc = a.etab + (size_t)c * NP2, *hc = a.h + (size_t)c * NP2;
+            const double *bc = a.etab + c2, *hc = a.h + c2;
             T gex2 = 0, gey2 = 0, ghx = 0, ghy = 0;
 #pragma unroll
             for (int m = 0; m < NP; ++m) {
@@ -407,8 +417,8 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, int c, uint3
         if (s == 2 && ey > 0) { nc = c - G.nx; nj = N; }
         if (s == 3 && ey < G.ny - 1) { nc = c + G.nx; nj = 0; }
         if (nc < 0) return false;
-        const size_t nb = (size_t)nc * ncn + (size_t)ez * NP3 + ni + NP * (nj + NP * k);
-        const size_t n2 = (size_t)nc * NP2 + ni + NP * nj;
+        const size_t nb = ((size_t)cv.off3 + (size_t)nc * ncn) + (size_t)ez * NP3 + ni + NP * (nj + NP * k);
+        const size_t n2 = ((size_t)cv.off2 + (size_t)nc * NP2) + ni + NP * nj;
 #pragma unroll
         for (int v = 0; v < 4; ++v) o.q[v] = a.qin[v][nb];
         if (a.corrU) {
@@ -429,7 +439,7 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, int c, uint3
         const int bcs = s == 0 ? G.bc[0] : (s == 1 ? G.bc[1] : (s == 2 ? G.bc[2] : G.bc[3]));
         if (bcs == DRF_BC_TIDE) {
             o.e = etide;
-            o.H = etide + (T)a.h[(size_t)c * NP2 + an];
+            o.H = etide + (T)a.h[c2 + an];
             const T r = o.H * sIH[an];
 #pragma unroll
             for (int v = 0; v < 4; ++v) o.q[v] = sQ[v * ncn + n] * r;
@@ -450,7 +460,7 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, int c, uint3
         hx0 = fetch_side(0, ez, 0, j, k, fx0);
         hxN = fetch_side(1, ez, N, j, k, fxN);
     }
-    if (threadIdx.x == 0) s_ok = a.bulk ? (int)mbar_wait(&bars[0], ph) : 1;
+    if (threadIdx.x == 0) s_ok = cv.bulk ? (int)mbar_wait(&bars[0], ph) : 1;
     __syncthreads();
     if (!s_ok) {
         if (threadIdx.x == 0) atomicExch(a.err, DRF_E_TIMEOUT);
@@ -460,9 +470,9 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, int c, uint3
     if (a.corrU) {  // pending transport correction of the previous step
         for (int n = threadIdx.x; n < ncn; n += blockDim.x) {
             const int an = n % NP2;
-            sQ[n] += (T)a.corrU[(size_t)c * NP2 + an];
-            sQ[ncn + n] += (T)a.corrV[(size_t)c * NP2 + an];
-            const T dr = (T)a.corrR[(size_t)c * NP2 + an];
+            sQ[n] += (T)a.corrU[c2 + an];
+            sQ[ncn + n] += (T)a.corrV[c2 + an];
+            const T dr = (T)a.corrR[c2 + an];
             sQ[2 * ncn + n] = fma(sQ[2 * ncn + n], dr, sQ[2 * ncn + n]);
             sQ[3 * ncn + n] = fma(sQ[3 * ncn + n], dr, sQ[3 * ncn + n]);
         }
@@ -516,13 +526,13 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, int c, uint3
                 int ni, nj;
                 const int nc = face_line(sd, tt, ni, nj);
                 if (nc < 0) continue;
-                const size_t n2 = (size_t)nc * NP2 + ni + NP * nj;
+                const size_t n2 = ((size_t)cv.off2 + (size_t)nc * NP2) + ni + NP * nj;
                 const double en = a.etab[n2], Hd = en + a.h[n2];
                 const T Hn = (T)Hd, etn = (T)en, iHn = (T)(1.0 / Hd);
                 // the neighbour's pending tracer volume correction, with the arithmetic of the
                 // neighbour's own load (or of the correction applied to the state)
                 const T dr = a.corrU ? (T)a.corrR[n2] : T(0);
-                const size_t nb = (size_t)nc * ncn + (size_t)ez * NP3 + ni + NP * nj;
+                const size_t nb = ((size_t)cv.off3 + (size_t)nc * ncn) + (size_t)ez * NP3 + ni + NP * nj;
 #pragma unroll
                 for (int m = 0; m < NP; ++m) {
                     const T Tr = fma(Trz, fma(sS1[ez * NP + m] - T(1), Hn, etn), Trs);
@@ -579,7 +589,7 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, int c, uint3
                 int ni, nj;
                 const int nc = face_line(sd, tt, ni, nj);
                 if (nc < 0) continue;
-                const size_t n2 = (size_t)nc * NP2 + ni + NP * nj;
+                const size_t n2 = ((size_t)cv.off2 + (size_t)nc * NP2) + ni + NP * nj;
                 const T Hn = (T)(a.etab[n2] + a.h[n2]);
                 const T *tl = sTbn + (sd * NP + tt) * nz;
                 T Tab = 0;
@@ -725,7 +735,7 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, int c, uint3
             const int nc = sd <= 1 ? (sd == 0 ? c - 1 : c + 1) : (sd == 2 ? c - G.nx : c + G.nx);
             ni = sd == 0 ? N : (sd == 1 ? 0 : tt);
             nj = sd == 2 ? N : (sd == 3 ? 0 : tt);
-            const size_t n2 = (size_t)nc * NP2 + ni + NP * nj;
+            const size_t n2 = ((size_t)cv.off2 + (size_t)nc * NP2) + ni + NP * nj;
             return (T)(a.etab[n2] + a.h[n2]) * sPn[((sd * NP + tt) * nz + ez) * NP + k];
         }
         const T HPm = sHb[anEnd] * sP[nEnd];
@@ -780,7 +790,7 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, int c, uint3
     __syncthreads();
     // the register of (HT, HS) now that P is no longer read from its shared memory
     if (late) {
-        if (a.bulk) {
+        if (cv.bulk) {
             if (threadIdx.x == 0) {
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                 const uint32_t bytes = (uint32_t)(ncn * sizeof(T));
@@ -808,12 +818,12 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, int c, uint3
     // and bed stresses, then the LSRK update and the FP64 column increments. Each thread
     // waits for the register halves itself: (Hu, Hv) here, (HT, HS) before its first (HT, HS)
     // pair; a wait that gives up clears s_ok2, checked at the barrier after the pass.
-    if (a.bulk && need_res && !mbar_wait(&bars[1], ph)) s_ok2 = 0;
-    bool w2 = !(a.bulk && need_res);
+    if (cv.bulk && need_res && !mbar_wait(&bars[1], ph)) s_ok2 = 0;
+    bool w2 = !(cv.bulk && need_res);
     for (int p = threadIdx.x; p < npen; p += blockDim.x) {
         const int ez = p / NP2, an = p % NP2;
         const int e0 = ez * NP3 + an;
-        const T iH = sIH[an], fa = (T)a.f[(size_t)c * NP2 + an];
+        const T iH = sIH[an], fa = (T)a.f[c2 + an];
         const bool bed = ez == 0, top = ez == nz - 1;
         // the sigma velocity consistent with the discrete divergence: per layer, bottom up,
         // H omega = y solves cs D y + Ls e_0 (y_0 - M0) = I - delta (the strong-form continuity
@@ -833,10 +843,10 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, int c, uint3
         T M0 = fma((T)ez * dsg, Iq, -Pq);
         const T M1 = top ? T(0) : M0 + (dsg * Iq - sQl[ez * NP2 + an]);
         if (bed) M0 = 0;
-        if (a.mode == 1 && a.deta_out && bed) a.deta_out[(size_t)c * NP2 + an] = -(double)Iq;
+        if (a.mode == 1 && a.deta_out && bed) a.deta_out[c2 + an] = -(double)Iq;
         if (a.mode == 0 && bed) {  // the stage elevation, advanced like the 3D state
-            const size_t i2 = (size_t)c * NP2 + an;
-            const double re = (a.first ? 0.0 : (double)a.A * a.rese[i2]) - (double)a.dt * (double)Iq;
+            const size_t i2 = c2 + an;
+            const double re = (a.first ? 0.0 : (double)a.A * a.rese[i2]) - (double)dtc * (double)Iq;
             a.rese[i2] = re;
             a.etab_out[i2] = a.etab[i2] + (double)a.B * re;
         }
@@ -864,8 +874,8 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, int c, uint3
         }
         T fsx = 0, fsy = 0;
         if (top) {
-            fsx = Ls * (T)(a.taux[(size_t)c * NP2 + an] / G.rho0);
-            fsy = Ls * (T)(a.tauy[(size_t)c * NP2 + an] / G.rho0);
+            fsx = Ls * (T)(a.taux[c2 + an] / G.rho0);
+            fsy = Ls * (T)(a.tauy[c2 + an] / G.rho0);
         }
         const T w0 = om[0] * T(-1), wN = om[N];
         const int nb0 = (ez - 1) * NP3 + an + NP2 * N, nbN = (ez + 1) * NP3 + an;
@@ -933,7 +943,7 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, int c, uint3
                 } else {
                     const P2<T> r0 = a.first ? bc(T(0))
                                              : p2mul(bc(a.A), P2<T>{sRes[v0 * ncn + n], sRes[v1 * ncn + n]});
-                    const P2<T> rn = p2fma(bc(a.dt), r, r0);
+                    const P2<T> rn = p2fma(bc(dtc), r, r0);
                     res0[gi] = rn.x;
                     res1[gi] = rn.y;
                     const P2<T> qn = p2fma(bc(a.B), rn, q[k]);
@@ -948,7 +958,7 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, int c, uint3
             sL2[ez * NP2 + an] = inc.y;
         }
     }
-    if (a.bulk && need_res) {
+    if (cv.bulk && need_res) {
         __syncthreads();
         if (!s_ok2) {
             if (threadIdx.x == 0) atomicExch(a.err, DRF_E_TIMEOUT);
@@ -971,7 +981,7 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, int c, uint3
             }
             for (; ez < nz; ++ez) s0 += (double)L[ez * NP2];
             const double sum = (s0 + s1) + (s2 + s3);
-            const size_t i2 = (size_t)c * NP2 + an;
+            const size_t i2 = c2 + an;
             double *out = v == 0 ? a.dHU3 : a.dHV3;
             out[i2] = (a.first ? 0.0 : sOld[t]) + 0.5 * G.dsig * sum;
         }
@@ -982,7 +992,7 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, int c, uint3
 // One model: one CTA per water column.
 template <typename T, int NP, int NZ>
 __global__ void __launch_bounds__(STAGE_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) dg3d_stage_kernel(StageArgs<T> a) {
-    stage_column<T, NP, NZ>(a, blockIdx.x, 0u, true);
+    stage_column<T, NP, NZ>(a, a.G, ColView{0, 0, 0, a.bulk, (double)a.dt}, blockIdx.x, 0u, true);
 }
 // Layer counts the single-model stage kernel is compiled for (others run the NZ = 0 form):
 // 4 (config C1) and 16 (C2) at orders 3 and 4.
@@ -1309,54 +1319,20 @@ struct EnsMember {
     int ncol, bulk;
 };
 
-template <typename T>
-__device__ __forceinline__ void shift_stage(StageArgs<T> &a, const EnsMember &m, int idx) {
-#pragma unroll
-    for (int v = 0; v < 4; ++v) {
-        a.qin[v] += m.off3;
-        a.qout[v] += m.off3;
-        a.res[v] += m.off3;
-    }
-    a.eta += m.off2; a.h += m.off2; a.f += m.off2; a.taux += m.off2; a.tauy += m.off2;
-    if (a.corrU) { a.corrU += m.off2; a.corrV += m.off2; a.corrR += m.off2; }
-    a.dHU3 += m.off2; a.dHV3 += m.off2;
-    a.etab += m.off2;
-    if (a.etab_out) { a.etab_out += m.off2; a.rese += m.off2; }
-    a.tdev += idx;
-    a.dt = (T)m.dt;
-    a.bulk = m.bulk;
-    a.G = m.G;
-}
-
-// Persistent stage launch over all members: CTA b takes work items b, b + gridDim.x, ...;
-// an item is (member, column), ordered tallest columns first so the tail of the launch is
-// made of the cheapest columns. Shared memory is sized for the tallest member.
+// Stage launch over all members: one CTA per work item (member, column), the items ordered
+// tallest columns first so the tail of the launch is made of the cheapest columns. The member's
+// geometry is staged in shared memory; its arrays are addressed through the column view
+// (element offsets into the pools). Shared memory is sized for the tallest member.
 template <typename T, int NP>
 __global__ void __launch_bounds__(STAGE_MAX_THREADS, sizeof(T) == 4 ? 2 : 1)
     dg3d_stage_ens_kernel(StageArgs<T> a, const EnsMember *mem, const int2 *items, int nitems) {
-    __shared__ StageArgs<T> sa;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    if (threadIdx.x == 0) {  // the column's three mbarriers, initialised once per CTA
-        uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw);
-        mbar_init(&bars[0], 1);
-        mbar_init(&bars[1], 1);
-        mbar_init(&bars[2], 1);
-    }
-    // each column staged by bulk copies completes one phase of every barrier (the two register
-    // barriers only in stages that read the register, which is the same for every item)
-    uint32_t ph = 0;
-    for (int w = blockIdx.x; w < nitems; w += gridDim.x) {
-        const int2 wi = items[w];
-        if (threadIdx.x == 0) {
-            StageArgs<T> b = a;
-            shift_stage(b, mem[wi.x], wi.x);
-            sa = b;
-        }
-        __syncthreads();
-        if (!stage_column<T, NP>(sa, wi.y, ph, false)) return;
-        if (sa.bulk) ph ^= 1u;
-        __syncthreads();  // the next item overwrites the column's shared memory and sa
-    }
+    __shared__ Geo sG;
+    if ((int)blockIdx.x >= nitems) return;
+    const int2 wi = items[blockIdx.x];
+    const EnsMember &m = mem[wi.x];
+    if (threadIdx.x == 0) sG = m.G;
+    __syncthreads();
+    stage_column<T, NP>(a, sG, ColView{m.off3, m.off2, wi.x, m.bulk, m.dt}, wi.y, 0u, true);
 }
 
 __device__ __forceinline__ void shift_baro(BaroArgs &a, const EnsMember &m, int idx) {
@@ -3122,7 +3098,7 @@ int drf_ens_create(int nmembers, const drf_mesh_desc *meshes, const drf_dg_param
         DRF_CUDA(cudaMemcpy(e->items.p, items.data(), items.size() * sizeof(int2), cudaMemcpyHostToDevice));
         e->tiles.alloc(tiles.size());
         DRF_CUDA(cudaMemcpy(e->tiles.p, tiles.data(), tiles.size() * sizeof(int2), cudaMemcpyHostToDevice));
-        // persistent grid: as many stage CTAs as fit on the device at once
+        // the stage kernel must fit on an SM with the tallest member's shared memory
         int dev = 0, nsm = 0, per_sm = 0;
         DRF_CUDA(cudaGetDevice(&dev));
         DRF_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
@@ -3136,7 +3112,7 @@ int drf_ens_create(int nmembers, const drf_mesh_desc *meshes, const drf_dg_param
                                                                    e->threads, e->smem));
         });
         DRF_CHECK(per_sm >= 1, DRF_E_UNSUPPORTED, "ensemble stage kernel does not fit on an SM");
-        e->grid = std::min(e->nitems, per_sm * nsm);
+        e->grid = e->nitems;  // one CTA per (member, column) item
         *out = e.release();
     });
 }

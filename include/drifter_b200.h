@@ -201,7 +201,8 @@ int drf_dg_info(drf_dg *m, int64_t *n3d_nodes, int64_t *n2d_nodes, int *precisio
 /* ------------------------------------------------------------------ ensembles
  * An ensemble of independent coupled DG runs with their own meshes (nx, ny, nz), bathymetry,
  * forcing, parameters and step sizes, stepped together: each LSRK stage of all members is ONE
- * persistent kernel launch over every member's water columns, each barotropic substep one
+ * kernel launch over every member's water columns (one CTA per column, tallest columns first),
+ * each barotropic substep one
  * launch over every member's 2D tiles, and each baroclinic step one CUDA graph. Per member
  * the result is that of ModeSplittingSolver::step (include/physics/mode_splitting.hpp:241)
  * as computed by drf_dg_step_modesplit. The reference runs members one after the other. */
@@ -222,7 +223,7 @@ int drf_ens_sync(drf_ens *e);
 /* nsteps baroclinic steps of every member, member i with step dt[i] and nsub subcycles. */
 int drf_ens_step(drf_ens *e, const double *dt, int nsub, int nsteps);
 /* Totals for the bench: 3D nodes over all members, stage work items (water columns) and the
- * persistent stage grid. */
+ * stage grid (one CTA per item). */
 int drf_ens_info(drf_ens *e, int64_t *n3d_nodes, int *items, int *grid);
 
 /* ------------------------------------------------------------------ Bezier smoother
