@@ -172,6 +172,21 @@ def test_constrained_solve_doc_known_answer(inner):
     assert np.abs(A @ x).max() < 1e-7
 
 
+def test_constrained_solve_matches_oracle_at_48():
+    """The constrained (C1, Schur-CG) solve on a 48 x 48 fBm case (21,025 control points, the
+    reference's edge constraints at 4 Gauss points): the GPU's Schur CG with inner multigrid-PCG
+    solves against the oracle's Schur CG with exact Q^-1 (SuperLU), 1e-7 relative."""
+    from test_oracle_bz import schur_solve
+    n = 48
+    g, o = pair(n)
+    g.mg_setup(2)
+    x, info = g.solve_constrained(4, tol=1e-10, inner="mg", inner_tol=1e-13)
+    xo, A = schur_solve(o)
+    assert info["relres"] < 1e-10 and info["outer_iters"] > 0
+    assert rel(x, xo) < 1e-7
+    assert np.abs(A @ x).max() < 1e-6 * np.abs(x).max()
+
+
 @pytest.mark.parametrize("ng", [3, 4, 5])
 def test_element_errors_match_oracle(ng):
     """AdaptiveCGCubicBezierSmoother::compute_element_l2_error for every element on the GPU
