@@ -243,6 +243,15 @@ inline size_t stage_smem_bytes(int nz, int np, size_t tsz) {
 // thread applies the 1D operators to registers, with the operator entries read as
 // warp-uniform constants: x pencils (j,k,layer), y pencils (i,k,layer), z pencils (i,j,layer).
 //
+// Layer-half thread mapping of the stage kernel instances with a compile-time, even layer count
+// (pencils per half HP, threads per half HT, a whole number of warps; 2 HT threads a CTA).
+template <int NP, int NZ>
+struct StageHalves {
+    static constexpr bool on = NZ > 0 && NZ % 2 == 0;
+    static constexpr int HP = on ? NZ * NP * NP / 2 : 0;
+    static constexpr int HT = on ? ((HP + 31) / 32) * 32 : 0;
+};
+
 // Where a column's data live: a single model's arrays (zero offsets, clock 0), or an ensemble
 // member's slices of the pooled arrays (element offsets of its 3D and 2D arrays, its clock, its
 // bulk-copy alignment and its baroclinic step).
@@ -265,6 +274,20 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, const Geo &G
     using B = BT<T, NP>;
     const int nz = NZ > 0 ? NZ : G.nz, ncn = nz * NP3, npen = nz * NP2;
     const int ex = c % G.nx, ey = c / G.nx;
+    // Pencils to threads. With the layer count a compile-time even number, the layers' two
+    // halves go to two groups of whole warps (StageHalves), each with one pencil per thread,
+    // and the horizontal passes synchronise each half alone (named barriers 1 and 2): a
+    // pass of a layer reads only that layer. Otherwise thread t takes pencils t, t + blockDim.
+    using SH = StageHalves<NP, NZ>;
+    const int hf = SH::on ? (int)threadIdx.x / SH::HT : 0;
+    const int my_p = SH::on ? hf * SH::HP + (int)threadIdx.x % SH::HT : (int)threadIdx.x;
+    const bool my_valid = SH::on ? (hf < 2 && (int)threadIdx.x % SH::HT < SH::HP) : (int)threadIdx.x < npen;
+    const int p_first = my_valid ? my_p : npen;
+    auto p_next = [&](int p) { return SH::on ? npen : p + (int)blockDim.x; };
+    auto half_sync = [&] {
+        if constexpr (SH::on) asm volatile("bar.sync %0, %1;" ::"r"(1 + hf), "r"(SH::HT) : "memory");
+        else __syncthreads();
+    };
     const size_t base = (size_t)cv.off3 + (size_t)c * ncn, c2 = (size_t)cv.off2 + (size_t)c * NP2;
     const T dtc = (T)cv.dt;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -455,8 +478,8 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, const Geo &G
     // copies are in flight (the x pass then starts without a global-load wait)
     Side fx0, fxN;
     bool hx0 = false, hxN = false;
-    if (threadIdx.x < npen) {
-        const int p = threadIdx.x, ez = p / NP2, j = p % NP, k = (p / NP) % NP;
+    if (my_valid) {
+        const int p = my_p, ez = p / NP2, j = p % NP, k = (p / NP) % NP;
         hx0 = fetch_side(0, ez, 0, j, k, fx0);
         hxN = fetch_side(1, ez, N, j, k, fxN);
     }
@@ -754,8 +777,8 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, const Geo &G
         const T PpN = pplus(hN, 1, j, ez, k, e0 + N, N + NP * j, oN);
         hpass(std::integral_constant<int, 0>{}, e0, 1, j, 0, o0, oN, Pp0, PpN);
     };
-    if (threadIdx.x < npen) xpencil(threadIdx.x, fx0, fxN, hx0, hxN);
-    for (int p = threadIdx.x + blockDim.x; p < npen; p += blockDim.x) {
+    if (my_valid) xpencil(my_p, fx0, fxN, hx0, hxN);
+    for (int p = SH::on ? npen : (int)threadIdx.x + (int)blockDim.x; p < npen; p += blockDim.x) {
         const int ez = p / NP2, j = p % NP, k = (p / NP) % NP;
         Side o0, oN;
         const bool h0 = fetch_side(0, ez, 0, j, k, o0), hN = fetch_side(1, ez, N, j, k, oN);
@@ -764,12 +787,12 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, const Geo &G
     // the first y pencil's neighbour faces are loaded across the barrier
     Side fy0, fyN;
     bool hy0 = false, hyN = false;
-    if (threadIdx.x < npen) {
-        const int p = threadIdx.x, ez = p / NP2, i = p % NP, k = (p / NP) % NP;
+    if (my_valid) {
+        const int p = my_p, ez = p / NP2, i = p % NP, k = (p / NP) % NP;
         hy0 = fetch_side(2, ez, i, 0, k, fy0);
         hyN = fetch_side(3, ez, i, N, k, fyN);
     }
-    __syncthreads();
+    half_sync();
     // y pencils (i, k, layer)
     auto ypencil = [&](int p, Side &o0, Side &oN, bool h0, bool hN) {
         const int ez = p / NP2, i = p % NP, k = (p / NP) % NP;
@@ -780,14 +803,16 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, const Geo &G
         const T PpN = pplus(hN, 3, i, ez, k, e0 + NP * N, i + NP * N, oN);
         hpass(std::integral_constant<int, 1>{}, e0, NP, 0, i, o0, oN, Pp0, PpN);
     };
-    if (threadIdx.x < npen) ypencil(threadIdx.x, fy0, fyN, hy0, hyN);
-    for (int p = threadIdx.x + blockDim.x; p < npen; p += blockDim.x) {
+    if (my_valid) ypencil(my_p, fy0, fyN, hy0, hyN);
+    for (int p = SH::on ? npen : (int)threadIdx.x + (int)blockDim.x; p < npen; p += blockDim.x) {
         const int ez = p / NP2, i = p % NP, k = (p / NP) % NP;
         Side o0, oN;
         const bool h0 = fetch_side(2, ez, i, 0, k, o0), hN = fetch_side(3, ez, i, N, k, oN);
         ypencil(p, o0, oN, h0, hN);
     }
-    __syncthreads();
+    // the late register half overwrites P, read by every layer's passes: a full barrier then
+    if (late) __syncthreads();
+    else half_sync();
     // the register of (HT, HS) now that P is no longer read from its shared memory
     if (late) {
         if (cv.bulk) {
@@ -804,7 +829,7 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, const Geo &G
     }
     // ---- layer quadrature totals of the horizontal divergence, Q = (dsig/2) sum_k w_k delta_k
     const T hds = (T)(0.5 * G.dsig);
-    for (int p = threadIdx.x; p < npen; p += blockDim.x) {
+    for (int p = p_first; p < npen; p = p_next(p)) {
         const int ez = p / NP2, an = p % NP2;
         const int e0 = ez * NP3 + an;
         T sq = 0;
@@ -820,7 +845,7 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, const Geo &G
     // pair; a wait that gives up clears s_ok2, checked at the barrier after the pass.
     if (cv.bulk && need_res && !mbar_wait(&bars[1], ph)) s_ok2 = 0;
     bool w2 = !(cv.bulk && need_res);
-    for (int p = threadIdx.x; p < npen; p += blockDim.x) {
+    for (int p = p_first; p < npen; p = p_next(p)) {
         const int ez = p / NP2, an = p % NP2;
         const int e0 = ez * NP3 + an;
         const T iH = sIH[an], fa = (T)a.f[c2 + an];
@@ -966,7 +991,7 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, const Geo &G
         }
     }
     if (a.mode == 0) {
-        __syncthreads();
+        if (!(cv.bulk && need_res)) __syncthreads();  // (else the barrier above)
         // one thread per (2D node, component): FP64 sum over the layers in four partial sums
         for (int t = threadIdx.x; t < 2 * NP2; t += blockDim.x) {
             const int v = t / NP2, an = t % NP2;
@@ -1902,7 +1927,14 @@ struct drf_dg {
         if (own) cudaStreamDestroy(own);
     }
 
+    // threads of the single-model stage CTA: the layer-half mapping of the instances compiled
+    // for a layer count (dispatch_stage_nz), else one thread per pencil up to the maximum
     int stage_threads() const {
+        const int npen = G.nz * np2;
+        if ((np == 4 || np == 5) && (G.nz == 4 || G.nz == 16)) return 2 * (((npen / 2) + 31) / 32) * 32;
+        return stage_threads_generic();
+    }
+    int stage_threads_generic() const {
         const int npen = G.nz * np2;
         int bs = ((npen + 31) / 32) * 32;
         return bs < 64 ? 64 : (bs > STAGE_MAX_THREADS ? STAGE_MAX_THREADS : bs);
@@ -3049,7 +3081,7 @@ int drf_ens_create(int nmembers, const drf_mesh_desc *meshes, const drf_dg_param
             off2[i] = e->n2tot;
             e->n3tot += (m->n3 + 63) / 64 * 64;
             e->n2tot += m->n2;
-            e->threads = std::max(e->threads, m->stage_threads());
+            e->threads = std::max(e->threads, m->stage_threads_generic());
             e->smem = std::max(e->smem, m->smem);
             e->mem.push_back(std::move(m));
         }
