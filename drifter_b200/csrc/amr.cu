@@ -27,6 +27,7 @@
 
 #include "amr_layout.hpp"
 #include "common.cuh"
+#include "mortar_internal.hpp"
 
 namespace drf {
 namespace {
@@ -49,7 +50,27 @@ struct AmrArgs {
     int64_t n_elem;
     double ax, ay, az;
     int flux;               // 0 central, 1 upwind, 2 Lax-Friedrichs
+    // the LSRK stage form (amr_rhs_kernel<NP, true>): the mortar lifts added in the lift
+    // kernel's order, then the mass inverse and res = A res + dt (-M^-1 R), Uout = U + B res
+    const double *contrib;  // staged mortar lifts (null: no interfaces)
+    const int64_t *lptr;    // lift entries of touched element u: lent[lptr[u] .. lptr[u + 1])
+    const int *lent;        // (interface, slot, face)
+    const int *e2u;         // touched-element index of each element, -1 if none
+    int slots;
+    double *res, *Uout;
+    double A, B, dt;
+    int first;
 };
+
+// One node's LSRK45 stage from its weak right-hand side R (before the mass inverse, the
+// diagonal LGL mass w_i w_j w_k): res = A res + dt (-M^-1 R), u += B res.
+__device__ __forceinline__ void amr_lsrk_node(double R, double wi, double wj, double wk, double &res, double &u,
+                                              double A, double B, double dt, int first) {
+    const double rhs = R * (1.0 / (wi * wj * wk));
+    const double rn = (first ? 0.0 : A * res) + dt * (-rhs);
+    res = rn;
+    u = u + B * rn;
+}
 
 __device__ __forceinline__ double amr_flux(int kind, double uL, double uR, double vn) {
     if (kind == 0) return 0.5 * (vn * uL + vn * uR);
@@ -73,8 +94,9 @@ constexpr int amr_epb() {  // elements per CTA: about 256 threads
 
 // R = volume term + conforming/boundary face lifts, one thread per node. The element's face
 // table and its conforming neighbours' face traces are loaded at the start (each thread takes
-// face-node slots n, n + NP^3, ...) so those global loads overlap the volume passes.
-template <int NP>
+// face-node slots n, n + NP^3, ...) so those global loads overlap the volume passes. STAGE:
+// the node's mortar lifts are added and the LSRK stage applied (U read, Uout written).
+template <int NP, bool STAGE = false>
 __global__ void __launch_bounds__(amr_epb<NP>() * NP * NP * NP) amr_rhs_kernel(AmrArgs a) {
     constexpr int NP2 = NP * NP, NP3 = NP2 * NP, EPB = amr_epb<NP>(), NFS = 6 * NP2;
     constexpr int SLOTS = (NFS + NP3 - 1) / NP3;  // face-node slots per thread
@@ -167,7 +189,26 @@ __global__ void __launch_bounds__(amr_epb<NP>() * NP * NP * NP) amr_rhs_kernel(A
         const double uR = kd == 1 ? sN[le * NFS + f * NP2 + it + NP * jt] : u;
         r += Bs.w[it] * Bs.w[jt] * amr_flux(a.flux, u, uR, vn);
     }
-    a.R[e * NP3 + n] = r;
+    if constexpr (STAGE) {
+        // mortar lifts of the interfaces touching this element, in the lift kernel's order
+        const int ut = a.e2u ? a.e2u[e] : -1;
+        if (ut >= 0)
+            for (int64_t q = a.lptr[ut]; q < a.lptr[ut + 1]; ++q) {
+                const int iface = a.lent[3 * q], slot = a.lent[3 * q + 1], f = a.lent[3 * q + 2];
+                const int axis = f >> 1, b = (f & 1) ? NP - 1 : 0;
+                const int on = axis == 0 ? i : (axis == 1 ? j : k);
+                if (on != b) continue;
+                const int it = axis == 0 ? j : i, jt = axis == 2 ? j : k;
+                r += a.contrib[((size_t)iface * a.slots + slot) * NP2 + it + NP * jt];
+            }
+        const size_t t = (size_t)e * NP3 + n;
+        double rs = a.first ? 0.0 : a.res[t], uo = u;
+        amr_lsrk_node(r, Bs.w[i], Bs.w[j], Bs.w[k], rs, uo, a.A, a.B, a.dt, a.first);
+        a.res[t] = rs;
+        a.Uout[t] = uo;
+    } else {
+        a.R[e * NP3 + n] = r;
+    }
 }
 
 // out = M^-1 R (the right-hand side the caller sees)
@@ -179,21 +220,6 @@ __global__ void amr_massinv_kernel(int64_t n, const double *R, double *out) {
     const int nn = (int)(t % NP3), i = nn % NP, j = (nn / NP) % NP, k = nn / (NP * NP);
     const AmrBasis &Bs = cAmr[NP];
     out[t] = R[t] * (1.0 / (Bs.w[i] * Bs.w[j] * Bs.w[k]));
-}
-
-// LSRK45 stage: res = A res + dt (-M^-1 R); U += B res
-template <int NP>
-__global__ void amr_lsrk_kernel(int64_t n, const double *R, double *res, double *U, double A, double B,
-                                double dt, int first) {
-    constexpr int NP3 = NP * NP * NP;
-    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (t >= n) return;
-    const int nn = (int)(t % NP3), i = nn % NP, j = (nn / NP) % NP, k = nn / (NP * NP);
-    const AmrBasis &Bs = cAmr[NP];
-    const double rhs = R[t] * (1.0 / (Bs.w[i] * Bs.w[j] * Bs.w[k]));
-    const double rn = (first ? 0.0 : A * res[t]) + dt * (-rhs);
-    res[t] = rn;
-    U[t] = U[t] + B * rn;
 }
 
 template <class F>
@@ -402,27 +428,36 @@ struct drf_amr {
     cudaStream_t stream = nullptr, own = nullptr;
     DevBuf<int64_t> nbe;
     DevBuf<int8_t> nbk, nbf;
-    DevBuf<double> U, R, res, out;  // device state, weak rhs, LSRK register, caller-visible rhs
+    // device state (two buffers: an LSRK stage reads one and writes the other; cur holds the
+    // state between steps), weak rhs, LSRK register, caller-visible rhs
+    DevBuf<double> U, R, res, out;
+    int cur = 0;
     drf_mortar *mortar = nullptr;
-    cudaGraphExec_t graph = nullptr;
-    uint64_t graph_kernels = 0;  // kernel nodes of the step graph
+    DevBuf<int> e2u;  // touched-element index of each element for the stage kernel's lifts
+    // step graphs for each starting buffer (a step's five stages flip it)
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    uint64_t graph_kernels = 0;  // kernel nodes of a step graph
     int g_mode = -1, g_flux = -1;
     double g_a[3] = {0, 0, 0}, g_dt = 0.0;
 
+    double *state() { return U.p + (size_t)cur * n_elem * nd; }
+    double *buf(int b) { return U.p + (size_t)b * n_elem * nd; }
     ~drf_amr() {
-        if (graph) cudaGraphExecDestroy(graph);
+        for (auto &g : graph)
+            if (g) cudaGraphExecDestroy(g);
         if (mortar) drf_mortar_destroy(mortar);
         if (own) cudaStreamDestroy(own);
     }
     void drop_graph() {
-        if (graph) cudaGraphExecDestroy(graph);
-        graph = nullptr;
+        for (auto &g : graph)
+            if (g) cudaGraphExecDestroy(g);
+        graph[0] = graph[1] = nullptr;
         g_mode = -1;
     }
     // R = weak right-hand side of U (volume + faces of the mode + mortar lifts)
     void enqueue_rhs(int mode, int flux, const double a[3]) {
         AmrArgs A{};
-        A.U = U.p; A.R = R.p; A.nbe = nbe.p; A.nbf = nbf.p; A.n_elem = n_elem;
+        A.U = state(); A.R = R.p; A.nbe = nbe.p; A.nbf = nbf.p; A.n_elem = n_elem;
         A.ax = a[0]; A.ay = a[1]; A.az = a[2]; A.flux = flux;
         // mode 0 reads an all-zero face table: the reference's TODO branches
         A.nbk = mode == 1 ? nbk.p : nbk.p + (size_t)6 * n_elem;
@@ -433,18 +468,30 @@ struct drf_amr {
             DRF_LAUNCHED();
         });
         if (mortar) {
-            const int rc = drf_mortar_apply_device(mortar, flux, a, U.p, R.p);
+            const int rc = drf_mortar_apply_device(mortar, flux, a, state(), R.p);
             DRF_CHECK(rc == DRF_OK, rc, "mortar apply failed");
         }
     }
-    void enqueue_step(int mode, int flux, const double a[3], double dt) {
-        const int64_t n = n_elem * nd;
+    // one LSRK45 step from buffer b0: per stage the mortar face kernel, then the stage kernel
+    // (volume, faces, mortar lifts, mass inverse and update) from one buffer into the other
+    void enqueue_step(int mode, int flux, const double a[3], double dt, int b0) {
+        const MortarLifts L = mortar ? mortar_lifts(mortar) : MortarLifts{};
         for (int s = 0; s < 5; ++s) {
-            enqueue_rhs(mode, flux, a);
+            const int src = (b0 + s) % 2;
+            if (mortar) mortar_stage_faces(mortar, flux, a, buf(src));
+            AmrArgs A{};
+            A.U = buf(src); A.Uout = buf(1 - src); A.res = res.p;
+            A.nbe = nbe.p; A.nbf = nbf.p; A.n_elem = n_elem;
+            A.nbk = mode == 1 ? nbk.p : nbk.p + (size_t)6 * n_elem;
+            A.ax = a[0]; A.ay = a[1]; A.az = a[2]; A.flux = flux;
+            A.contrib = mortar ? L.contrib : nullptr; A.lptr = L.ptr; A.lent = L.ent;
+            A.e2u = mortar ? e2u.p : nullptr; A.slots = L.slots;
+            A.A = AMR_LSRK_A[s]; A.B = AMR_LSRK_B[s]; A.dt = dt; A.first = s == 0;
             amr_dispatch(np, [&](auto npc) {
                 constexpr int NP = decltype(npc)::value;
-                amr_lsrk_kernel<NP><<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(
-                    n, R.p, res.p, U.p, AMR_LSRK_A[s], AMR_LSRK_B[s], dt, s == 0);
+                constexpr int EPB = amr_epb<NP>();
+                amr_rhs_kernel<NP, true>
+                    <<<(unsigned)((n_elem + EPB - 1) / EPB), EPB * NP * NP * NP, 0, stream>>>(A);
                 DRF_LAUNCHED();
             });
         }
@@ -580,17 +627,26 @@ int drf_amr_create(int order, int64_t n_elem, int64_t n_conf, const int64_t *con
         DRF_CUDA(cudaMemcpy(h->nbk.p, nbk.data(), nbk.size(), cudaMemcpyHostToDevice));
         DRF_CUDA(cudaMemcpy(h->nbf.p, nbf.data(), nbf.size(), cudaMemcpyHostToDevice));
         const size_t n = (size_t)n_elem * h->nd;
-        h->U.alloc(n);
+        h->U.alloc(2 * n);
         h->R.alloc(n);
         h->res.alloc(n);
         h->out.alloc(n);
-        DRF_CUDA(cudaMemset(h->U.p, 0, n * 8));
+        DRF_CUDA(cudaMemset(h->U.p, 0, 2 * n * 8));
         DRF_CUDA(cudaMemset(h->res.p, 0, n * 8));
         if (n_if > 0) {
             const int rc = drf_mortar_create(order, n_if, type, coarse_elem, coarse_face, fine_elem, fine_face,
                                              n_elem, &h->mortar);
             DRF_CHECK(rc == DRF_OK, rc, "mortar interfaces rejected");
             DRF_CHECK(drf_mortar_set_stream(h->mortar, h->stream) == DRF_OK, DRF_E_CUDA, "mortar stream");
+            // each element's index in the mortar space's touched-element list (-1: none)
+            const MortarLifts L = mortar_lifts(h->mortar);
+            std::vector<int64_t> touched((size_t)std::max<int64_t>(L.n_touched, 1));
+            if (L.n_touched > 0)
+                DRF_CUDA(cudaMemcpy(touched.data(), L.touched, L.n_touched * 8, cudaMemcpyDeviceToHost));
+            std::vector<int> e2u((size_t)n_elem, -1);
+            for (int64_t u = 0; u < L.n_touched; ++u) e2u[touched[u]] = (int)u;
+            h->e2u.alloc(n_elem);
+            DRF_CUDA(cudaMemcpy(h->e2u.p, e2u.data(), n_elem * 4, cudaMemcpyHostToDevice));
         }
         *out = h.release();
     });
@@ -620,7 +676,7 @@ int drf_amr_upload(drf_amr *h, const double *U) {
         DRF_CHECK(U, DRF_E_INVALID, "null argument");
         const size_t n = (size_t)h->n_elem * h->nd;
         DRF_CHECK(all_finite(U, n), DRF_E_NONFINITE, "non-finite state");
-        DRF_CUDA(cudaMemcpyAsync(h->U.p, U, n * 8, cudaMemcpyHostToDevice, h->stream));
+        DRF_CUDA(cudaMemcpyAsync(h->state(), U, n * 8, cudaMemcpyHostToDevice, h->stream));
         DRF_CUDA(cudaStreamSynchronize(h->stream));
     });
 }
@@ -630,7 +686,7 @@ int drf_amr_download(drf_amr *h, double *U) {
         amr_check(h);
         DRF_CHECK(U, DRF_E_INVALID, "null argument");
         const size_t n = (size_t)h->n_elem * h->nd;
-        DRF_CUDA(cudaMemcpyAsync(U, h->U.p, n * 8, cudaMemcpyDeviceToHost, h->stream));
+        DRF_CUDA(cudaMemcpyAsync(U, h->state(), n * 8, cudaMemcpyDeviceToHost, h->stream));
         DRF_CUDA(cudaStreamSynchronize(h->stream));
         DRF_CHECK(all_finite(U, n), DRF_E_NONFINITE, "non-finite state (the run blew up)");
     });
@@ -644,7 +700,7 @@ int drf_amr_compute_rhs(drf_amr *h, int mode, int flux_kind, const double *a, co
         const int64_t n = h->n_elem * h->nd;
         if (U) {
             DRF_CHECK(all_finite(U, (size_t)n), DRF_E_NONFINITE, "non-finite state");
-            DRF_CUDA(cudaMemcpyAsync(h->U.p, U, n * 8, cudaMemcpyHostToDevice, h->stream));
+            DRF_CUDA(cudaMemcpyAsync(h->state(), U, n * 8, cudaMemcpyHostToDevice, h->stream));
         }
         h->enqueue_rhs(mode, flux_kind, a);
         amr_dispatch(h->np, [&](auto npc) {
@@ -663,19 +719,21 @@ int drf_amr_step(drf_amr *h, int mode, int flux_kind, const double *a, double dt
         amr_check_args(mode, flux_kind, a);
         DRF_CHECK(dt > 0.0 && std::isfinite(dt), DRF_E_INVALID, "dt must be positive");
         DRF_CHECK(nsteps >= 0, DRF_E_INVALID, "nsteps must be >= 0");
-        if (!h->graph || h->g_mode != mode || h->g_flux != flux_kind || h->g_dt != dt ||
+        if (!h->graph[0] || h->g_mode != mode || h->g_flux != flux_kind || h->g_dt != dt ||
             std::memcmp(h->g_a, a, sizeof(h->g_a)) != 0) {
             h->drop_graph();
-            h->graph = capture_graph(h->stream, [&] { h->enqueue_step(mode, flux_kind, a, dt); },
-                                     &h->graph_kernels);
+            for (int b = 0; b < 2; ++b)
+                h->graph[b] = capture_graph(h->stream, [&] { h->enqueue_step(mode, flux_kind, a, dt, b); },
+                                            &h->graph_kernels);
             h->g_mode = mode;
             h->g_flux = flux_kind;
             h->g_dt = dt;
             std::memcpy(h->g_a, a, sizeof(h->g_a));
         }
         for (int s = 0; s < nsteps; ++s) {
-            DRF_CUDA(cudaGraphLaunch(h->graph, h->stream));
+            DRF_CUDA(cudaGraphLaunch(h->graph[h->cur], h->stream));
             launch_counter().fetch_add(h->graph_kernels);
+            h->cur = 1 - h->cur;  // five stages leave the state in the other buffer
         }
     });
 }
@@ -731,7 +789,7 @@ int drf_amr_estimate(drf_amr *h, const double *hchar, double refine_threshold, d
         amr_dispatch(h->np, [&](auto npc) {
             constexpr int NP = decltype(npc)::value;
             amr_estimate_kernel<NP><<<(unsigned)nb, 32 * AMR_EST_WARPS, 0, h->stream>>>(
-                ne, h->U.p, dh.p, smoothness_factor, dv.p, dm.p, part.p);
+                ne, h->state(), dh.p, smoothness_factor, dv.p, dm.p, part.p);
         });
         DRF_LAUNCHED();
         amr_max_kernel<<<1, 1024, 0, h->stream>>>(part.p, nb, part.p + nb);
@@ -813,7 +871,7 @@ int drf_amr_transfer(drf_amr *from, drf_amr *to, int nx, int ny, const int *old_
         DRF_CUDA(cudaMemcpyAsync(doffn.p, offn.data(), offn.size() * 8, cudaMemcpyHostToDevice, st));
         DRF_CUDA(cudaMemcpyAsync(drows.p, rows.data(), rows.size() * 8, cudaMemcpyHostToDevice, st));
         AmrTransferArgs A{};
-        A.Uo = from->U.p; A.Un = to->U.p; A.col_of = dcol.p; A.lvo = dlvo.p; A.lvn = dlvn.p;
+        A.Uo = from->state(); A.Un = to->state(); A.col_of = dcol.p; A.lvo = dlvo.p; A.lvn = dlvn.p;
         A.offo = doffo.p; A.offn = doffn.p; A.rows = drows.p; A.n_new = nn;
         for (int i = 0; i < b.np; ++i) A.xn[i] = b.x[i];
         const int64_t nthr = nn * from->nd;

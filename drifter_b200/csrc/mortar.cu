@@ -22,6 +22,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "mortar_internal.hpp"
 
 namespace drf {
 namespace {
@@ -338,6 +339,14 @@ struct drf_mortar {
     }
     void run(int kind, const double a[3], const double *dU, double *drhs) {
         if (n_if == 0) return;
+        stage_faces(kind, a, dU);
+        const int64_t nt = n_touched * nd;
+        mortar_lift_kernel<<<(unsigned)((nt + 255) / 256), 256, 0, stream>>>(np, nd, n_touched, touched.p, ptr.p,
+                                                                             ent.p, contrib.p, drhs);
+        DRF_LAUNCHED();
+    }
+    void stage_faces(int kind, const double a[3], const double *dU) {
+        if (n_if == 0) return;
         const unsigned g = (unsigned)std::min<int64_t>((n_if + MW - 1) / MW, 148 * 16);
         switch (np) {
         case 2: mortar_face_kernel<2><<<g, 32 * MW, 0, stream>>>(dev(), kind, a[0], a[1], a[2], dU, contrib.p); break;
@@ -347,12 +356,24 @@ struct drf_mortar {
         default: mortar_face_kernel<6><<<g, 32 * MW, 0, stream>>>(dev(), kind, a[0], a[1], a[2], dU, contrib.p); break;
         }
         DRF_LAUNCHED();
-        const int64_t nt = n_touched * nd;
-        mortar_lift_kernel<<<(unsigned)((nt + 255) / 256), 256, 0, stream>>>(np, nd, n_touched, touched.p, ptr.p,
-                                                                             ent.p, contrib.p, drhs);
-        DRF_LAUNCHED();
     }
 };
+
+namespace drf {
+void mortar_stage_faces(drf_mortar *h, int kind, const double a[3], const double *d_U) {
+    h->stage_faces(kind, a, d_U);
+}
+MortarLifts mortar_lifts(const drf_mortar *h) {
+    MortarLifts L;
+    L.contrib = h->contrib.p;
+    L.touched = h->touched.p;
+    L.ptr = h->ptr.p;
+    L.ent = h->ent.p;
+    L.n_touched = h->n_touched;
+    L.slots = SLOTS;
+    return L;
+}
+}  // namespace drf
 
 namespace {
 template <class T>

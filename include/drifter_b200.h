@@ -454,8 +454,8 @@ int drf_amr_compute_rhs(drf_amr *h, int mode, int flux_kind, const double *a, co
 int drf_amr_upload(drf_amr *h, const double *U);
 int drf_amr_download(drf_amr *h, double *U);
 /* nsteps of LSRK45 (LSRK45::step, src/solver/time_stepper.cpp:126) on du/dt = -compute_rhs(u)
- * of the device state, each step one CUDA graph (5 x (volume/face kernel, mortar kernels,
- * update)). */
+ * of the device state, each step one CUDA graph (5 x (mortar face kernel; one kernel for the
+ * volume, faces, mortar lifts and update)). */
 int drf_amr_step(drf_amr *h, int mode, int flux_kind, const double *a, double dt, int nsteps);
 /* Device time of one right-hand side (mean of nrep, CUDA events) and its algorithmic bytes. */
 int drf_amr_time_rhs(drf_amr *h, int mode, int flux_kind, const double *a, int nrep, double *ms,
