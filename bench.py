@@ -239,7 +239,7 @@ def run_cg(stream, reps=3):
     c = configs.c4()
     t0 = time.perf_counter()
     net, info = train_preconditioner(n=64, dx=c["L"] / c["n"], lam=c["lam"], eps=c["eps"],
-                                     steps=1500, rhs_count=16, seed=1)
+                                     steps=10000, rhs_count=16, seed=1)
     train_s = time.perf_counter() - t0
     s = BezierSmoother(c["n"], c["n"], c["L"], c["L"], c["d"], lam=c["lam"], ridge_epsilon=c["eps"])
     s.set_stream(stream.cuda_stream)

@@ -185,7 +185,7 @@ def bathymetry_rhs(n: int, L: float, lam: float, eps: float, count: int, seed: i
     return out
 
 
-def train_preconditioner(n=64, dx=100.0, lam=1.0, eps=1e-4, d=None, rhs_count=16, steps=1500,
+def train_preconditioner(n=64, dx=100.0, lam=1.0, eps=1e-4, d=None, rhs_count=16, steps=10000,
                          seed=1, lr=2e-3, crop=48, batch=16):
     """Trains a network on a training grid of n x n elements with element size dx (the same
     element operator as the target grid) and returns it with its output scale set. Training
