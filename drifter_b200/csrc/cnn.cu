@@ -74,7 +74,9 @@ constexpr size_t conv_smem_bytes() {
 template <int CIN, int COUT, bool RELU, bool OUTF32>
 __global__ void __launch_bounds__(256) conv3x3_kernel(int B, int H, int W, const bf16 *__restrict__ X,
                                                       const bf16 *__restrict__ Wt,
-                                                      const float *__restrict__ bias, void *Yv) {
+                                                      const float *__restrict__ bias, void *Yv,
+                                                      const int *stop) {
+    if (stop && *stop) return;  // a preconditioner apply queued after its solve converged
     constexpr int PS = CIN + 8, WS = 9 * CIN + 8, HP = TH + 2, WP = CTW + 2, C8 = CIN / 8;
     extern __shared__ __align__(16) unsigned char conv_smem[];
     bf16 *Xs0 = reinterpret_cast<bf16 *>(conv_smem);  // double-buffered input halo
@@ -290,7 +292,11 @@ __device__ __forceinline__ void tc_bar_init(uint64_t *bar, uint32_t count) {
 template <int CIN, int COUT, bool RELU, bool OUTF32>
 __global__ void __launch_bounds__(192) conv3x3_tc_kernel(int B, int H, int W, const __grid_constant__ CUtensorMap xmap,
                                                          const bf16 *__restrict__ Wt,
-                                                         const float *__restrict__ bias, void *Yv, int *err) {
+                                                         const float *__restrict__ bias, void *Yv, int *err,
+                                                         const int *stop) {
+    // a preconditioner apply queued after its solve converged: every thread leaves before any
+    // barrier, copy or tensor-memory allocation
+    if (stop && *stop) return;
     using P = TcConv<CIN, COUT>;
     constexpr int C8 = P::C8, WP = P::WP, NS = P::NS, NA = P::NA;
     constexpr uint32_t IDESC = umma_idesc_bf16<128, COUT>();
@@ -575,7 +581,9 @@ __global__ void crop_kernel(int B, int ch, int cw, int H, int W, const int *sel,
 }
 
 // superpixel packing of a control-point field (nd x nd, nd = 3n + 1) scaled by 1/rms
-__global__ void pack_kernel(int n, const double *r, const double *rr_ptr, double inv_len, bf16 *X) {
+__global__ void pack_kernel(int n, const double *r, const double *rr_ptr, double inv_len, bf16 *X,
+                            const int *stop) {
+    if (stop && *stop) return;
     // one thread per superpixel (I, J): its 9 control points 3I..3I+2 x 3J..3J+2 (three runs of
     // three consecutive values) become channels 0..8, channels 9..15 are zero; one 32-byte store
     const int S = n + 1, nd = 3 * n + 1;
@@ -694,7 +702,7 @@ CUtensorMap conv_halo_map(const bf16 *X, int B, int H, int W) {
 
 template <int CIN, int COUT, bool RELU, bool OUTF32>
 void conv_tc(cudaStream_t s, int B, int H, int W, const bf16 *X, const bf16 *Wt, const float *bias, void *Y,
-             int *err) {
+             int *err, const int *stop) {
     constexpr size_t smem = TcConv<CIN, COUT>::SMEM;
     static int resident = 0;
     if (!resident) {
@@ -719,7 +727,7 @@ void conv_tc(cudaStream_t s, int B, int H, int W, const bf16 *X, const bf16 *Wt,
     DRF_CHECK(reinterpret_cast<uintptr_t>(X) % 16 == 0, DRF_E_INVALID, "conv input not 16-byte aligned");
     const CUtensorMap xmap = conv_halo_map<CIN>(X, B, H, W);
     conv3x3_tc_kernel<CIN, COUT, RELU, OUTF32><<<grid, TcConv<CIN, COUT>::THREADS, smem, s>>>(B, H, W, xmap, Wt, bias,
-                                                                                          Y, err);
+                                                                                          Y, err, stop);
     DRF_LAUNCHED();
 }
 
@@ -754,9 +762,9 @@ int conv_form(int l, int B, int H, int W) {
 
 template <int CIN, int COUT, bool RELU, bool OUTF32>
 void conv(cudaStream_t s, int B, int H, int W, const bf16 *X, const bf16 *Wt, const float *bias,
-          void *Y, int *err, int form) {
+          void *Y, int *err, int form, const int *stop = nullptr) {
     if (form == 1) {
-        conv_tc<CIN, COUT, RELU, OUTF32>(s, B, H, W, X, Wt, bias, Y, err);
+        conv_tc<CIN, COUT, RELU, OUTF32>(s, B, H, W, X, Wt, bias, Y, err, stop);
         return;
     }
     // persistent grid: as many CTAs as are resident at once (the weights are staged once each)
@@ -773,19 +781,20 @@ void conv(cudaStream_t s, int B, int H, int W, const bf16 *X, const bf16 *Wt, co
     }
     const int64_t ntiles = (int64_t)((W + CTW - 1) / CTW) * ((H + TH - 1) / TH) * B;
     const unsigned grid = (unsigned)std::min<int64_t>(ntiles, resident);
-    conv3x3_kernel<CIN, COUT, RELU, OUTF32><<<grid, 256, smem, s>>>(B, H, W, X, Wt, bias, Y);
+    conv3x3_kernel<CIN, COUT, RELU, OUTF32><<<grid, 256, smem, s>>>(B, H, W, X, Wt, bias, Y, stop);
     DRF_LAUNCHED();
 }
 
-// form -1: the tuned (or forced, or default) form of this layer and shape
+// form -1: the tuned (or forced, or default) form of this layer and shape; stop (device, may be
+// null): the launch returns at once when it is set
 void conv_layer(cudaStream_t s, int l, int B, int H, int W, const bf16 *X, const bf16 *Wt,
-                const float *bias, void *Y, int *err, int form = -1) {
+                const float *bias, void *Y, int *err, int form = -1, const int *stop = nullptr) {
     if (form < 0) form = conv_form(l, B, H, W);
     switch (l) {
-    case 0: conv<16, 32, true, false>(s, B, H, W, X, Wt, bias, Y, err, form); break;
-    case 1: conv<32, 32, true, false>(s, B, H, W, X, Wt, bias, Y, err, form); break;
-    case 2: conv<32, 32, true, false>(s, B, H, W, X, Wt, bias, Y, err, form); break;
-    default: conv<32, 16, false, true>(s, B, H, W, X, Wt, bias, Y, err, form); break;
+    case 0: conv<16, 32, true, false>(s, B, H, W, X, Wt, bias, Y, err, form, stop); break;
+    case 1: conv<32, 32, true, false>(s, B, H, W, X, Wt, bias, Y, err, form, stop); break;
+    case 2: conv<32, 32, true, false>(s, B, H, W, X, Wt, bias, Y, err, form, stop); break;
+    default: conv<32, 16, false, true>(s, B, H, W, X, Wt, bias, Y, err, form, stop); break;
     }
 }
 
@@ -874,11 +883,12 @@ struct CnnNet {
         lpart.alloc(1024);
         cap_pix = pix;
     }
-    // forward from act[0]; output f32 in `out`
-    void forward(int B, int H, int W) {
+    // forward from act[0]; output f32 in `out` (every launch skipped when *stop is set)
+    void forward(int B, int H, int W, const int *stop = nullptr) {
         for (int l = 0; l < 3; ++l)
-            conv_layer(stream, l, B, H, W, act[l].p, wb.p + off_wb[l], wm.p + off_b[l], act[l + 1].p, status.p);
-        conv_layer(stream, 3, B, H, W, act[3].p, wb.p + off_wb[3], wm.p + off_b[3], out.p, status.p);
+            conv_layer(stream, l, B, H, W, act[l].p, wb.p + off_wb[l], wm.p + off_b[l], act[l + 1].p, status.p,
+                       -1, stop);
+        conv_layer(stream, 3, B, H, W, act[3].p, wb.p + off_wb[3], wm.p + off_b[3], out.p, status.p, -1, stop);
     }
     // backward of the mean-square loss against tgt; fills grad; returns device loss partials
     void backward(int B, int H, int W, const float *tgt) {
@@ -923,9 +933,10 @@ int cnn_precondition(CnnNet *net, cudaStream_t s, int n, const double *r, const 
     cudaStream_t keep = net->stream;
     net->stream = s;
     net->ensure(pix);
-    pack_kernel<<<nb(pix), 256, 0, s>>>(n, r, rr_dev, 1.0 / (double)(nd * nd), net->act[0].p);
+    // after convergence (stop set) every launch of the apply returns at once
+    pack_kernel<<<nb(pix), 256, 0, s>>>(n, r, rr_dev, 1.0 / (double)(nd * nd), net->act[0].p, stop);
     DRF_LAUNCHED();
-    net->forward(1, S, S);
+    net->forward(1, S, S, stop);
     DRF_CHECK(!part || jac_diag, DRF_E_INVALID, "the fused dot products need the Jacobi base (r)");
     unpack_kernel<<<nb(pix), 256, 0, s>>>(n, net->out.p, rr_dev, 1.0 / (double)(nd * nd), out_scale,
                                               z, add, stop, jac_diag ? r : nullptr, jac_diag, dq, part);
