@@ -186,11 +186,13 @@ def bathymetry_rhs(n: int, L: float, lam: float, eps: float, count: int, seed: i
 
 
 def train_preconditioner(n=64, dx=100.0, lam=1.0, eps=1e-4, d=None, rhs_count=16, steps=10000,
-                         seed=1, lr=2e-3, crop=48, batch=16):
+                         seed=1, lr=2e-3, crop=48, batch=16, rounds=3, fcg_iters=14):
     """Trains a network on a training grid of n x n elements with element size dx (the same
     element operator as the target grid) and returns it with its output scale set. Training
     pairs come from the multigrid iterations of smoothing problems (bathymetry right-hand
-    sides) and of random fields."""
+    sides) and of random fields; each later round (rounds - 1 of them) adds the residuals the
+    current network meets inside flexible CG on every right-hand side (fcg_iters iterations
+    each) and trains on, for half the steps at half the rate."""
     L = n * dx
     if d is None:
         from . import configs
@@ -203,9 +205,10 @@ def train_preconditioner(n=64, dx=100.0, lam=1.0, eps=1e-4, d=None, rhs_count=16
     net.set_dataset(X, T)
     loss = net.train(steps, batch=batch, crop=min(crop, n + 1), lr=lr, seed=seed)
     net.out_scale = scale
-    # second round: add the residuals the network meets inside flexible CG
-    X2, T2, _ = build_dataset(fcg_pairs(s, net, rhs[: max(2, rhs_count // 2)]), n, s, scale)
-    net.set_dataset(np.concatenate([X, X2]), np.concatenate([T, T2]))
-    loss = net.train(steps // 2, batch=batch, crop=min(crop, n + 1), lr=lr * 0.5, seed=seed + 1)
+    for r in range(1, rounds):
+        X2, T2, _ = build_dataset(fcg_pairs(s, net, rhs, iters=fcg_iters), n, s, scale)
+        X, T = np.concatenate([X, X2]), np.concatenate([T, T2])
+        net.set_dataset(X, T)
+        loss = net.train(steps // 2, batch=batch, crop=min(crop, n + 1), lr=lr * 0.5, seed=seed + r)
     s.close()
-    return net, dict(loss=loss, scale=scale, pairs=len(X) + len(X2))
+    return net, dict(loss=loss, scale=scale, pairs=len(X))
