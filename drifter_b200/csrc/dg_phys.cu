@@ -129,6 +129,12 @@ __device__ __forceinline__ void bulk_prefetch_l2(const void *src, uint32_t bytes
     asm volatile("cvta.to.global.u64 %0, %1;" : "=l"(g) : "l"(src));
     asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(g), "r"(bytes) : "memory");
 }
+// Prefetch of the 128-byte line holding a global address into L2 (no completion to wait for).
+__device__ __forceinline__ void line_prefetch_l2(const void *p) {
+    uint64_t g;
+    asm volatile("cvta.to.global.u64 %0, %1;" : "=l"(g) : "l"(p));
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(g));
+}
 // Spins on the barrier's phase with an iteration limit; false when it gave up.
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t phase) {
     const uint32_t a = smem_addr(bar);
@@ -219,10 +225,14 @@ template <int NP>
 struct StageTail {
     static constexpr bool pn_in_res = 4 * NP * NP <= NP * NP * NP;  // sides' P in sRes[3]
     static constexpr bool tb_in_d = NP + 4 <= NP * NP;             // layer totals in sD
-    static size_t elems(int nz) {
+    static constexpr size_t elems(int nz) {
         return (pn_in_res ? 0 : (size_t)4 * nz * NP * NP) + (tb_in_d ? 0 : (size_t)nz * NP * (NP + 4));
     }
 };
+// Per side and face node, the neighbouring column's 2D values a face flux needs (its elevation
+// e, depth H = e + h, pending corrections of Hu, Hv and the tracers, and the baroclinic
+// pressure's depth etab + h), staged once per column instead of loaded by every pencil end.
+constexpr int STAGE_NF = 6;
 inline size_t stage_tail_elems(int nz, int np) {
     switch (np) {
     case 2: return StageTail<2>::elems(nz);
@@ -235,7 +245,8 @@ inline size_t stage_tail_elems(int nz, int np) {
 inline size_t stage_smem_bytes(int nz, int np, size_t tsz) {
     const int np2 = np * np, ncn = nz * np2 * np;
     return 32 + (size_t)2 * np2 * 8 +
-           ((size_t)13 * ncn + (size_t)3 * nz * np2 + 12 * np2 + (size_t)nz * np + stage_tail_elems(nz, np)) *
+           ((size_t)13 * ncn + (size_t)3 * nz * np2 + 12 * np2 + (size_t)nz * np + stage_tail_elems(nz, np) +
+            (size_t)4 * np * STAGE_NF) *
                tsz;
 }
 
@@ -317,40 +328,18 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, const Geo &G
     T *sPn = Tl::pn_in_res ? sRes + 3 * ncn : tail;
     T *sTb = Tl::tb_in_d ? sD : tail + (Tl::pn_in_res ? 0 : 4 * nz * NP2);
     T *sTbn = sTb + nz * NP2;
+    // the neighbours' 2D face values [side][face node][STAGE_NF]
+    T *sNF = tail + Tl::elems(nz);
     __shared__ int s_ok, s_ok2;
 
-    // tidal elevation: evaluated once per CTA, and only by a column on a tidal side
-    __shared__ T s_etide;
-    if (threadIdx.x == 0) {
-        s_ok2 = 1;
-        const bool tidal = (ex == 0 && G.bc[0] == DRF_BC_TIDE) || (ex == G.nx - 1 && G.bc[1] == DRF_BC_TIDE) ||
-                           (ey == 0 && G.bc[2] == DRF_BC_TIDE) || (ey == G.ny - 1 && G.bc[3] == DRF_BC_TIDE);
-        s_etide = tidal ? (T)tide_at(G, a.tdev[cv.tidx] + a.toff) : T(0);
-    }
-    T etide = 0;  // read after the first barrier
-    const T cx = (T)G.cx, cy = (T)G.cy, cs = (T)G.cs;
-    const T Lx = (T)G.Lx, Ly = (T)G.Ly, Ls = (T)G.Ls;
-    const T g = (T)G.g;
     const bool need_res = a.mode == 0 && !a.first;
     // with the baroclinic pressure on, the register of (HT, HS) is staged after the horizontal
     // passes (its shared memory holds P until then)
     const bool late = need_res && G.eos;
-    // the column increments of the earlier stages, read while the column is being staged
-    if (a.mode == 0 && !a.first)
-        for (int t = threadIdx.x; t < NP2; t += blockDim.x) {
-            sOld[t] = a.dHU3[c2 + t];
-            sOld[NP2 + t] = a.dHV3[c2 + t];
-        }
 
-    // ---- stage the column: state (and the 2N register) by TMA bulk copies when aligned
-    if (cv.bulk && a.pf > 0 && threadIdx.x >= 32 && threadIdx.x < 40 && c + a.pf < G.nx * G.ny) {
-        // the state and register blocks of the column a later CTA takes, into L2
-        const int v = threadIdx.x - 32;
-        const size_t pb = (size_t)(c + a.pf) * ncn;
-        const uint32_t bytes = (uint32_t)(ncn * sizeof(T));
-        if (v < 4) bulk_prefetch_l2(a.qin[v] + pb, bytes);
-        else if (need_res) bulk_prefetch_l2(a.res[v - 4] + pb, bytes);
-    }
+    // ---- stage the column: state by TMA bulk copies when aligned (the 2N register follows after
+    // the first barrier). They are issued first: any global load thread 0 made before them
+    // would hold them back by its latency.
     if (cv.bulk) {
         if (threadIdx.x == 0) {
             if (init) {
@@ -366,17 +355,60 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, const Geo &G
             mbar_expect_tx(&bars[0], 4 * bytes);
 #pragma unroll
             for (int v = 0; v < 4; ++v) bulk_g2s(sQ + v * ncn, a.qin[v] + base, bytes, &bars[0]);
-            // the register in two halves, each completing one phase of its own barrier
-            if (need_res) {
-                mbar_expect_tx(&bars[1], 2 * bytes);
-                for (int v = 0; v < 2; ++v) bulk_g2s(sRes + v * ncn, a.res[v] + base, bytes, &bars[1]);
-                if (!late) {
-                    mbar_expect_tx(&bars[2], 2 * bytes);
-                    for (int v = 2; v < 4; ++v) bulk_g2s(sRes + v * ncn, a.res[v] + base, bytes, &bars[2]);
-                }
-            }
         }
-    } else {
+    }
+    // tidal elevation: evaluated once per CTA, and only by a column on a tidal side
+    __shared__ T s_etide;
+    if (threadIdx.x == 0) {
+        s_ok2 = 1;
+        const bool tidal = (ex == 0 && G.bc[0] == DRF_BC_TIDE) || (ex == G.nx - 1 && G.bc[1] == DRF_BC_TIDE) ||
+                           (ey == 0 && G.bc[2] == DRF_BC_TIDE) || (ey == G.ny - 1 && G.bc[3] == DRF_BC_TIDE);
+        s_etide = tidal ? (T)tide_at(G, a.tdev[cv.tidx] + a.toff) : T(0);
+    }
+    T etide = 0;  // read after the first barrier
+    const T cx = (T)G.cx, cy = (T)G.cy, cs = (T)G.cs;
+    const T Lx = (T)G.Lx, Ly = (T)G.Ly, Ls = (T)G.Ls;
+    const T g = (T)G.g;
+    // the column a CTA launched about pf columns later takes, into L2: its state and register
+    // blocks (bulk prefetches, threads 32-39) and the lines of its 2D blocks (threads 40-87:
+    // four probes per block of NP2 doubles, the first and last at its ends and less than 128
+    // bytes apart, so every 128-byte line of the block holds one)
+    if (a.pf > 0 && threadIdx.x >= 32 && threadIdx.x < 88 && c + a.pf < G.nx * G.ny) {
+        const int l = threadIdx.x - 32;
+        if (l < 8) {
+            if (cv.bulk) {
+                const size_t pb = (size_t)(c + a.pf) * ncn;
+                const uint32_t bytes = (uint32_t)(ncn * sizeof(T));
+                if (l < 4) bulk_prefetch_l2(a.qin[l] + pb, bytes);
+                else if (need_res) bulk_prefetch_l2(a.res[l - 4] + pb, bytes);
+            }
+        } else {
+            const int k = (l - 8) / 4, pr = (l - 8) % 4;
+            const double *arr = nullptr;
+            switch (k) {
+            case 0: arr = a.eta; break;
+            case 1: arr = a.h; break;
+            case 2: arr = a.f; break;
+            case 3: arr = a.dHU3; break;
+            case 4: arr = a.dHV3; break;
+            case 5: arr = a.taux; break;
+            case 6: arr = a.tauy; break;
+            case 7: arr = a.etab; break;
+            case 8: arr = a.rese; break;
+            case 9: arr = a.corrU; break;
+            case 10: arr = a.corrV; break;
+            default: arr = a.corrR; break;
+            }
+            if (arr) line_prefetch_l2(arr + (size_t)cv.off2 + (size_t)(c + a.pf) * NP2 + pr * (NP2 - 1) / 3);
+        }
+    }
+    // the column increments of the earlier stages, read while the column is being staged
+    if (a.mode == 0 && !a.first)
+        for (int t = threadIdx.x; t < NP2; t += blockDim.x) {
+            sOld[t] = a.dHU3[c2 + t];
+            sOld[NP2 + t] = a.dHV3[c2 + t];
+        }
+    if (!cv.bulk) {
         for (int n = threadIdx.x; n < ncn; n += blockDim.x) {
 #pragma unroll
             for (int v = 0; v < 4; ++v) sQ[v * ncn + n] = a.qin[v][base + n];
@@ -428,11 +460,36 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, const Geo &G
         const int ez = t / NP, k = t % NP;
         sS1[t] = (ez == nz - 1 && k == N) ? T(1) : (T)(G.dsig * (ez + 0.5 * ((double)B::x(k) + 1.0)));
     }
+    // the neighbours' 2D face values, side sd, face node tt (threads from 96 on where the CTA
+    // has them, clear of the first warps' 2D loads and prefetches)
+    {
+        const int so = (int)blockDim.x >= 96 + 4 * NP ? 96 : 0;
+        for (int t = (int)threadIdx.x - so; t >= 0 && t < 4 * NP; t += blockDim.x) {
+            const int sd = t / NP, tt = t % NP;
+            int nc = -1, ni = tt, nj = tt;
+            if (sd == 0 && ex > 0) { nc = c - 1; ni = N; }
+            if (sd == 1 && ex < G.nx - 1) { nc = c + 1; ni = 0; }
+            if (sd == 2 && ey > 0) { nc = c - G.nx; nj = N; }
+            if (sd == 3 && ey < G.ny - 1) { nc = c + G.nx; nj = 0; }
+            if (nc < 0) continue;
+            const size_t n2 = ((size_t)cv.off2 + (size_t)nc * NP2) + ni + NP * nj;
+            T *f = sNF + t * STAGE_NF;
+            const double e = a.eta[n2], hn = a.h[n2];
+            f[0] = (T)e;
+            f[1] = (T)(e + hn);
+            if (a.corrU) {
+                f[2] = (T)a.corrU[n2];
+                f[3] = (T)a.corrV[n2];
+                f[4] = (T)a.corrR[n2];
+            }
+            if (G.eos) f[5] = (T)(a.etab[n2] + hn);
+        }
+    }
     // state across horizontal side s at own node (ez,i,j,k): q+ (4), eta+, H+
     struct Side {
         T q[4], e, H;
     };
-    // the neighbouring column's values across side s (global loads); false on a basin side
+    // the neighbouring column's state across side s (global loads); false on a basin side
     auto fetch_side = [&](int s, int ez, int i, int j, int k, Side &o) -> bool {
         int nc = -1, ni = i, nj = j;
         if (s == 0 && ex > 0) { nc = c - 1; ni = N; }
@@ -441,20 +498,23 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, const Geo &G
         if (s == 3 && ey < G.ny - 1) { nc = c + G.nx; nj = 0; }
         if (nc < 0) return false;
         const size_t nb = ((size_t)cv.off3 + (size_t)nc * ncn) + (size_t)ez * NP3 + ni + NP * (nj + NP * k);
-        const size_t n2 = ((size_t)cv.off2 + (size_t)nc * NP2) + ni + NP * nj;
 #pragma unroll
         for (int v = 0; v < 4; ++v) o.q[v] = a.qin[v][nb];
+        return true;
+    };
+    // completes a fetched side at face node tt from the staged 2D face values (after the first
+    // barrier): the neighbour's pending transport correction, its elevation and depth
+    auto finish_side = [&](int s, int tt, Side &o) {
+        const T *f = sNF + (s * NP + tt) * STAGE_NF;
         if (a.corrU) {
-            o.q[0] += (T)a.corrU[n2];
-            o.q[1] += (T)a.corrV[n2];
-            const T dr = (T)a.corrR[n2];
+            o.q[0] += f[2];
+            o.q[1] += f[3];
+            const T dr = f[4];
             o.q[2] = fma(o.q[2], dr, o.q[2]);
             o.q[3] = fma(o.q[3], dr, o.q[3]);
         }
-        const double e = a.eta[n2];
-        o.e = (T)e;
-        o.H = (T)(e + a.h[n2]);
-        return true;
+        o.e = f[0];
+        o.H = f[1];
     };
     // the exterior state on a basin side (wall mirror or tidal elevation) at own node n
     auto basin_side = [&](int s, int i, int j, int n, Side &o) {
@@ -490,6 +550,18 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, const Geo &G
         return false;
     }
     etide = s_etide;
+    // the register in two halves, each completing one phase of its own barrier; issued once the
+    // state is in, so the state's copies do not share the memory system with them (the register
+    // is first read in the z pass)
+    if (cv.bulk && need_res && threadIdx.x == 0) {
+        const uint32_t bytes = (uint32_t)(ncn * sizeof(T));
+        mbar_expect_tx(&bars[1], 2 * bytes);
+        for (int v = 0; v < 2; ++v) bulk_g2s(sRes + v * ncn, a.res[v] + base, bytes, &bars[1]);
+        if (!late) {
+            mbar_expect_tx(&bars[2], 2 * bytes);
+            for (int v = 2; v < 4; ++v) bulk_g2s(sRes + v * ncn, a.res[v] + base, bytes, &bars[2]);
+        }
+    }
     if (a.corrU) {  // pending transport correction of the previous step
         for (int n = threadIdx.x; n < ncn; n += blockDim.x) {
             const int an = n % NP2;
@@ -753,14 +825,7 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, const Geo &G
     // column's B
     auto pplus = [&](bool has, int sd, int tt, int ez, int k, int nEnd, int anEnd, const Side &o) -> T {
         if (!G.eos) return T(0);
-        if (has) {
-            int ni, nj;
-            const int nc = sd <= 1 ? (sd == 0 ? c - 1 : c + 1) : (sd == 2 ? c - G.nx : c + G.nx);
-            ni = sd == 0 ? N : (sd == 1 ? 0 : tt);
-            nj = sd == 2 ? N : (sd == 3 ? 0 : tt);
-            const size_t n2 = ((size_t)cv.off2 + (size_t)nc * NP2) + ni + NP * nj;
-            return (T)(a.etab[n2] + a.h[n2]) * sPn[((sd * NP + tt) * nz + ez) * NP + k];
-        }
+        if (has) return sNF[(sd * NP + tt) * STAGE_NF + 5] * sPn[((sd * NP + tt) * nz + ez) * NP + k];
         const T HPm = sHb[anEnd] * sP[nEnd];
         const int bcs = sd == 0 ? G.bc[0] : (sd == 1 ? G.bc[1] : (sd == 2 ? G.bc[2] : G.bc[3]));
         if (bcs != DRF_BC_TIDE) return HPm;
@@ -772,7 +837,9 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, const Geo &G
         const int ez = p / NP2, j = p % NP, k = (p / NP) % NP;
         const int e0 = ez * NP3 + NP * (j + NP * k);
         if (!h0) basin_side(0, 0, j, e0, o0);
+        else finish_side(0, j, o0);
         if (!hN) basin_side(1, N, j, e0 + N, oN);
+        else finish_side(1, j, oN);
         const T Pp0 = pplus(h0, 0, j, ez, k, e0, NP * j, o0);
         const T PpN = pplus(hN, 1, j, ez, k, e0 + N, N + NP * j, oN);
         hpass(std::integral_constant<int, 0>{}, e0, 1, j, 0, o0, oN, Pp0, PpN);
@@ -798,7 +865,9 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, const Geo &G
         const int ez = p / NP2, i = p % NP, k = (p / NP) % NP;
         const int e0 = ez * NP3 + i + NP2 * k;
         if (!h0) basin_side(2, i, 0, e0, o0);
+        else finish_side(2, i, o0);
         if (!hN) basin_side(3, i, N, e0 + NP * N, oN);
+        else finish_side(3, i, oN);
         const T Pp0 = pplus(h0, 2, i, ez, k, e0, i, o0);
         const T PpN = pplus(hN, 3, i, ez, k, e0 + NP * N, i + NP * N, oN);
         hpass(std::integral_constant<int, 1>{}, e0, NP, 0, i, o0, oN, Pp0, PpN);
