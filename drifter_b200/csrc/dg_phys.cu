@@ -231,8 +231,9 @@ struct StageTail {
 };
 // Per side and face node, the neighbouring column's 2D values a face flux needs (its elevation
 // e, depth H = e + h, pending corrections of Hu, Hv and the tracers, and the baroclinic
-// pressure's depth etab + h), staged once per column instead of loaded by every pencil end.
-constexpr int STAGE_NF = 6;
+// pressure's depth Hb = etab + h, stage elevation etab and 1 / Hb), staged once per column
+// instead of loaded by every pencil end and face line.
+constexpr int STAGE_NF = 8;
 inline size_t stage_tail_elems(int nz, int np) {
     switch (np) {
     case 2: return StageTail<2>::elems(nz);
@@ -482,7 +483,12 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, const Geo &G
                 f[3] = (T)a.corrV[n2];
                 f[4] = (T)a.corrR[n2];
             }
-            if (G.eos) f[5] = (T)(a.etab[n2] + hn);
+            if (G.eos) {
+                const double eb = a.etab[n2], Hd = eb + hn;
+                f[5] = (T)Hd;
+                f[6] = (T)eb;
+                f[7] = (T)(1.0 / Hd);
+            }
         }
     }
     // state across horizontal side s at own node (ez,i,j,k): q+ (4), eta+, H+
@@ -621,12 +627,11 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, const Geo &G
                 int ni, nj;
                 const int nc = face_line(sd, tt, ni, nj);
                 if (nc < 0) continue;
-                const size_t n2 = ((size_t)cv.off2 + (size_t)nc * NP2) + ni + NP * nj;
-                const double en = a.etab[n2], Hd = en + a.h[n2];
-                const T Hn = (T)Hd, etn = (T)en, iHn = (T)(1.0 / Hd);
+                const T *nf = sNF + (sd * NP + tt) * STAGE_NF;
+                const T Hn = nf[5], etn = nf[6], iHn = nf[7];
                 // the neighbour's pending tracer volume correction, with the arithmetic of the
                 // neighbour's own load (or of the correction applied to the state)
-                const T dr = a.corrU ? (T)a.corrR[n2] : T(0);
+                const T dr = a.corrU ? nf[4] : T(0);
                 const size_t nb = ((size_t)cv.off3 + (size_t)nc * ncn) + (size_t)ez * NP3 + ni + NP * nj;
 #pragma unroll
                 for (int m = 0; m < NP; ++m) {
@@ -684,8 +689,9 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, const Geo &G
                 int ni, nj;
                 const int nc = face_line(sd, tt, ni, nj);
                 if (nc < 0) continue;
-                const size_t n2 = ((size_t)cv.off2 + (size_t)nc * NP2) + ni + NP * nj;
-                const T Hn = (T)(a.etab[n2] + a.h[n2]);
+                (void)ni;
+                (void)nj;
+                const T Hn = sNF[(sd * NP + tt) * STAGE_NF + 5];
                 const T *tl = sTbn + (sd * NP + tt) * nz;
                 T Tab = 0;
                 for (int e = nz - 1; e >= ez; --e) Tab += tl[e];
@@ -1938,10 +1944,11 @@ struct drf_dg {
     double baro_ms[4] = {0.0, 0.0, 0.0, 0.0};
     int graph_nsub = 0;
     size_t smem = 0;
-    // L2 prefetch distance of the stage launch in columns, 0 for none: stage_waves waves of
-    // stage_pf_unit resident stage CTAs. Tuned at the first step (0, 1 or 2 waves, each timed:
-    // stage_ms) unless DRIFTER_B200_STAGE_PREFETCH=<waves> fixes it (DRIFTER_B200_TUNE=0: 1)
-    int stage_pf = 0, stage_pf_unit = 0, stage_waves = -1;
+    // L2 prefetch distance of the stage launch in columns, 0 for none: stage_hw half waves of
+    // stage_pf_unit resident stage CTAs. Tuned at the first step (0, 1 or 2 half waves, each
+    // timed: stage_ms) unless DRIFTER_B200_STAGE_PREFETCH=<half waves> fixes it
+    // (DRIFTER_B200_TUNE=0: 1)
+    int stage_pf = 0, stage_pf_unit = 0, stage_hw = -1;
     double stage_ms[3] = {0.0, 0.0, 0.0};
     // asynchronous output staging: FP64 snapshot buffers (4 3D fields, 4 2D fields and the
     // time), a copy stream and its events; allocated at the first drf_dg_output_stage
@@ -2330,8 +2337,8 @@ void drf_dg::setup(const drf_mesh_desc *mesh, const drf_dg_params *params, const
             stage_pf_unit = per_sm * nsm;
             const char *pe = std::getenv("DRIFTER_B200_STAGE_PREFETCH");
             const char *tn = std::getenv("DRIFTER_B200_TUNE");
-            stage_waves = pe ? std::max(std::atoi(pe), 0) : ((tn && tn[0] == '0') ? 1 : -1);
-            stage_pf = (stage_waves < 0 ? 1 : stage_waves) * stage_pf_unit;
+            stage_hw = pe ? std::max(std::atoi(pe), 0) : ((tn && tn[0] == '0') ? 1 : -1);
+            stage_pf = (stage_hw < 0 ? 1 : stage_hw) * stage_pf_unit / 2;
         });
     });
 }
@@ -2403,12 +2410,12 @@ void drf_dg::tune_baro() {
     cache[key] = {best, {baro_ms[0], baro_ms[1], baro_ms[2], baro_ms[3]}};
 }
 
-// Stage-launch tuner: the L2 prefetch distance (0, 1 or 2 waves of resident CTAs), each timed
+// Stage-launch tuner: the L2 prefetch distance (0, 1/2 or 1 wave of resident CTAs), each timed
 // on a non-first LSRK stage written into the spare buffers (two warm-up launches, then five
 // between CUDA events; the model state is not modified), the fastest kept. Cached per
 // (device, order, layers, columns, precision, equation of state).
 void drf_dg::tune_stage() {
-    if (stage_waves >= 0) return;
+    if (stage_hw >= 0) return;
     static std::mutex mu;
     static std::map<std::tuple<int, int, int, int, int, int>, std::pair<int, std::array<double, 3>>> cache;
     int dev = 0;
@@ -2418,9 +2425,9 @@ void drf_dg::tune_stage() {
         std::lock_guard<std::mutex> lk(mu);
         auto it = cache.find(key);
         if (it != cache.end()) {
-            stage_waves = it->second.first;
+            stage_hw = it->second.first;
             for (int i = 0; i < 3; ++i) stage_ms[i] = it->second.second[i];
-            stage_pf = stage_waves * stage_pf_unit;
+            stage_pf = stage_hw * stage_pf_unit / 2;
             return;
         }
     }
@@ -2433,7 +2440,7 @@ void drf_dg::tune_stage() {
         using T = decltype(tv);
         constexpr int NP = decltype(npc)::value;
         for (int w = 0; w < 3; ++w) {
-            stage_pf = w * stage_pf_unit;
+            stage_pf = w * stage_pf_unit / 2;
             auto launch = [&] {
                 launch_stage<T, NP>(cur, 1 - cur, 1, 1e-6, 0, nullptr, nullptr, nullptr, eta, 0.0);
             };
@@ -2454,8 +2461,8 @@ void drf_dg::tune_stage() {
     });
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    stage_waves = best;
-    stage_pf = best * stage_pf_unit;
+    stage_hw = best;
+    stage_pf = best * stage_pf_unit / 2;
     std::lock_guard<std::mutex> lk(mu);
     cache[key] = {best, {stage_ms[0], stage_ms[1], stage_ms[2]}};
 }
@@ -3004,12 +3011,12 @@ int drf_dg_tuning(drf_dg *m, int *baro_cols_per_cta, double *baro_ms4) {
     });
 }
 
-int drf_dg_stage_tuning(drf_dg *m, int *prefetch_waves, int *prefetch_columns, double *stage_ms3) {
+int drf_dg_stage_tuning(drf_dg *m, int *prefetch_half_waves, int *prefetch_columns, double *stage_ms3) {
     return guard([&] {
         check_model(m);
         DRF_CHECK(!m->view, DRF_E_INVALID, "ensemble members use the ensemble's stage launch");
         m->tune_stage();
-        if (prefetch_waves) *prefetch_waves = m->stage_waves;
+        if (prefetch_half_waves) *prefetch_half_waves = m->stage_hw;
         if (prefetch_columns) *prefetch_columns = m->stage_pf;
         if (stage_ms3)
             for (int i = 0; i < 3; ++i) stage_ms3[i] = m->stage_ms[i];

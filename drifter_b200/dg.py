@@ -267,14 +267,15 @@ class OceanModel:
 
     def tuning(self) -> dict:
         """The autotuned launch shapes with each candidate's time (ms): the barotropic tile
-        (columns per CTA) and the stage kernel's L2 prefetch distance (waves of resident CTAs)."""
+        (columns per CTA) and the stage kernel's L2 prefetch distance (half waves of resident
+        CTAs)."""
         cpb, ms = C.c_int(), np.zeros(4)
         check(lib().drf_dg_tuning(self.handle, C.byref(cpb), dptr(ms)))
-        waves, cols, sms = C.c_int(), C.c_int(), np.zeros(3)
-        check(lib().drf_dg_stage_tuning(self.handle, C.byref(waves), C.byref(cols), dptr(sms)))
+        hw, cols, sms = C.c_int(), C.c_int(), np.zeros(3)
+        check(lib().drf_dg_stage_tuning(self.handle, C.byref(hw), C.byref(cols), dptr(sms)))
         return dict(baro_cols_per_cta=cpb.value,
                     candidates_ms={str(c): round(float(t), 5) for c, t in zip((2, 4, 8, 16), ms)},
-                    stage_prefetch_waves=waves.value, stage_prefetch_columns=cols.value,
+                    stage_prefetch_half_waves=hw.value, stage_prefetch_columns=cols.value,
                     stage_candidates_ms={str(w): round(float(t), 5) for w, t in enumerate(sms)})
 
     def time_copy(self, nrep: int = 20) -> dict:

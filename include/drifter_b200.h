@@ -188,12 +188,12 @@ int drf_dg_download_surface(drf_dg *m, double *eta);
  * the candidates' times in ms (baro_ms4 may be NULL). No counterpart in the reference, which
  * has no kernels; DRIFTER_B200_TUNE=0 keeps the default tile of 8. */
 int drf_dg_tuning(drf_dg *m, int *baro_cols_per_cta, double *baro_ms4);
-/* Autotuned stage launch: how far ahead (in waves of resident CTAs, 0..2, and in columns) each
- * stage CTA prefetches a later column into L2, chosen by timing the three on this model (at
+/* Autotuned stage launch: how far ahead (in half waves of resident CTAs, 0..2, and in columns)
+ * each stage CTA prefetches a later column into L2, chosen by timing the three on this model (at
  * the first step, or here), and the candidates' times in ms (stage_ms3 may be NULL; zeros when
  * the distance was fixed by DRIFTER_B200_STAGE_PREFETCH or DRIFTER_B200_TUNE=0). No counterpart
  * in the reference. */
-int drf_dg_stage_tuning(drf_dg *m, int *prefetch_waves, int *prefetch_columns, double *stage_ms3);
+int drf_dg_stage_tuning(drf_dg *m, int *prefetch_half_waves, int *prefetch_columns, double *stage_ms3);
 
 /* Size and pointer introspection for the bench (device-resident timing). */
 int drf_dg_info(drf_dg *m, int64_t *n3d_nodes, int64_t *n2d_nodes, int *precision);

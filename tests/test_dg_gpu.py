@@ -259,7 +259,7 @@ def test_time_stage_reports_positive_rate():
 def test_autotuned_barotropic_tile_matches_default_tile(monkeypatch):
     """The autotuner picks one of the candidate tiles by timing; every tile does the same
     arithmetic per 2D node, so the tuned step equals the default-tile step exactly. The stage
-    kernel's L2 prefetch distance is tuned too (0, 1 or 2 waves); a prefetch changes no
+    kernel's L2 prefetch distance is tuned too (0, 1/2 or 1 wave); a prefetch changes no
     arithmetic."""
     case = _tidal_small("fp64", nx=9, ny=7)
     tuned = OceanModel(case["cfg"], case["h"], case["f"], case["taux"], case["tauy"])
@@ -268,14 +268,14 @@ def test_autotuned_barotropic_tile_matches_default_tile(monkeypatch):
     t = tuned.tuning()
     assert t["baro_cols_per_cta"] in (2, 4, 8, 16)
     assert all(v > 0 for v in t["candidates_ms"].values())
-    assert t["stage_prefetch_waves"] in (0, 1, 2)
+    assert t["stage_prefetch_half_waves"] in (0, 1, 2)
     assert all(v > 0 for v in t["stage_candidates_ms"].values())
     monkeypatch.setenv("DRIFTER_B200_TUNE", "0")
     fixed = OceanModel(case["cfg"], case["h"], case["f"], case["taux"], case["tauy"])
     fixed.upload_state(case["q"], case["eta"])
     fixed.step(case["dt"], case["nsub"], 2)
     ft = fixed.tuning()
-    assert ft["baro_cols_per_cta"] == 8 and ft["stage_prefetch_waves"] == 1
+    assert ft["baro_cols_per_cta"] == 8 and ft["stage_prefetch_half_waves"] == 1
     a, b = tuned.download_state(), fixed.download_state()
     for k in ("eta", "HU", "HV", "Hu", "HT"):
         assert relerr(a[k], b[k]) <= 1e-15, k
