@@ -1,5 +1,6 @@
 """Builds libdrifter_b200.so in-tree with nvcc for sm_100a (no JIT, no torch extension)."""
 import os
+import re
 import subprocess
 import sys
 
@@ -55,7 +56,8 @@ def _wait(item):
     if p.returncode != 0:
         sys.stderr.write(text)
         raise RuntimeError(f"nvcc failed on {src}")
-    if "spill" in text and "0 bytes spill" not in text:
+    # ptxas -warn-spills names each function that spills ("N bytes spill stores", N > 0)
+    if re.search(r"\b[1-9][0-9]* bytes spill", text):
         sys.stderr.write(text)
 
 

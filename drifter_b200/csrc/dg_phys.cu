@@ -245,9 +245,9 @@ inline size_t stage_tail_elems(int nz, int np) {
 }
 inline size_t stage_smem_bytes(int nz, int np, size_t tsz) {
     const int np2 = np * np, ncn = nz * np2 * np;
-    return 32 + (size_t)2 * np2 * 8 +
+    return 32 + (size_t)4 * np2 * 8 +
            ((size_t)13 * ncn + (size_t)3 * nz * np2 + 12 * np2 + (size_t)nz * np + stage_tail_elems(nz, np) +
-            (size_t)4 * np * STAGE_NF) *
+            (size_t)4 * np * STAGE_NF + (size_t)3 * np2) *
                tsz;
 }
 
@@ -306,7 +306,8 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, const Geo &G
     // mbarriers: state, register of (Hu, Hv), register of (HT, HS)
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw);
     double *sOld = reinterpret_cast<double *>(smem_raw + 32);  // [2][NP2] column increments so far
-    T *sQ = reinterpret_cast<T *>(smem_raw + 32 + 2 * NP2 * sizeof(double));  // [4][ncn]
+    double *sRe = sOld + 2 * NP2, *sEtb = sRe + NP2;  // the bed's 2D register and stage elevation
+    T *sQ = reinterpret_cast<T *>(smem_raw + 32 + 4 * NP2 * sizeof(double));  // [4][ncn]
     T *sRes = sQ + 4 * ncn;                        // [4][ncn]
     T *sR = sRes + 4 * ncn;                        // [4][ncn]
     T *sD = sR + 4 * ncn;                          // [ncn] divergence -> layer integrals
@@ -331,6 +332,8 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, const Geo &G
     T *sTbn = sTb + nz * NP2;
     // the neighbours' 2D face values [side][face node][STAGE_NF]
     T *sNF = tail + Tl::elems(nz);
+    // the z pass's 2D fields per 2D node: Coriolis, surface stress / rho0 (x, y)
+    T *sFc = sNF + 4 * NP * STAGE_NF, *sTx = sFc + NP2, *sTy = sTx + NP2;
     __shared__ int s_ok, s_ok2;
 
     const bool need_res = a.mode == 0 && !a.first;
@@ -491,6 +494,20 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, const Geo &G
             }
         }
     }
+    // the z pass's 2D fields, staged now so that no z pencil waits for a global load (threads
+    // from 128 on where the CTA has them)
+    {
+        const int so = (int)blockDim.x >= 128 + NP2 ? 128 : 0;
+        for (int t = (int)threadIdx.x - so; t >= 0 && t < NP2; t += blockDim.x) {
+            sFc[t] = (T)a.f[c2 + t];
+            sTx[t] = (T)(a.taux[c2 + t] / G.rho0);
+            sTy[t] = (T)(a.tauy[c2 + t] / G.rho0);
+            if (a.mode == 0) {
+                sRe[t] = a.first ? 0.0 : a.rese[c2 + t];
+                sEtb[t] = a.etab[c2 + t];
+            }
+        }
+    }
     // state across horizontal side s at own node (ez,i,j,k): q+ (4), eta+, H+
     struct Side {
         T q[4], e, H;
@@ -549,6 +566,32 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, const Geo &G
         hx0 = fetch_side(0, ez, 0, j, k, fx0);
         hxN = fetch_side(1, ez, N, j, k, fxN);
     }
+    // with the baroclinic pressure on: the tracers along this thread's first neighbour face line
+    // of the pre-pass below (item npen + fl0 of its strided loop), loaded now like the x faces;
+    // FP32 instances with a compile-time layer count only (the others have no registers to spare)
+    constexpr bool PRE = NZ > 0 && sizeof(T) == 4;
+    const int nfl = 4 * NP * nz;  // neighbour face lines: (side, face node, layer)
+    int fl0 = -1;
+    T flT[NP], flS[NP];
+    if (PRE && G.eos) {
+        const int x = (int)threadIdx.x, bd = (int)blockDim.x;
+        const int i0 = x >= npen ? x : x + bd * ((npen - x + bd - 1) / bd);
+        const int f = i0 - npen, sd = f / (NP * nz), tt = (f / nz) % NP, ez = f % nz;
+        int nc = -1, ni = tt, nj = tt;
+        if (sd == 0 && ex > 0) { nc = c - 1; ni = N; }
+        if (sd == 1 && ex < G.nx - 1) { nc = c + 1; ni = 0; }
+        if (sd == 2 && ey > 0) { nc = c - G.nx; nj = N; }
+        if (sd == 3 && ey < G.ny - 1) { nc = c + G.nx; nj = 0; }
+        if (f < nfl && nc >= 0) {
+            fl0 = f;
+            const size_t nb = ((size_t)cv.off3 + (size_t)nc * ncn) + (size_t)ez * NP3 + ni + NP * nj;
+#pragma unroll
+            for (int m = 0; m < NP; ++m) {
+                flT[m] = a.qin[2][nb + NP2 * m];
+                flS[m] = a.qin[3][nb + NP2 * m];
+            }
+        }
+    }
     if (threadIdx.x == 0) s_ok = cv.bulk ? (int)mbar_wait(&bars[0], ph) : 1;
     __syncthreads();
     if (!s_ok) {
@@ -594,7 +637,6 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, const Geo &G
         const T al = (T)G.alpha, be = (T)G.beta, S0 = (T)G.S0;
         const T Trs = (T)G.Tref_s, Trz = (T)G.Tref_dz;
         const T hd2 = (T)(0.5 * G.dsig);
-        const int nfl = 4 * NP * nz;  // neighbour face lines: (side, face node, layer)
         // the neighbouring column across side sd and the face node (ni, nj) of face line tt
         auto face_line = [&](int sd, int tt, int &ni, int &nj) -> int {
             int nc = -1;
@@ -633,10 +675,11 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, const Geo &G
                 // neighbour's own load (or of the correction applied to the state)
                 const T dr = a.corrU ? nf[4] : T(0);
                 const size_t nb = ((size_t)cv.off3 + (size_t)nc * ncn) + (size_t)ez * NP3 + ni + NP * nj;
+                const bool pre = PRE && f == fl0;  // loaded before the first barrier
 #pragma unroll
                 for (int m = 0; m < NP; ++m) {
                     const T Tr = fma(Trz, fma(sS1[ez * NP + m] - T(1), Hn, etn), Trs);
-                    const T hs = a.qin[3][nb + NP2 * m], ht = a.qin[2][nb + NP2 * m];
+                    const T hs = pre ? flS[m] : a.qin[3][nb + NP2 * m], ht = pre ? flT[m] : a.qin[2][nb + NP2 * m];
                     bv[m] = fma(be, fma(fma(hs, dr, hs), iHn, -S0), -al * fma(fma(ht, dr, ht), iHn, -Tr));
                 }
                 dst = sPn + ((sd * NP + tt) * nz + ez) * NP;
@@ -923,7 +966,7 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, const Geo &G
     for (int p = p_first; p < npen; p = p_next(p)) {
         const int ez = p / NP2, an = p % NP2;
         const int e0 = ez * NP3 + an;
-        const T iH = sIH[an], fa = (T)a.f[c2 + an];
+        const T iH = sIH[an], fa = sFc[an];
         const bool bed = ez == 0, top = ez == nz - 1;
         // the sigma velocity consistent with the discrete divergence: per layer, bottom up,
         // H omega = y solves cs D y + Ls e_0 (y_0 - M0) = I - delta (the strong-form continuity
@@ -946,9 +989,9 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, const Geo &G
         if (a.mode == 1 && a.deta_out && bed) a.deta_out[c2 + an] = -(double)Iq;
         if (a.mode == 0 && bed) {  // the stage elevation, advanced like the 3D state
             const size_t i2 = c2 + an;
-            const double re = (a.first ? 0.0 : (double)a.A * a.rese[i2]) - (double)dtc * (double)Iq;
+            const double re = (a.first ? 0.0 : (double)a.A * sRe[an]) - (double)dtc * (double)Iq;
             a.rese[i2] = re;
-            a.etab_out[i2] = a.etab[i2] + (double)a.B * re;
+            a.etab_out[i2] = sEtb[an] + (double)a.B * re;
         }
         T om[NP];
         {
@@ -974,8 +1017,8 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, const Geo &G
         }
         T fsx = 0, fsy = 0;
         if (top) {
-            fsx = Ls * (T)(a.taux[c2 + an] / G.rho0);
-            fsy = Ls * (T)(a.tauy[c2 + an] / G.rho0);
+            fsx = Ls * sTx[an];
+            fsy = Ls * sTy[an];
         }
         const T w0 = om[0] * T(-1), wN = om[N];
         const int nb0 = (ez - 1) * NP3 + an + NP2 * N, nbN = (ez + 1) * NP3 + an;
