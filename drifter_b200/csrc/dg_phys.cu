@@ -247,7 +247,7 @@ inline size_t stage_smem_bytes(int nz, int np, size_t tsz) {
     const int np2 = np * np, ncn = nz * np2 * np;
     return 32 + (size_t)4 * np2 * 8 +
            ((size_t)13 * ncn + (size_t)3 * nz * np2 + 12 * np2 + (size_t)nz * np + stage_tail_elems(nz, np) +
-            (size_t)4 * np * STAGE_NF + (size_t)3 * np2) *
+            (size_t)4 * np * STAGE_NF + (size_t)6 * np2) *
                tsz;
 }
 
@@ -332,8 +332,10 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, const Geo &G
     T *sTbn = sTb + nz * NP2;
     // the neighbours' 2D face values [side][face node][STAGE_NF]
     T *sNF = tail + Tl::elems(nz);
-    // the z pass's 2D fields per 2D node: Coriolis, surface stress / rho0 (x, y)
+    // the z pass's 2D fields per 2D node: Coriolis, surface stress / rho0 (x, y); and the pending
+    // transport correction of the column (Hu, Hv, tracers)
     T *sFc = sNF + 4 * NP * STAGE_NF, *sTx = sFc + NP2, *sTy = sTx + NP2;
+    T *sCu = sTy + NP2, *sCv = sCu + NP2, *sCr = sCv + NP2;
     __shared__ int s_ok, s_ok2;
 
     const bool need_res = a.mode == 0 && !a.first;
@@ -406,12 +408,15 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, const Geo &G
             if (arr) line_prefetch_l2(arr + (size_t)cv.off2 + (size_t)(c + a.pf) * NP2 + pr * (NP2 - 1) / 3);
         }
     }
-    // the column increments of the earlier stages, read while the column is being staged
-    if (a.mode == 0 && !a.first)
-        for (int t = threadIdx.x; t < NP2; t += blockDim.x) {
-            sOld[t] = a.dHU3[c2 + t];
-            sOld[NP2 + t] = a.dHV3[c2 + t];
-        }
+    // the column increments of the earlier stages, read while the column is being staged: loaded
+    // here and stored after the column's 2D loads below, so the first warp waits for one global
+    // round trip instead of two
+    const bool old = a.mode == 0 && !a.first;
+    double old0 = 0.0, old1 = 0.0;
+    if (old && (int)threadIdx.x < NP2) {
+        old0 = a.dHU3[c2 + threadIdx.x];
+        old1 = a.dHV3[c2 + threadIdx.x];
+    }
     if (!cv.bulk) {
         for (int n = threadIdx.x; n < ncn; n += blockDim.x) {
 #pragma unroll
@@ -460,6 +465,16 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, const Geo &G
             sGHy[t] = g * cy * ghy;
         }
     }
+    if (old) {
+        if ((int)threadIdx.x < NP2) {
+            sOld[threadIdx.x] = old0;
+            sOld[NP2 + threadIdx.x] = old1;
+        }
+        for (int t = threadIdx.x + blockDim.x; t < NP2; t += blockDim.x) {
+            sOld[t] = a.dHU3[c2 + t];
+            sOld[NP2 + t] = a.dHV3[c2 + t];
+        }
+    }
     for (int t = threadIdx.x; t < nz * NP; t += blockDim.x) {
         const int ez = t / NP, k = t % NP;
         sS1[t] = (ez == nz - 1 && k == N) ? T(1) : (T)(G.dsig * (ez + 0.5 * ((double)B::x(k) + 1.0)));
@@ -494,8 +509,8 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, const Geo &G
             }
         }
     }
-    // the z pass's 2D fields, staged now so that no z pencil waits for a global load (threads
-    // from 128 on where the CTA has them)
+    // the z pass's 2D fields and the column's pending correction, staged now so that no pass
+    // after the column load waits for a global load (threads from 128 on where the CTA has them)
     {
         const int so = (int)blockDim.x >= 128 + NP2 ? 128 : 0;
         for (int t = (int)threadIdx.x - so; t >= 0 && t < NP2; t += blockDim.x) {
@@ -505,6 +520,11 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, const Geo &G
             if (a.mode == 0) {
                 sRe[t] = a.first ? 0.0 : a.rese[c2 + t];
                 sEtb[t] = a.etab[c2 + t];
+            }
+            if (a.corrU) {
+                sCu[t] = (T)a.corrU[c2 + t];
+                sCv[t] = (T)a.corrV[c2 + t];
+                sCr[t] = (T)a.corrR[c2 + t];
             }
         }
     }
@@ -614,9 +634,9 @@ __device__ __forceinline__ bool stage_column(const StageArgs<T> &a, const Geo &G
     if (a.corrU) {  // pending transport correction of the previous step
         for (int n = threadIdx.x; n < ncn; n += blockDim.x) {
             const int an = n % NP2;
-            sQ[n] += (T)a.corrU[c2 + an];
-            sQ[ncn + n] += (T)a.corrV[c2 + an];
-            const T dr = (T)a.corrR[c2 + an];
+            sQ[n] += sCu[an];
+            sQ[ncn + n] += sCv[an];
+            const T dr = sCr[an];
             sQ[2 * ncn + n] = fma(sQ[2 * ncn + n], dr, sQ[2 * ncn + n]);
             sQ[3 * ncn + n] = fma(sQ[3 * ncn + n], dr, sQ[3 * ncn + n]);
         }
