@@ -334,8 +334,9 @@ def run_baroclinic(stream, steps=10, warmup=3):
 
 def run_ensemble(stream, steps=5, warmup=3):
     """C5: 64 independent N=3 runs of uneven size stepped together (one stage launch per LSRK
-    stage over all members' columns, one graph per baroclinic step), against the same members
-    stepped one model after another on the same stream. Device time with CUDA events."""
+    stage and layer count over all members' columns, one graph per baroclinic step), against the
+    same members stepped one model after another on the same stream. Device time with CUDA
+    events."""
     import torch
     from drifter_b200 import configs
     from drifter_b200.dg import Ensemble, OceanModel

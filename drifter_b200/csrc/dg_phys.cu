@@ -1482,10 +1482,10 @@ struct EnsMember {
     int ncol, bulk;
 };
 
-// Stage launch over all members: one CTA per work item (member, column), the items ordered
-// tallest columns first so the tail of the launch is made of the cheapest columns. The member's
-// geometry is staged in shared memory; its arrays are addressed through the column view
-// (element offsets into the pools). Shared memory is sized for the tallest member.
+// Stage launch over the members of one layer count: one CTA per work item (member, column),
+// the CTA size and shared memory those columns need (one such launch per layer count, tallest
+// first). The member's geometry is staged in shared memory; its arrays are addressed through the
+// column view (element offsets into the pools).
 template <typename T, int NP>
 __global__ void __launch_bounds__(STAGE_MAX_THREADS, sizeof(T) == 4 ? 2 : 1)
     dg3d_stage_ens_kernel(StageArgs<T> a, const EnsMember *mem, const int2 *items, int nitems) {
@@ -3112,8 +3112,14 @@ struct drf_ens {
     DevBuf<EnsMember> table;
     DevBuf<int2> items, tiles;
     std::vector<EnsMember> htab;
-    int nitems = 0, ntiles = 0, grid = 0, threads = 0;
-    size_t smem = 0;
+    // the stage items of one layer count (a contiguous run of the sorted item list), launched
+    // with that height's CTA size and shared memory
+    struct Group {
+        int start, count, nz, threads;
+        size_t smem;
+    };
+    std::vector<Group> groups;
+    int nitems = 0, ntiles = 0, grid = 0;
     int64_t n3tot = 0, n2tot = 0;
     cudaStream_t stream = nullptr, own = nullptr;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
@@ -3142,8 +3148,11 @@ struct drf_ens {
             StageArgs<T> a = m0->template stage_args<T>(src, dst, s, 0.0, 0, nullptr, nullptr, nullptr,
                                                         m0->eta, 0.0, s == 0);
             a.pf = 0;  // the work items are not in column order
-            dg3d_stage_ens_kernel<T, NP><<<grid, threads, smem, stream>>>(a, table.p, items.p, nitems);
-            DRF_LAUNCHED();
+            for (const Group &g : groups) {
+                dg3d_stage_ens_kernel<T, NP><<<g.count, g.threads, g.smem, stream>>>(a, table.p, items.p + g.start,
+                                                                                     g.count);
+                DRF_LAUNCHED();
+            }
             src = dst;
         }
         if (baro_persist) {
@@ -3220,8 +3229,6 @@ int drf_ens_create(int nmembers, const drf_mesh_desc *meshes, const drf_dg_param
             off2[i] = e->n2tot;
             e->n3tot += (m->n3 + 63) / 64 * 64;
             e->n2tot += m->n2;
-            e->threads = std::max(e->threads, m->stage_threads_generic());
-            e->smem = std::max(e->smem, m->smem);
             e->mem.push_back(std::move(m));
         }
         drf_dg &m0 = *e->mem[0];
@@ -3263,6 +3270,13 @@ int drf_ens_create(int nmembers, const drf_mesh_desc *meshes, const drf_dg_param
         });
         e->nitems = (int)items.size();
         e->ntiles = (int)tiles.size();
+        // one stage launch per layer count, with that height's CTA size and shared memory
+        for (int i = 0; i < e->nitems; ++i) {
+            const drf_dg &m = *e->mem[items[i].x];
+            if (e->groups.empty() || e->groups.back().nz != m.G.nz)
+                e->groups.push_back({i, 0, m.G.nz, m.stage_threads_generic(), m.smem});
+            ++e->groups.back().count;
+        }
         e->table.alloc(nmembers);
         DRF_CUDA(cudaMemcpy(e->table.p, e->htab.data(), nmembers * sizeof(EnsMember), cudaMemcpyHostToDevice));
         e->items.alloc(items.size());
@@ -3279,11 +3293,13 @@ int drf_ens_create(int nmembers, const drf_mesh_desc *meshes, const drf_dg_param
             int maxsm = 0;
             DRF_CUDA(cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
             allow_max_dynamic_smem(reinterpret_cast<const void *>(dg3d_stage_ens_kernel<T, NP>), maxsm);
-            DRF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dg3d_stage_ens_kernel<T, NP>,
-                                                                   e->threads, e->smem));
+            for (const auto &g : e->groups) {
+                DRF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dg3d_stage_ens_kernel<T, NP>,
+                                                                       g.threads, g.smem));
+                DRF_CHECK(per_sm >= 1, DRF_E_UNSUPPORTED, "ensemble stage kernel does not fit on an SM");
+            }
         });
-        DRF_CHECK(per_sm >= 1, DRF_E_UNSUPPORTED, "ensemble stage kernel does not fit on an SM");
-        e->grid = e->nitems;  // one CTA per (member, column) item
+        e->grid = e->nitems;  // one CTA per (member, column) item, over the groups' launches
         *out = e.release();
     });
 }

@@ -291,9 +291,9 @@ class OceanModel:
 
 
 class Ensemble:
-    """Independent coupled DG runs stepped together (one launch per LSRK stage over all
-    members' water columns, one launch per barotropic substep, one CUDA graph per baroclinic
-    step).
+    """Independent coupled DG runs stepped together (one launch per LSRK stage and layer count
+    over all members' water columns, one launch per barotropic substep, one CUDA graph per
+    baroclinic step).
 
     `members[i]` is an OceanModel view of member i (upload/download/diagnostics); the members
     are stepped only through `step`. Each member's result equals OceanModel.step on it alone.

@@ -1,6 +1,6 @@
 """Uneven ensembles (C5 layout) on the GPU, through the C ABI.
 
-An ensemble steps all members with one persistent stage launch per LSRK stage and one launch
+An ensemble steps all members with one stage launch per LSRK stage and layer count and one launch
 per barotropic pass over every member's tiles; each member must end where the same model stepped
 alone ends (both evaluate the same formulas per node; the ensemble's barotropic kernels are
 separately compiled instances, whose multiply-add fusion may differ, so they agree to 1e-11
@@ -48,8 +48,10 @@ def test_ensemble_members_equal_single_runs(precision):
     before = launch_count()
     ens.step(dts, 20, 3)
     ens.sync()
-    # 5 stage launches + force + 2 per subcycle + finish per step, for all members together
-    assert launch_count() - before == 3 * (5 + 2 + 2 * 20)
+    # per step: 5 stages, each one launch per layer count of the members, then force, 2 per
+    # subcycle and finish, for all members together
+    groups = len({c["cfg"].nz for c in cases})
+    assert launch_count() - before == 3 * (5 * groups + 2 + 2 * 20)
     for m, c in zip(ens.members, cases):
         g = m.download_state()
         solo = OceanModel(c["cfg"], c["h"], c["f"], c["taux"], c["tauy"])
@@ -86,7 +88,7 @@ def test_ensemble_persistent_barotropic_agrees_with_per_pass_launches(monkeypatc
     before = launch_count()
     pers.step(dts, 20, 3)
     pers.sync()
-    assert launch_count() - before == 3 * 6
+    assert launch_count() - before == 3 * (5 * len({c["cfg"].nz for c in cases}) + 1)
     for ma, mb in zip(pers.members, per.members):
         a, b = ma.download_state(), mb.download_state()
         assert a["t"] == b["t"]
